@@ -1,0 +1,140 @@
+/*
+ * pwgpu -- B200 (sm_100a) SCF hot path of a plane-wave Kohn-Sham DFT code,
+ * exported as a plain C ABI.
+ *
+ * The entry points replace, one for one, the per-iteration calls of the
+ * reference solver (Ron-Leizrowice/pwdft-rs, paths relative to
+ * pwdft/pwdft-core/src/):
+ *
+ *   pwgpu_set_veff_g   <- the V_eff(G) handed from assemble_v_eff
+ *                         (scf/energy.rs:293-301) to the per-k H build
+ *                         (scf/driver.rs:459-468)
+ *   pwgpu_apply_h      <- H|psi> with H = fill_hamiltonian_with_v_eff
+ *                         (scf/potentials.rs:163-190) +
+ *                         NonlocalPotential::add_to_hamiltonian
+ *                         (potential/nonlocal.rs:432-450), applied
+ *                         matrix-free
+ *
+ * Units are the reference's: eV, Å, e/Å³.  Complex arrays are interleaved
+ * (re, im) doubles.  Wavefunction blocks are column-major n_pw x n_bands
+ * in the basis order of BasisSet::new (basis.rs:36-63), as faer::Mat.
+ *
+ * Conventions: every function returns a pwgpu_status (0 = success,
+ * negative = error, one code per reference error family); the message of
+ * the calling thread's last failure is returned by pwgpu_last_error().
+ * The library never aborts the process and never traps the device.
+ * Host arrays are borrowed for the duration of a call only; device state
+ * is owned by the handle.  A handle is bound to one device and one CUDA
+ * stream and must not be used from two threads at once; distinct handles
+ * are independent.
+ */
+#ifndef PWGPU_H
+#define PWGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t pwgpu_status;
+
+#define PWGPU_OK 0
+#define PWGPU_E_INVALID (-1)          /* PwdftError::InvalidParam / InvalidCrystal */
+#define PWGPU_E_CUDA (-2)             /* PwdftError::Gpu */
+#define PWGPU_E_OOM (-3)              /* device allocation failed */
+#define PWGPU_E_NOT_CONVERGED (-4)    /* PwdftError::ConvergenceFailure */
+#define PWGPU_E_TIMEOUT (-5)          /* a bounded device wait ran out */
+#define PWGPU_E_NOT_IMPLEMENTED (-6)  /* PwdftError::NotImplemented */
+#define PWGPU_E_STATE (-7)            /* call order violated (e.g. no V_eff set) */
+
+#define PWGPU_PRECISION_FP64 0  /* plain: every H|psi> stage in FP64 */
+#define PWGPU_PRECISION_MIXED 1 /* FFTs and V_eff product in FP32 */
+
+typedef struct pwgpu_handle pwgpu_handle;
+
+/*
+ * Per-calculation invariants: the data contract of ScfContext::new
+ * (scf/context.rs:102-231).  All pointers are host pointers, read during
+ * pwgpu_create only.
+ */
+typedef struct pwgpu_system {
+  int32_t dims[3];             /* FFT grid (FftGrid::new, scf/grid.rs:44-87) */
+  int32_t n_pw;                /* basis size (k-independent sphere) */
+  const int32_t* miller;       /* n_pw x 3 Miller indices, basis order */
+  int32_t n_k;                 /* number of (IBZ) k-points */
+  const double* k_weights;     /* n_k, sum 1 */
+  const double* kinetic;       /* n_k x n_pw: (hbar^2/2m)|k+G|^2, eV */
+  int32_t n_ch;                /* KB channels (atom, projector, m) */
+  const double* proj_b;        /* n_k x (n_pw x n_ch) complex, column-major:
+                                  B[G,c] = e^{-iG.tau} F(|k+G|) Y_lm / sqrt(Omega)
+                                  (nonlocal.rs:311-338) */
+  int32_t n_atoms;             /* atoms carrying channels */
+  const int32_t* atom_ch_start;/* n_atoms+1: first channel of each atom */
+  const double* d_blocks;      /* per atom, the dense nc_a x nc_a block of D
+                                  (row-major, eV), concatenated */
+  const double* v_local_g;     /* N complex: V_loc(G) on the full grid, G=0 kept */
+  const double* g_squared;     /* N: |G|^2, Å^-2 */
+  const double* rho_core_r;    /* N: NLCC core density, or NULL */
+  int32_t n_sym;               /* symmetry operations (1 = identity only) */
+  const int32_t* sym_src;      /* n_sym x N gather map (symmetry/density/g_space.rs) */
+  const double* sym_arg;       /* n_sym x N phase arguments 2 pi n.tau */
+  double n_electrons;
+  double omega;                /* cell volume, Å^3 */
+  double e_ewald;              /* eV */
+  int32_t nspin;               /* 1 or 2 */
+} pwgpu_system;
+
+typedef struct pwgpu_options {
+  int32_t device;     /* CUDA device ordinal */
+  int32_t precision;  /* PWGPU_PRECISION_FP64 or PWGPU_PRECISION_MIXED */
+} pwgpu_options;
+
+/* Message of the calling thread's most recent failure ("" if none). */
+const char* pwgpu_last_error(void);
+
+/* Library version string. */
+const char* pwgpu_version(void);
+
+/* Build a handle: uploads the system, plans the FFTs, sizes scratch.
+ * Replaces ScfContext::new's device-facing part (scf/context.rs:102-231). */
+pwgpu_status pwgpu_create(const pwgpu_system* sys, const pwgpu_options* opt, pwgpu_handle** out);
+
+/* Release every device allocation of the handle.  NULL is accepted. */
+pwgpu_status pwgpu_destroy(pwgpu_handle* h);
+
+/* Set V_eff(G) (N complex, eV) for one spin channel; the library forms
+ * V_eff(r) by one unnormalised inverse FFT.  Replaces the V_eff hand-off of
+ * scf/driver.rs:427-468. */
+pwgpu_status pwgpu_set_veff_g(pwgpu_handle* h, int32_t spin, const double* veff_g);
+
+/* hpsi = H psi for a block of nb bands at k-point ik (host arrays,
+ * column-major n_pw x nb, complex).  Equals the dense H of
+ * scf/potentials.rs:163-190 + potential/nonlocal.rs:432-450 applied to psi. */
+pwgpu_status pwgpu_apply_h(pwgpu_handle* h, int32_t spin, int32_t ik, const double* psi, int32_t nb,
+                           double* hpsi);
+
+/* Same on device pointers (leading dimensions in complex elements), on the
+ * CUDA stream `stream` (cudaStream_t, NULL = the handle's stream). */
+pwgpu_status pwgpu_apply_h_device(pwgpu_handle* h, int32_t spin, int32_t ik, const void* psi_dev, int64_t ldpsi,
+                                  int32_t nb, void* hpsi_dev, int64_t ldh, void* stream);
+
+/* pwgpu_apply_h_device on the handle's stream with a CUDA event after every
+ * launch; stage_ms[8] / launches[8] receive the summed device time and the
+ * launch count per stage: 0..4 the five FFT kernels (z-inverse+scatter,
+ * y-inverse, x-inverse*V*x-forward, y-forward, z-forward+gather+kinetic),
+ * 5 B^H psi, 6 D apply, 7 B Q.  Diagnostic; no reference counterpart. */
+pwgpu_status pwgpu_profile_apply_h(pwgpu_handle* h, int32_t spin, int32_t ik, const void* psi_dev, int64_t ldpsi,
+                                   int32_t nb, void* hpsi_dev, int64_t ldh, double* stage_ms, int32_t* launches);
+
+/* Select the arithmetic of subsequent H|psi> calls (PWGPU_PRECISION_*). */
+pwgpu_status pwgpu_set_precision(pwgpu_handle* h, int32_t precision);
+
+/* Basis size, grid size and channel count of a handle. */
+pwgpu_status pwgpu_get_dims(const pwgpu_handle* h, int32_t* n_pw, int64_t* n_grid, int32_t* n_ch);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PWGPU_H */

@@ -1,0 +1,458 @@
+"""ORACLE -- test infrastructure only.
+
+CPU FP64 restatement (numpy/scipy) of the reference's per-iteration SCF
+algorithm, used by tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline leg as the checker.  It is never part of the product path.
+
+Each function cites the reference file:line it restates (paths relative to
+pwdft/pwdft-core/src/ of Ron-Leizrowice/pwdft-rs).  The reference's own
+Rust crate cannot be built here (no Rust toolchain, and the snapshot does
+not compile), so parity is pinned through the reference's golden numbers:
+  * SCF golden  -- tests/cpu_scf_baseline.rs:43-44 (E=-213.028339 eV,
+                   E_F=8.052064 eV, Si prim, 100 eV, 16^3, Γ, 4 bands)
+  * component CSVs -- data/csv/{vloc_g,beta_q,dij,rho_core_g}_si_reference.csv
+  * basis counts   -- basis.rs:139-148 (259 G at 200 eV)
+Third-party numerics: rustfft 6.4.1 (restated by numpy.fft, same sign and
+normalisation conventions), faer 0.24 self_adjoint_eigen (restated by
+LAPACK zheevd via numpy.linalg.eigh), puruspe 0.4.4 erf/erfc (scipy.special).
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import scipy.fft as sfft
+from scipy.special import erfc
+
+HA_TO_EV = 27.211386245988
+BOHR_TO_ANG = 0.529177210903
+BOHR3_TO_ANG3 = BOHR_TO_ANG ** 3
+E2_COULOMB = 14.399645351950548
+G2_ZERO_THRESHOLD = 1e-12
+RHO_FLOOR = 1e-30
+
+_WORKERS = -1
+
+
+def set_workers(n: int):
+    """Thread count for the oracle's FFTs (-1 = all cores)."""
+    global _WORKERS
+    _WORKERS = n
+
+
+# ---------------------------------------------------------------------------
+# FFT conventions (fft.rs:19-114): both directions unnormalised.
+# ---------------------------------------------------------------------------
+
+def ifft3(x, dims):
+    return sfft.ifftn(x.reshape(dims), norm="forward", workers=_WORKERS).ravel()
+
+
+def fft3(x, dims):
+    return sfft.fftn(x.reshape(dims), workers=_WORKERS).ravel()
+
+
+def density_r_to_g(rho_r, dims):
+    """ρ(G) = (1/N) Σ_r ρ(r) e^{-iG·r} (energy.rs:250-259)."""
+    return fft3(rho_r.astype(np.complex128), dims) / rho_r.size
+
+
+# ---------------------------------------------------------------------------
+# Hamiltonian (potentials.rs:163-190, nonlocal.rs:432-450)
+# ---------------------------------------------------------------------------
+
+def miller_to_idx(dims, m):
+    d0, d1, d2 = dims
+    return (np.mod(m[..., 0], d0) * d1 + np.mod(m[..., 1], d1)) * d2 + np.mod(m[..., 2], d2)
+
+
+def dense_hamiltonian(miller, kinetic, veff_g, dims, b, d_dense):
+    """H[i,j] = V_eff(G_i−G_j) + δ_ij T_i, then H += B·(D·B^H).
+
+    fill_hamiltonian_with_v_eff (potentials.rs:163-190) followed by
+    NonlocalPotential::add_to_hamiltonian (nonlocal.rs:432-450)."""
+    m = miller.astype(np.int64)
+    dm = m[:, None, :] - m[None, :, :]
+    h = veff_g[miller_to_idx(dims, dm)].astype(np.complex128)
+    h[np.diag_indices_from(h)] += kinetic
+    if b.shape[1]:
+        h += b @ (d_dense @ b.conj().T)
+    return h
+
+
+def apply_h_fft(g_to_fft, kinetic, veff_g, dims, b, d_dense, psi):
+    """H·ψ by the FFT form, identical to the dense form of potentials.rs:163-190:
+    (Vψ)(G_i) = (1/N) Σ_r e^{-iG_i·r} V(r) ψ(r), V(r) and ψ(r) unnormalised
+    inverse transforms; plus the nonlocal B·(D·(B^H ψ))."""
+    n = int(np.prod(dims))
+    vr = ifft3(veff_g, dims)
+    out = np.empty_like(psi)
+    for j in range(psi.shape[1]):
+        grid = np.zeros(n, dtype=np.complex128)
+        grid[g_to_fft] = psi[:, j]
+        pr = ifft3(grid, dims)
+        hg = fft3(pr * vr, dims) / n
+        out[:, j] = hg[g_to_fft] + kinetic * psi[:, j]
+    if b.shape[1]:
+        out += b @ (d_dense @ (b.conj().T @ psi))
+    return out
+
+
+def lowest_eigenpairs(h, n_bands):
+    """Lowest n_bands eigenpairs, ascending (eigensolver/dense.rs:50-98)."""
+    w, v = np.linalg.eigh(h)
+    return w[:n_bands].copy(), v[:, :n_bands].copy()
+
+
+# ---------------------------------------------------------------------------
+# Occupations (smearing.rs:38-252)
+# ---------------------------------------------------------------------------
+
+def _step(e, ef):
+    return np.where(e < ef, 1.0, np.where(np.abs(e - ef) < 1e-12, 0.5, 0.0))
+
+
+def occupation01(scheme, e, ef, sigma):
+    e = np.asarray(e, dtype=np.float64)
+    if sigma < 1e-15:
+        return _step(e, ef)
+    x = (e - ef) / sigma
+    if scheme in ("fermi_dirac", "fixed"):
+        with np.errstate(over="ignore"):
+            v = 1.0 / (1.0 + np.exp(np.clip(x, -40.0, 40.0)))
+        return np.where(x > 40.0, 0.0, np.where(x < -40.0, 1.0, v))
+    if scheme == "gaussian":
+        return erfc(x) / 2.0
+    if scheme == "methfessel_paxton":
+        return erfc(x) / 2.0 - 0.5 * x * np.exp(-x * x) / math.sqrt(math.pi)
+    if scheme == "cold":
+        a = x + 1.0 / math.sqrt(2.0)
+        return 0.5 * erfc(a) + np.exp(-a * a) / math.sqrt(2.0 * math.pi)
+    raise ValueError(scheme)
+
+
+def find_fermi_energy(evals, weights, n_el, sigma, scheme, spin_factor):
+    """Bisection, ≤200 steps, stop at 1e-14 (smearing.rs:49-90)."""
+    flat = np.concatenate([np.asarray(e) for e in evals])
+    wk = np.concatenate([np.full(len(e), w) for e, w in zip(evals, weights)])
+    lo = flat.min() - 10.0 * max(sigma, 0.1)
+    hi = flat.max() + 10.0 * max(sigma, 0.1)
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        n = float(np.sum(wk * occupation01(scheme, flat, mid, sigma) * spin_factor))
+        if n < n_el:
+            lo = mid
+        else:
+            hi = mid
+        if abs(hi - lo) < 1e-14:
+            break
+    return 0.5 * (lo + hi)
+
+
+def entropy_ts(evals, weights, ef, sigma, scheme, spin_factor):
+    """T·S (smearing.rs:202-252)."""
+    if sigma < 1e-15:
+        return 0.0
+    s = 0.0
+    for e, w in zip(evals, weights):
+        x = (np.asarray(e) - ef) / sigma
+        if scheme in ("fermi_dirac", "fixed"):
+            f = 1.0 / (1.0 + np.exp(np.clip(x, -700, 700)))
+            f = np.clip(f, 1e-30, 1.0 - 1e-30)
+            with np.errstate(divide="ignore", invalid="ignore"):
+                sw = np.where(np.abs(x) > 30.0, 0.0, -(f * np.log(f) + (1.0 - f) * np.log(1.0 - f)))
+        elif scheme == "gaussian":
+            sw = np.exp(-x * x) / math.sqrt(math.pi)
+        elif scheme == "methfessel_paxton":
+            sw = (0.5 - x * x) * np.exp(-x * x) / math.sqrt(math.pi)
+        else:
+            a = x + 1.0 / math.sqrt(2.0)
+            sw = a * np.exp(-a * a) / math.sqrt(math.pi)
+        s += w * float(np.sum(sw))
+    return s * sigma * spin_factor
+
+
+# ---------------------------------------------------------------------------
+# Density (density.rs:41-111)
+# ---------------------------------------------------------------------------
+
+def compute_density(g_to_fft, dims, psis, occs, weights, n_el, omega):
+    n = int(np.prod(dims))
+    rho = np.zeros(n)
+    for psi, occ, w in zip(psis, occs, weights):
+        for ib in range(len(occ)):
+            f = occ[ib] * w
+            if f < 1e-15:
+                continue
+            grid = np.zeros(n, dtype=np.complex128)
+            grid[g_to_fft] = psi[:, ib]
+            pr = ifft3(grid, dims)
+            rho += f * (pr.real * pr.real + pr.imag * pr.imag)
+    integ = rho.sum() * (omega / n)
+    if abs(integ) > 1e-15:
+        rho *= n_el / integ
+    return rho
+
+
+def gather_map(dims, ops):
+    """Source index ρ(R^T n mod N) and phase argument 2π n·τ per op and grid
+    point (g_space.rs:21-91 rotate_miller/miller_to_flat/flat_to_miller)."""
+    d0, d1, d2 = dims
+    ax = [np.where(np.arange(d) > d // 2, np.arange(d) - d, np.arange(d)) for d in dims]
+    n1, n2, n3 = [a.ravel() for a in np.meshgrid(*ax, indexing="ij")]
+    srcs, args = [], []
+    for rot, tau in ops:
+        s = [rot[0][i] * n1 + rot[1][i] * n2 + rot[2][i] * n3 for i in range(3)]
+        srcs.append(((np.mod(s[0], d0) * d1 + np.mod(s[1], d1)) * d2 + np.mod(s[2], d2)).astype(np.int32))
+        args.append(2.0 * math.pi * ((n1 * tau[0] + n2 * tau[1]) + n3 * tau[2]))
+    return np.stack(srcs), np.stack(args)
+
+
+def symmetrize_density(rho_r, dims, src, arg):
+    """G-space symmetrisation (symmetry/density/g_space.rs:147-252).
+
+    src/arg: gather map [n_ops, N] (source flat index, 2π n·τ)."""
+    n_ops = src.shape[0]
+    if n_ops <= 1:
+        return rho_r.copy()
+    rg = fft3(rho_r.astype(np.complex128), dims)
+    acc = np.zeros(rg.size, dtype=np.complex128)
+    for s in range(n_ops):
+        acc += (np.cos(arg[s]) - 1j * np.sin(arg[s])) * rg[src[s]]
+    acc *= 1.0 / n_ops
+    return (ifft3(acc, dims) / rg.size).real.copy()
+
+
+# ---------------------------------------------------------------------------
+# Potentials and XC (energy.rs:293-358, xc.rs:129-596)
+# ---------------------------------------------------------------------------
+
+def hartree(rho_g, g2):
+    fpe = 4.0 * math.pi * E2_COULOMB
+    out = np.zeros_like(rho_g)
+    m = g2 > G2_ZERO_THRESHOLD
+    out[m] = rho_g[m] * fpe / g2[m]
+    return out
+
+
+def hartree_energy(rho_g, g2, omega):
+    fpe = 4.0 * math.pi * E2_COULOMB
+    m = g2 > G2_ZERO_THRESHOLD
+    return float(np.sum((rho_g[m].real ** 2 + rho_g[m].imag ** 2) * fpe / g2[m])) * 0.5 * omega
+
+
+def _pz_rs(rs, polarized):
+    if polarized:
+        g, b1, b2 = -0.0843, 1.3981, 0.2611
+        a, b, c, d = 0.01555, -0.0269, 0.0007, -0.0048
+    else:
+        g, b1, b2 = -0.1423, 1.0529, 0.3334
+        a, b, c, d = 0.0311, -0.048, 0.0020, -0.0116
+    rs = np.asarray(rs)
+    hi = rs >= 1.0
+    sq = np.sqrt(np.where(hi, rs, 1.0))
+    den = 1.0 + b1 * sq + b2 * rs
+    ec_h = g / den
+    dec_h = -g * (b1 / (2.0 * sq) + b2) / (den * den)
+    vc_h = ec_h - rs / 3.0 * dec_h
+    lr = np.log(np.where(hi, 1.0, rs))
+    ec_l = a * lr + b + c * rs * lr + d * rs
+    dec_l = a / np.where(hi, 1.0, rs) + c * (lr + 1.0) + d
+    vc_l = ec_l - rs / 3.0 * dec_l
+    return np.where(hi, ec_h, ec_l), np.where(hi, vc_h, vc_l)
+
+
+def lda_xc(rho):
+    """PZ81 LDA: (ε_xc, v_xc) in eV for ρ in e/Å³ (xc.rs:129-288)."""
+    rho = np.asarray(rho, dtype=np.float64)
+    ok = rho >= RHO_FLOOR
+    rb = np.where(ok, rho, 1.0) * BOHR3_TO_ANG3
+    ex = -0.75 * np.cbrt(3.0 * rb / math.pi)
+    vx = (4.0 / 3.0) * ex
+    rs = np.cbrt(3.0 / (4.0 * math.pi * rb))
+    ec, vc = _pz_rs(rs, False)
+    exc = np.where(ok, (ex + ec) * HA_TO_EV, 0.0)
+    vxc = np.where(ok, (vx + vc) * HA_TO_EV, 0.0)
+    return exc, vxc
+
+
+def lsda_xc(rho_up, rho_dn):
+    """LSDA: Slater spin scaling + PZ von Barth-Hedin interpolation (xc.rs:374-596)."""
+    ru = np.asarray(rho_up, dtype=np.float64)
+    rd = np.asarray(rho_dn, dtype=np.float64)
+    rho = ru + rd
+    ok = rho >= RHO_FLOOR
+    rhs = np.where(ok, rho, 1.0)
+    rub, rdb = ru * BOHR3_TO_ANG3, rd * BOHR3_TO_ANG3
+    exu = np.where(rub > RHO_FLOOR, -0.75 * np.cbrt(6.0 * np.maximum(rub, 0) / math.pi), 0.0)
+    exd = np.where(rdb > RHO_FLOOR, -0.75 * np.cbrt(6.0 * np.maximum(rdb, 0) / math.pi), 0.0)
+    rb = rhs * BOHR3_TO_ANG3
+    ex = (rub * exu + rdb * exd) / rb
+    vxu, vxd = (4.0 / 3.0) * exu, (4.0 / 3.0) * exd
+    rs = np.cbrt(3.0 / (4.0 * math.pi * rb))
+    zeta = np.clip((ru - rd) / rhs, -1.0, 1.0)
+    ecu, vcu = _pz_rs(rs, False)
+    ecp, vcp = _pz_rs(rs, True)
+    fden = 2.0 * np.cbrt(2.0) - 2.0
+    op, om = np.maximum(1.0 + zeta, 0.0), np.maximum(1.0 - zeta, 0.0)
+    cop, com = np.cbrt(op), np.cbrt(om)
+    fz = (cop * op + com * om - 2.0) / fden
+    dfz = (4.0 / 3.0) * (cop - com) / fden
+    ec = ecu + fz * (ecp - ecu)
+    vrs = vcu + fz * (vcp - vcu)
+    dz = dfz * (ecp - ecu)
+    vcu_ = vrs + (1.0 - zeta) * dz
+    vcd_ = vrs - (1.0 + zeta) * dz
+    z = lambda x: np.where(ok, x * HA_TO_EV, 0.0)
+    return z(ex + ec), z(vxu + vcu_), z(vxd + vcd_)
+
+
+def add_core(rho, rho_core):
+    if rho_core.size == 0:
+        return rho.copy()
+    return np.maximum(rho + rho_core, 0.0)
+
+
+def xc_energy_corrected(rho_xc, rho_val, exc, vxc, omega):
+    dv = omega / rho_xc.size
+    return float(np.sum(rho_xc * exc * dv)) - float(np.sum(rho_val * vxc * dv))
+
+
+def density_diff(a, b, omega):
+    n = a.size
+    dv = omega / n
+    return math.sqrt(float(np.sum((a - b) ** 2 * dv)) / omega)
+
+
+# ---------------------------------------------------------------------------
+# Mixing (mixing/anderson.rs:170-266, kerker.rs:18-49, linalg.rs:124-152)
+# ---------------------------------------------------------------------------
+
+def auto_q_tf_squared(n_el, omega):
+    rho_b = n_el / omega * BOHR_TO_ANG ** 3
+    q2 = 4.0 * np.cbrt(3.0 * math.pi * math.pi * rho_b) / math.pi
+    return q2 / (BOHR_TO_ANG * BOHR_TO_ANG)
+
+
+class AndersonMixer:
+    def __init__(self, beta, ndim, dims, kerker_weights=None):
+        self.beta, self.ndim, self.dims = beta, ndim, dims
+        self.kw = kerker_weights
+        self.hin, self.hres = [], []
+
+    def mix(self, rho_in, rho_out):
+        res = rho_out - rho_in
+        if self.kw is not None:
+            rg = fft3(res.astype(np.complex128), self.dims) * self.kw
+            res = (ifft3(rg, self.dims) / res.size).real.copy()
+        self.hin.append(rho_in.copy())
+        self.hres.append(res)
+        if len(self.hin) > self.ndim:
+            self.hin.pop(0)
+            self.hres.pop(0)
+        m = len(self.hin)
+        if m < 2:
+            return self.hin[-1] + self.beta * self.hres[-1]
+        rl = self.hres[-1]
+        dr = [self.hres[i] - rl for i in range(m - 1)]
+        mm = m - 1
+        a = np.array([[float(dr[i] @ dr[j]) for j in range(mm)] for i in range(mm)])
+        b = np.array([-float(dr[i] @ rl) for i in range(mm)])
+        alpha = solve_small(a, b)
+        al = 1.0 - alpha.sum()
+        out = al * (self.hin[-1] + self.beta * rl)
+        for i in range(mm):
+            out = out + alpha[i] * (self.hin[i] + self.beta * self.hres[i])
+        return out
+
+
+def solve_small(a, b):
+    """Partial-pivot LU with the 1e-15 singular-pivot fallback (linalg.rs:124-152)."""
+    import scipy.linalg as sl
+    n = b.size
+    if n == 0:
+        return b
+    lu, piv = sl.lu_factor(a, check_finite=False)
+    if np.any(np.abs(np.diag(lu)) < 1e-15):
+        return np.full(n, 1.0 / (n + 1))
+    return sl.lu_solve((lu, piv), b, check_finite=False)
+
+
+# ---------------------------------------------------------------------------
+# SCF driver (driver.rs:266-742)
+# ---------------------------------------------------------------------------
+
+@dataclass
+class OracleResult:
+    total_energy: float
+    harris_foulkes_energy: float
+    fermi_energy: float
+    eigenvalues: list
+    n_iterations: int
+    final_delta: float
+    rho_r: np.ndarray
+    entropy_ts: float = 0.0
+    history: list = field(default_factory=list)
+
+
+def run_scf_unpolarized(sys, n_bands, max_iter=100, conv_threshold=1e-6, energy_threshold=1e-5,
+                        mixing_beta=0.3, mixing_ndim=8, smearing="fermi_dirac", sigma=0.01,
+                        kerker=False, q_tf=None, verbose=False):
+    """Dense-H SCF loop of driver.rs:353-735 on an ScfSystem (pwgpu.context)."""
+    dims = sys.dims
+    n = sys.n_grid
+    omega = sys.omega
+    weights = sys.kpt_weights
+    spin_factor = 2.0
+    if sys.symmetry.n_ops > 1:
+        src, arg = gather_map(dims, [(op.rotation, op.translation) for op in sys.symmetry.operations])
+    else:
+        src = arg = np.zeros((1, 0))
+    kw = None
+    if kerker:
+        q2 = q_tf * q_tf if q_tf is not None else auto_q_tf_squared(sys.n_electrons, omega)
+        kw = np.where(sys.g_squared < G2_ZERO_THRESHOLD, 0.0, sys.g_squared / (sys.g_squared + q2))
+    mixer = AndersonMixer(mixing_beta, mixing_ndim, dims, kw)
+    d_dense = [p.d_dense() for p in sys.projectors]
+    rho = sys.rho_init_r.copy()
+    rho_g = density_r_to_g(rho, dims)
+    e_prev = None
+    hist = []
+    for it in range(max_iter):
+        vh = hartree(rho_g, sys.g_squared)
+        rxc = add_core(rho, sys.rho_core_r)
+        exc_in, vxc_in = lda_xc(rxc)
+        veff = sys.v_local_g + vh + density_r_to_g(vxc_in, dims)
+        evals, psis = [], []
+        for ik in range(len(sys.kpoints)):
+            h = dense_hamiltonian(sys.basis.miller, sys.kinetic[ik], veff, dims, sys.projectors[ik].b, d_dense[ik])
+            w, v = lowest_eigenpairs(h, n_bands)
+            evals.append(w)
+            psis.append(v)
+        ef = find_fermi_energy(evals, weights, sys.n_electrons, sigma, smearing, spin_factor)
+        occs = [spin_factor * occupation01(smearing, e, ef, sigma) for e in evals]
+        rho_new = compute_density(sys.g_to_fft, dims, psis, occs, weights, sys.n_electrons, omega)
+        if src.shape[0] > 1:
+            rho_new = symmetrize_density(rho_new, dims, src, arg)
+        delta = density_diff(rho, rho_new, omega)
+        rho_g_new = density_r_to_g(rho_new, dims)
+        rxc_new = add_core(rho_new, sys.rho_core_r)
+        exc_o, vxc_o = lda_xc(rxc_new)
+        e_band = float(sum(np.sum(o * w * e) for o, w, e in zip(occs, weights, evals)))
+        ts = entropy_ts(evals, weights, ef, sigma, smearing, spin_factor)
+        e_tot = (e_band - hartree_energy(rho_g_new, sys.g_squared, omega)
+                 + xc_energy_corrected(rxc_new, rho_new, exc_o, vxc_o, omega) + sys.e_ewald - ts)
+        e_hf = (e_band - hartree_energy(rho_g, sys.g_squared, omega)
+                + xc_energy_corrected(rxc, rho, exc_in, vxc_in, omega) + sys.e_ewald - ts)
+        de = None if e_prev is None else abs(e_tot - e_prev)
+        e_prev = e_tot
+        hist.append((it, e_tot, delta))
+        if verbose:
+            print(f"iter {it:3d} E={e_tot:.10f} dE={de} drho={delta:.3e}")
+        if delta < conv_threshold and de is not None and de < energy_threshold:
+            return OracleResult(e_tot, e_hf, ef, evals, it + 1, delta, rho_new, ts, hist)
+        rho = mixer.mix(rho, rho_new)
+        rho_g = density_r_to_g(rho, dims)
+    raise RuntimeError(f"SCF did not converge in {max_iter} iterations (delta={delta})")

@@ -1,0 +1,249 @@
+// C-ABI entry points of libpwgpu (declared in include/pwgpu.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "handle.hpp"
+#include "../../include/pwgpu.h"
+
+struct pwgpu_handle {
+  pwgpu::Handle h;
+  int precision = 0;
+};
+
+namespace pwgpu {
+
+static thread_local std::string t_last_error;
+
+Status fail(int code, const std::string& msg) {
+  t_last_error = msg;
+  return (Status)code;
+}
+
+template <typename T> static Status upload(T** dst, const T* src, size_t count) {
+  const size_t n = std::max<size_t>(count, 1);
+  cudaError_t e = cudaMalloc((void**)dst, n * sizeof(T));
+  if (e != cudaSuccess) return fail(kOom, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  if (src && count) {
+    e = cudaMemcpy(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(kCuda, std::string("cudaMemcpy: ") + cudaGetErrorString(e));
+  }
+  return kOk;
+}
+
+static void release(Handle& h) {
+  auto f = [](void* p) { if (p) cudaFree(p); };
+  GridMaps& g = h.g;
+  for (int a = 0; a < 3; ++a) { f(g.tw64[a]); f(g.tw32[a]); }
+  f(g.col_start); f(g.pt_ig); f(g.pt_col); f(g.pt_z); f(g.g_to_fft);
+  for (auto& k : h.kp) { f(k.kinetic); f(k.b); f(k.b32); }
+  h.kp.clear();
+  f(h.ch_atom); f(h.atom_ch_start); f(h.d_off); f(h.d_vals);
+  f(h.v_local_g); f(h.g_squared); f(h.rho_core_r); f(h.sym_src); f(h.sym_arg);
+  for (int s = 0; s < 2; ++s) { f(h.veff_r[s]); f(h.veff_r32[s]); }
+  f(h.work_a); f(h.work_b); f(h.nl_p); f(h.nl_q); f(h.tmp_grid);
+  if (h.blas) cublasDestroy(h.blas);
+  if (h.stream) cudaStreamDestroy(h.stream);
+  h = Handle();
+}
+
+static Status create(const pwgpu_system* s, const pwgpu_options* o, pwgpu_handle* ph) {
+  Handle& h = ph->h;
+  if (!s || !s->miller || !s->kinetic || !s->k_weights || !s->v_local_g || !s->g_squared)
+    return fail(kInvalid, "pwgpu_create: required system array is NULL");
+  if (s->n_pw <= 0 || s->n_k <= 0 || s->dims[0] <= 0 || s->dims[1] <= 0 || s->dims[2] <= 0)
+    return fail(kInvalid, "pwgpu_create: n_pw, n_k and dims must be positive");
+  if (s->dims[0] > 1024 || s->dims[1] > 1024 || s->dims[2] > 1024)
+    return fail(kInvalid, "pwgpu_create: FFT grid dimension exceeds MAX_FFT_DIM=1024");
+  if (s->nspin != 1 && s->nspin != 2) return fail(kInvalid, "pwgpu_create: nspin must be 1 or 2");
+  if (s->n_ch < 0 || (s->n_ch > 0 && (!s->proj_b || !s->atom_ch_start || !s->d_blocks || s->n_atoms <= 0)))
+    return fail(kInvalid, "pwgpu_create: projector arrays missing");
+  if (s->n_sym < 0 || (s->n_sym > 1 && (!s->sym_src || !s->sym_arg)))
+    return fail(kInvalid, "pwgpu_create: symmetry map missing");
+  h.device = o ? o->device : 0;
+  ph->precision = o ? o->precision : 0;
+  PW_CUDA_TRY(cudaSetDevice(h.device));
+  h.n_pw = s->n_pw;
+  h.n_k = s->n_k;
+  h.n_ch = s->n_ch;
+  h.n_atoms = s->n_ch > 0 ? s->n_atoms : 0;
+  h.nspin = s->nspin;
+  h.n_sym = std::max(1, s->n_sym);
+  h.n_electrons = s->n_electrons;
+  h.omega = s->omega;
+  h.e_ewald = s->e_ewald;
+  for (int a = 0; a < 3; ++a) h.g.d[a] = s->dims[a];
+  PW_CUDA_TRY(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
+  if (cublasCreate(&h.blas) != CUBLAS_STATUS_SUCCESS) return fail(kCuda, "cublasCreate failed");
+  cublasSetStream(h.blas, h.stream);
+  Status st = build_grid_maps(h, s->miller);
+  if (st != kOk) return st;
+  const long N = h.g.N;
+  h.kp.resize(h.n_k);
+  for (int k = 0; k < h.n_k; ++k) {
+    KPointData& kd = h.kp[k];
+    kd.weight = s->k_weights[k];
+    if ((st = upload(&kd.kinetic, s->kinetic + (long)k * h.n_pw, h.n_pw)) != kOk) return st;
+    if (h.n_ch > 0) {
+      const double2* bsrc = reinterpret_cast<const double2*>(s->proj_b) + (long)k * h.n_pw * h.n_ch;
+      if ((st = upload(&kd.b, bsrc, (size_t)h.n_pw * h.n_ch)) != kOk) return st;
+    }
+  }
+  if (h.n_ch > 0) {
+    std::vector<int> starts(s->atom_ch_start, s->atom_ch_start + h.n_atoms + 1);
+    if (starts[0] != 0 || starts[h.n_atoms] != h.n_ch) return fail(kInvalid, "atom_ch_start must span [0, n_ch]");
+    std::vector<int> ch_atom(h.n_ch), d_off(h.n_atoms);
+    long off = 0;
+    for (int a = 0; a < h.n_atoms; ++a) {
+      const int nc = starts[a + 1] - starts[a];
+      if (nc < 0) return fail(kInvalid, "atom_ch_start must be non-decreasing");
+      d_off[a] = (int)off;
+      off += (long)nc * nc;
+      for (int c = starts[a]; c < starts[a + 1]; ++c) ch_atom[c] = a;
+    }
+    if ((st = upload(&h.atom_ch_start, starts.data(), starts.size())) != kOk) return st;
+    if ((st = upload(&h.ch_atom, ch_atom.data(), ch_atom.size())) != kOk) return st;
+    if ((st = upload(&h.d_off, d_off.data(), d_off.size())) != kOk) return st;
+    if ((st = upload(&h.d_vals, s->d_blocks, (size_t)off)) != kOk) return st;
+  }
+  if ((st = upload(&h.v_local_g, reinterpret_cast<const double2*>(s->v_local_g), (size_t)N)) != kOk) return st;
+  if ((st = upload(&h.g_squared, s->g_squared, (size_t)N)) != kOk) return st;
+  if (s->rho_core_r && (st = upload(&h.rho_core_r, s->rho_core_r, (size_t)N)) != kOk) return st;
+  if (h.n_sym > 1) {
+    if ((st = upload(&h.sym_src, s->sym_src, (size_t)h.n_sym * N)) != kOk) return st;
+    if ((st = upload(&h.sym_arg, s->sym_arg, (size_t)h.n_sym * N)) != kOk) return st;
+  }
+  for (int sp = 0; sp < h.nspin; ++sp) {
+    if ((st = upload<double>(&h.veff_r[sp], nullptr, (size_t)N)) != kOk) return st;
+    if ((st = upload<float>(&h.veff_r32[sp], nullptr, (size_t)N)) != kOk) return st;
+    PW_CUDA_TRY(cudaMemset(h.veff_r[sp], 0, N * sizeof(double)));
+    PW_CUDA_TRY(cudaMemset(h.veff_r32[sp], 0, N * sizeof(float)));
+  }
+  PW_CUDA_TRY(cudaDeviceSynchronize());
+  return kOk;
+}
+
+}  // namespace pwgpu
+
+using namespace pwgpu;
+
+extern "C" {
+
+const char* pwgpu_last_error(void) { return t_last_error.c_str(); }
+
+const char* pwgpu_version(void) { return "pwgpu 0.1 (sm_100a)"; }
+
+pwgpu_status pwgpu_create(const pwgpu_system* sys, const pwgpu_options* opt, pwgpu_handle** out) {
+  if (!out) return fail(kInvalid, "pwgpu_create: out is NULL");
+  *out = nullptr;
+  pwgpu_handle* ph = new (std::nothrow) pwgpu_handle();
+  if (!ph) return fail(kOom, "pwgpu_create: host allocation failed");
+  Status st = create(sys, opt, ph);
+  if (st != kOk) {
+    release(ph->h);
+    delete ph;
+    return st;
+  }
+  *out = ph;
+  return kOk;
+}
+
+pwgpu_status pwgpu_destroy(pwgpu_handle* ph) {
+  if (!ph) return kOk;
+  cudaSetDevice(ph->h.device);
+  if (ph->h.stream) cudaStreamSynchronize(ph->h.stream);
+  release(ph->h);
+  delete ph;
+  return kOk;
+}
+
+pwgpu_status pwgpu_set_veff_g(pwgpu_handle* ph, int32_t spin, const double* veff_g) {
+  if (!ph || !veff_g) return fail(kInvalid, "pwgpu_set_veff_g: NULL argument");
+  Handle& h = ph->h;
+  if (spin < 0 || spin >= h.nspin) return fail(kInvalid, "pwgpu_set_veff_g: spin out of range");
+  PW_CUDA_TRY(cudaSetDevice(h.device));
+  PW_CUDA_TRY(cudaMemcpyAsync(h.tmp_grid, veff_g, h.g.N * sizeof(double2), cudaMemcpyHostToDevice, h.stream));
+  Status st = set_veff_from_g(h, spin, h.tmp_grid, h.stream);
+  if (st != kOk) return st;
+  PW_CUDA_TRY(cudaStreamSynchronize(h.stream));
+  return kOk;
+}
+
+pwgpu_status pwgpu_apply_h(pwgpu_handle* ph, int32_t spin, int32_t ik, const double* psi, int32_t nb,
+                           double* hpsi) {
+  if (!ph || !psi || !hpsi) return fail(kInvalid, "pwgpu_apply_h: NULL argument");
+  if (nb < 0) return fail(kInvalid, "pwgpu_apply_h: nb must be non-negative");
+  Handle& h = ph->h;
+  if (nb == 0) return kOk;
+  PW_CUDA_TRY(cudaSetDevice(h.device));
+  const size_t bytes = (size_t)h.n_pw * nb * sizeof(double2);
+  double2 *dp = nullptr, *dh = nullptr;
+  PW_CUDA_TRY(cudaMallocAsync((void**)&dp, bytes, h.stream));
+  cudaError_t e = cudaMallocAsync((void**)&dh, bytes, h.stream);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(dp, h.stream);
+    return fail(kOom, "pwgpu_apply_h: device allocation failed");
+  }
+  Status st = kOk;
+  e = cudaMemcpyAsync(dp, psi, bytes, cudaMemcpyHostToDevice, h.stream);
+  if (e != cudaSuccess) st = fail(kCuda, cudaGetErrorString(e));
+  if (st == kOk) st = apply_h_device(h, spin, ik, dp, h.n_pw, nb, dh, h.n_pw, ph->precision, h.stream);
+  if (st == kOk) {
+    e = cudaMemcpyAsync(hpsi, dh, bytes, cudaMemcpyDeviceToHost, h.stream);
+    if (e != cudaSuccess) st = fail(kCuda, cudaGetErrorString(e));
+  }
+  cudaFreeAsync(dp, h.stream);
+  cudaFreeAsync(dh, h.stream);
+  e = cudaStreamSynchronize(h.stream);
+  if (st == kOk && e != cudaSuccess) st = fail(kCuda, cudaGetErrorString(e));
+  return st;
+}
+
+pwgpu_status pwgpu_apply_h_device(pwgpu_handle* ph, int32_t spin, int32_t ik, const void* psi_dev, int64_t ldpsi,
+                                  int32_t nb, void* hpsi_dev, int64_t ldh, void* stream) {
+  if (!ph || !psi_dev || !hpsi_dev) return fail(kInvalid, "pwgpu_apply_h_device: NULL argument");
+  Handle& h = ph->h;
+  cudaStream_t s = stream ? (cudaStream_t)stream : h.stream;
+  return apply_h_device(h, spin, ik, (const double2*)psi_dev, ldpsi, nb, (double2*)hpsi_dev, ldh, ph->precision, s);
+}
+
+pwgpu_status pwgpu_profile_apply_h(pwgpu_handle* ph, int32_t spin, int32_t ik, const void* psi_dev, int64_t ldpsi,
+                                   int32_t nb, void* hpsi_dev, int64_t ldh, double* stage_ms, int32_t* launches) {
+  if (!ph || !psi_dev || !hpsi_dev || !stage_ms || !launches) return fail(kInvalid, "pwgpu_profile_apply_h: NULL");
+  Handle& h = ph->h;
+  StageTimer tm;
+  Status st = apply_h_device(h, spin, ik, (const double2*)psi_dev, ldpsi, nb, (double2*)hpsi_dev, ldh, ph->precision,
+                             h.stream, &tm);
+  cudaError_t e = cudaStreamSynchronize(h.stream);
+  for (int k = 0; k < 8; ++k) { stage_ms[k] = 0.0; launches[k] = 0; }
+  for (size_t i = 1; i < tm.events.size() && st == kOk && e == cudaSuccess; ++i) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, tm.events[i - 1], tm.events[i]);
+    const int sg = tm.stage[i];
+    if (sg >= 0 && sg < 8) { stage_ms[sg] += ms; launches[sg] += 1; }
+  }
+  for (cudaEvent_t ev : tm.events) cudaEventDestroy(ev);
+  if (st != kOk) return st;
+  if (e != cudaSuccess) return fail(kCuda, cudaGetErrorString(e));
+  return kOk;
+}
+
+pwgpu_status pwgpu_set_precision(pwgpu_handle* ph, int32_t precision) {
+  if (!ph) return fail(kInvalid, "pwgpu_set_precision: NULL handle");
+  if (precision != 0 && precision != 1) return fail(kInvalid, "pwgpu_set_precision: unknown precision");
+  ph->precision = precision;
+  return kOk;
+}
+
+pwgpu_status pwgpu_get_dims(const pwgpu_handle* ph, int32_t* n_pw, int64_t* n_grid, int32_t* n_ch) {
+  if (!ph) return fail(kInvalid, "pwgpu_get_dims: NULL handle");
+  if (n_pw) *n_pw = ph->h.n_pw;
+  if (n_grid) *n_grid = ph->h.g.N;
+  if (n_ch) *n_ch = ph->h.n_ch;
+  return kOk;
+}
+
+}  // extern "C"

@@ -1,0 +1,96 @@
+// Device-resident state of one pwgpu handle: FFT grid plans and sphere
+// maps, per-k projector matrices, potentials and scratch buffers.
+#pragma once
+
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "pw_common.cuh"
+
+namespace pwgpu {
+
+Status fail(int code, const std::string& msg);  // records the thread's last error, returns code
+
+// Sphere <-> grid maps and per-axis FFT plans.  Grid flat index is
+// (i0*d1 + i1)*d2 + i2, x slowest, as in the reference's miller_to_idx.
+// The sphere occupies |n_i| <= m_i; the "compact" x range holds Xp = 2*m0+1
+// planes and the compact y range Yp = 2*m1+1 rows, so the z-direction FFTs
+// run only on the Xp*Yp columns that can carry plane-wave coefficients.
+struct GridMaps {
+  int d[3] = {0, 0, 0};
+  long N = 0;
+  int m[3] = {0, 0, 0};
+  int Xp = 0, Yp = 0, ncol = 0;
+  FftPlan plan[3];
+  double2* tw64[3] = {nullptr, nullptr, nullptr};
+  float2* tw32[3] = {nullptr, nullptr, nullptr};
+  // points sorted by column c = (n0+m0)*Yp + (n1+m1), then by basis order
+  int* col_start = nullptr;  // ncol+1
+  int* pt_ig = nullptr;      // n_pw: basis index of sorted point
+  int* pt_col = nullptr;     // n_pw: column of sorted point
+  int* pt_z = nullptr;       // n_pw: wrapped z index
+  int* g_to_fft = nullptr;   // n_pw (basis order): flat grid index
+  // tile widths chosen for the FFT kernels (lines per block)
+  int wz = 1, wy = 1, wx = 1;
+};
+
+struct KPointData {
+  double* kinetic = nullptr;    // n_pw
+  double2* b = nullptr;         // n_pw x n_ch, column-major
+  float2* b32 = nullptr;        // FP32 copy for the mixed form (lazily made)
+  double weight = 0.0;
+};
+
+struct Handle {
+  int device = 0;
+  int n_pw = 0, n_k = 0, n_ch = 0, n_atoms = 0, nspin = 1, n_sym = 0;
+  double n_electrons = 0.0, omega = 0.0, e_ewald = 0.0;
+  GridMaps g;
+  std::vector<KPointData> kp;
+  int* ch_atom = nullptr;          // n_ch: atom of channel
+  int* atom_ch_start = nullptr;    // n_atoms+1
+  int* d_off = nullptr;            // n_atoms: offset of atom block in d_vals
+  double* d_vals = nullptr;        // concatenated blocks
+  double2* v_local_g = nullptr;    // N
+  double* g_squared = nullptr;     // N
+  double* rho_core_r = nullptr;    // N or null
+  int* sym_src = nullptr;          // n_sym x N
+  double* sym_arg = nullptr;       // n_sym x N
+  // effective potential per spin in real space
+  double* veff_r[2] = {nullptr, nullptr};
+  float* veff_r32[2] = {nullptr, nullptr};
+  // H|psi> scratch: band-chunked compact grids (L2-resident per chunk)
+  int chunk = 1;
+  void* work_a = nullptr;   // chunk * ncol * d2 complex (FP64 size)
+  void* work_b = nullptr;   // chunk * Xp * d1 * d2 complex
+  double2* nl_p = nullptr;  // n_ch x max_nb
+  double2* nl_q = nullptr;
+  int nl_cap = 0;
+  double2* tmp_grid = nullptr;  // N complex scratch
+  cudaStream_t stream = nullptr;
+  cublasHandle_t blas = nullptr;
+  std::string last_error;
+};
+
+// Optional per-launch event trail of an H|psi> call (profiling entry point).
+// stage ids: -1 start, 0..4 the five FFT kernels, 5 B^H psi, 6 D apply, 7 B Q.
+struct StageTimer {
+  std::vector<cudaEvent_t> events;
+  std::vector<int> stage;
+};
+
+// Grid-map construction and the H|psi> launcher (hpsi.cu).
+Status build_grid_maps(Handle& h, const int* miller_host);
+Status apply_h_device(Handle& h, int spin, int ik, const double2* psi, long ldpsi, int nb, double2* hpsi,
+                      long ldh, int precision, cudaStream_t stream, StageTimer* timer = nullptr);
+Status set_veff_from_g(Handle& h, int spin, const double2* veff_g_dev, cudaStream_t stream);
+Status ensure_nl_capacity(Handle& h, int nb);
+
+// 3-D FFT of a full grid (unnormalised), sign -1 forward / +1 inverse,
+// in place on device memory (used for potentials and density paths).
+Status fft3d_full(Handle& h, double2* data, int sign, cudaStream_t stream);
+
+}  // namespace pwgpu

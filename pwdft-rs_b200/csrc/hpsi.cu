@@ -1,0 +1,519 @@
+// H|psi> for a block of bands: kinetic diagonal + local potential through
+// sphere-pruned batched 3-D FFTs + Kleinman-Bylander nonlocal GEMMs.
+//
+// Replaces the dense per-k Hamiltonian of the reference
+// (fill_hamiltonian_with_v_eff, scf/potentials.rs:163-190, plus
+// NonlocalPotential::add_to_hamiltonian, potential/nonlocal.rs:432-450).
+// The FFT form is exactly the dense form: with psi(r) and V(r) the
+// unnormalised inverse transforms, (V psi)(G_i) = (1/N) FFT(V psi)[G_i]
+// collects V(G) psi_j for every G == G_i - G_j on the wrapped grid, which
+// is V_eff[miller_to_idx(m_i - m_j)] of the dense matrix.
+//
+// Pipeline per chunk of bands (intermediates sized to stay in L2):
+//   K1 z-inverse on the Xp*Yp sphere columns, scattering psi(G)   -> A
+//   K2 y-inverse per compact x-plane                               A -> B
+//   K3 x-inverse, multiply by V(r), x-forward (in place)           B
+//   K4 y-forward, keep the Yp sphere rows                          B -> A
+//   K5 z-forward, gather the sphere, scale 1/N, add T psi          A -> Hpsi
+// then  P = B^H psi,  Q = D P (block diagonal),  Hpsi += B Q.
+#include <cublas_v2.h>
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <type_traits>
+#include <vector>
+
+#include "fft_smem.cuh"
+#include "handle.hpp"
+
+namespace pwgpu {
+
+namespace {
+
+constexpr int kThreads = 128;
+constexpr int kTileElems = 1024;
+
+__device__ __forceinline__ int wrap_idx(int n, int d) { return n < 0 ? n + d : n; }
+
+template <typename C> __device__ __forceinline__ C to_c(double2 v) { return cmake<C>(v.x, v.y); }
+
+// K1: scatter sphere coefficients of W columns and z-inverse-FFT them.
+template <typename R>
+__global__ void __launch_bounds__(kThreads) k_zinv(const double2* __restrict__ psi, long ldpsi,
+                                                  cplx<R>* __restrict__ A, const int* __restrict__ col_start,
+                                                  const int* __restrict__ pt_ig, const int* __restrict__ pt_col,
+                                                  const int* __restrict__ pt_z, int ncol, int d2, int W,
+                                                  FftPlan pz, const cplx<R>* __restrict__ twz) {
+  using C = cplx<R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int c0 = blockIdx.x * W;
+  const int b = blockIdx.y;
+  const int nl = min(W, ncol - c0);
+  const int tile = W * d2;
+  C* scr = buf + tile;
+  for (int i = threadIdx.x; i < tile; i += blockDim.x) buf[i] = cmake<C>(0.0, 0.0);
+  __syncthreads();
+  const double2* ps = psi + (long)b * ldpsi;
+  const int i0 = col_start[c0], i1 = col_start[c0 + nl];
+  for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+    buf[(pt_col[i] - c0) * d2 + pt_z[i]] = to_c<C>(ps[pt_ig[i]]);
+  }
+  __syncthreads();
+  const C* res = fft_lines<+1>(buf, scr, pz, W, LineMap{d2, 1}, twz);
+  C* out = A + ((long)b * ncol + c0) * d2;
+  for (int i = threadIdx.x; i < nl * d2; i += blockDim.x) out[i] = res[i];
+}
+
+// K5: z-forward-FFT W columns, gather the sphere, Hpsi = buf/N + T psi.
+template <typename R>
+__global__ void __launch_bounds__(kThreads) k_zfwd(const cplx<R>* __restrict__ A, const double2* __restrict__ psi,
+                                                  long ldpsi, double2* __restrict__ hpsi, long ldh,
+                                                  const double* __restrict__ kin, double scale,
+                                                  const int* __restrict__ col_start, const int* __restrict__ pt_ig,
+                                                  const int* __restrict__ pt_col, const int* __restrict__ pt_z,
+                                                  int ncol, int d2, int W, FftPlan pz,
+                                                  const cplx<R>* __restrict__ twz) {
+  using C = cplx<R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int c0 = blockIdx.x * W;
+  const int b = blockIdx.y;
+  const int nl = min(W, ncol - c0);
+  const C* in = A + ((long)b * ncol + c0) * d2;
+  C* scr = buf + W * d2;
+  for (int i = threadIdx.x; i < W * d2; i += blockDim.x) buf[i] = (i < nl * d2) ? in[i] : cmake<C>(0.0, 0.0);
+  __syncthreads();
+  const C* res = fft_lines<-1>(buf, scr, pz, W, LineMap{d2, 1}, twz);
+  const double2* ps = psi + (long)b * ldpsi;
+  double2* hs = hpsi + (long)b * ldh;
+  const int i0 = col_start[c0], i1 = col_start[c0 + nl];
+  for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+    const int ig = pt_ig[i];
+    const C v = res[(pt_col[i] - c0) * d2 + pt_z[i]];
+    const double2 p = ps[ig];
+    const double t = kin[ig];
+    hs[ig] = make_double2((double)v.x * scale + t * p.x, (double)v.y * scale + t * p.y);
+  }
+}
+
+// K2 (S=+1): rows q<Yp of A -> y-inverse -> all d1 rows of B.
+// K4 (S=-1): all d1 rows of B -> y-forward -> rows q<Yp of A.
+template <typename R, int S>
+__global__ void __launch_bounds__(kThreads) k_y(cplx<R>* __restrict__ A, cplx<R>* __restrict__ B, int Xp, int Yp,
+                                               int m1, int d1, int d2, int W, FftPlan py,
+                                               const cplx<R>* __restrict__ twy) {
+  using C = cplx<R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int p = blockIdx.x;
+  const int z0 = blockIdx.y * W;
+  const int b = blockIdx.z;
+  const int zn = min(W, d2 - z0);
+  const long ncol = (long)Xp * Yp;
+  C* scr = buf + d1 * W;
+  C* a_base = A + ((long)b * ncol + (long)p * Yp) * d2 + z0;
+  C* b_base = B + (((long)b * Xp + p) * d1) * d2 + z0;
+  if (S > 0) {
+    for (int i = threadIdx.x; i < d1 * W; i += blockDim.x) buf[i] = cmake<C>(0.0, 0.0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < Yp * W; i += blockDim.x) {
+      const int q = i / W, w = i - q * W;
+      if (w < zn) buf[wrap_idx(q - m1, d1) * W + w] = a_base[(long)q * d2 + w];
+    }
+  } else {
+    for (int i = threadIdx.x; i < d1 * W; i += blockDim.x) {
+      const int y = i / W, w = i - y * W;
+      buf[i] = (w < zn) ? b_base[(long)y * d2 + w] : cmake<C>(0.0, 0.0);
+    }
+  }
+  __syncthreads();
+  const C* res = fft_lines<S>(buf, scr, py, W, LineMap{1, W}, twy);
+  if (S > 0) {
+    for (int i = threadIdx.x; i < d1 * W; i += blockDim.x) {
+      const int y = i / W, w = i - y * W;
+      if (w < zn) b_base[(long)y * d2 + w] = res[i];
+    }
+  } else {
+    for (int i = threadIdx.x; i < Yp * W; i += blockDim.x) {
+      const int q = i / W, w = i - q * W;
+      if (w < zn) a_base[(long)q * d2 + w] = res[wrap_idx(q - m1, d1) * W + w];
+    }
+  }
+}
+
+// K3: compact x rows of B -> x-inverse -> * V(r) -> x-forward -> compact rows.
+template <typename R>
+__global__ void __launch_bounds__(kThreads) k_xv(cplx<R>* __restrict__ B, const R* __restrict__ vr, int Xp, int m0,
+                                                int d0, int d1, int d2, int W, FftPlan px,
+                                                const cplx<R>* __restrict__ twx) {
+  using C = cplx<R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int y = blockIdx.x;
+  const int z0 = blockIdx.y * W;
+  const int b = blockIdx.z;
+  const int zn = min(W, d2 - z0);
+  const long plane = (long)d1 * d2;
+  C* base = B + (long)b * Xp * plane + (long)y * d2 + z0;
+  C* scr = buf + d0 * W;
+  for (int i = threadIdx.x; i < d0 * W; i += blockDim.x) buf[i] = cmake<C>(0.0, 0.0);
+  __syncthreads();
+  for (int i = threadIdx.x; i < Xp * W; i += blockDim.x) {
+    const int p = i / W, w = i - p * W;
+    if (w < zn) buf[wrap_idx(p - m0, d0) * W + w] = base[(long)p * plane + w];
+  }
+  __syncthreads();
+  C* r1 = fft_lines<+1>(buf, scr, px, W, LineMap{1, W}, twx);
+  const R* vb = vr + (long)y * d2 + z0;
+  for (int i = threadIdx.x; i < d0 * W; i += blockDim.x) {
+    const int x = i / W, w = i - x * W;
+    if (w < zn) r1[i] = r1[i] * vb[(long)x * plane + w];
+  }
+  __syncthreads();
+  const C* r2 = fft_lines<-1>(r1, r1 == buf ? scr : buf, px, W, LineMap{1, W}, twx);
+  for (int i = threadIdx.x; i < Xp * W; i += blockDim.x) {
+    const int p = i / W, w = i - p * W;
+    if (w < zn) base[(long)p * plane + w] = r2[wrap_idx(p - m0, d0) * W + w];
+  }
+}
+
+// Full-grid line FFT along one axis, grid viewed as [outer][L][inner].
+// inner == 1: a tile is W consecutive rows (contiguous lines);
+// inner > 1:  a tile is one outer index and W consecutive inner offsets.
+template <int S>
+__global__ void __launch_bounds__(kThreads) k_fft_axis(double2* __restrict__ g, long nbatch_stride, int outer, int L,
+                                                      int inner, int W, FftPlan p, const double2* __restrict__ tw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* buf = reinterpret_cast<double2*>(smem_raw);
+  double2* gb = g + (long)blockIdx.z * nbatch_stride;
+  if (inner == 1) {
+    const int r0 = blockIdx.x * W;
+    const int nl = min(W, outer - r0);
+    double2* src = gb + (long)r0 * L;
+    for (int i = threadIdx.x; i < W * L; i += blockDim.x) buf[i] = (i < nl * L) ? src[i] : make_double2(0.0, 0.0);
+    __syncthreads();
+    const double2* res = fft_lines<S>(buf, buf + W * L, p, W, LineMap{L, 1}, tw);
+    for (int i = threadIdx.x; i < nl * L; i += blockDim.x) src[i] = res[i];
+  } else {
+    const int o = blockIdx.y;
+    const int i0 = blockIdx.x * W;
+    const int zn = min(W, inner - i0);
+    double2* src = gb + (long)o * L * inner + i0;
+    for (int i = threadIdx.x; i < L * W; i += blockDim.x) {
+      const int l = i / W, w = i - l * W;
+      buf[i] = (w < zn) ? src[(long)l * inner + w] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    const double2* res = fft_lines<S>(buf, buf + W * L, p, W, LineMap{1, W}, tw);
+    for (int i = threadIdx.x; i < L * W; i += blockDim.x) {
+      const int l = i / W, w = i - l * W;
+      if (w < zn) src[(long)l * inner + w] = res[i];
+    }
+  }
+}
+
+// Q = D P with D block-diagonal over atoms (each block dense, row-major).
+__global__ void k_apply_d(const double2* __restrict__ P, double2* __restrict__ Q, int n_ch, int nb,
+                          const int* __restrict__ ch_atom, const int* __restrict__ atom_ch_start,
+                          const int* __restrict__ d_off, const double* __restrict__ d_vals) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)n_ch * nb) return;
+  const int c = (int)(t % n_ch);
+  const int b = (int)(t / n_ch);
+  const int a = ch_atom[c];
+  const int s = atom_ch_start[a];
+  const int nc = atom_ch_start[a + 1] - s;
+  const double* drow = d_vals + d_off[a] + (long)(c - s) * nc;
+  const double2* pcol = P + (long)b * n_ch + s;
+  double re = 0.0, im = 0.0;
+  for (int j = 0; j < nc; ++j) {
+    const double dv = drow[j];
+    re += dv * pcol[j].x;
+    im += dv * pcol[j].y;
+  }
+  Q[(long)b * n_ch + c] = make_double2(re, im);
+}
+
+__global__ void k_real_to_r32(const double2* __restrict__ in, double* __restrict__ out64, float* __restrict__ out32,
+                              long n) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    out64[i] = in[i].x;
+    out32[i] = (float)in[i].x;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host helpers
+// ---------------------------------------------------------------------------
+
+bool make_plan(int L, FftPlan& p) {
+  p.L = L;
+  p.nstages = 0;
+  int rem = L;
+  std::vector<int> rad;
+  while (rem % 8 == 0 && rem > 1) { rad.push_back(8); rem /= 8; }
+  while (rem % 4 == 0) { rad.push_back(4); rem /= 4; }
+  while (rem % 2 == 0) { rad.push_back(2); rem /= 2; }
+  while (rem % 5 == 0) { rad.push_back(5); rem /= 5; }
+  while (rem % 3 == 0) { rad.push_back(3); rem /= 3; }
+  if (rem != 1 || (int)rad.size() > kMaxStages) return false;
+  int ns = 1;
+  for (size_t s = 0; s < rad.size(); ++s) {
+    p.radix[s] = rad[s];
+    p.ns[s] = ns;
+    ns *= rad[s];
+  }
+  p.nstages = (int)rad.size();
+  return true;
+}
+
+// Tile width (lines per block): about kTileElems elements per tile.
+int pick_w(const FftPlan& p, int cap) {
+  return std::max(1, std::min(cap, kTileElems / std::max(1, p.L)));
+}
+
+// Balance W over n items: ceil(n / ceil(n / wmax)).
+int balance_w(int n, int wmax) {
+  if (n <= 0) return 1;
+  const int chunks = (n + wmax - 1) / wmax;
+  return (n + chunks - 1) / chunks;
+}
+
+template <typename T> Status dalloc(T** p, size_t count) {
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (e != cudaSuccess) return fail(kOom, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  return kOk;
+}
+
+}  // namespace
+
+Status build_grid_maps(Handle& h, const int* miller) {
+  GridMaps& g = h.g;
+  for (int a = 0; a < 3; ++a) {
+    if (!make_plan(g.d[a], g.plan[a]))
+      return fail(kNotImplemented, "FFT length " + std::to_string(g.d[a]) + " is not 2,3,5-smooth (or too long)");
+  }
+  g.N = (long)g.d[0] * g.d[1] * g.d[2];
+  int m[3] = {0, 0, 0};
+  for (int i = 0; i < h.n_pw; ++i)
+    for (int a = 0; a < 3; ++a) m[a] = std::max(m[a], std::abs(miller[3 * i + a]));
+  for (int a = 0; a < 3; ++a) {
+    if (2 * m[a] + 1 > g.d[a])
+      return fail(kInvalid, "FFT grid dimension " + std::to_string(g.d[a]) + " on axis " + std::to_string(a) +
+                                " is smaller than 2*max|n|+1 = " + std::to_string(2 * m[a] + 1) +
+                                "; sphere points would alias");
+    g.m[a] = m[a];
+  }
+  g.Xp = 2 * m[0] + 1;
+  g.Yp = 2 * m[1] + 1;
+  g.ncol = g.Xp * g.Yp;
+  // sort points by column, stable in basis order
+  std::vector<int> col(h.n_pw), order(h.n_pw), zi(h.n_pw), gf(h.n_pw);
+  for (int i = 0; i < h.n_pw; ++i) {
+    const int n0 = miller[3 * i], n1 = miller[3 * i + 1], n2 = miller[3 * i + 2];
+    col[i] = (n0 + m[0]) * g.Yp + (n1 + m[1]);
+    zi[i] = n2 < 0 ? n2 + g.d[2] : n2;
+    const int x = n0 < 0 ? n0 + g.d[0] : n0, y = n1 < 0 ? n1 + g.d[1] : n1;
+    gf[i] = (x * g.d[1] + y) * g.d[2] + zi[i];
+  }
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return col[a] < col[b]; });
+  std::vector<int> cs(g.ncol + 1, 0), pig(h.n_pw), pcol(h.n_pw), pz(h.n_pw);
+  for (int s = 0; s < h.n_pw; ++s) {
+    const int i = order[s];
+    pig[s] = i;
+    pcol[s] = col[i];
+    pz[s] = zi[i];
+    cs[col[i] + 1]++;
+  }
+  for (int c = 0; c < g.ncol; ++c) cs[c + 1] += cs[c];
+  Status st;
+  if ((st = dalloc(&g.col_start, g.ncol + 1)) != kOk) return st;
+  if ((st = dalloc(&g.pt_ig, h.n_pw)) != kOk) return st;
+  if ((st = dalloc(&g.pt_col, h.n_pw)) != kOk) return st;
+  if ((st = dalloc(&g.pt_z, h.n_pw)) != kOk) return st;
+  if ((st = dalloc(&g.g_to_fft, h.n_pw)) != kOk) return st;
+  PW_CUDA_TRY(cudaMemcpy(g.col_start, cs.data(), cs.size() * sizeof(int), cudaMemcpyHostToDevice));
+  PW_CUDA_TRY(cudaMemcpy(g.pt_ig, pig.data(), h.n_pw * sizeof(int), cudaMemcpyHostToDevice));
+  PW_CUDA_TRY(cudaMemcpy(g.pt_col, pcol.data(), h.n_pw * sizeof(int), cudaMemcpyHostToDevice));
+  PW_CUDA_TRY(cudaMemcpy(g.pt_z, pz.data(), h.n_pw * sizeof(int), cudaMemcpyHostToDevice));
+  PW_CUDA_TRY(cudaMemcpy(g.g_to_fft, gf.data(), h.n_pw * sizeof(int), cudaMemcpyHostToDevice));
+  // twiddle tables tw[m] = exp(-2 pi i m / L) in extended precision
+  for (int a = 0; a < 3; ++a) {
+    const int L = g.d[a];
+    std::vector<double2> t64(L);
+    std::vector<float2> t32(L);
+    for (int k = 0; k < L; ++k) {
+      const long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)k / (long double)L;
+      t64[k] = make_double2((double)cosl(ang), (double)sinl(ang));
+      t32[k] = make_float2((float)t64[k].x, (float)t64[k].y);
+    }
+    if ((st = dalloc(&g.tw64[a], L)) != kOk) return st;
+    if ((st = dalloc(&g.tw32[a], L)) != kOk) return st;
+    PW_CUDA_TRY(cudaMemcpy(g.tw64[a], t64.data(), L * sizeof(double2), cudaMemcpyHostToDevice));
+    PW_CUDA_TRY(cudaMemcpy(g.tw32[a], t32.data(), L * sizeof(float2), cudaMemcpyHostToDevice));
+  }
+  g.wz = balance_w(g.ncol, pick_w(g.plan[2], 64));
+  g.wy = balance_w(g.d[2], pick_w(g.plan[1], 64));
+  g.wx = balance_w(g.d[2], pick_w(g.plan[0], 64));
+  // band chunk: keep A + B of one chunk within ~48 MB (FP64) of L2
+  const double per_band = 16.0 * ((double)g.ncol * g.d[2] + (double)g.Xp * g.d[1] * g.d[2]);
+  h.chunk = std::max(1, std::min(64, (int)(48.0e6 / per_band)));
+  if ((st = dalloc((double2**)&h.work_a, (size_t)h.chunk * g.ncol * g.d[2])) != kOk) return st;
+  if ((st = dalloc((double2**)&h.work_b, (size_t)h.chunk * g.Xp * g.d[1] * g.d[2])) != kOk) return st;
+  if ((st = dalloc(&h.tmp_grid, (size_t)g.N)) != kOk) return st;
+  return kOk;
+}
+
+Status ensure_nl_capacity(Handle& h, int nb) {
+  if (nb <= h.nl_cap) return kOk;
+  if (h.nl_p) cudaFree(h.nl_p);
+  if (h.nl_q) cudaFree(h.nl_q);
+  h.nl_p = h.nl_q = nullptr;
+  Status st;
+  if ((st = dalloc(&h.nl_p, (size_t)std::max(1, h.n_ch) * nb)) != kOk) return st;
+  if ((st = dalloc(&h.nl_q, (size_t)std::max(1, h.n_ch) * nb)) != kOk) return st;
+  h.nl_cap = nb;
+  return kOk;
+}
+
+Status fft3d_full(Handle& h, double2* data, int sign, cudaStream_t stream) {
+  GridMaps& g = h.g;
+  const int d0 = g.d[0], d1 = g.d[1], d2 = g.d[2];
+  struct Ax { int outer, L, inner, a; };
+  const Ax axes[3] = {{d0 * d1, d2, 1, 2}, {d0, d1, d2, 1}, {1, d0, d1 * d2, 0}};
+  for (const Ax& ax : axes) {
+    const FftPlan& p = g.plan[ax.a];
+    if (p.nstages == 0) continue;
+    int W;
+    dim3 grid;
+    if (ax.inner == 1) {
+      W = balance_w(ax.outer, pick_w(p, 64));
+      grid = dim3((ax.outer + W - 1) / W, 1, 1);
+    } else {
+      W = balance_w(ax.inner, pick_w(p, 64));
+      grid = dim3((ax.inner + W - 1) / W, ax.outer, 1);
+    }
+    const size_t sm = 2 * (size_t)W * ax.L * sizeof(double2);
+    if (sign < 0)
+      k_fft_axis<-1><<<grid, kThreads, sm, stream>>>(data, 0, ax.outer, ax.L, ax.inner, W, p, g.tw64[ax.a]);
+    else
+      k_fft_axis<+1><<<grid, kThreads, sm, stream>>>(data, 0, ax.outer, ax.L, ax.inner, W, p, g.tw64[ax.a]);
+  }
+  PW_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
+Status set_veff_from_g(Handle& h, int spin, const double2* veff_g_dev, cudaStream_t stream) {
+  const long N = h.g.N;
+  PW_CUDA_TRY(cudaMemcpyAsync(h.tmp_grid, veff_g_dev, N * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
+  Status st = fft3d_full(h, h.tmp_grid, +1, stream);
+  if (st != kOk) return st;
+  k_real_to_r32<<<(unsigned)((N + 255) / 256), 256, 0, stream>>>(h.tmp_grid, h.veff_r[spin], h.veff_r32[spin], N);
+  PW_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
+// Records an event after each launch when profiling (stage timings).
+static inline void mark(StageTimer* t, int stage, cudaStream_t s) {
+  if (!t) return;
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  cudaEventRecord(e, s);
+  t->events.push_back(e);
+  t->stage.push_back(stage);
+}
+
+template <typename R>
+static Status local_chunk(Handle& h, int spin, int ik, const double2* psi, long ldpsi, int nb, double2* hpsi,
+                          long ldh, cudaStream_t s, StageTimer* tm) {
+  using C = cplx<R>;
+  GridMaps& g = h.g;
+  const int d0 = g.d[0], d1 = g.d[1], d2 = g.d[2];
+  C* A = reinterpret_cast<C*>(h.work_a);
+  C* B = reinterpret_cast<C*>(h.work_b);
+  const C* tw0 = std::is_same<R, double>::value ? (const C*)g.tw64[0] : (const C*)g.tw32[0];
+  const C* tw1 = std::is_same<R, double>::value ? (const C*)g.tw64[1] : (const C*)g.tw32[1];
+  const C* tw2 = std::is_same<R, double>::value ? (const C*)g.tw64[2] : (const C*)g.tw32[2];
+  const R* vr = std::is_same<R, double>::value ? (const R*)h.veff_r[spin] : (const R*)h.veff_r32[spin];
+  const double scale = 1.0 / (double)g.N;
+  {
+    dim3 grid((g.ncol + g.wz - 1) / g.wz, nb);
+    k_zinv<R><<<grid, kThreads, 2 * (size_t)g.wz * d2 * sizeof(C), s>>>(psi, ldpsi, A, g.col_start, g.pt_ig, g.pt_col,
+                                                                      g.pt_z, g.ncol, d2, g.wz, g.plan[2], tw2);
+    mark(tm, 0, s);
+  }
+  {
+    dim3 grid(g.Xp, (d2 + g.wy - 1) / g.wy, nb);
+    k_y<R, +1><<<grid, kThreads, 2 * (size_t)g.wy * d1 * sizeof(C), s>>>(A, B, g.Xp, g.Yp, g.m[1], d1, d2, g.wy,
+                                                                       g.plan[1], tw1);
+    mark(tm, 1, s);
+  }
+  {
+    dim3 grid(d1, (d2 + g.wx - 1) / g.wx, nb);
+    k_xv<R><<<grid, kThreads, 2 * (size_t)g.wx * d0 * sizeof(C), s>>>(B, vr, g.Xp, g.m[0], d0, d1, d2, g.wx, g.plan[0],
+                                                                    tw0);
+    mark(tm, 2, s);
+  }
+  {
+    dim3 grid(g.Xp, (d2 + g.wy - 1) / g.wy, nb);
+    k_y<R, -1><<<grid, kThreads, 2 * (size_t)g.wy * d1 * sizeof(C), s>>>(A, B, g.Xp, g.Yp, g.m[1], d1, d2, g.wy,
+                                                                       g.plan[1], tw1);
+    mark(tm, 3, s);
+  }
+  {
+    dim3 grid((g.ncol + g.wz - 1) / g.wz, nb);
+    k_zfwd<R><<<grid, kThreads, 2 * (size_t)g.wz * d2 * sizeof(C), s>>>(A, psi, ldpsi, hpsi, ldh, h.kp[ik].kinetic,
+                                                                      scale, g.col_start, g.pt_ig, g.pt_col, g.pt_z,
+                                                                      g.ncol, d2, g.wz, g.plan[2], tw2);
+    mark(tm, 4, s);
+  }
+  PW_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
+Status apply_h_device(Handle& h, int spin, int ik, const double2* psi, long ldpsi, int nb, double2* hpsi, long ldh,
+                      int precision, cudaStream_t s, StageTimer* tm) {
+  if (ik < 0 || ik >= h.n_k) return fail(kInvalid, "apply_h: k-point index out of range");
+  if (spin < 0 || spin >= h.nspin) return fail(kInvalid, "apply_h: spin index out of range");
+  if (nb <= 0) return kOk;
+  if (ldpsi < h.n_pw || ldh < h.n_pw) return fail(kInvalid, "apply_h: leading dimension smaller than n_pw");
+  Status st;
+  mark(tm, -1, s);
+  for (int c0 = 0; c0 < nb; c0 += h.chunk) {
+    const int cnt = std::min(h.chunk, nb - c0);
+    if (precision == 0)
+      st = local_chunk<double>(h, spin, ik, psi + (long)c0 * ldpsi, ldpsi, cnt, hpsi + (long)c0 * ldh, ldh, s, tm);
+    else
+      st = local_chunk<float>(h, spin, ik, psi + (long)c0 * ldpsi, ldpsi, cnt, hpsi + (long)c0 * ldh, ldh, s, tm);
+    if (st != kOk) return st;
+  }
+  if (h.n_ch > 0) {
+    if ((st = ensure_nl_capacity(h, nb)) != kOk) return st;
+    cublasSetStream(h.blas, s);
+    const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+    const cuDoubleComplex* Bm = reinterpret_cast<const cuDoubleComplex*>(h.kp[ik].b);
+    cublasStatus_t cs = cublasZgemm(h.blas, CUBLAS_OP_C, CUBLAS_OP_N, h.n_ch, nb, h.n_pw, &one, Bm, h.n_pw,
+                                    reinterpret_cast<const cuDoubleComplex*>(psi), (int)ldpsi, &zero,
+                                    reinterpret_cast<cuDoubleComplex*>(h.nl_p), h.n_ch);
+    if (cs != CUBLAS_STATUS_SUCCESS) return fail(kCuda, "cublasZgemm (B^H psi) failed");
+    mark(tm, 5, s);
+    const long tot = (long)h.n_ch * nb;
+    k_apply_d<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(h.nl_p, h.nl_q, h.n_ch, nb, h.ch_atom, h.atom_ch_start,
+                                                            h.d_off, h.d_vals);
+    mark(tm, 6, s);
+    cs = cublasZgemm(h.blas, CUBLAS_OP_N, CUBLAS_OP_N, h.n_pw, nb, h.n_ch, &one, Bm, h.n_pw,
+                     reinterpret_cast<const cuDoubleComplex*>(h.nl_q), h.n_ch, &one,
+                     reinterpret_cast<cuDoubleComplex*>(hpsi), (int)ldh);
+    if (cs != CUBLAS_STATUS_SUCCESS) return fail(kCuda, "cublasZgemm (B Q) failed");
+    mark(tm, 7, s);
+    PW_CUDA_TRY(cudaGetLastError());
+  }
+  return kOk;
+}
+
+}  // namespace pwgpu

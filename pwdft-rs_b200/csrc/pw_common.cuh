@@ -1,0 +1,78 @@
+// Common device/host helpers for the pwgpu library: complex arithmetic on
+// double2/float2, error plumbing, and the per-length FFT plan descriptor.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+namespace pwgpu {
+
+template <typename R> struct cvec;
+template <> struct cvec<double> { using type = double2; };
+template <> struct cvec<float> { using type = float2; };
+template <typename R> using cplx = typename cvec<R>::type;
+
+template <typename C> __host__ __device__ __forceinline__ C cmake(double re, double im) {
+  C c; c.x = re; c.y = im; return c;
+}
+__host__ __device__ __forceinline__ double2 operator+(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ double2 operator-(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ double2 operator*(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__host__ __device__ __forceinline__ float2 operator+(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ float2 operator-(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ float2 operator*(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+
+template <typename C> __host__ __device__ __forceinline__ C cmul(C a, C b) {
+  C c; c.x = a.x * b.x - a.y * b.y; c.y = a.x * b.y + a.y * b.x; return c;
+}
+// a * conj(b)
+template <typename C> __host__ __device__ __forceinline__ C cmulc(C a, C b) {
+  C c; c.x = a.x * b.x + a.y * b.y; c.y = a.y * b.x - a.x * b.y; return c;
+}
+// multiply by S*i where S = +1 or -1
+template <int S, typename C> __host__ __device__ __forceinline__ C mul_si(C a) {
+  C c;
+  if (S > 0) { c.x = -a.y; c.y = a.x; } else { c.x = a.y; c.y = -a.x; }
+  return c;
+}
+
+// Maximum number of radix stages per 1-D length (1024 = 8^3 * 2 needs 4).
+constexpr int kMaxStages = 8;
+
+// 1-D FFT plan for one length L = prod(radix[s]), radices in {2,3,4,5,8}.
+// ns[s] = product of the radices of the stages before s (Stockham stride).
+struct FftPlan {
+  int L;
+  int nstages;
+  int radix[kMaxStages];
+  int ns[kMaxStages];
+};
+
+// Status codes shared with include/pwgpu.h.
+enum Status : int {
+  kOk = 0,
+  kInvalid = -1,
+  kCuda = -2,
+  kOom = -3,
+  kNotConverged = -4,
+  kTimeout = -5,
+  kNotImplemented = -6,
+  kState = -7,
+};
+
+struct Error {
+  int code = kOk;
+  std::string msg;
+};
+
+}  // namespace pwgpu
+
+#define PW_CUDA_TRY(expr)                                                              \
+  do {                                                                                 \
+    cudaError_t _e = (expr);                                                           \
+    if (_e != cudaSuccess) {                                                           \
+      return ::pwgpu::fail(::pwgpu::kCuda, std::string(#expr ": ") + cudaGetErrorString(_e)); \
+    }                                                                                  \
+  } while (0)

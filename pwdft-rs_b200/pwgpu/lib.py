@@ -1,0 +1,224 @@
+"""ctypes binding of libpwgpu.so (include/pwgpu.h).
+
+`PwGpu(system)` uploads an ScfSystem (pwgpu.context) and exposes the C-ABI
+entry points with numpy arrays.  Loading fails loudly when the shared
+library is missing: there is no CPU fallback in the product path.
+"""
+
+from __future__ import annotations
+
+import ctypes as ct
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libpwgpu.so")
+
+PWGPU_OK = 0
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+
+ERROR_NAMES = {
+    -1: "PWGPU_E_INVALID", -2: "PWGPU_E_CUDA", -3: "PWGPU_E_OOM", -4: "PWGPU_E_NOT_CONVERGED",
+    -5: "PWGPU_E_TIMEOUT", -6: "PWGPU_E_NOT_IMPLEMENTED", -7: "PWGPU_E_STATE",
+}
+
+
+class PwGpuError(RuntimeError):
+    """A pwgpu entry point returned a negative status (PwdftError analogue)."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"{ERROR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+_i32p = ct.POINTER(ct.c_int32)
+_f64p = ct.POINTER(ct.c_double)
+
+
+class PwgpuSystem(ct.Structure):
+    _fields_ = [
+        ("dims", ct.c_int32 * 3),
+        ("n_pw", ct.c_int32),
+        ("miller", _i32p),
+        ("n_k", ct.c_int32),
+        ("k_weights", _f64p),
+        ("kinetic", _f64p),
+        ("n_ch", ct.c_int32),
+        ("proj_b", _f64p),
+        ("n_atoms", ct.c_int32),
+        ("atom_ch_start", _i32p),
+        ("d_blocks", _f64p),
+        ("v_local_g", _f64p),
+        ("g_squared", _f64p),
+        ("rho_core_r", _f64p),
+        ("n_sym", ct.c_int32),
+        ("sym_src", _i32p),
+        ("sym_arg", _f64p),
+        ("n_electrons", ct.c_double),
+        ("omega", ct.c_double),
+        ("e_ewald", ct.c_double),
+        ("nspin", ct.c_int32),
+    ]
+
+
+class PwgpuOptions(ct.Structure):
+    _fields_ = [("device", ct.c_int32), ("precision", ct.c_int32)]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libpwgpu.so; raises OSError if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise OSError(f"libpwgpu.so not found at {path}; build it with `python -m pwgpu.build`")
+    lib = ct.CDLL(path)
+    vp = ct.c_void_p
+    lib.pwgpu_last_error.restype = ct.c_char_p
+    lib.pwgpu_version.restype = ct.c_char_p
+    lib.pwgpu_create.argtypes = [ct.POINTER(PwgpuSystem), ct.POINTER(PwgpuOptions), ct.POINTER(vp)]
+    lib.pwgpu_destroy.argtypes = [vp]
+    lib.pwgpu_set_veff_g.argtypes = [vp, ct.c_int32, _f64p]
+    lib.pwgpu_apply_h.argtypes = [vp, ct.c_int32, ct.c_int32, _f64p, ct.c_int32, _f64p]
+    lib.pwgpu_apply_h_device.argtypes = [vp, ct.c_int32, ct.c_int32, vp, ct.c_int64, ct.c_int32, vp, ct.c_int64, vp]
+    lib.pwgpu_set_precision.argtypes = [vp, ct.c_int32]
+    lib.pwgpu_profile_apply_h.argtypes = [vp, ct.c_int32, ct.c_int32, vp, ct.c_int64, ct.c_int32, vp, ct.c_int64,
+                                          _f64p, _i32p]
+    lib.pwgpu_get_dims.argtypes = [vp, _i32p, ct.POINTER(ct.c_int64), _i32p]
+    for name in ("pwgpu_create", "pwgpu_destroy", "pwgpu_set_veff_g", "pwgpu_apply_h", "pwgpu_apply_h_device",
+                 "pwgpu_set_precision", "pwgpu_get_dims", "pwgpu_profile_apply_h"):
+        getattr(lib, name).restype = ct.c_int32
+    _lib = lib
+    return lib
+
+
+def _check(lib, rc):
+    if rc != PWGPU_OK:
+        raise PwGpuError(rc, lib.pwgpu_last_error().decode(errors="replace"))
+
+
+def _f64(a):
+    return a.ctypes.data_as(_f64p)
+
+
+def _i32(a):
+    return a.ctypes.data_as(_i32p)
+
+
+def pack_system(sys_) -> tuple:
+    """Flatten an ScfSystem into the pwgpu_system POD.  Returns (struct, keepalive)."""
+    keep = []
+
+    def hold(a):
+        keep.append(a)
+        return a
+
+    n_pw = sys_.n_pw
+    miller = hold(np.ascontiguousarray(sys_.basis.miller, dtype=np.int32))
+    kw = hold(np.ascontiguousarray(sys_.kpt_weights, dtype=np.float64))
+    kin = hold(np.ascontiguousarray(np.stack(sys_.kinetic), dtype=np.float64))
+    projs = sys_.projectors
+    n_ch = projs[0].n_ch if projs else 0
+    s = PwgpuSystem()
+    s.dims[:] = list(sys_.dims)
+    s.n_pw = n_pw
+    s.miller = _i32(miller)
+    s.n_k = len(sys_.kpoints)
+    s.k_weights = _f64(kw)
+    s.kinetic = _f64(kin)
+    s.n_ch = n_ch
+    if n_ch:
+        b = hold(np.concatenate([np.asfortranarray(p.b).ravel(order="F") for p in projs]).astype(np.complex128))
+        starts = hold(np.ascontiguousarray(projs[0].atom_ch_start, dtype=np.int32))
+        blocks = hold(np.concatenate([blk.ravel() for blk in projs[0].d_blocks]).astype(np.float64))
+        s.proj_b = b.view(np.float64).ctypes.data_as(_f64p)
+        s.n_atoms = len(projs[0].d_blocks)
+        s.atom_ch_start = _i32(starts)
+        s.d_blocks = _f64(blocks)
+    vl = hold(np.ascontiguousarray(sys_.v_local_g, dtype=np.complex128))
+    s.v_local_g = vl.view(np.float64).ctypes.data_as(_f64p)
+    g2 = hold(np.ascontiguousarray(sys_.g_squared, dtype=np.float64))
+    s.g_squared = _f64(g2)
+    if sys_.rho_core_r.size:
+        rc = hold(np.ascontiguousarray(sys_.rho_core_r, dtype=np.float64))
+        s.rho_core_r = _f64(rc)
+    n_sym = sys_.symmetry.n_ops
+    s.n_sym = n_sym
+    if n_sym > 1:
+        from .symmetry import g_space_gather_map
+        src, arg = g_space_gather_map(sys_.dims, sys_.symmetry)
+        src = hold(np.ascontiguousarray(src, dtype=np.int32))
+        arg = hold(np.ascontiguousarray(arg, dtype=np.float64))
+        s.sym_src = _i32(src)
+        s.sym_arg = _f64(arg)
+    s.n_electrons = sys_.n_electrons
+    s.omega = sys_.omega
+    s.e_ewald = sys_.e_ewald
+    s.nspin = sys_.nspin
+    return s, keep
+
+
+class PwGpu:
+    """One device handle (pwgpu_create .. pwgpu_destroy)."""
+
+    def __init__(self, sys_, precision: int = PRECISION_FP64, device: int = 0):
+        self.lib = load_library()
+        self.sys = sys_
+        st, keep = pack_system(sys_)
+        opt = PwgpuOptions(device, precision)
+        h = ct.c_void_p()
+        _check(self.lib, self.lib.pwgpu_create(ct.byref(st), ct.byref(opt), ct.byref(h)))
+        self.h = h
+        self.n_pw = sys_.n_pw
+
+    def close(self):
+        if self.h:
+            self.lib.pwgpu_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_precision(self, precision: int):
+        _check(self.lib, self.lib.pwgpu_set_precision(self.h, precision))
+
+    def set_veff_g(self, veff_g: np.ndarray, spin: int = 0):
+        v = np.ascontiguousarray(veff_g, dtype=np.complex128)
+        _check(self.lib, self.lib.pwgpu_set_veff_g(self.h, spin, v.view(np.float64).ctypes.data_as(_f64p)))
+
+    def apply_h(self, psi: np.ndarray, ik: int = 0, spin: int = 0) -> np.ndarray:
+        p = np.asfortranarray(psi, dtype=np.complex128)
+        if p.ndim == 1:
+            p = p[:, None]
+        nb = p.shape[1]
+        out = np.empty((self.n_pw, nb), dtype=np.complex128, order="F")
+        _check(self.lib, self.lib.pwgpu_apply_h(self.h, spin, ik, p.ravel(order="F").view(np.float64).ctypes.data_as(_f64p),
+                                                nb, out.ravel(order="F").view(np.float64).ctypes.data_as(_f64p)))
+        return out
+
+    def apply_h_device(self, psi_ptr: int, ldpsi: int, nb: int, hpsi_ptr: int, ldh: int, ik: int = 0, spin: int = 0,
+                       stream: int = 0):
+        _check(self.lib, self.lib.pwgpu_apply_h_device(self.h, spin, ik, ct.c_void_p(psi_ptr), ldpsi, nb,
+                                                       ct.c_void_p(hpsi_ptr), ldh, ct.c_void_p(stream or None)))
+
+    def profile_apply_h(self, psi_ptr: int, ldpsi: int, nb: int, hpsi_ptr: int, ldh: int, ik: int = 0, spin: int = 0):
+        """Per-stage device ms and launch counts of one H|psi> call (8 stages)."""
+        ms = np.zeros(8)
+        n = np.zeros(8, dtype=np.int32)
+        _check(self.lib, self.lib.pwgpu_profile_apply_h(self.h, spin, ik, ct.c_void_p(psi_ptr), ldpsi, nb,
+                                                        ct.c_void_p(hpsi_ptr), ldh, _f64(ms), _i32(n)))
+        return ms, n

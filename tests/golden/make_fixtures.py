@@ -1,0 +1,35 @@
+"""Copy the reference's test fixtures used by the parity tests into tests/golden/.
+
+Run once in a checkout that has the reference tree available:
+
+    python tests/golden/make_fixtures.py /root/reference
+
+Copied verbatim (data files, not source):
+  * pseudopotentials/nc/lda/{Si,Si_hgh,C}.upf   -> tests/golden/upf/
+  * data/csv/{vloc_g_si,beta_q_si,dij_si,rho_core_g,vgcmp_phase4}_reference.csv
+                                                 -> tests/golden/csv/
+The SCF goldens (E_total, E_F) are constants in tests/test_oracle_pins.py
+with their reference file:line.
+"""
+
+import os
+import shutil
+import sys
+
+UPFS = ["Si.upf", "Si_hgh.upf", "C.upf"]
+CSVS = ["vloc_g_si_reference.csv", "beta_q_si_reference.csv", "dij_si_reference.csv",
+        "rho_core_g_reference.csv", "vgcmp_phase4_reference.csv"]
+
+
+def main(ref_root: str):
+    here = os.path.dirname(os.path.abspath(__file__))
+    os.makedirs(os.path.join(here, "upf"), exist_ok=True)
+    os.makedirs(os.path.join(here, "csv"), exist_ok=True)
+    for f in UPFS:
+        shutil.copyfile(os.path.join(ref_root, "pseudopotentials", "nc", "lda", f), os.path.join(here, "upf", f))
+    for f in CSVS:
+        shutil.copyfile(os.path.join(ref_root, "data", "csv", f), os.path.join(here, "csv", f))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

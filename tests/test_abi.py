@@ -1,0 +1,46 @@
+"""The C-ABI library loads and exports every entry point include/*.h declares.
+CPU only: symbols are resolved, nothing is computed."""
+
+import ctypes
+import glob
+import os
+import re
+
+from conftest import ROOT
+from pwgpu import lib as L
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b(pwgpu_\w+)\s*\(", text):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    for n in ("pwgpu_create", "pwgpu_destroy", "pwgpu_apply_h", "pwgpu_set_veff_g", "pwgpu_last_error"):
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = L.load_library()
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, f"symbols declared in include/ but not exported: {missing}"
+
+
+def test_version_and_error_strings_callable_without_gpu():
+    lib = L.load_library()
+    assert lib.pwgpu_version().startswith(b"pwgpu")
+    assert isinstance(lib.pwgpu_last_error(), bytes)
+
+
+def test_create_rejects_null_system_without_touching_device():
+    lib = L.load_library()
+    h = ctypes.c_void_p()
+    rc = lib.pwgpu_create(None, None, ctypes.byref(h))
+    assert rc == -1
+    assert b"NULL" in lib.pwgpu_last_error()

@@ -1,0 +1,105 @@
+"""Pins the oracle (and the host setup it consumes) to the reference's own
+golden numbers and component fixtures.  CPU only."""
+
+import math
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from oracle import pwdft_oracle as O
+from pwgpu.consts import BOHR_TO_ANG, RY_TO_EV
+from pwgpu.context import build_system
+from pwgpu.crystal import BasisSet, diamond_primitive, gamma_only
+from pwgpu.symmetry import SymmetryInfo
+from pwgpu.upf import beta_form_factor, sinc_transform, v_local_of_g
+
+
+def _csv(name):
+    path = os.path.join(GOLDEN, "csv", name)
+    with open(path) as f:
+        head = f.readline().strip().split(",")
+        rows = [line.strip().split(",") for line in f if line.strip()]
+    return head, rows
+
+
+def si_omega():
+    return diamond_primitive("Si", 5.431).lattice.volume()
+
+
+def test_vloc_g_matches_reference_csv(si_pp):
+    # tests/vgcmp_vloc_cross_check.rs: tol 1e-4 Ry on 20 shells
+    _, rows = _csv("vloc_g_si_reference.csv")
+    assert len(rows) == 20
+    g = np.array([float(r[1]) for r in rows]) / BOHR_TO_ANG
+    ref = np.array([float(r[3]) for r in rows])
+    got = v_local_of_g(si_pp, g, si_omega()) / RY_TO_EV
+    assert np.max(np.abs(got - ref)) < 1e-4
+
+
+def test_beta_q_matches_reference_csv(si_pp):
+    # tests/vgcmp_beta_q_cross_check.rs: tol 1e-4 Bohr^(3/2)
+    _, rows = _csv("beta_q_si_reference.csv")
+    worst = 0.0
+    for r in rows:
+        ip, l, q = int(r[0]), int(r[1]), float(r[2])
+        assert si_pp.beta_l[ip] == l
+        f = beta_form_factor(si_pp, ip, np.array([q / BOHR_TO_ANG]))[0] / BOHR_TO_ANG ** 1.5
+        worst = max(worst, abs(f - float(r[3])))
+    assert worst < 1e-4
+
+
+def test_dij_matches_reference_csv(si_pp):
+    # tests/vgcmp_dij_cross_check.rs: tol 1e-12 eV
+    _, rows = _csv("dij_si_reference.csv")
+    n = si_pp.n_proj
+    for r in rows:
+        i, j, d = int(r[0]), int(r[1]), float(r[2])
+        assert abs(si_pp.dij[i * n + j] - d * RY_TO_EV) < 1e-12
+
+
+def test_rho_core_g_matches_reference_csv(si_pp):
+    # pseudopotential/upf/parse.rs:236-296 pins; CSV column e/Å³
+    _, rows = _csv("rho_core_g_reference.csv")
+    om = 5.431 ** 3 / 4.0
+    si_rows = [r for r in rows if r[0] == "si"]
+    g = np.array([float(r[2]) for r in si_rows]) / BOHR_TO_ANG
+    ref = np.array([float(r[5]) for r in si_rows])
+    got = 4.0 * math.pi * sinc_transform(si_pp, si_pp.core_charge, True, g) / om
+    assert np.max(np.abs(got - ref)) < 1e-5
+
+
+def test_assembled_h_diagonal_matches_reference_csv(si_pp):
+    # tests/vgcmp_assembled_h_cross_check.rs: kinetic + V_NL diagonal, tol 1e-4 Ry
+    _, rows = _csv("vgcmp_phase4_reference.csv")
+    cr = diamond_primitive("Si", 5.431)
+    sys_ = build_system(cr, {"Si": si_pp}, 200.0, gamma_only(), with_initial_density=False)
+    assert sys_.n_pw == 259
+    p = sys_.projectors[0]
+    hnl = p.b @ (p.d_dense() @ p.b.conj().T)
+    for r in rows:
+        idx = sys_.basis.index_of(int(r[1]), int(r[2]), int(r[3]))
+        kin = sys_.kinetic[0][idx] / RY_TO_EV
+        vnl = hnl[idx, idx].real / RY_TO_EV
+        assert abs(kin - float(r[7])) < 1e-4
+        assert abs(vnl - float(r[8])) < 1e-4
+
+
+def test_basis_counts():
+    # basis.rs:139-148 (259 at 200 eV); tests/cpu_scf_baseline.rs (89 at 100 eV)
+    lat = diamond_primitive("Si", 5.431).lattice
+    assert len(BasisSet(lat, 200.0)) == 259
+    assert len(BasisSet(lat, 100.0)) == 89
+
+
+@pytest.mark.slow
+def test_cpu_scf_baseline_golden(si_pp):
+    # tests/cpu_scf_baseline.rs:43-44, 105-165
+    cr = diamond_primitive("Si", 5.431)
+    s = build_system(cr, {"Si": si_pp}, 100.0, gamma_only(), SymmetryInfo.identity_only(), fft_grid=(16, 16, 16))
+    r = O.run_scf_unpolarized(s, 4, max_iter=40, conv_threshold=1e-6, energy_threshold=1e-5, mixing_beta=0.3,
+                              mixing_ndim=4, smearing="fermi_dirac", sigma=0.05)
+    assert r.n_iterations < 40
+    assert abs(r.total_energy - (-213.028339)) < 1e-3
+    assert abs(r.fermi_energy - 8.052064) < 1e-3
