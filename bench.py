@@ -140,6 +140,27 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_once():
+    """Three H|psi> calls of the bench workload per precision, mixed first
+    (a short, bounded program for profiler captures)."""
+    import torch
+
+    from pwgpu.lib import PRECISION_FP64, PRECISION_MIXED, PwGpu
+    from pwgpu.workloads import hpsi_system, si64_crystal
+    sys_, veff_g, psi = hpsi_system(si64_crystal())
+    nb, n_pw = psi.shape[1], sys_.n_pw
+    with PwGpu(sys_) as dev:
+        dev.set_veff_g(veff_g)
+        d_psi = torch.from_numpy(np.ascontiguousarray(psi.T)).cuda()
+        d_h = torch.empty_like(d_psi)
+        for prec in (PRECISION_MIXED, PRECISION_FP64):
+            dev.set_precision(prec)
+            for _ in range(3):
+                dev.apply_h_device(d_psi.data_ptr(), n_pw, nb, d_h.data_ptr(), n_pw)
+        torch.cuda.synchronize()
+    print("once: ok")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -147,8 +168,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="pwgpu", choices=["pwgpu", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="full", choices=["full", "once"],
+                    help="once: three untimed H|psi> calls per precision (for profiler captures)")
     args = ap.parse_args()
     world, rank, local = dist_env()
+    if args.mode == "once":
+        run_once()
+        return
     if args.impl == "reference":
         if world > 1:
             import torch.distributed as dist

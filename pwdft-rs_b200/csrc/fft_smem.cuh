@@ -1,8 +1,8 @@
 // In-shared-memory batched 1-D FFTs for 2,3,5-smooth lengths.
 //
-// A thread block holds a tile of `nlines` lines of length L in shared
+// A thread block holds a tile of W interleaved lines of length L in shared
 // memory, plus a scratch tile of the same size.  Each Stockham stage
-// (radix R in {2,3,4,5,8}, stride Ns) reads one tile and writes the other
+// (radix R in {2,3,4,5,8,9}, stride Ns) reads one tile and writes the other
 // in auto-sorted order, one butterfly per thread at a time, so only R
 // complex values live in registers.  Twiddles come from
 // a per-length table tw[m] = exp(-2*pi*i*m/L), m < L, computed on the host
@@ -76,71 +76,111 @@ template <int S, typename C> __device__ __forceinline__ void dft8(C* v) {
   v[3] = e3 + t3; v[7] = e3 - t3;
 }
 
+#define PW_C1_9 0.76604444311897803520    // cos(2pi/9)
+#define PW_S1_9 0.64278760968653932632    // sin(2pi/9)
+#define PW_C2_9 0.17364817766693034885    // cos(4pi/9)
+#define PW_S2_9 0.98480775301220805936    // sin(4pi/9)
+#define PW_C4_9 (-0.93969262078590838405) // cos(8pi/9)
+#define PW_S4_9 0.34202014332566873304    // sin(8pi/9)
+
+// 9-point DFT as 3 x 3: inner DFT3 over n1 (stride 3), twiddle w9^(n2*k1),
+// outer DFT3 over n2; X[k1 + 3 k2].
+template <int S, typename C> __device__ __forceinline__ void dft9(C* v) {
+  using R = decltype(v[0].x);
+  C y[3][3];
+#pragma unroll
+  for (int n2 = 0; n2 < 3; ++n2) {
+    C t[3] = {v[n2], v[n2 + 3], v[n2 + 6]};
+    dft3<S>(t);
+    y[n2][0] = t[0]; y[n2][1] = t[1]; y[n2][2] = t[2];
+  }
+  // w9^m = cos(2 pi m/9) + S i sin(2 pi m/9), m in {1, 2, 4}
+  const C w1 = cmake<C>(PW_C1_9, S * PW_S1_9);
+  const C w2 = cmake<C>(PW_C2_9, S * PW_S2_9);
+  const C w4 = cmake<C>(PW_C4_9, S * PW_S4_9);
+  y[1][1] = cmul(y[1][1], w1);
+  y[1][2] = cmul(y[1][2], w2);
+  y[2][1] = cmul(y[2][1], w2);
+  y[2][2] = cmul(y[2][2], w4);
+  (void)sizeof(R);
+#pragma unroll
+  for (int k1 = 0; k1 < 3; ++k1) {
+    C t[3] = {y[0][k1], y[1][k1], y[2][k1]};
+    dft3<S>(t);
+    v[k1] = t[0]; v[k1 + 3] = t[1]; v[k1 + 6] = t[2];
+  }
+}
+
 template <int R_, int S, typename C> __device__ __forceinline__ void dft(C* v) {
   if constexpr (R_ == 2) dft2<S>(v);
   else if constexpr (R_ == 3) dft3<S>(v);
   else if constexpr (R_ == 4) dft4<S>(v[0], v[1], v[2], v[3]);
   else if constexpr (R_ == 5) dft5<S>(v);
+  else if constexpr (R_ == 9) dft9<S>(v);
   else dft8<S>(v);
 }
 
-// Maps a tile line index to its base offset in shared memory and gives the
-// element stride along the line.
-struct LineMap {
-  int lmul;     // base offset = line * lmul
-  int estride;  // stride between consecutive elements of a line
-};
+// Exact j / d for 0 <= j, j*d < 2^32 with m = ceil(2^32 / d) (d >= 2).
+__device__ __forceinline__ int fast_div(int j, int d, unsigned m) {
+  return d == 1 ? j : (int)__umulhi((unsigned)j, m);
+}
 
-// One Stockham stage over all lines of the tile, src -> dst (both tiles of
-// the same shape).  Each thread takes butterflies tid, tid+T, ... and holds
-// only the R values of the current one in registers.
+// One Stockham stage, src -> dst.  Tile layout: element e of line l sits at
+// e*W + l (lines interleaved, W = blockDim.x); threadIdx.x is the line and
+// threadIdx.y strides the L/R butterflies, so a warp reads and writes
+// adjacent shared-memory words and shares one twiddle.
 template <int R_, int S, typename C>
-__device__ __forceinline__ void fft_stage(const C* __restrict__ src, C* __restrict__ dst, int L, int Ns, int nlines,
-                                          LineMap lm, const C* __restrict__ tw) {
+__device__ __forceinline__ void fft_stage(const C* __restrict__ src, C* __restrict__ dst, int L, int Ns,
+                                          unsigned nsm, int W, const C* __restrict__ tw) {
   const int LR = L / R_;
-  const int nbf = nlines * LR;
   const int twstep = L / (Ns * R_);
-  for (int bf = threadIdx.x; bf < nbf; bf += blockDim.x) {
-    const int line = bf / LR;
-    const int j = bf - line * LR;
-    const int k = j % Ns;
-    const int base = line * lm.lmul;
+  const int line = threadIdx.x;
+  for (int j = threadIdx.y; j < LR; j += blockDim.y) {
+    const int jq = fast_div(j, Ns, nsm);
+    const int k = j - jq * Ns;
     C v[R_];
 #pragma unroll
     for (int r = 0; r < R_; ++r) {
-      C x = src[base + (j + r * LR) * lm.estride];
-      if (r > 0) {
+      C x = src[(j + r * LR) * W + line];
+      if (r > 0 && Ns > 1) {
         const C w = tw[k * r * twstep];
         x = (S < 0) ? cmul(x, w) : cmulc(x, w);
       }
       v[r] = x;
     }
     dft<R_, S>(v);
-    const int ob = base + ((j / Ns) * Ns * R_ + k) * lm.estride;
-    const int os = Ns * lm.estride;
+    const int ob = (jq * Ns * R_ + k) * W + line;
+    const int os = Ns * W;
 #pragma unroll
     for (int q = 0; q < R_; ++q) dst[ob + q * os] = v[q];
   }
   __syncthreads();
 }
 
-// Full 1-D transform of every line of the tile (S = -1 forward, +1 inverse).
-// The data starts in `a`; `b` is scratch of the same size.  Returns the
-// buffer that holds the result (a or b, by the parity of the stage count).
+// Full 1-D transform of the W interleaved lines of a tile (S = -1 forward,
+// +1 inverse).  The data starts in `a`; `b` is scratch of the same size.
+// Returns the buffer holding the result (by the parity of the stage count).
 template <int S, typename C>
-__device__ __forceinline__ C* fft_lines(C* a, C* b, const FftPlan& p, int nlines, LineMap lm,
-                                        const C* __restrict__ tw) {
+__device__ __forceinline__ C* fft_lines(C* a, C* b, const FftPlan& p, int W, const C* __restrict__ tw) {
   C* src = a;
   C* dst = b;
-  for (int s = 0; s < p.nstages; ++s) {
-    switch (p.radix[s]) {
-      case 2: fft_stage<2, S>(src, dst, p.L, p.ns[s], nlines, lm, tw); break;
-      case 3: fft_stage<3, S>(src, dst, p.L, p.ns[s], nlines, lm, tw); break;
-      case 4: fft_stage<4, S>(src, dst, p.L, p.ns[s], nlines, lm, tw); break;
-      case 5: fft_stage<5, S>(src, dst, p.L, p.ns[s], nlines, lm, tw); break;
-      default: fft_stage<8, S>(src, dst, p.L, p.ns[s], nlines, lm, tw); break;
+  // Unrolled over the stage slots so every plan field is read at a fixed
+  // parameter-bank offset (a runtime index would go through the slow
+  // indexed-constant path), and if-chains instead of a jump table.
+#pragma unroll
+  for (int s = 0; s < kMaxStages; ++s) {
+    if (s < p.nstages) {
+      const int Ns = p.ns[s];
+      const unsigned m = p.nsm[s];
+      const int R = p.radix[s];
+      if (R == 8) fft_stage<8, S>(src, dst, p.L, Ns, m, W, tw);
+      else if (R == 9) fft_stage<9, S>(src, dst, p.L, Ns, m, W, tw);
+      else if (R == 4) fft_stage<4, S>(src, dst, p.L, Ns, m, W, tw);
+      else if (R == 5) fft_stage<5, S>(src, dst, p.L, Ns, m, W, tw);
+      else if (R == 3) fft_stage<3, S>(src, dst, p.L, Ns, m, W, tw);
+      else fft_stage<2, S>(src, dst, p.L, Ns, m, W, tw);
+      C* t = src; src = dst; dst = t;
     }
-    C* t = src; src = dst; dst = t;
   }
   return src;
 }

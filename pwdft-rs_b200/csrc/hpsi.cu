@@ -31,39 +31,46 @@ namespace pwgpu {
 
 namespace {
 
-constexpr int kThreads = 128;
-constexpr int kTileElems = 1024;
+constexpr int kThreads = 256;
+constexpr int kTileElems = 2048;
+constexpr int kMaxDynSmem = 2 * (kTileElems + 1024) * 16;  // worst case: two FP64 tiles
 
 __device__ __forceinline__ int wrap_idx(int n, int d) { return n < 0 ? n + d : n; }
 
 template <typename C> __device__ __forceinline__ C to_c(double2 v) { return cmake<C>(v.x, v.y); }
+
+// Every FFT kernel runs on a (W, TY) thread block: threadIdx.x indexes the W
+// interleaved lines of the tile, threadIdx.y strides along the lines.
 
 // K1: scatter sphere coefficients of W columns and z-inverse-FFT them.
 template <typename R>
 __global__ void __launch_bounds__(kThreads) k_zinv(const double2* __restrict__ psi, long ldpsi,
                                                   cplx<R>* __restrict__ A, const int* __restrict__ col_start,
                                                   const int* __restrict__ pt_ig, const int* __restrict__ pt_col,
-                                                  const int* __restrict__ pt_z, int ncol, int d2, int W,
+                                                  const int* __restrict__ pt_z, int ncol, int d2, unsigned md2,
                                                   FftPlan pz, const cplx<R>* __restrict__ twz) {
   using C = cplx<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int W = blockDim.x;
   C* buf = reinterpret_cast<C*>(smem_raw);
+  C* scr = buf + W * d2;
   const int c0 = blockIdx.x * W;
   const int b = blockIdx.y;
   const int nl = min(W, ncol - c0);
-  const int tile = W * d2;
-  C* scr = buf + tile;
-  for (int i = threadIdx.x; i < tile; i += blockDim.x) buf[i] = cmake<C>(0.0, 0.0);
+  const int tid = threadIdx.y * W + threadIdx.x;
+  const int T = W * blockDim.y;
+  for (int e = threadIdx.y; e < d2; e += blockDim.y) buf[e * W + threadIdx.x] = cmake<C>(0.0, 0.0);
   __syncthreads();
   const double2* ps = psi + (long)b * ldpsi;
   const int i0 = col_start[c0], i1 = col_start[c0 + nl];
-  for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
-    buf[(pt_col[i] - c0) * d2 + pt_z[i]] = to_c<C>(ps[pt_ig[i]]);
-  }
+  for (int i = i0 + tid; i < i1; i += T) buf[pt_z[i] * W + (pt_col[i] - c0)] = to_c<C>(ps[pt_ig[i]]);
   __syncthreads();
-  const C* res = fft_lines<+1>(buf, scr, pz, W, LineMap{d2, 1}, twz);
+  const C* res = fft_lines<+1>(buf, scr, pz, W, twz);
   C* out = A + ((long)b * ncol + c0) * d2;
-  for (int i = threadIdx.x; i < nl * d2; i += blockDim.x) out[i] = res[i];
+  for (int i = tid; i < nl * d2; i += T) {
+    const int c = fast_div(i, d2, md2), e = i - c * d2;
+    out[i] = res[e * W + c];
+  }
 }
 
 // K5: z-forward-FFT W columns, gather the sphere, Hpsi = buf/N + T psi.
@@ -73,25 +80,31 @@ __global__ void __launch_bounds__(kThreads) k_zfwd(const cplx<R>* __restrict__ A
                                                   const double* __restrict__ kin, double scale,
                                                   const int* __restrict__ col_start, const int* __restrict__ pt_ig,
                                                   const int* __restrict__ pt_col, const int* __restrict__ pt_z,
-                                                  int ncol, int d2, int W, FftPlan pz,
+                                                  int ncol, int d2, unsigned md2, FftPlan pz,
                                                   const cplx<R>* __restrict__ twz) {
   using C = cplx<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int W = blockDim.x;
   C* buf = reinterpret_cast<C*>(smem_raw);
+  C* scr = buf + W * d2;
   const int c0 = blockIdx.x * W;
   const int b = blockIdx.y;
   const int nl = min(W, ncol - c0);
+  const int tid = threadIdx.y * W + threadIdx.x;
+  const int T = W * blockDim.y;
   const C* in = A + ((long)b * ncol + c0) * d2;
-  C* scr = buf + W * d2;
-  for (int i = threadIdx.x; i < W * d2; i += blockDim.x) buf[i] = (i < nl * d2) ? in[i] : cmake<C>(0.0, 0.0);
+  for (int i = tid; i < W * d2; i += T) {
+    const int c = fast_div(i, d2, md2), e = i - c * d2;
+    buf[e * W + c] = (c < nl) ? in[i] : cmake<C>(0.0, 0.0);
+  }
   __syncthreads();
-  const C* res = fft_lines<-1>(buf, scr, pz, W, LineMap{d2, 1}, twz);
+  const C* res = fft_lines<-1>(buf, scr, pz, W, twz);
   const double2* ps = psi + (long)b * ldpsi;
   double2* hs = hpsi + (long)b * ldh;
   const int i0 = col_start[c0], i1 = col_start[c0 + nl];
-  for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+  for (int i = i0 + tid; i < i1; i += T) {
     const int ig = pt_ig[i];
-    const C v = res[(pt_col[i] - c0) * d2 + pt_z[i]];
+    const C v = res[pt_z[i] * W + (pt_col[i] - c0)];
     const double2 p = ps[ig];
     const double t = kin[ig];
     hs[ig] = make_double2((double)v.x * scale + t * p.x, (double)v.y * scale + t * p.y);
@@ -100,117 +113,114 @@ __global__ void __launch_bounds__(kThreads) k_zfwd(const cplx<R>* __restrict__ A
 
 // K2 (S=+1): rows q<Yp of A -> y-inverse -> all d1 rows of B.
 // K4 (S=-1): all d1 rows of B -> y-forward -> rows q<Yp of A.
+// A tile is one compact x-plane p and W consecutive z offsets.
 template <typename R, int S>
 __global__ void __launch_bounds__(kThreads) k_y(cplx<R>* __restrict__ A, cplx<R>* __restrict__ B, int Xp, int Yp,
-                                               int m1, int d1, int d2, int W, FftPlan py,
-                                               const cplx<R>* __restrict__ twy) {
+                                               int m1, int d1, int d2, FftPlan py, const cplx<R>* __restrict__ twy) {
   using C = cplx<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int W = blockDim.x;
+  const int w = threadIdx.x;
   C* buf = reinterpret_cast<C*>(smem_raw);
+  C* scr = buf + d1 * W;
   const int p = blockIdx.x;
   const int z0 = blockIdx.y * W;
   const int b = blockIdx.z;
-  const int zn = min(W, d2 - z0);
+  const bool live = w < d2 - z0;
   const long ncol = (long)Xp * Yp;
-  C* scr = buf + d1 * W;
-  C* a_base = A + ((long)b * ncol + (long)p * Yp) * d2 + z0;
-  C* b_base = B + (((long)b * Xp + p) * d1) * d2 + z0;
+  C* a_base = A + ((long)b * ncol + (long)p * Yp) * d2 + z0 + w;
+  C* b_base = B + (((long)b * Xp + p) * d1) * d2 + z0 + w;
   if (S > 0) {
-    for (int i = threadIdx.x; i < d1 * W; i += blockDim.x) buf[i] = cmake<C>(0.0, 0.0);
-    __syncthreads();
-    for (int i = threadIdx.x; i < Yp * W; i += blockDim.x) {
-      const int q = i / W, w = i - q * W;
-      if (w < zn) buf[wrap_idx(q - m1, d1) * W + w] = a_base[(long)q * d2 + w];
+    // row y holds compact row q = y + m1 (y <= m1) or y - d1 + m1 (y >= d1 - m1), else zero
+    for (int y = threadIdx.y; y < d1; y += blockDim.y) {
+      const int q = y <= m1 ? y + m1 : (y >= d1 - m1 ? y - d1 + m1 : -1);
+      buf[y * W + w] = (live && q >= 0) ? a_base[(long)q * d2] : cmake<C>(0.0, 0.0);
     }
   } else {
-    for (int i = threadIdx.x; i < d1 * W; i += blockDim.x) {
-      const int y = i / W, w = i - y * W;
-      buf[i] = (w < zn) ? b_base[(long)y * d2 + w] : cmake<C>(0.0, 0.0);
-    }
+    for (int y = threadIdx.y; y < d1; y += blockDim.y)
+      buf[y * W + w] = live ? b_base[(long)y * d2] : cmake<C>(0.0, 0.0);
   }
   __syncthreads();
-  const C* res = fft_lines<S>(buf, scr, py, W, LineMap{1, W}, twy);
+  const C* res = fft_lines<S>(buf, scr, py, W, twy);
+  if (!live) return;
   if (S > 0) {
-    for (int i = threadIdx.x; i < d1 * W; i += blockDim.x) {
-      const int y = i / W, w = i - y * W;
-      if (w < zn) b_base[(long)y * d2 + w] = res[i];
-    }
+    for (int y = threadIdx.y; y < d1; y += blockDim.y) b_base[(long)y * d2] = res[y * W + w];
   } else {
-    for (int i = threadIdx.x; i < Yp * W; i += blockDim.x) {
-      const int q = i / W, w = i - q * W;
-      if (w < zn) a_base[(long)q * d2 + w] = res[wrap_idx(q - m1, d1) * W + w];
-    }
+    for (int q = threadIdx.y; q < Yp; q += blockDim.y) a_base[(long)q * d2] = res[wrap_idx(q - m1, d1) * W + w];
   }
 }
 
 // K3: compact x rows of B -> x-inverse -> * V(r) -> x-forward -> compact rows.
+// A tile is one y row and W consecutive z offsets.
 template <typename R>
 __global__ void __launch_bounds__(kThreads) k_xv(cplx<R>* __restrict__ B, const R* __restrict__ vr, int Xp, int m0,
-                                                int d0, int d1, int d2, int W, FftPlan px,
-                                                const cplx<R>* __restrict__ twx) {
+                                                int d0, int d1, int d2, FftPlan px, const cplx<R>* __restrict__ twx) {
   using C = cplx<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int W = blockDim.x;
+  const int w = threadIdx.x;
   C* buf = reinterpret_cast<C*>(smem_raw);
+  C* scr = buf + d0 * W;
   const int y = blockIdx.x;
   const int z0 = blockIdx.y * W;
   const int b = blockIdx.z;
-  const int zn = min(W, d2 - z0);
+  const bool live = w < d2 - z0;
   const long plane = (long)d1 * d2;
-  C* base = B + (long)b * Xp * plane + (long)y * d2 + z0;
-  C* scr = buf + d0 * W;
-  for (int i = threadIdx.x; i < d0 * W; i += blockDim.x) buf[i] = cmake<C>(0.0, 0.0);
-  __syncthreads();
-  for (int i = threadIdx.x; i < Xp * W; i += blockDim.x) {
-    const int p = i / W, w = i - p * W;
-    if (w < zn) buf[wrap_idx(p - m0, d0) * W + w] = base[(long)p * plane + w];
+  C* base = B + (long)b * Xp * plane + (long)y * d2 + z0 + w;
+  for (int x = threadIdx.y; x < d0; x += blockDim.y) {
+    const int q = x <= m0 ? x + m0 : (x >= d0 - m0 ? x - d0 + m0 : -1);
+    buf[x * W + w] = (live && q >= 0) ? base[(long)q * plane] : cmake<C>(0.0, 0.0);
   }
   __syncthreads();
-  C* r1 = fft_lines<+1>(buf, scr, px, W, LineMap{1, W}, twx);
-  const R* vb = vr + (long)y * d2 + z0;
-  for (int i = threadIdx.x; i < d0 * W; i += blockDim.x) {
-    const int x = i / W, w = i - x * W;
-    if (w < zn) r1[i] = r1[i] * vb[(long)x * plane + w];
-  }
+  C* r1 = fft_lines<+1>(buf, scr, px, W, twx);
+  const R* vb = vr + (long)y * d2 + z0 + w;
+  for (int x = threadIdx.y; x < d0; x += blockDim.y)
+    if (live) r1[x * W + w] = r1[x * W + w] * vb[(long)x * plane];
   __syncthreads();
-  const C* r2 = fft_lines<-1>(r1, r1 == buf ? scr : buf, px, W, LineMap{1, W}, twx);
-  for (int i = threadIdx.x; i < Xp * W; i += blockDim.x) {
-    const int p = i / W, w = i - p * W;
-    if (w < zn) base[(long)p * plane + w] = r2[wrap_idx(p - m0, d0) * W + w];
-  }
+  const C* r2 = fft_lines<-1>(r1, r1 == buf ? scr : buf, px, W, twx);
+  if (!live) return;
+  for (int q = threadIdx.y; q < Xp; q += blockDim.y) base[(long)q * plane] = r2[wrap_idx(q - m0, d0) * W + w];
 }
 
 // Full-grid line FFT along one axis, grid viewed as [outer][L][inner].
-// inner == 1: a tile is W consecutive rows (contiguous lines);
-// inner > 1:  a tile is one outer index and W consecutive inner offsets.
+// inner == 1: a tile is W consecutive rows (contiguous lines, transposed
+// into the interleaved layout); inner > 1: one outer index and W
+// consecutive inner offsets.
 template <int S>
-__global__ void __launch_bounds__(kThreads) k_fft_axis(double2* __restrict__ g, long nbatch_stride, int outer, int L,
-                                                      int inner, int W, FftPlan p, const double2* __restrict__ tw) {
+__global__ void __launch_bounds__(kThreads) k_fft_axis(double2* __restrict__ g, int outer, int L, int inner,
+                                                      unsigned mL, FftPlan p, const double2* __restrict__ tw) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int W = blockDim.x;
   double2* buf = reinterpret_cast<double2*>(smem_raw);
-  double2* gb = g + (long)blockIdx.z * nbatch_stride;
+  double2* scr = buf + W * L;
+  const int tid = threadIdx.y * W + threadIdx.x;
+  const int T = W * blockDim.y;
   if (inner == 1) {
     const int r0 = blockIdx.x * W;
     const int nl = min(W, outer - r0);
-    double2* src = gb + (long)r0 * L;
-    for (int i = threadIdx.x; i < W * L; i += blockDim.x) buf[i] = (i < nl * L) ? src[i] : make_double2(0.0, 0.0);
+    double2* src = g + (long)r0 * L;
+    for (int i = tid; i < W * L; i += T) {
+      const int c = fast_div(i, L, mL), e = i - c * L;
+      buf[e * W + c] = (c < nl) ? src[i] : make_double2(0.0, 0.0);
+    }
     __syncthreads();
-    const double2* res = fft_lines<S>(buf, buf + W * L, p, W, LineMap{L, 1}, tw);
-    for (int i = threadIdx.x; i < nl * L; i += blockDim.x) src[i] = res[i];
+    const double2* res = fft_lines<S>(buf, scr, p, W, tw);
+    for (int i = tid; i < nl * L; i += T) {
+      const int c = fast_div(i, L, mL), e = i - c * L;
+      src[i] = res[e * W + c];
+    }
   } else {
     const int o = blockIdx.y;
+    const int w = threadIdx.x;
     const int i0 = blockIdx.x * W;
-    const int zn = min(W, inner - i0);
-    double2* src = gb + (long)o * L * inner + i0;
-    for (int i = threadIdx.x; i < L * W; i += blockDim.x) {
-      const int l = i / W, w = i - l * W;
-      buf[i] = (w < zn) ? src[(long)l * inner + w] : make_double2(0.0, 0.0);
-    }
+    const bool live = w < inner - i0;
+    double2* src = g + (long)o * L * inner + i0 + w;
+    for (int l = threadIdx.y; l < L; l += blockDim.y)
+      buf[l * W + w] = live ? src[(long)l * inner] : make_double2(0.0, 0.0);
     __syncthreads();
-    const double2* res = fft_lines<S>(buf, buf + W * L, p, W, LineMap{1, W}, tw);
-    for (int i = threadIdx.x; i < L * W; i += blockDim.x) {
-      const int l = i / W, w = i - l * W;
-      if (w < zn) src[(long)l * inner + w] = res[i];
-    }
+    const double2* res = fft_lines<S>(buf, scr, p, W, tw);
+    if (!live) return;
+    for (int l = threadIdx.y; l < L; l += blockDim.y) src[(long)l * inner] = res[l * W + w];
   }
 }
 
@@ -255,6 +265,7 @@ bool make_plan(int L, FftPlan& p) {
   int rem = L;
   std::vector<int> rad;
   while (rem % 8 == 0 && rem > 1) { rad.push_back(8); rem /= 8; }
+  while (rem % 9 == 0) { rad.push_back(9); rem /= 9; }
   while (rem % 4 == 0) { rad.push_back(4); rem /= 4; }
   while (rem % 2 == 0) { rad.push_back(2); rem /= 2; }
   while (rem % 5 == 0) { rad.push_back(5); rem /= 5; }
@@ -264,6 +275,7 @@ bool make_plan(int L, FftPlan& p) {
   for (size_t s = 0; s < rad.size(); ++s) {
     p.radix[s] = rad[s];
     p.ns[s] = ns;
+    p.nsm[s] = div_magic(ns);
     ns *= rad[s];
   }
   p.nstages = (int)rad.size();
@@ -282,10 +294,37 @@ int balance_w(int n, int wmax) {
   return (n + chunks - 1) / chunks;
 }
 
+// (W, TY) block for a tile of W lines: TY = kThreads / W rows of threads.
+dim3 block_for(int W) { return dim3(W, std::max(1, kThreads / W), 1); }
+
+// Odd tile width for tiles whose lines are filled by a transposing load
+// (keeps the strided shared-memory stores at most 2-way bank conflicted).
+int odd_w(int w) { return (w > 1 && (w % 2 == 0)) ? w - 1 : w; }
+
 template <typename T> Status dalloc(T** p, size_t count) {
   if (count == 0) count = 1;
   cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
   if (e != cudaSuccess) return fail(kOom, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  return kOk;
+}
+
+// Opt every FFT kernel into the dynamic shared memory its largest tile needs.
+Status configure_kernels() {
+  static bool done = false;
+  if (done) return kOk;
+  const int sm = kMaxDynSmem;
+  cudaError_t e = cudaSuccess;
+  auto set = [&](const void* f) {
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  };
+  set((const void*)k_zinv<double>); set((const void*)k_zinv<float>);
+  set((const void*)k_zfwd<double>); set((const void*)k_zfwd<float>);
+  set((const void*)k_y<double, 1>); set((const void*)k_y<double, -1>);
+  set((const void*)k_y<float, 1>); set((const void*)k_y<float, -1>);
+  set((const void*)k_xv<double>); set((const void*)k_xv<float>);
+  set((const void*)k_fft_axis<1>); set((const void*)k_fft_axis<-1>);
+  if (e != cudaSuccess) return fail(kCuda, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+  done = true;
   return kOk;
 }
 
@@ -357,9 +396,10 @@ Status build_grid_maps(Handle& h, const int* miller) {
     PW_CUDA_TRY(cudaMemcpy(g.tw64[a], t64.data(), L * sizeof(double2), cudaMemcpyHostToDevice));
     PW_CUDA_TRY(cudaMemcpy(g.tw32[a], t32.data(), L * sizeof(float2), cudaMemcpyHostToDevice));
   }
-  g.wz = balance_w(g.ncol, pick_w(g.plan[2], 64));
-  g.wy = balance_w(g.d[2], pick_w(g.plan[1], 64));
-  g.wx = balance_w(g.d[2], pick_w(g.plan[0], 64));
+  g.wz = odd_w(balance_w(g.ncol, pick_w(g.plan[2], 64)));
+  g.wy = balance_w(g.d[2], pick_w(g.plan[1], 32));
+  g.wx = balance_w(g.d[2], pick_w(g.plan[0], 32));
+  if (Status st0 = configure_kernels(); st0 != kOk) return st0;
   // band chunk: keep A + B of one chunk within ~48 MB (FP64) of L2
   const double per_band = 16.0 * ((double)g.ncol * g.d[2] + (double)g.Xp * g.d[1] * g.d[2]);
   h.chunk = std::max(1, std::min(64, (int)(48.0e6 / per_band)));
@@ -392,17 +432,19 @@ Status fft3d_full(Handle& h, double2* data, int sign, cudaStream_t stream) {
     int W;
     dim3 grid;
     if (ax.inner == 1) {
-      W = balance_w(ax.outer, pick_w(p, 64));
+      W = odd_w(balance_w(ax.outer, pick_w(p, 64)));
       grid = dim3((ax.outer + W - 1) / W, 1, 1);
     } else {
       W = balance_w(ax.inner, pick_w(p, 64));
       grid = dim3((ax.inner + W - 1) / W, ax.outer, 1);
     }
     const size_t sm = 2 * (size_t)W * ax.L * sizeof(double2);
+    const dim3 blk = block_for(W);
+    const unsigned mL = div_magic(ax.L);
     if (sign < 0)
-      k_fft_axis<-1><<<grid, kThreads, sm, stream>>>(data, 0, ax.outer, ax.L, ax.inner, W, p, g.tw64[ax.a]);
+      k_fft_axis<-1><<<grid, blk, sm, stream>>>(data, ax.outer, ax.L, ax.inner, mL, p, g.tw64[ax.a]);
     else
-      k_fft_axis<+1><<<grid, kThreads, sm, stream>>>(data, 0, ax.outer, ax.L, ax.inner, W, p, g.tw64[ax.a]);
+      k_fft_axis<+1><<<grid, blk, sm, stream>>>(data, ax.outer, ax.L, ax.inner, mL, p, g.tw64[ax.a]);
   }
   PW_CUDA_TRY(cudaGetLastError());
   return kOk;
@@ -443,33 +485,33 @@ static Status local_chunk(Handle& h, int spin, int ik, const double2* psi, long 
   const double scale = 1.0 / (double)g.N;
   {
     dim3 grid((g.ncol + g.wz - 1) / g.wz, nb);
-    k_zinv<R><<<grid, kThreads, 2 * (size_t)g.wz * d2 * sizeof(C), s>>>(psi, ldpsi, A, g.col_start, g.pt_ig, g.pt_col,
-                                                                      g.pt_z, g.ncol, d2, g.wz, g.plan[2], tw2);
+    k_zinv<R><<<grid, block_for(g.wz), 2 * (size_t)g.wz * d2 * sizeof(C), s>>>(
+        psi, ldpsi, A, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2, div_magic(d2), g.plan[2], tw2);
     mark(tm, 0, s);
   }
   {
     dim3 grid(g.Xp, (d2 + g.wy - 1) / g.wy, nb);
-    k_y<R, +1><<<grid, kThreads, 2 * (size_t)g.wy * d1 * sizeof(C), s>>>(A, B, g.Xp, g.Yp, g.m[1], d1, d2, g.wy,
-                                                                       g.plan[1], tw1);
+    k_y<R, +1><<<grid, block_for(g.wy), 2 * (size_t)g.wy * d1 * sizeof(C), s>>>(A, B, g.Xp, g.Yp, g.m[1], d1, d2,
+                                                                              g.plan[1], tw1);
     mark(tm, 1, s);
   }
   {
     dim3 grid(d1, (d2 + g.wx - 1) / g.wx, nb);
-    k_xv<R><<<grid, kThreads, 2 * (size_t)g.wx * d0 * sizeof(C), s>>>(B, vr, g.Xp, g.m[0], d0, d1, d2, g.wx, g.plan[0],
-                                                                    tw0);
+    k_xv<R><<<grid, block_for(g.wx), 2 * (size_t)g.wx * d0 * sizeof(C), s>>>(B, vr, g.Xp, g.m[0], d0, d1, d2,
+                                                                           g.plan[0], tw0);
     mark(tm, 2, s);
   }
   {
     dim3 grid(g.Xp, (d2 + g.wy - 1) / g.wy, nb);
-    k_y<R, -1><<<grid, kThreads, 2 * (size_t)g.wy * d1 * sizeof(C), s>>>(A, B, g.Xp, g.Yp, g.m[1], d1, d2, g.wy,
-                                                                       g.plan[1], tw1);
+    k_y<R, -1><<<grid, block_for(g.wy), 2 * (size_t)g.wy * d1 * sizeof(C), s>>>(A, B, g.Xp, g.Yp, g.m[1], d1, d2,
+                                                                              g.plan[1], tw1);
     mark(tm, 3, s);
   }
   {
     dim3 grid((g.ncol + g.wz - 1) / g.wz, nb);
-    k_zfwd<R><<<grid, kThreads, 2 * (size_t)g.wz * d2 * sizeof(C), s>>>(A, psi, ldpsi, hpsi, ldh, h.kp[ik].kinetic,
-                                                                      scale, g.col_start, g.pt_ig, g.pt_col, g.pt_z,
-                                                                      g.ncol, d2, g.wz, g.plan[2], tw2);
+    k_zfwd<R><<<grid, block_for(g.wz), 2 * (size_t)g.wz * d2 * sizeof(C), s>>>(
+        A, psi, ldpsi, hpsi, ldh, h.kp[ik].kinetic, scale, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2,
+        div_magic(d2), g.plan[2], tw2);
     mark(tm, 4, s);
   }
   PW_CUDA_TRY(cudaGetLastError());
@@ -484,8 +526,10 @@ Status apply_h_device(Handle& h, int spin, int ik, const double2* psi, long ldps
   if (ldpsi < h.n_pw || ldh < h.n_pw) return fail(kInvalid, "apply_h: leading dimension smaller than n_pw");
   Status st;
   mark(tm, -1, s);
-  for (int c0 = 0; c0 < nb; c0 += h.chunk) {
-    const int cnt = std::min(h.chunk, nb - c0);
+  // the work buffers are sized for h.chunk FP64 bands; FP32 fits twice as many
+  const int chunk = precision == 0 ? h.chunk : 2 * h.chunk;
+  for (int c0 = 0; c0 < nb; c0 += chunk) {
+    const int cnt = std::min(chunk, nb - c0);
     if (precision == 0)
       st = local_chunk<double>(h, spin, ik, psi + (long)c0 * ldpsi, ldpsi, cnt, hpsi + (long)c0 * ldh, ldh, s, tm);
     else

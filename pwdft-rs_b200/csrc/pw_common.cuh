@@ -38,17 +38,24 @@ template <int S, typename C> __host__ __device__ __forceinline__ C mul_si(C a) {
   return c;
 }
 
-// Maximum number of radix stages per 1-D length (1024 = 8^3 * 2 needs 4).
-constexpr int kMaxStages = 8;
+// Maximum number of radix stages per 1-D length (2,3,5-smooth lengths up to
+// 1024 need at most 5 with radices 2,3,4,5,8,9).
+constexpr int kMaxStages = 6;
 
-// 1-D FFT plan for one length L = prod(radix[s]), radices in {2,3,4,5,8}.
+// 1-D FFT plan for one length L = prod(radix[s]), radices in {2,3,4,5,8,9}.
 // ns[s] = product of the radices of the stages before s (Stockham stride).
 struct FftPlan {
   int L;
   int nstages;
   int radix[kMaxStages];
   int ns[kMaxStages];
+  unsigned nsm[kMaxStages];  // ceil(2^32 / ns[s]) for division by ns (0 if ns == 1)
 };
+
+// Division magic for 0 <= j < 2^32 / d: j / d == __umulhi(j, magic(d)).
+inline unsigned div_magic(int d) {
+  return d <= 1 ? 0u : (unsigned)((((unsigned long long)1 << 32) + (unsigned long long)d - 1) / (unsigned long long)d);
+}
 
 // Status codes shared with include/pwgpu.h.
 enum Status : int {

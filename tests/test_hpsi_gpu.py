@@ -85,4 +85,6 @@ def test_apply_h_block_is_independent_of_band_chunking(pps):
         dev.set_veff_g(veff)
         full = dev.apply_h(psi)
         one = dev.apply_h(psi[:, 97:98])
-    assert np.array_equal(full[:, 97:98], one)
+    # the FFT part is bit-identical; the projector GEMM may pick another
+    # reduction order for a 1-column operand, hence a 1e-13 relative bound
+    assert np.max(np.abs(full[:, 97:98] - one)) < 1e-13 * np.max(np.abs(one))
