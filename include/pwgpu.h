@@ -133,6 +133,76 @@ pwgpu_status pwgpu_set_precision(pwgpu_handle* h, int32_t precision);
 /* Basis size, grid size and channel count of a handle. */
 pwgpu_status pwgpu_get_dims(const pwgpu_handle* h, int32_t* n_pw, int64_t* n_grid, int32_t* n_ch);
 
+/* SCF controls: the fields of ScfParams (scf/mod.rs:228-252) that the
+ * unpolarised loop reads, plus the eigensolver and precision controls of
+ * the matrix-free form. */
+typedef struct pwgpu_scf_params {
+  int32_t n_bands;
+  int32_t max_iter;
+  double conv_threshold;    /* density rms, e/Å^3 (energy.rs:227-235) */
+  double energy_threshold;  /* |E_n - E_{n-1}|, eV */
+  double mixing_beta;
+  int32_t mixing_ndim;
+  int32_t mixing_mode;      /* 0 plain Anderson, 1 Anderson + Kerker */
+  double kerker_q_tf;       /* Å^-1; <= 0 selects the Thomas-Fermi estimate */
+  int32_t smearing;         /* 0 Fermi-Dirac, 1 Gaussian, 2 Methfessel-Paxton, 3 cold, 4 fixed */
+  double smearing_sigma;    /* eV */
+  double diag_tol;          /* eigen-residual floor |H psi - e psi|, eV */
+  int32_t diag_max_iter;    /* Davidson iterations per SCF step */
+  int32_t diag_extra_bands; /* < 0: automatic */
+  int32_t precision;        /* PWGPU_PRECISION_* for H|psi> */
+  double fp64_switch;       /* mixed: FP64 H|psi> once the density rms < this */
+  int32_t verbose;          /* per-iteration line on stderr */
+} pwgpu_scf_params;
+
+/* ScfResult (scf/mod.rs:269-322) scalars. */
+typedef struct pwgpu_scf_result {
+  double total_energy, harris_foulkes_energy, free_energy, energy_sigma0, entropy_ts;
+  double fermi_energy, final_delta;
+  double e_band, e_hartree, e_xc, e_vxc, e_ewald;
+  int32_t n_iterations, converged, nspin;
+  double magnetization;
+  int64_t h_applications;   /* band applications of H over the run */
+  double max_residual;      /* largest eigen-residual of the last eigensolve */
+} pwgpu_scf_result;
+
+/* Run the SCF loop from rho_init_r (N doubles, e/Å^3).  Replaces
+ * run_scf_unpolarized (scf/driver.rs:266-742) with the dense per-k
+ * eigensolve replaced by block Davidson on the device.  Outputs may be
+ * NULL: eigenvalues n_k x n_bands (eV), rho_r_out N, rho_g_basis_out n_pw
+ * complex (rho(G) in basis order, as ScfResult::rho_g).
+ * Returns PWGPU_E_NOT_CONVERGED (result filled) if max_iter is reached. */
+pwgpu_status pwgpu_scf_run(pwgpu_handle* h, const pwgpu_scf_params* params, const double* rho_init_r,
+                           pwgpu_scf_result* result, double* eigenvalues, double* rho_r_out,
+                           double* rho_g_basis_out);
+
+/* Lowest n_bands eigenpairs of H at (spin, ik) for the current V_eff
+ * (diagonalize_dispatch, scf/driver.rs:125-184, lowest-n contract of
+ * eigensolver/dense.rs:87-98).  psi_in: optional warm start (n_pw x n_bands
+ * complex); evals ascending; psi_out optional. */
+pwgpu_status pwgpu_eigensolve(pwgpu_handle* h, int32_t spin, int32_t ik, int32_t n_bands, double tol,
+                              int32_t max_iter, const double* psi_in, double* evals, double* psi_out,
+                              int32_t* iters, double* max_residual);
+
+/* rho(r) = sum_k w_k sum_b occ f |IFFT psi|^2, renormalised to N_el and
+ * symmetrised (compute_density, scf/density.rs:41-111, then
+ * symmetrize_density_g).  occ: n_k x n_bands; psi: n_k blocks n_pw x n_bands. */
+pwgpu_status pwgpu_density(pwgpu_handle* h, int32_t n_bands, const double* occ, const double* psi, double* rho_r);
+
+/* In-place G-space symmetrisation of a real density (symmetry/density/g_space.rs:147-252). */
+pwgpu_status pwgpu_symmetrize(pwgpu_handle* h, double* rho_r);
+
+/* V_eff(G) = V_loc + V_H + V_xc from rho (energy.rs:293-358, xc.rs:129-288)
+ * and sets it as the H|psi> potential of spin 0; energies[3] = E_H, E_xc,
+ * int rho_val v_xc (eV). */
+pwgpu_status pwgpu_potentials(pwgpu_handle* h, const double* rho_r, double* veff_g, double* energies);
+
+/* Batched small generalized Hermitian eigensolve H c = e S c (m <= 64,
+ * column-major complex, batch consecutive problems): the Rayleigh-Ritz
+ * kernel, exposed for testing.  evals batch x nev ascending; C batch x m x nev. */
+pwgpu_status pwgpu_small_geneig(int32_t batch, int32_t m, int32_t nev, const double* H, const double* S,
+                                double* evals, double* C);
+
 #ifdef __cplusplus
 }
 #endif

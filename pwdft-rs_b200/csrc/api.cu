@@ -7,6 +7,8 @@
 #include <vector>
 
 #include "handle.hpp"
+#include "linalg.hpp"
+#include "scf.hpp"
 #include "../../include/pwgpu.h"
 
 struct pwgpu_handle {
@@ -45,6 +47,9 @@ static void release(Handle& h) {
   f(h.v_local_g); f(h.g_squared); f(h.rho_core_r); f(h.sym_src); f(h.sym_arg);
   for (int s = 0; s < 2; ++s) { f(h.veff_r[s]); f(h.veff_r32[s]); }
   f(h.work_a); f(h.work_b); f(h.nl_p); f(h.nl_q); f(h.tmp_grid);
+  release_scf(h);
+  f(h.solver_work); f(h.solver_info);
+  if (h.solver) cusolverDnDestroy(h.solver);
   if (h.blas) cublasDestroy(h.blas);
   if (h.stream) cudaStreamDestroy(h.stream);
   h = Handle();
@@ -236,6 +241,114 @@ pwgpu_status pwgpu_set_precision(pwgpu_handle* ph, int32_t precision) {
   if (precision != 0 && precision != 1) return fail(kInvalid, "pwgpu_set_precision: unknown precision");
   ph->precision = precision;
   return kOk;
+}
+
+pwgpu_status pwgpu_scf_run(pwgpu_handle* ph, const pwgpu_scf_params* p, const double* rho_init_r,
+                           pwgpu_scf_result* result, double* eigenvalues, double* rho_r_out,
+                           double* rho_g_basis_out) {
+  if (!ph || !p || !rho_init_r || !result) return fail(kInvalid, "pwgpu_scf_run: NULL argument");
+  ScfParams q;
+  q.n_bands = p->n_bands;
+  q.max_iter = p->max_iter;
+  q.conv_threshold = p->conv_threshold;
+  q.energy_threshold = p->energy_threshold;
+  q.mixing_beta = p->mixing_beta;
+  q.mixing_ndim = p->mixing_ndim;
+  q.mixing_mode = p->mixing_mode;
+  q.kerker_q_tf = p->kerker_q_tf;
+  q.smearing = p->smearing;
+  q.sigma = p->smearing_sigma;
+  q.diag_tol = p->diag_tol > 0.0 ? p->diag_tol : 1e-8;
+  q.diag_max_iter = p->diag_max_iter > 0 ? p->diag_max_iter : 60;
+  q.diag_extra_bands = p->diag_extra_bands;
+  q.precision = p->precision;
+  q.fp64_switch = p->fp64_switch;
+  q.verbose = p->verbose;
+  if (q.smearing < 0 || q.smearing > 4) return fail(kInvalid, "pwgpu_scf_run: unknown smearing scheme");
+  if (q.mixing_mode < 0 || q.mixing_mode > 1) return fail(kInvalid, "pwgpu_scf_run: unknown mixing mode");
+  ScfResult r;
+  Status st = scf_run(ph->h, q, rho_init_r, r, eigenvalues, rho_r_out, rho_g_basis_out);
+  result->total_energy = r.total_energy;
+  result->harris_foulkes_energy = r.harris_foulkes_energy;
+  result->free_energy = r.free_energy;
+  result->energy_sigma0 = r.energy_sigma0;
+  result->entropy_ts = r.entropy_ts;
+  result->fermi_energy = r.fermi_energy;
+  result->final_delta = r.final_delta;
+  result->e_band = r.e_band;
+  result->e_hartree = r.e_hartree;
+  result->e_xc = r.e_xc;
+  result->e_vxc = r.e_vxc;
+  result->e_ewald = r.e_ewald;
+  result->n_iterations = r.n_iterations;
+  result->converged = r.converged;
+  result->nspin = r.nspin;
+  result->magnetization = r.magnetization;
+  result->h_applications = r.h_applications;
+  result->max_residual = r.max_residual;
+  return st;
+}
+
+pwgpu_status pwgpu_eigensolve(pwgpu_handle* ph, int32_t spin, int32_t ik, int32_t n_bands, double tol,
+                              int32_t max_iter, const double* psi_in, double* evals, double* psi_out,
+                              int32_t* iters, double* max_residual) {
+  if (!ph || !evals) return fail(kInvalid, "pwgpu_eigensolve: NULL argument");
+  PW_CUDA_TRY(cudaSetDevice(ph->h.device));
+  return eigensolve_k(ph->h, spin, ik, n_bands, tol, max_iter, psi_in, evals, psi_out, iters, max_residual);
+}
+
+pwgpu_status pwgpu_density(pwgpu_handle* ph, int32_t n_bands, const double* occ, const double* psi, double* rho_r) {
+  if (!ph || !occ || !psi || !rho_r) return fail(kInvalid, "pwgpu_density: NULL argument");
+  PW_CUDA_TRY(cudaSetDevice(ph->h.device));
+  return density_from_host(ph->h, n_bands, occ, psi, rho_r);
+}
+
+pwgpu_status pwgpu_symmetrize(pwgpu_handle* ph, double* rho_r) {
+  if (!ph || !rho_r) return fail(kInvalid, "pwgpu_symmetrize: NULL argument");
+  PW_CUDA_TRY(cudaSetDevice(ph->h.device));
+  return symmetrize_host(ph->h, rho_r);
+}
+
+pwgpu_status pwgpu_potentials(pwgpu_handle* ph, const double* rho_r, double* veff_g, double* energies) {
+  if (!ph || !rho_r) return fail(kInvalid, "pwgpu_potentials: NULL argument");
+  PW_CUDA_TRY(cudaSetDevice(ph->h.device));
+  return potentials_host(ph->h, rho_r, veff_g, energies);
+}
+
+pwgpu_status pwgpu_small_geneig(int32_t batch, int32_t m, int32_t nev, const double* H, const double* S,
+                                double* evals, double* C) {
+  if (!H || !S || !evals || !C || batch < 1) return fail(kInvalid, "pwgpu_small_geneig: bad argument");
+  if (m < 1 || m > 64 || nev < 1 || nev > m) return fail(kInvalid, "pwgpu_small_geneig: need 1 <= nev <= m <= 64");
+  const size_t mm = (size_t)m * m * batch;
+  double2 *dh = nullptr, *ds = nullptr, *dc = nullptr;
+  double* de = nullptr;
+  int* dst = nullptr;
+  Status st = kOk;
+  auto cleanup = [&]() { cudaFree(dh); cudaFree(ds); cudaFree(dc); cudaFree(de); cudaFree(dst); };
+  if (cudaMalloc((void**)&dh, mm * sizeof(double2)) != cudaSuccess || cudaMalloc((void**)&ds, mm * sizeof(double2)) != cudaSuccess ||
+      cudaMalloc((void**)&dc, (size_t)m * nev * batch * sizeof(double2)) != cudaSuccess ||
+      cudaMalloc((void**)&de, (size_t)nev * batch * sizeof(double)) != cudaSuccess ||
+      cudaMalloc((void**)&dst, batch * sizeof(int)) != cudaSuccess) {
+    cleanup();
+    return fail(kOom, "pwgpu_small_geneig: allocation failed");
+  }
+  cudaMemcpy(dh, H, mm * sizeof(double2), cudaMemcpyHostToDevice);
+  cudaMemcpy(ds, S, mm * sizeof(double2), cudaMemcpyHostToDevice);
+  st = small_geneig_batched(dh, ds, m, (long)m * m, m, nev, batch, de, dc, m, (long)m * nev, dst, 0);
+  std::vector<int> stat(batch, 0);
+  if (st == kOk) {
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) st = fail(kCuda, cudaGetErrorString(e));
+  }
+  if (st == kOk) {
+    cudaMemcpy(evals, de, (size_t)nev * batch * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaMemcpy(C, dc, (size_t)m * nev * batch * sizeof(double2), cudaMemcpyDeviceToHost);
+    cudaMemcpy(stat.data(), dst, batch * sizeof(int), cudaMemcpyDeviceToHost);
+    for (int b = 0; b < batch; ++b)
+      if (stat[b] == 1) { st = fail(kInvalid, "pwgpu_small_geneig: S is not positive definite"); break; }
+  }
+  cleanup();
+  return st;
 }
 
 pwgpu_status pwgpu_get_dims(const pwgpu_handle* ph, int32_t* n_pw, int64_t* n_grid, int32_t* n_ch) {

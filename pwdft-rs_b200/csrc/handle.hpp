@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cublas_v2.h>
+#include <cusolverDn.h>
 #include <cuda_runtime.h>
 
 #include <string>
@@ -72,8 +73,15 @@ struct Handle {
   double2* tmp_grid = nullptr;  // N complex scratch
   cudaStream_t stream = nullptr;
   cublasHandle_t blas = nullptr;
+  cusolverDnHandle_t solver = nullptr;
+  double2* solver_work = nullptr;
+  size_t solver_work_len = 0;
+  int* solver_info = nullptr;
+  struct ScfState* scf = nullptr;  // device state of the SCF loop (scf.cu)
   std::string last_error;
 };
+
+void release_scf(Handle& h);
 
 // Optional per-launch event trail of an H|psi> call (profiling entry point).
 // stage ids: -1 start, 0..4 the five FFT kernels, 5 B^H psi, 6 D apply, 7 B Q.
@@ -88,6 +96,10 @@ Status apply_h_device(Handle& h, int spin, int ik, const double2* psi, long ldps
                       long ldh, int precision, cudaStream_t stream, StageTimer* timer = nullptr);
 Status set_veff_from_g(Handle& h, int spin, const double2* veff_g_dev, cudaStream_t stream);
 Status ensure_nl_capacity(Handle& h, int nb);
+
+// rho(r) += sum_b fw[b] |psi_b(r)|^2 over nb bands (FP64 FFTs); fw on device.
+Status density_accumulate(Handle& h, const double2* psi, long ldpsi, int nb, const double* fw_dev, double* rho,
+                          cudaStream_t stream);
 
 // 3-D FFT of a full grid (unnormalised), sign -1 forward / +1 inverse,
 // in place on device memory (used for potentials and density paths).

@@ -182,6 +182,54 @@ __global__ void __launch_bounds__(kThreads) k_xv(cplx<R>* __restrict__ B, const 
   for (int q = threadIdx.y; q < Xp; q += blockDim.y) base[(long)q * plane] = r2[wrap_idx(q - m0, d0) * W + w];
 }
 
+// Density: for each band of the chunk, compact x rows of B -> x-inverse ->
+// rho(x, y, z) += fw[b] |psi_b(r)|^2 (compute_density, scf/density.rs:59-97).
+// One block per (y row, W z offsets) owns its rho tile, so no atomics.
+__global__ void __launch_bounds__(kThreads) k_x_density(const double2* __restrict__ B, const double* __restrict__ fw,
+                                                       int nb, double* __restrict__ rho, int Xp, int m0, int d0,
+                                                       int d1, int d2, FftPlan px, const double2* __restrict__ twx) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int W = blockDim.x;
+  const int w = threadIdx.x;
+  double2* buf = reinterpret_cast<double2*>(smem_raw);
+  double2* scr = buf + d0 * W;
+  const int y = blockIdx.x;
+  const int z0 = blockIdx.y * W;
+  const bool live = w < d2 - z0;
+  const long plane = (long)d1 * d2;
+  // each thread accumulates the rows x = threadIdx.y + k*blockDim.y it owns
+  constexpr int kMaxRows = 16;
+  double acc[kMaxRows];
+#pragma unroll
+  for (int k = 0; k < kMaxRows; ++k) acc[k] = 0.0;
+  for (int b = 0; b < nb; ++b) {
+    const double2* base = B + (long)b * Xp * plane + (long)y * d2 + z0 + w;
+    for (int x = threadIdx.y; x < d0; x += blockDim.y) {
+      const int q = x <= m0 ? x + m0 : (x >= d0 - m0 ? x - d0 + m0 : -1);
+      buf[x * W + w] = (live && q >= 0) ? base[(long)q * plane] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    const double2* res = fft_lines<+1>(buf, scr, px, W, twx);
+    const double f = fw[b];
+#pragma unroll
+    for (int k = 0; k < kMaxRows; ++k) {
+      const int x = threadIdx.y + k * blockDim.y;
+      if (x < d0) {
+        const double2 v = res[x * W + w];
+        acc[k] += f * (v.x * v.x + v.y * v.y);
+      }
+    }
+    __syncthreads();
+  }
+  if (!live) return;
+  double* rb = rho + (long)y * d2 + z0 + w;
+#pragma unroll
+  for (int k = 0; k < kMaxRows; ++k) {
+    const int x = threadIdx.y + k * blockDim.y;
+    if (x < d0) rb[(long)x * plane] += acc[k];
+  }
+}
+
 // Full-grid line FFT along one axis, grid viewed as [outer][L][inner].
 // inner == 1: a tile is W consecutive rows (contiguous lines, transposed
 // into the interleaved layout); inner > 1: one outer index and W
@@ -323,6 +371,7 @@ Status configure_kernels() {
   set((const void*)k_y<float, 1>); set((const void*)k_y<float, -1>);
   set((const void*)k_xv<double>); set((const void*)k_xv<float>);
   set((const void*)k_fft_axis<1>); set((const void*)k_fft_axis<-1>);
+  set((const void*)k_x_density);
   if (e != cudaSuccess) return fail(kCuda, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
   done = true;
   return kOk;
@@ -513,6 +562,36 @@ static Status local_chunk(Handle& h, int spin, int ik, const double2* psi, long 
         A, psi, ldpsi, hpsi, ldh, h.kp[ik].kinetic, scale, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2,
         div_magic(d2), g.plan[2], tw2);
     mark(tm, 4, s);
+  }
+  PW_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
+Status density_accumulate(Handle& h, const double2* psi, long ldpsi, int nb, const double* fw_dev, double* rho,
+                          cudaStream_t s) {
+  GridMaps& g = h.g;
+  const int d0 = g.d[0], d1 = g.d[1], d2 = g.d[2];
+  double2* A = reinterpret_cast<double2*>(h.work_a);
+  double2* B = reinterpret_cast<double2*>(h.work_b);
+  if ((d0 + (kThreads / g.wx) - 1) / (kThreads / g.wx) > 16) return fail(kNotImplemented, "density: x tile too tall");
+  for (int c0 = 0; c0 < nb; c0 += h.chunk) {
+    const int cnt = std::min(h.chunk, nb - c0);
+    {
+      dim3 grid((g.ncol + g.wz - 1) / g.wz, cnt);
+      k_zinv<double><<<grid, block_for(g.wz), 2 * (size_t)g.wz * d2 * sizeof(double2), s>>>(
+          psi + (long)c0 * ldpsi, ldpsi, A, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2, div_magic(d2),
+          g.plan[2], g.tw64[2]);
+    }
+    {
+      dim3 grid(g.Xp, (d2 + g.wy - 1) / g.wy, cnt);
+      k_y<double, +1><<<grid, block_for(g.wy), 2 * (size_t)g.wy * d1 * sizeof(double2), s>>>(
+          A, B, g.Xp, g.Yp, g.m[1], d1, d2, g.plan[1], g.tw64[1]);
+    }
+    {
+      dim3 grid(d1, (d2 + g.wx - 1) / g.wx, 1);
+      k_x_density<<<grid, block_for(g.wx), 2 * (size_t)g.wx * d0 * sizeof(double2), s>>>(
+          B, fw_dev + c0, cnt, rho, g.Xp, g.m[0], d0, d1, d2, g.plan[0], g.tw64[0]);
+    }
   }
   PW_CUDA_TRY(cudaGetLastError());
   return kOk;

@@ -1,0 +1,21 @@
+// Dense linear-algebra helpers of the Rayleigh-Ritz step (linalg.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "handle.hpp"
+
+namespace pwgpu {
+
+// Batched small generalized Hermitian eigenproblems (m <= 64): lowest nev
+// eigenpairs of H c = lambda S c, ascending; C is S-orthonormal.
+// status_dev[b]: 0 ok, 1 S not positive definite, 2 Jacobi sweep cap hit.
+Status small_geneig_batched(const double2* H, const double2* S, long ld, long stride, int m, int nev, int batch,
+                            double* evals, double2* C, long ldc, long cstride, int* status_dev, cudaStream_t s);
+size_t small_geneig_smem(int m);
+
+// One large problem through cuSOLVER zhegvd (H, S overwritten; w ascending,
+// eigenvectors in H).
+Status large_geneig(Handle& h, double2* Hm, double2* Sm, int m, double* w, cudaStream_t s);
+
+}  // namespace pwgpu

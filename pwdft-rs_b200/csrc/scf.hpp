@@ -1,0 +1,54 @@
+// SCF loop on the device: block Davidson eigensolver, density, G-space
+// symmetrisation, Hartree + LDA potentials, energies and Anderson/Kerker
+// mixing (scf.cu).
+#pragma once
+
+#include <vector>
+
+#include "handle.hpp"
+
+namespace pwgpu {
+
+struct ScfParams {
+  int n_bands = 8;
+  int max_iter = 100;
+  double conv_threshold = 1e-6;     // density rms, e/Å³ (energy.rs:227-235)
+  double energy_threshold = 1e-5;   // |E_n - E_{n-1}|, eV
+  double mixing_beta = 0.3;
+  int mixing_ndim = 8;
+  int mixing_mode = 0;              // 0 plain Anderson, 1 Anderson + Kerker
+  double kerker_q_tf = 0.0;         // Å⁻¹; <= 0 selects the Thomas-Fermi estimate
+  int smearing = 0;                 // 0 Fermi-Dirac, 1 Gaussian, 2 Methfessel-Paxton, 3 cold, 4 fixed
+  double sigma = 0.01;              // eV
+  double diag_tol = 1e-8;           // eigen-residual norm floor, eV
+  int diag_max_iter = 60;
+  int diag_extra_bands = -1;        // < 0: automatic
+  int precision = 0;                // 0 FP64, 1 mixed
+  double fp64_switch = 1e-6;        // mixed: FP64 H|psi> once delta rho < this
+  int verbose = 0;
+};
+
+struct ScfResult {
+  double total_energy = 0, harris_foulkes_energy = 0, free_energy = 0, energy_sigma0 = 0, entropy_ts = 0;
+  double fermi_energy = 0, final_delta = 0;
+  double e_band = 0, e_hartree = 0, e_xc = 0, e_vxc = 0, e_ewald = 0;
+  int n_iterations = 0, converged = 0, nspin = 1;
+  double magnetization = 0;
+  long h_applications = 0;
+  double max_residual = 0;
+};
+
+// Whole SCF (driver.rs:266-742 for nspin = 1).  rho_init: N doubles on the
+// host (start density).  evals_out: n_k*n_bands (may be null); rho_out: N
+// (may be null); rho_g_basis_out: n_pw complex (may be null).
+Status scf_run(Handle& h, const ScfParams& p, const double* rho_init, ScfResult& res, double* evals_out,
+               double* rho_out, double* rho_g_basis_out);
+
+// Pieces exposed through the C-ABI for parity tests.
+Status eigensolve_k(Handle& h, int spin, int ik, int n_bands, double tol, int max_iter, const double* psi_in,
+                    double* evals, double* psi_out, int* iters, double* max_res);
+Status density_from_host(Handle& h, int n_bands, const double* occ, const double* psi_all, double* rho_out);
+Status symmetrize_host(Handle& h, double* rho);
+Status potentials_host(Handle& h, const double* rho, double* veff_g, double* energies);
+
+}  // namespace pwgpu

@@ -19,7 +19,7 @@ INCLUDE = os.path.join(os.path.dirname(PKG_ROOT), "include")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libpwgpu.so")
 
-SOURCES = ["api.cu", "hpsi.cu"]
+SOURCES = ["api.cu", "hpsi.cu", "linalg.cu", "scf.cu"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -53,7 +53,7 @@ def build(verbose: bool = False, extra_flags=None) -> str:
         objs.append(obj)
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
         cmd = [nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", LIB,
-               "-lcublas", "-lcudart"]
+               "-lcublas", "-lcusolver", "-lcudart"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

@@ -67,6 +67,34 @@ class PwgpuOptions(ct.Structure):
     _fields_ = [("device", ct.c_int32), ("precision", ct.c_int32)]
 
 
+SMEARING = {"fermi_dirac": 0, "gaussian": 1, "methfessel_paxton": 2, "cold": 3, "fixed": 4}
+
+
+class PwgpuScfParams(ct.Structure):
+    _fields_ = [
+        ("n_bands", ct.c_int32), ("max_iter", ct.c_int32), ("conv_threshold", ct.c_double),
+        ("energy_threshold", ct.c_double), ("mixing_beta", ct.c_double), ("mixing_ndim", ct.c_int32),
+        ("mixing_mode", ct.c_int32), ("kerker_q_tf", ct.c_double), ("smearing", ct.c_int32),
+        ("smearing_sigma", ct.c_double), ("diag_tol", ct.c_double), ("diag_max_iter", ct.c_int32),
+        ("diag_extra_bands", ct.c_int32), ("precision", ct.c_int32), ("fp64_switch", ct.c_double),
+        ("verbose", ct.c_int32),
+    ]
+
+
+class PwgpuScfResult(ct.Structure):
+    _fields_ = [
+        ("total_energy", ct.c_double), ("harris_foulkes_energy", ct.c_double), ("free_energy", ct.c_double),
+        ("energy_sigma0", ct.c_double), ("entropy_ts", ct.c_double), ("fermi_energy", ct.c_double),
+        ("final_delta", ct.c_double), ("e_band", ct.c_double), ("e_hartree", ct.c_double), ("e_xc", ct.c_double),
+        ("e_vxc", ct.c_double), ("e_ewald", ct.c_double), ("n_iterations", ct.c_int32), ("converged", ct.c_int32),
+        ("nspin", ct.c_int32), ("magnetization", ct.c_double), ("h_applications", ct.c_int64),
+        ("max_residual", ct.c_double),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -90,8 +118,18 @@ def load_library(path: str = LIB_PATH):
     lib.pwgpu_profile_apply_h.argtypes = [vp, ct.c_int32, ct.c_int32, vp, ct.c_int64, ct.c_int32, vp, ct.c_int64,
                                           _f64p, _i32p]
     lib.pwgpu_get_dims.argtypes = [vp, _i32p, ct.POINTER(ct.c_int64), _i32p]
+    lib.pwgpu_scf_run.argtypes = [vp, ct.POINTER(PwgpuScfParams), _f64p, ct.POINTER(PwgpuScfResult), _f64p, _f64p,
+                                  _f64p]
+    lib.pwgpu_eigensolve.argtypes = [vp, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_double, ct.c_int32, _f64p, _f64p,
+                                     _f64p, _i32p, _f64p]
+    lib.pwgpu_density.argtypes = [vp, ct.c_int32, _f64p, _f64p, _f64p]
+    lib.pwgpu_symmetrize.argtypes = [vp, _f64p]
+    lib.pwgpu_potentials.argtypes = [vp, _f64p, _f64p, _f64p]
+    lib.pwgpu_small_geneig.argtypes = [ct.c_int32, ct.c_int32, ct.c_int32, _f64p, _f64p, _f64p, _f64p]
     for name in ("pwgpu_create", "pwgpu_destroy", "pwgpu_set_veff_g", "pwgpu_apply_h", "pwgpu_apply_h_device",
-                 "pwgpu_set_precision", "pwgpu_get_dims", "pwgpu_profile_apply_h"):
+                 "pwgpu_set_precision", "pwgpu_get_dims", "pwgpu_profile_apply_h", "pwgpu_scf_run",
+                 "pwgpu_eigensolve", "pwgpu_density", "pwgpu_symmetrize", "pwgpu_potentials",
+                 "pwgpu_small_geneig"):
         getattr(lib, name).restype = ct.c_int32
     _lib = lib
     return lib
@@ -222,3 +260,80 @@ class PwGpu:
         _check(self.lib, self.lib.pwgpu_profile_apply_h(self.h, spin, ik, ct.c_void_p(psi_ptr), ldpsi, nb,
                                                         ct.c_void_p(hpsi_ptr), ldh, _f64(ms), _i32(n)))
         return ms, n
+
+    # -- SCF pieces ---------------------------------------------------------
+
+    def scf_run(self, rho_init: np.ndarray, n_bands: int, max_iter: int = 100, conv_threshold: float = 1e-6,
+                energy_threshold: float = 1e-5, mixing_beta: float = 0.3, mixing_ndim: int = 8, kerker: bool = False,
+                q_tf: float = 0.0, smearing: str = "fermi_dirac", sigma: float = 0.01, diag_tol: float = 1e-8,
+                diag_max_iter: int = 60, diag_extra_bands: int = -1, precision: int = PRECISION_FP64,
+                fp64_switch: float = 1e-6, verbose: bool = False, raise_on_unconverged: bool = True):
+        """run_scf_unpolarized on the device; returns (result dict, eigenvalues [n_k, n_bands],
+        rho_r [N], rho_g in basis order [n_pw])."""
+        p = PwgpuScfParams(n_bands, max_iter, conv_threshold, energy_threshold, mixing_beta, mixing_ndim,
+                           1 if kerker else 0, q_tf, SMEARING[smearing], sigma, diag_tol, diag_max_iter,
+                           diag_extra_bands, precision, fp64_switch, 1 if verbose else 0)
+        rho0 = np.ascontiguousarray(rho_init, dtype=np.float64)
+        res = PwgpuScfResult()
+        nk = len(self.sys.kpoints)
+        ev = np.zeros((nk, n_bands))
+        rho = np.zeros(self.sys.n_grid)
+        rg = np.zeros(self.n_pw, dtype=np.complex128)
+        rc = self.lib.pwgpu_scf_run(self.h, ct.byref(p), _f64(rho0), ct.byref(res), _f64(ev), _f64(rho),
+                                    rg.view(np.float64).ctypes.data_as(_f64p))
+        if rc != PWGPU_OK and (raise_on_unconverged or rc != -4):
+            raise PwGpuError(rc, self.lib.pwgpu_last_error().decode(errors="replace"))
+        return res.as_dict(), ev, rho, rg
+
+    def eigensolve(self, n_bands: int, ik: int = 0, spin: int = 0, tol: float = 1e-9, max_iter: int = 300,
+                   psi_in=None):
+        ev = np.zeros(n_bands)
+        psi = np.zeros((self.n_pw, n_bands), dtype=np.complex128, order="F")
+        it = ct.c_int32()
+        mr = ct.c_double()
+        pin = None
+        if psi_in is not None:
+            pin = np.asfortranarray(psi_in, dtype=np.complex128)
+            pin = pin.ravel(order="F").view(np.float64).ctypes.data_as(_f64p)
+        _check(self.lib, self.lib.pwgpu_eigensolve(self.h, spin, ik, n_bands, tol, max_iter, pin, _f64(ev),
+                                                   psi.ravel(order="F").view(np.float64).ctypes.data_as(_f64p),
+                                                   ct.byref(it), ct.byref(mr)))
+        return ev, psi, it.value, mr.value
+
+    def density(self, occ: np.ndarray, psis) -> np.ndarray:
+        """occ [n_k, n_bands]; psis: list of n_k blocks (n_pw, n_bands)."""
+        occ = np.ascontiguousarray(occ, dtype=np.float64)
+        nb = occ.shape[1]
+        allp = np.concatenate([np.asfortranarray(p, dtype=np.complex128).ravel(order="F") for p in psis])
+        rho = np.zeros(self.sys.n_grid)
+        _check(self.lib, self.lib.pwgpu_density(self.h, nb, _f64(occ), allp.view(np.float64).ctypes.data_as(_f64p),
+                                                _f64(rho)))
+        return rho
+
+    def symmetrize(self, rho: np.ndarray) -> np.ndarray:
+        r = np.ascontiguousarray(rho, dtype=np.float64).copy()
+        _check(self.lib, self.lib.pwgpu_symmetrize(self.h, _f64(r)))
+        return r
+
+    def potentials(self, rho: np.ndarray):
+        r = np.ascontiguousarray(rho, dtype=np.float64)
+        vg = np.zeros(self.sys.n_grid, dtype=np.complex128)
+        en = np.zeros(3)
+        _check(self.lib, self.lib.pwgpu_potentials(self.h, _f64(r), vg.view(np.float64).ctypes.data_as(_f64p),
+                                                   _f64(en)))
+        return vg, {"e_hartree": en[0], "e_xc": en[1], "e_vxc": en[2]}
+
+
+def small_geneig(H: np.ndarray, S: np.ndarray, nev: int):
+    """Batched generalized Hermitian eigensolve through the device kernel.
+    H, S: (batch, m, m) complex.  Returns (evals [batch, nev], C [batch, m, nev])."""
+    lib = load_library()
+    b, m, _ = H.shape
+    hf = np.ascontiguousarray(np.transpose(H, (0, 2, 1)), dtype=np.complex128)  # column-major per matrix
+    sf = np.ascontiguousarray(np.transpose(S, (0, 2, 1)), dtype=np.complex128)
+    ev = np.zeros((b, nev))
+    c = np.zeros((b, nev, m), dtype=np.complex128)
+    _check(lib, lib.pwgpu_small_geneig(b, m, nev, hf.view(np.float64).ctypes.data_as(_f64p),
+                                       sf.view(np.float64).ctypes.data_as(_f64p), _f64(ev),
+                                       c.view(np.float64).ctypes.data_as(_f64p)))
+    return ev, np.transpose(c, (0, 2, 1))

@@ -1,0 +1,154 @@
+"""SCF components and whole SCF on the GPU vs the oracle (same seeded inputs).
+
+Tolerances (FP64 plain form): eigenvalues 1e-7 Ha (2.7e-6 eV) against the
+dense diagonalisation; total energy 1e-8 Ha (2.7e-7 eV) against the oracle
+SCF; grid quantities (potentials, density, symmetrisation) 1e-10 relative;
+the reference's SCF golden (cpu_scf_baseline.rs) to its own 1e-3 eV."""
+
+import numpy as np
+import pytest
+import scipy.linalg as sl
+
+from conftest import rng
+from oracle import pwdft_oracle as O
+from pwgpu.consts import HA_TO_EV, RY_TO_EV
+from pwgpu.context import build_system
+from pwgpu.crystal import KPoint, diamond_primitive, gamma_only, monkhorst_pack
+from pwgpu.lib import PwGpu, small_geneig
+from pwgpu.symmetry import SymmetryInfo, reduce_kpoints
+
+pytestmark = pytest.mark.gpu
+
+HA = HA_TO_EV
+
+
+def si2_100ev(pp):
+    return build_system(diamond_primitive("Si", 5.431), {"Si": pp}, 100.0, gamma_only(), SymmetryInfo.identity_only(),
+                        fft_grid=(16, 16, 16))
+
+
+def sad_veff(s):
+    rho_g = O.density_r_to_g(s.rho_init_r, s.dims)
+    _, vxc = O.lda_xc(O.add_core(s.rho_init_r, s.rho_core_r))
+    return s.v_local_g + O.hartree(rho_g, s.g_squared) + O.density_r_to_g(vxc, s.dims)
+
+
+def test_small_geneig_matches_lapack():
+    g = rng(5)
+    b, m, nev = 3, 20, 9
+    H = np.empty((b, m, m), dtype=complex)
+    S = np.empty((b, m, m), dtype=complex)
+    for i in range(b):
+        a = g.standard_normal((m, m)) + 1j * g.standard_normal((m, m))
+        H[i] = a + a.conj().T
+        c = g.standard_normal((m, m)) + 1j * g.standard_normal((m, m))
+        S[i] = c @ c.conj().T + m * np.eye(m)
+    ev, C = small_geneig(H, S, nev)
+    for i in range(b):
+        w = sl.eigh(H[i], S[i], eigvals_only=True)[:nev]
+        assert np.max(np.abs(ev[i] - w)) < 1e-11 * np.max(np.abs(w))
+        resid = H[i] @ C[i] - S[i] @ C[i] * ev[i][None, :]
+        assert np.max(np.abs(resid)) < 1e-10 * np.max(np.abs(H[i]))
+        assert np.max(np.abs(C[i].conj().T @ S[i] @ C[i] - np.eye(nev))) < 1e-11
+
+
+def test_eigensolve_matches_dense(si_pp):
+    s = build_system(diamond_primitive("Si", 5.431), {"Si": si_pp}, 150.0,
+                     [KPoint(np.array([0.1, -0.2, 0.15]), 1.0)], SymmetryInfo.identity_only())
+    veff = sad_veff(s)
+    p = s.projectors[0]
+    h = O.dense_hamiltonian(s.basis.miller, s.kinetic[0], veff, s.dims, p.b, p.d_dense())
+    w, _ = O.lowest_eigenpairs(h, 10)
+    with PwGpu(s) as dev:
+        dev.set_veff_g(veff)
+        ev, psi, its, res = dev.eigensolve(10, tol=1e-9)
+    assert np.max(np.abs(ev - w)) < 1e-7 * HA
+    # eigenvectors: residual against the dense H and orthonormality
+    r = h @ psi - psi * ev[None, :]
+    assert np.max(np.linalg.norm(r, axis=0)) < 1e-7
+    assert np.max(np.abs(psi.conj().T @ psi - np.eye(10))) < 1e-10
+
+
+def test_potentials_match_oracle(si_pp):
+    s = si2_100ev(si_pp)
+    ref_v = sad_veff(s)
+    rho = s.rho_init_r
+    rho_g = O.density_r_to_g(rho, s.dims)
+    rxc = O.add_core(rho, s.rho_core_r)
+    exc, vxc = O.lda_xc(rxc)
+    with PwGpu(s) as dev:
+        vg, en = dev.potentials(rho)
+    assert np.max(np.abs(vg - ref_v)) < 1e-10 * np.max(np.abs(ref_v))
+    assert abs(en["e_hartree"] - O.hartree_energy(rho_g, s.g_squared, s.omega)) < 1e-10 * abs(en["e_hartree"])
+    dv = s.omega / rho.size
+    assert abs(en["e_xc"] - np.sum(rxc * exc) * dv) < 1e-10 * abs(en["e_xc"])
+    assert abs(en["e_vxc"] - np.sum(rho * vxc) * dv) < 1e-10 * abs(en["e_vxc"])
+
+
+def test_density_matches_oracle(si_pp):
+    cr = diamond_primitive("Si", 5.431)
+    kp = [KPoint(np.array([0.0, 0.0, 0.0]), 0.25), KPoint(np.array([0.2, 0.1, -0.3]), 0.75)]
+    s = build_system(cr, {"Si": si_pp}, 120.0, kp, SymmetryInfo.identity_only())
+    g = rng(9)
+    nb = 6
+    psis = []
+    for _ in kp:
+        q, _ = np.linalg.qr(g.standard_normal((s.n_pw, nb)) + 1j * g.standard_normal((s.n_pw, nb)))
+        psis.append(np.asfortranarray(q))
+    occ = np.array([[2.0, 2.0, 2.0, 1.5, 0.3, 0.0], [2.0, 2.0, 1.9, 1.0, 1e-17, 0.0]])
+    ref = O.compute_density(s.g_to_fft, s.dims, psis, occ, s.kpt_weights, s.n_electrons, s.omega)
+    with PwGpu(s) as dev:
+        got = dev.density(occ, psis)
+    assert np.max(np.abs(got - ref)) < 1e-11 * np.max(np.abs(ref))
+
+
+def test_symmetrize_matches_oracle(si_pp):
+    cr = diamond_primitive("Si", 5.431)
+    sym = SymmetryInfo.from_crystal(cr, 1e-5)
+    assert sym.n_ops == 48
+    s = build_system(cr, {"Si": si_pp}, 15 * RY_TO_EV, gamma_only(), sym)
+    g = rng(13)
+    rho = s.rho_init_r * (1.0 + 0.1 * g.standard_normal(s.n_grid))
+    src, arg = O.gather_map(s.dims, [(op.rotation, op.translation) for op in sym.operations])
+    ref = O.symmetrize_density(rho, s.dims, src, arg)
+    with PwGpu(s) as dev:
+        got = dev.symmetrize(rho)
+        twice = dev.symmetrize(got)
+    assert np.max(np.abs(got - ref)) < 1e-11 * np.max(np.abs(ref))
+    assert np.max(np.abs(twice - got)) < 1e-11 * np.max(np.abs(got))  # idempotent (g_space.rs tests)
+
+
+def test_scf_reproduces_reference_golden(si_pp):
+    # tests/cpu_scf_baseline.rs:43-44: E=-213.028339 eV, E_F=8.052064 eV (+-1e-3)
+    s = si2_100ev(si_pp)
+    with PwGpu(s) as dev:
+        res, ev, rho, _ = dev.scf_run(s.rho_init_r, 4, max_iter=40, conv_threshold=1e-6, energy_threshold=1e-5,
+                                      mixing_beta=0.3, mixing_ndim=4, smearing="fermi_dirac", sigma=0.05)
+    assert res["converged"] == 1
+    assert abs(res["total_energy"] - (-213.028339)) < 1e-3
+    assert abs(res["fermi_energy"] - 8.052064) < 1e-3
+
+
+def config1_system(pp, ecut_ry=20.0):
+    """Si fcc primitive a=10.26 bohr, shifted 4x4x4 MP reduced by symmetry (10 IBZ k)."""
+    from pwgpu.consts import BOHR_TO_ANG
+    cr = diamond_primitive("Si", 10.26 * BOHR_TO_ANG)
+    sym = SymmetryInfo.from_crystal(cr, 1e-5)
+    kp = reduce_kpoints((4, 4, 4), "mp1976", sym, cr.lattice)
+    return build_system(cr, {"Si": pp}, ecut_ry * RY_TO_EV, kp, sym)
+
+
+@pytest.mark.parametrize("ppname", ["Si_hgh", "Si"])
+def test_scf_config1_matches_oracle(ppname, si_pp, si_hgh_pp):
+    pp = si_pp if ppname == "Si" else si_hgh_pp
+    s = config1_system(pp)
+    assert len(s.kpoints) == 10 and s.n_pw == 411 and s.dims == (24, 24, 24)
+    kw = dict(max_iter=60, conv_threshold=1e-10, energy_threshold=1e-10 * RY_TO_EV, mixing_beta=0.7,
+              mixing_ndim=8)
+    ref = O.run_scf_unpolarized(s, 8, smearing="fixed", sigma=0.0, **kw)
+    with PwGpu(s) as dev:
+        res, ev, rho, _ = dev.scf_run(s.rho_init_r, 8, smearing="fixed", sigma=0.0, diag_tol=1e-9, **kw)
+    assert res["converged"] == 1
+    assert abs(res["total_energy"] - ref.total_energy) < 1e-8 * HA
+    assert np.max(np.abs(ev - np.array(ref.eigenvalues))) < 1e-7 * HA
+    assert np.max(np.abs(rho - ref.rho_r)) < 1e-6 * np.max(ref.rho_r)
