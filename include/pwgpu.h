@@ -197,6 +197,21 @@ pwgpu_status pwgpu_symmetrize(pwgpu_handle* h, double* rho_r);
  * int rho_val v_xc (eV). */
 pwgpu_status pwgpu_potentials(pwgpu_handle* h, const double* rho_r, double* veff_g, double* energies);
 
+/* Local part of H|psi> (kinetic diagonal + V_eff through the FFT pipeline;
+ * no Kleinman-Bylander term) on device pointers, allocating nothing.  No
+ * counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * code living inside a host framework whose memory manager owns all device
+ * memory, and serving loops that cannot afford cudaMalloc's implicit
+ * device-wide synchronisation.  The FFT intermediates go to one fixed
+ * 32 MiB device array inside the library (held by every GPU that loads
+ * it); a grid whose single band needs more than that is rejected with
+ * PWGPU_E_INVALID.  The first call on a device looks the array's address
+ * up, so make it before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU race.  Result equals pwgpu_apply_h_device
+ * for a system without projectors. */
+pwgpu_status pwgpu_apply_h_local_noalloc(pwgpu_handle* h, int32_t spin, int32_t ik, const void* psi_dev,
+                                         int64_t ldpsi, int32_t nb, void* hpsi_dev, int64_t ldh, void* stream);
+
 /* Batched small generalized Hermitian eigensolve H c = e S c (m <= 64,
  * column-major complex, batch consecutive problems): the Rayleigh-Ritz
  * kernel, exposed for testing.  evals batch x nev ascending; C batch x m x nev. */

@@ -133,6 +133,16 @@ static Status create(const pwgpu_system* s, const pwgpu_options* o, pwgpu_handle
 
 }  // namespace pwgpu
 
+namespace pwgpu {
+// Internal state and precision of an opaque handle (for entry points
+// defined in other translation units).
+Handle* handle_state(pwgpu_handle* ph, int* precision) {
+  if (!ph) return nullptr;
+  if (precision) *precision = ph->precision;
+  return &ph->h;
+}
+}  // namespace pwgpu
+
 using namespace pwgpu;
 
 extern "C" {

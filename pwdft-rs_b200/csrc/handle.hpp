@@ -97,6 +97,12 @@ Status apply_h_device(Handle& h, int spin, int ik, const double2* psi, long ldps
 Status set_veff_from_g(Handle& h, int spin, const double2* veff_g_dev, cudaStream_t stream);
 Status ensure_nl_capacity(Handle& h, int nb);
 
+// Local part of H|psi> (kinetic + V_eff, no projectors) with the FFT
+// intermediates in caller-provided device scratch; fails with kInvalid when
+// one band does not fit.
+Status local_apply_on_scratch(Handle& h, int spin, int ik, const double2* psi, long ldpsi, int nb, double2* hpsi,
+                              long ldh, int precision, cudaStream_t s, void* scratch, size_t scratch_bytes);
+
 // rho(r) += sum_b fw[b] |psi_b(r)|^2 over nb bands (FP64 FFTs); fw on device.
 Status density_accumulate(Handle& h, const double2* psi, long ldpsi, int nb, const double* fw_dev, double* rho,
                           cudaStream_t stream);

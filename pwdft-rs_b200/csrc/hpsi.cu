@@ -567,6 +567,63 @@ static Status local_chunk(Handle& h, int spin, int ik, const double2* psi, long 
   return kOk;
 }
 
+// The five local kernels on explicit scratch A / B (used by the
+// allocation-free entry point; the handle's own buffers are not touched).
+template <typename R>
+static void local_chunk_on(Handle& h, int spin, int ik, const double2* psi, long ldpsi, int nb, double2* hpsi,
+                           long ldh, cudaStream_t s, cplx<R>* A, cplx<R>* B) {
+  using C = cplx<R>;
+  GridMaps& g = h.g;
+  const int d0 = g.d[0], d1 = g.d[1], d2 = g.d[2];
+  const bool dbl = std::is_same<R, double>::value;
+  const C* tw0 = dbl ? (const C*)g.tw64[0] : (const C*)g.tw32[0];
+  const C* tw1 = dbl ? (const C*)g.tw64[1] : (const C*)g.tw32[1];
+  const C* tw2 = dbl ? (const C*)g.tw64[2] : (const C*)g.tw32[2];
+  const R* vr = dbl ? (const R*)h.veff_r[spin] : (const R*)h.veff_r32[spin];
+  k_zinv<R><<<dim3((g.ncol + g.wz - 1) / g.wz, nb), block_for(g.wz), 2 * (size_t)g.wz * d2 * sizeof(C), s>>>(
+      psi, ldpsi, A, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2, div_magic(d2), g.plan[2], tw2);
+  k_y<R, +1><<<dim3(g.Xp, (d2 + g.wy - 1) / g.wy, nb), block_for(g.wy), 2 * (size_t)g.wy * d1 * sizeof(C), s>>>(
+      A, B, g.Xp, g.Yp, g.m[1], d1, d2, g.plan[1], tw1);
+  k_xv<R><<<dim3(d1, (d2 + g.wx - 1) / g.wx, nb), block_for(g.wx), 2 * (size_t)g.wx * d0 * sizeof(C), s>>>(
+      B, vr, g.Xp, g.m[0], d0, d1, d2, g.plan[0], tw0);
+  k_y<R, -1><<<dim3(g.Xp, (d2 + g.wy - 1) / g.wy, nb), block_for(g.wy), 2 * (size_t)g.wy * d1 * sizeof(C), s>>>(
+      A, B, g.Xp, g.Yp, g.m[1], d1, d2, g.plan[1], tw1);
+  k_zfwd<R><<<dim3((g.ncol + g.wz - 1) / g.wz, nb), block_for(g.wz), 2 * (size_t)g.wz * d2 * sizeof(C), s>>>(
+      A, psi, ldpsi, hpsi, ldh, h.kp[ik].kinetic, 1.0 / (double)g.N, g.col_start, g.pt_ig, g.pt_col, g.pt_z,
+      g.ncol, d2, div_magic(d2), g.plan[2], tw2);
+}
+
+Status local_apply_on_scratch(Handle& h, int spin, int ik, const double2* psi, long ldpsi, int nb, double2* hpsi,
+                              long ldh, int precision, cudaStream_t s, void* scratch, size_t scratch_bytes) {
+  if (ik < 0 || ik >= h.n_k) return fail(kInvalid, "k-point index out of range");
+  if (spin < 0 || spin >= h.nspin) return fail(kInvalid, "spin index out of range");
+  if (ldpsi < h.n_pw || ldh < h.n_pw) return fail(kInvalid, "leading dimension smaller than n_pw");
+  if (nb <= 0) return kOk;
+  GridMaps& g = h.g;
+  const size_t cb = precision == 0 ? sizeof(double2) : sizeof(float2);
+  const size_t a_elems = (size_t)g.ncol * g.d[2];
+  const size_t b_elems = (size_t)g.Xp * g.d[1] * g.d[2];
+  const size_t per_band = (a_elems + b_elems) * cb;
+  // 256 bytes of margin for aligning B behind A
+  const int chunk = scratch_bytes > 256 ? (int)std::min<size_t>(64, (scratch_bytes - 256) / per_band) : 0;
+  if (chunk < 1)
+    return fail(kInvalid, "grid too large for the fixed scratch: one band needs " + std::to_string(per_band) +
+                              " bytes, the scratch holds " + std::to_string(scratch_bytes));
+  unsigned char* base = static_cast<unsigned char*>(scratch);
+  const size_t a_bytes = ((a_elems * chunk * cb) + 255) / 256 * 256;
+  for (int c0 = 0; c0 < nb; c0 += chunk) {
+    const int cnt = std::min(chunk, nb - c0);
+    if (precision == 0)
+      local_chunk_on<double>(h, spin, ik, psi + (long)c0 * ldpsi, ldpsi, cnt, hpsi + (long)c0 * ldh, ldh, s,
+                             reinterpret_cast<double2*>(base), reinterpret_cast<double2*>(base + a_bytes));
+    else
+      local_chunk_on<float>(h, spin, ik, psi + (long)c0 * ldpsi, ldpsi, cnt, hpsi + (long)c0 * ldh, ldh, s,
+                            reinterpret_cast<float2*>(base), reinterpret_cast<float2*>(base + a_bytes));
+  }
+  PW_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
 Status density_accumulate(Handle& h, const double2* psi, long ldpsi, int nb, const double* fw_dev, double* rho,
                           cudaStream_t s) {
   GridMaps& g = h.g;

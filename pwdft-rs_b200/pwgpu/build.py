@@ -19,7 +19,7 @@ INCLUDE = os.path.join(os.path.dirname(PKG_ROOT), "include")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libpwgpu.so")
 
-SOURCES = ["api.cu", "hpsi.cu", "linalg.cu", "scf.cu"]
+SOURCES = ["api.cu", "hpsi.cu", "linalg.cu", "scf.cu", "noalloc.cu"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
