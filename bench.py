@@ -1,17 +1,26 @@
 """Benchmark of the SCF hot path on B200 (one JSON line on stdout).
 
-Workload: the synthetic H|psi> kernel bench -- 64-atom Si cubic supercell,
-Γ, ecutwfc 30 Ry (n_pw 23,847, 72^3 grid), 160 bands, 256 KB channels,
-seeded inputs (pwgpu.workloads.hpsi_system).  One step = one H|psi> of the
-160-band block, inputs resident in HBM, L2 flushed (256 MB write) before
-every timed step.  `value` is the mixed form (FP32 FFT / V_eff product);
-the FP64 plain form is reported beside it.
+Headline: SCF solves/s of the 64-atom Si cell (2x2x2 conventional cells of
+a = 10.26 bohr, seeded ±0.05 bohr displacements, Si UPF, ecutwfc 30 Ry,
+n_pw 23,847 on 72^3, Γ, 160 bands, Gaussian 0.01 Ry, Anderson beta 0.4 +
+Kerker) run to convergence in the mixed form (FP32 FFT/V_eff product, FP64
+subspace algebra and energies, FP64 H|psi> after the density rms passes
+1e-6), next to the FP64 plain form of the same solve, with |ΔE| per atom
+and the eigenvalue deviation between the two.  One step = one solve from
+the SAD start density; the device time of a step is CUDA events on the
+library's stream, the end-to-end time the same C-ABI call by wall clock
+(it includes the host->device copy of the start density and the
+device->host copies of eigenvalues and density).
+
+Beside it, the synthetic H|psi> kernel bench of the same cell (160 seeded
+bands, 256 Gaussian KB channels, V_eff seeded in [-1, 0] Ha) gives the
+per-stage device times and the roofline of the dominant own kernel.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pwgpu|reference]
 
-Multi-GPU: one process per GPU (torchrun), independent replicas of the
-workload (the path has no cross-GPU exchange at this size), barrier and
-max-over-ranks device time.
+Multi-GPU: one process per GPU (torchrun); every rank solves its own replica
+(weak scaling: the solve has no cross-GPU exchange at this size), barrier,
+max-over-ranks device time, aggregate solves/s.
 """
 
 from __future__ import annotations
@@ -30,8 +39,10 @@ sys.path.insert(0, os.path.join(ROOT, "pwdft-rs_b200"))
 
 import numpy as np  # noqa: E402
 
-METRIC = "H|psi> 160-band blocks/s (Si64 Γ 30 Ry synthetic kernel bench of the SCF solves/s metric)"
-UNIT = "blocks/s"
+METRIC = "SCF solves/s (Si64 Γ 30 Ry, 160 bands; mixed vs FP64 plain GPU, |ΔE| per atom reported)"
+UNIT = "solves/s"
+HA_TO_EV = 27.211386245988
+SI_UPF = os.path.join(ROOT, "tests", "golden", "upf", "Si.upf")
 
 
 def load_peaks():
@@ -80,68 +91,95 @@ class ClockSampler:
     def summary(self):
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [v for v in (num(s[0]) for s in self.samples) if v is not None]
+        mx = [v for v in (num(s[1]) for s in self.samples) if v is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and "Active" in s[3 + i]
-                          and "Not" not in s[3 + i]})
+        reasons = sorted({names[i] for s in self.samples for i in range(4)
+                          if len(s) > 3 + i and s[3 + i].strip() == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.samples)}
 
 
 def dist_env():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
 
 
-def cpu_baseline_sample(sys_, veff_g, psi, nb_sample=8):
-    """Oracle FP64 H|psi> (FFT form, all host threads) on a band sample."""
+def scf_kwargs():
+    from pwgpu.config3 import FP64_SWITCH, SCF_KW
+    kw = dict(SCF_KW)
+    nb = kw.pop("n_bands")
+    return nb, kw, FP64_SWITCH
+
+
+def sad_veff(sys_):
+    """V_eff(G) of the start density, as the solve's first iteration builds it (for CPU sampling)."""
+    from oracle import pwdft_oracle as O
+    rho_g = O.density_r_to_g(sys_.rho_init_r, sys_.dims)
+    _, vxc = O.lda_xc(O.add_core(sys_.rho_init_r, sys_.rho_core_r))
+    return sys_.v_local_g + O.hartree(rho_g, sys_.g_squared) + O.density_r_to_g(vxc, sys_.dims)
+
+
+def cpu_solve_sample(sys_, h_applications: int, nb_sample: int = 8):
+    """Oracle FP64 H|psi> (FFT form + projector GEMMs, all host threads) on a
+    band sample, scaled by the band applications of the FP64 GPU solve."""
     from oracle import pwdft_oracle as O
     O.set_workers(-1)
     p = sys_.projectors[0]
     d = p.d_dense()
-    sub = np.ascontiguousarray(psi[:, :nb_sample])
-    O.apply_h_fft(sys_.g_to_fft, sys_.kinetic[0], veff_g, sys_.dims, p.b, d, sub[:, :1])  # warm
+    veff = sad_veff(sys_)
+    rng = np.random.default_rng(1)
+    psi = rng.standard_normal((sys_.n_pw, nb_sample)) + 1j * rng.standard_normal((sys_.n_pw, nb_sample))
+    O.apply_h_fft(sys_.g_to_fft, sys_.kinetic[0], veff, sys_.dims, p.b, d, psi[:, :1])  # warm
     t0 = time.perf_counter()
     reps = 0
     while True:
-        O.apply_h_fft(sys_.g_to_fft, sys_.kinetic[0], veff_g, sys_.dims, p.b, d, sub)
+        O.apply_h_fft(sys_.g_to_fft, sys_.kinetic[0], veff, sys_.dims, p.b, d, psi)
         reps += 1
         if time.perf_counter() - t0 > 10.0 or reps >= 3:
             break
-    dt = (time.perf_counter() - t0) / reps
-    per_block = dt * psi.shape[1] / nb_sample
-    return {"value": 1.0 / per_block, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-            "sample": f"{nb_sample} of {psi.shape[1]} bands, {reps} rep(s), scaled to a 160-band block"}
+    per_band = (time.perf_counter() - t0) / reps / nb_sample
+    solve_s = per_band * h_applications
+    return {"value": 1.0 / solve_s, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": (f"oracle FP64 H|psi> on {nb_sample} bands x {reps} rep(s) ({per_band * 1e3:.2f} ms/band), "
+                       f"scaled by the {h_applications} band applications of the FP64 GPU solve; "
+                       "subspace algebra, density and potentials not counted (lower bound on CPU time)")}
 
 
 def run_reference(args, world, rank):
+    """CPU arm: the oracle restatement of the reference's per-iteration operator
+    on all host cores, bounded samples scaled to one solve."""
     if rank != 0:
         return
-    from pwgpu.workloads import hpsi_system, si64_crystal
-    sys_, veff_g, psi = hpsi_system(si64_crystal())
-    times = []
+    from pwgpu.config3 import config3_system
+    from pwgpu.upf import load_upf
+    sys_ = config3_system(load_upf(SI_UPF))
+    h_apps = 84240  # band applications of the FP64 GPU solve of this cell (measured, bench "fp64" line)
+    vals = []
     base = None
     for i in range(args.warmup + args.steps):
-        b = cpu_baseline_sample(sys_, veff_g, psi, nb_sample=4)
+        base = cpu_solve_sample(sys_, h_apps, nb_sample=4)
         if i >= args.warmup:
-            times.append(1.0 / b["value"])
-        base = b
-    v = 1.0 / statistics.mean(times)
+            vals.append(1.0 / base["value"])
+    v = 1.0 / statistics.mean(vals)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-            "config": {"workload": "si64_hpsi_gamma_30ry", "n_pw": sys_.n_pw, "grid": list(sys_.dims),
-                       "n_bands": 160, "n_ch": 256},
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded Si64 cell)",
+            "config": {"workload": "si64_scf_gamma_30ry", "n_pw": sys_.n_pw, "grid": list(sys_.dims),
+                       "n_bands": 160, "n_ch": sys_.projectors[0].n_ch},
             "cpu_baseline": {**base, "value": v},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 def run_once():
-    """Three H|psi> calls of the bench workload per precision, mixed first
+    """Three H|psi> calls of the kernel-bench block per precision, mixed first
     (a short, bounded program for profiler captures)."""
     import torch
 
@@ -161,19 +199,104 @@ def run_once():
     print("once: ok")
 
 
+def run_scf_once():
+    """One mixed-form solve of the headline cell (for profiler launch lists)."""
+    from pwgpu.config3 import config3_system
+    from pwgpu.lib import PRECISION_MIXED, PwGpu
+    from pwgpu.upf import load_upf
+    sys_ = config3_system(load_upf(SI_UPF))
+    nb, kw, sw = scf_kwargs()
+    with PwGpu(sys_) as dev:
+        res, _, _, _ = dev.scf_run(sys_.rho_init_r, nb, precision=PRECISION_MIXED, fp64_switch=sw, **kw)
+    print("scf once: ok", res["n_iterations"], res["total_energy"])
+
+
+def kernel_bench(local, steps, warmup, flush, hbm_peak, peak_kind):
+    """H|psi> of the 160-band block (mixed and FP64): device ms per block and
+    the per-stage profile; roofline of the dominant own kernel."""
+    import torch
+
+    from pwgpu.lib import PRECISION_FP64, PRECISION_MIXED, PwGpu
+    from pwgpu.workloads import hpsi_system, si64_crystal
+    sys_, veff_g, psi = hpsi_system(si64_crystal())
+    nb = psi.shape[1]
+    n_pw, N = sys_.n_pw, sys_.n_grid
+    out = {}
+    with PwGpu(sys_, device=local) as dev:
+        dev.set_veff_g(veff_g)
+        d_psi = torch.from_numpy(np.ascontiguousarray(psi.T)).to(f"cuda:{local}")
+        d_h = torch.empty_like(d_psi)
+        stream = torch.cuda.Stream()
+        for prec, tag in ((PRECISION_FP64, "fp64"), (PRECISION_MIXED, "mixed")):
+            dev.set_precision(prec)
+            ms = []
+            with torch.cuda.stream(stream):
+                for i in range(warmup + steps):
+                    flush.fill_(float(i))
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    dev.apply_h_device(d_psi.data_ptr(), n_pw, nb, d_h.data_ptr(), n_pw, stream=stream.cuda_stream)
+                    e1.record(stream)
+                    if i >= warmup:
+                        ms.append((e0, e1))
+            torch.cuda.synchronize()
+            out[tag] = {"ms_per_block": statistics.mean(a.elapsed_time(b) for a, b in ms)}
+        names = ["fft_z_inv_scatter", "fft_y_inv", "fft_x_inv_v_fwd", "fft_y_fwd", "fft_z_fwd_gather",
+                 "nl_bh_psi_zgemm", "nl_d_apply", "nl_b_q_zgemm"]
+        for prec, tag in ((PRECISION_MIXED, "mixed"), (PRECISION_FP64, "fp64")):
+            dev.set_precision(prec)
+            acc = np.zeros(8)
+            for _ in range(3):
+                flush.fill_(1.0)
+                torch.cuda.synchronize()
+                st_ms, st_n = dev.profile_apply_h(d_psi.data_ptr(), n_pw, nb, d_h.data_ptr(), n_pw)
+                acc += st_ms
+            acc /= 3
+            out[tag]["stage_ms"] = dict(zip(names, [round(float(x), 5) for x in acc]))
+            out[tag]["launches"] = dict(zip(names, [int(x) for x in st_n]))
+    p = out["mixed"]
+    own = {k: v for k, v in p["stage_ms"].items() if not k.endswith("zgemm")}
+    dom = max(own, key=own.get)
+    nl = max(1, p["launches"][dom])
+    m = np.abs(sys_.basis.miller).max(axis=0)
+    Xp, Yp = 2 * int(m[0]) + 1, 2 * int(m[1]) + 1
+    d0, d1, d2 = sys_.dims
+    cb = 8  # complex FP32 in the mixed form
+    per_band = {
+        "fft_z_inv_scatter": 16 * n_pw + cb * Xp * Yp * d2,
+        "fft_y_inv": cb * Xp * Yp * d2 + cb * Xp * d1 * d2,
+        "fft_x_inv_v_fwd": 2 * cb * Xp * d1 * d2 + 4.0 * N / (nb / nl),
+        "fft_y_fwd": cb * Xp * d1 * d2 + cb * Xp * Yp * d2,
+        "fft_z_fwd_gather": cb * Xp * Yp * d2 + 3 * 16 * n_pw,
+        "nl_d_apply": 2 * 16 * 256,
+    }[dom]
+    alg = per_band * nb / nl
+    ms_launch = own[dom] / nl
+    achieved = alg / (ms_launch * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "traffic": None, "peak_kind": peak_kind,
+                "alg_bytes_per_launch": alg, "ms_per_launch": ms_launch,
+                "note": "dominant own kernel of H|psi> (the inner operator of every SCF step); "
+                        "alg bytes = compact-grid read+write per band x bands per launch, V(r) FP32 read"}
+    return out, roofline, {"n_pw": n_pw, "grid": [d0, d1, d2], "n_bands": nb, "n_ch": 256}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="pwgpu", choices=["pwgpu", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="full", choices=["full", "once"],
-                    help="once: three untimed H|psi> calls per precision (for profiler captures)")
+    ap.add_argument("--mode", default="full", choices=["full", "once", "scf-once"],
+                    help="once: three untimed H|psi> calls per precision; scf-once: one mixed solve")
     args = ap.parse_args()
     world, rank, local = dist_env()
     if args.mode == "once":
         run_once()
+        return
+    if args.mode == "scf-once":
+        run_scf_once()
         return
     if args.impl == "reference":
         if world > 1:
@@ -189,155 +312,90 @@ def main():
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=300))
 
-    from pwgpu.lib import PRECISION_FP64, PRECISION_MIXED, PwGpu
-    from pwgpu.workloads import hpsi_algorithmic_bytes, hpsi_system, nonlocal_flops, si64_crystal
-
-    sys_, veff_g, psi = hpsi_system(si64_crystal())
-    nb = psi.shape[1]
-    n_pw, N = sys_.n_pw, sys_.n_grid
-    dev = PwGpu(sys_, device=local)
-    dev.set_veff_g(veff_g)
-    d_psi = torch.from_numpy(np.ascontiguousarray(psi.T)).to(f"cuda:{local}")  # row b = band b (column-major view)
-    d_h = torch.empty_like(d_psi)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
-    stream = torch.cuda.Stream()
-
-    def timed(precision, steps, warmup):
-        dev.set_precision(precision)
-        ms = []
-        with torch.cuda.stream(stream):
-            for i in range(warmup + steps):
-                flush.fill_(float(i))
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                dev.apply_h_device(d_psi.data_ptr(), n_pw, nb, d_h.data_ptr(), n_pw, stream=stream.cuda_stream)
-                e1.record(stream)
-                if i >= warmup:
-                    ms.append((e0, e1))
-        torch.cuda.synchronize()
-        return [a.elapsed_time(b) for a, b in ms]
+    from pwgpu.config3 import config3_system
+    from pwgpu.lib import PRECISION_FP64, PRECISION_MIXED, PwGpu, kernel_launches
+    from pwgpu.upf import load_upf
 
     hbm_peak, bf16_peak, peak_kind = load_peaks()
-    # untimed correctness spot check against the FP64 form
-    timed(PRECISION_FP64, 1, 0)
-    ref_h = d_h.clone()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        t64 = timed(PRECISION_FP64, args.steps, args.warmup)
-        t32 = timed(PRECISION_MIXED, args.steps, args.warmup)
-    mixed_err = float((d_h - ref_h).abs().max() / ref_h.abs().max())
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    ms32 = statistics.mean(t32)
-    ms64 = statistics.mean(t64)
-    if dist:
-        t = torch.tensor([ms32, ms64], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms32, ms64 = t.tolist()
+    sys_ = config3_system(load_upf(SI_UPF))
+    nb, kw, sw = scf_kwargs()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    dev = PwGpu(sys_, device=local)
+    hstream = torch.cuda.ExternalStream(dev.stream(), device=f"cuda:{local}")
 
-    # per-stage profile (events after every launch, on the handle's stream)
-    stage_names = ["fft_z_inv_scatter", "fft_y_inv", "fft_x_inv_v_fwd", "fft_y_fwd", "fft_z_fwd_gather",
-                   "nl_bh_psi_zgemm", "nl_d_apply", "nl_b_q_zgemm"]
-    prof = {}
-    launches = 0
-    for prec, tag in ((PRECISION_MIXED, "mixed"), (PRECISION_FP64, "fp64")):
-        dev.set_precision(prec)
-        acc = np.zeros(8)
-        for _ in range(3):
-            flush.fill_(1.0)
-            torch.cuda.synchronize()
-            st_ms, st_n = dev.profile_apply_h(d_psi.data_ptr(), n_pw, nb, d_h.data_ptr(), n_pw)
-            acc += st_ms
-        acc /= 3
-        prof[tag] = {"stage_ms": dict(zip(stage_names, [round(x, 5) for x in acc])),
-                     "launches": dict(zip(stage_names, [int(x) for x in st_n]))}
-        if tag == "mixed":
-            launches = int(st_n[[0, 1, 2, 3, 4, 6]].sum())
-
-    # roofline of the dominant own kernel in the mixed form (HBM-bound FFT stage)
-    g = dev_grid = None
-    p = prof["mixed"]
-    own = {k: v for k, v in p["stage_ms"].items() if not k.endswith("zgemm")}
-    dom = max(own, key=own.get)
-    dom_ms_per_launch = own[dom] / max(1, p["launches"][dom])
-    cb = 8  # complex FP32 in the mixed form
-    from pwgpu.crystal import BasisSet  # noqa: F401
-    m = np.abs(sys_.basis.miller).max(axis=0)
-    Xp, Yp = 2 * m[0] + 1, 2 * m[1] + 1
-    d0, d1, d2 = sys_.dims
-    nb_launch = nb / max(1, p["launches"][dom])
-    per_band = {
-        "fft_z_inv_scatter": 16 * n_pw + cb * Xp * Yp * d2,
-        "fft_y_inv": cb * Xp * Yp * d2 + cb * Xp * d1 * d2,
-        "fft_x_inv_v_fwd": 2 * cb * Xp * d1 * d2 + 4 * N / nb,
-        "fft_y_fwd": cb * Xp * d1 * d2 + cb * Xp * Yp * d2,
-        "fft_z_fwd_gather": cb * Xp * Yp * d2 + 3 * 16 * n_pw,
-        "nl_d_apply": 2 * 16 * 256,
-    }[dom]
-    alg_bytes = per_band * nb_launch
-    achieved = alg_bytes / (dom_ms_per_launch * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "traffic": None, "peak_kind": peak_kind,
-                "alg_bytes_per_launch": alg_bytes, "ms_per_launch": dom_ms_per_launch}
-
-    # end to end through the C-ABI with host buffers (pinned), mixed form
-    dev.set_precision(PRECISION_MIXED)
-    h_psi = torch.from_numpy(np.ascontiguousarray(psi.T)).pin_memory()
-    h_out = torch.empty_like(h_psi).pin_memory()
-    import ctypes as ct
-    lib = dev.lib
-    f64p = ct.POINTER(ct.c_double)
-    e2e_t = []
-    for i in range(args.warmup + args.steps):
-        flush.fill_(float(i))
+    def solve(prec):
+        flush.fill_(1.0)
         torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(hstream)
         t0 = time.perf_counter()
-        rc = lib.pwgpu_apply_h(dev.h, 0, 0, ct.cast(h_psi.data_ptr(), f64p), nb, ct.cast(h_out.data_ptr(), f64p))
+        res, ev, rho, _ = dev.scf_run(sys_.rho_init_r, nb, precision=prec, fp64_switch=sw, **kw)
         t1 = time.perf_counter()
-        if rc != 0:
-            raise RuntimeError(lib.pwgpu_last_error())
-        if i >= args.warmup:
-            e2e_t.append(t1 - t0)
-    e2e_s = statistics.mean(e2e_t)
+        e1.record(hstream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), t1 - t0, res, ev
+
+    for _ in range(args.warmup):
+        solve(PRECISION_MIXED)
     if dist:
-        t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
+        dist.barrier()
+    torch.cuda.synchronize()
+    n0 = kernel_launches()
+    with ClockSampler(local) as clk:
+        runs = [solve(PRECISION_MIXED) for _ in range(args.steps)]
+    n_launch = kernel_launches() - n0
+    fp64_runs = [solve(PRECISION_FP64) for _ in range(max(1, min(2, args.steps)))]
+    ms = statistics.mean(r[0] for r in runs)
+    wall = statistics.mean(r[1] for r in runs)
+    ms64 = statistics.mean(r[0] for r in fp64_runs)
+    if dist:
+        t = torch.tensor([ms, wall, ms64], device=f"cuda:{local}", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = t.item()
+        ms, wall, ms64 = t.tolist()
+    rm, em = runs[-1][2], runs[-1][3]
+    r64, e64 = fp64_runs[-1][2], fp64_runs[-1][3]
+    n_at = len(sys_.crystal.atoms)
+    accuracy = {"dE_total_per_atom_ha": abs(rm["total_energy"] - r64["total_energy"]) / n_at / HA_TO_EV,
+                "max_eigenvalue_dev_ha": float(np.max(np.abs(em - e64))) / HA_TO_EV,
+                "bar": "|dE| <= 1e-6 Ha/atom, eigenvalues <= 1e-5 Ha vs the FP64 form",
+                "e_total_mixed_ev": rm["total_energy"], "e_total_fp64_ev": r64["total_energy"],
+                "iterations_mixed": rm["n_iterations"], "iterations_fp64": r64["n_iterations"],
+                "h_band_applications_mixed": rm["h_applications"],
+                "h_band_applications_fp64": r64["h_applications"]}
+
+    kb, roofline, kb_cfg = kernel_bench(local, 5, 3, flush, hbm_peak, peak_kind)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(sys_, veff_g, psi)
-
+        cpu = cpu_solve_sample(sys_, int(r64["h_applications"]))
+    dev.close()
     if rank == 0:
-        nl_gflop = nonlocal_flops(n_pw, 256, nb) / 1e9
         line = {
-            "metric": METRIC, "value": world * 1e3 / ms32, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "c64 FFT/V_eff + c128 projector GEMMs (mixed form)",
-            "data": "synthetic (seeded; shapes of the Si64 Γ 30 Ry kernel bench)",
-            "config": {"workload": "si64_hpsi_gamma_30ry", "n_pw": n_pw, "grid": [d0, d1, d2], "n_bands": nb,
-                       "n_ch": 256, "l2": "flushed before every timed step (256 MB write)",
+            "metric": METRIC, "value": world * 1e3 / ms, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "mixed: c64 FFT/V_eff product, c128 projector GEMMs, f64 subspace/energies/mixing",
+            "data": "synthetic (seeded Si64 cell; reference Si.upf)",
+            "config": {"workload": "si64_scf_gamma_30ry", "n_pw": sys_.n_pw, "grid": list(sys_.dims),
+                       "n_bands": nb, "n_ch": sys_.projectors[0].n_ch, "n_atoms": n_at,
+                       "smearing": "gaussian 0.01 Ry", "mixing": "anderson beta 0.4 + kerker",
+                       "l2": "flushed before every solve (256 MB write); working set > L2",
                        "parallelism": f"replicas x{world}"},
             "fp64": {"value": world * 1e3 / ms64, "unit": UNIT, "ms_per_step": ms64},
-            "mixed_vs_fp64_max_rel_err": mixed_err,
+            "accuracy": accuracy,
             "roofline": roofline,
-            "stages": prof,
-            "gpu_launches": launches * args.steps,
-            "e2e": {"value": world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(16 * n_pw * nb),
-                    "d2h_bytes_per_step": int(16 * n_pw * nb), "path": "pwgpu_apply_h (C-ABI, pinned host)"},
-            "nonlocal_gflop_per_step": nl_gflop,
-            "alg_local_bytes_per_step_fp32": hpsi_algorithmic_bytes(n_pw, N, 8) * nb,
+            "kernel_bench": {"workload": "si64_hpsi_gamma_30ry", **kb_cfg, **kb},
+            "gpu_launches": n_launch,
+            "e2e": {"value": world / wall, "unit": UNIT, "h2d_bytes_per_step": int(8 * sys_.n_grid),
+                    "d2h_bytes_per_step": int(8 * sys_.n_grid + 8 * nb + 16 * sys_.n_pw),
+                    "path": "pwgpu_scf_run (C-ABI, host start density in, host eigenvalues/density out)"},
             "clocks": clk.summary(),
         }
         if cpu:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
-    dev.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

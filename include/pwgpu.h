@@ -130,6 +130,14 @@ pwgpu_status pwgpu_profile_apply_h(pwgpu_handle* h, int32_t spin, int32_t ik, co
 /* Select the arithmetic of subsequent H|psi> calls (PWGPU_PRECISION_*). */
 pwgpu_status pwgpu_set_precision(pwgpu_handle* h, int32_t precision);
 
+/* Number of this library's kernel launches since it was loaded (all
+ * handles, all threads); library GEMMs (cuBLAS/cuSOLVER) are not counted. */
+pwgpu_status pwgpu_kernel_launches(int64_t* count);
+
+/* The CUDA stream (cudaStream_t) a handle runs on, for callers that time or
+ * order work against it. */
+pwgpu_status pwgpu_get_stream(const pwgpu_handle* h, void** stream);
+
 /* Basis size, grid size and channel count of a handle. */
 pwgpu_status pwgpu_get_dims(const pwgpu_handle* h, int32_t* n_pw, int64_t* n_grid, int32_t* n_ch);
 

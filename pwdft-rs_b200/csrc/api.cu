@@ -361,6 +361,18 @@ pwgpu_status pwgpu_small_geneig(int32_t batch, int32_t m, int32_t nev, const dou
   return st;
 }
 
+pwgpu_status pwgpu_kernel_launches(int64_t* count) {
+  if (!count) return fail(kInvalid, "pwgpu_kernel_launches: NULL argument");
+  *count = launch_counter().load();
+  return kOk;
+}
+
+pwgpu_status pwgpu_get_stream(const pwgpu_handle* ph, void** stream) {
+  if (!ph || !stream) return fail(kInvalid, "pwgpu_get_stream: NULL argument");
+  *stream = (void*)ph->h.stream;
+  return kOk;
+}
+
 pwgpu_status pwgpu_get_dims(const pwgpu_handle* ph, int32_t* n_pw, int64_t* n_grid, int32_t* n_ch) {
   if (!ph) return fail(kInvalid, "pwgpu_get_dims: NULL handle");
   if (n_pw) *n_pw = ph->h.n_pw;

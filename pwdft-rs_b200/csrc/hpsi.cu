@@ -494,6 +494,7 @@ Status fft3d_full(Handle& h, double2* data, int sign, cudaStream_t stream) {
       k_fft_axis<-1><<<grid, blk, sm, stream>>>(data, ax.outer, ax.L, ax.inner, mL, p, g.tw64[ax.a]);
     else
       k_fft_axis<+1><<<grid, blk, sm, stream>>>(data, ax.outer, ax.L, ax.inner, mL, p, g.tw64[ax.a]);
+    count_launch();
   }
   PW_CUDA_TRY(cudaGetLastError());
   return kOk;
@@ -504,7 +505,7 @@ Status set_veff_from_g(Handle& h, int spin, const double2* veff_g_dev, cudaStrea
   PW_CUDA_TRY(cudaMemcpyAsync(h.tmp_grid, veff_g_dev, N * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
   Status st = fft3d_full(h, h.tmp_grid, +1, stream);
   if (st != kOk) return st;
-  k_real_to_r32<<<(unsigned)((N + 255) / 256), 256, 0, stream>>>(h.tmp_grid, h.veff_r[spin], h.veff_r32[spin], N);
+  k_real_to_r32<<<(unsigned)((N + 255) / 256), 256, 0, stream>>>(h.tmp_grid, h.veff_r[spin], h.veff_r32[spin], N); count_launch();
   PW_CUDA_TRY(cudaGetLastError());
   return kOk;
 }
@@ -535,32 +536,32 @@ static Status local_chunk(Handle& h, int spin, int ik, const double2* psi, long 
   {
     dim3 grid((g.ncol + g.wz - 1) / g.wz, nb);
     k_zinv<R><<<grid, block_for(g.wz), 2 * (size_t)g.wz * d2 * sizeof(C), s>>>(
-        psi, ldpsi, A, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2, div_magic(d2), g.plan[2], tw2);
+        psi, ldpsi, A, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2, div_magic(d2), g.plan[2], tw2); count_launch();
     mark(tm, 0, s);
   }
   {
     dim3 grid(g.Xp, (d2 + g.wy - 1) / g.wy, nb);
     k_y<R, +1><<<grid, block_for(g.wy), 2 * (size_t)g.wy * d1 * sizeof(C), s>>>(A, B, g.Xp, g.Yp, g.m[1], d1, d2,
-                                                                              g.plan[1], tw1);
+                                                                              g.plan[1], tw1); count_launch();
     mark(tm, 1, s);
   }
   {
     dim3 grid(d1, (d2 + g.wx - 1) / g.wx, nb);
     k_xv<R><<<grid, block_for(g.wx), 2 * (size_t)g.wx * d0 * sizeof(C), s>>>(B, vr, g.Xp, g.m[0], d0, d1, d2,
-                                                                           g.plan[0], tw0);
+                                                                           g.plan[0], tw0); count_launch();
     mark(tm, 2, s);
   }
   {
     dim3 grid(g.Xp, (d2 + g.wy - 1) / g.wy, nb);
     k_y<R, -1><<<grid, block_for(g.wy), 2 * (size_t)g.wy * d1 * sizeof(C), s>>>(A, B, g.Xp, g.Yp, g.m[1], d1, d2,
-                                                                              g.plan[1], tw1);
+                                                                              g.plan[1], tw1); count_launch();
     mark(tm, 3, s);
   }
   {
     dim3 grid((g.ncol + g.wz - 1) / g.wz, nb);
     k_zfwd<R><<<grid, block_for(g.wz), 2 * (size_t)g.wz * d2 * sizeof(C), s>>>(
         A, psi, ldpsi, hpsi, ldh, h.kp[ik].kinetic, scale, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2,
-        div_magic(d2), g.plan[2], tw2);
+        div_magic(d2), g.plan[2], tw2); count_launch();
     mark(tm, 4, s);
   }
   PW_CUDA_TRY(cudaGetLastError());
@@ -581,16 +582,16 @@ static void local_chunk_on(Handle& h, int spin, int ik, const double2* psi, long
   const C* tw2 = dbl ? (const C*)g.tw64[2] : (const C*)g.tw32[2];
   const R* vr = dbl ? (const R*)h.veff_r[spin] : (const R*)h.veff_r32[spin];
   k_zinv<R><<<dim3((g.ncol + g.wz - 1) / g.wz, nb), block_for(g.wz), 2 * (size_t)g.wz * d2 * sizeof(C), s>>>(
-      psi, ldpsi, A, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2, div_magic(d2), g.plan[2], tw2);
+      psi, ldpsi, A, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2, div_magic(d2), g.plan[2], tw2); count_launch();
   k_y<R, +1><<<dim3(g.Xp, (d2 + g.wy - 1) / g.wy, nb), block_for(g.wy), 2 * (size_t)g.wy * d1 * sizeof(C), s>>>(
-      A, B, g.Xp, g.Yp, g.m[1], d1, d2, g.plan[1], tw1);
+      A, B, g.Xp, g.Yp, g.m[1], d1, d2, g.plan[1], tw1); count_launch();
   k_xv<R><<<dim3(d1, (d2 + g.wx - 1) / g.wx, nb), block_for(g.wx), 2 * (size_t)g.wx * d0 * sizeof(C), s>>>(
-      B, vr, g.Xp, g.m[0], d0, d1, d2, g.plan[0], tw0);
+      B, vr, g.Xp, g.m[0], d0, d1, d2, g.plan[0], tw0); count_launch();
   k_y<R, -1><<<dim3(g.Xp, (d2 + g.wy - 1) / g.wy, nb), block_for(g.wy), 2 * (size_t)g.wy * d1 * sizeof(C), s>>>(
-      A, B, g.Xp, g.Yp, g.m[1], d1, d2, g.plan[1], tw1);
+      A, B, g.Xp, g.Yp, g.m[1], d1, d2, g.plan[1], tw1); count_launch();
   k_zfwd<R><<<dim3((g.ncol + g.wz - 1) / g.wz, nb), block_for(g.wz), 2 * (size_t)g.wz * d2 * sizeof(C), s>>>(
       A, psi, ldpsi, hpsi, ldh, h.kp[ik].kinetic, 1.0 / (double)g.N, g.col_start, g.pt_ig, g.pt_col, g.pt_z,
-      g.ncol, d2, div_magic(d2), g.plan[2], tw2);
+      g.ncol, d2, div_magic(d2), g.plan[2], tw2); count_launch();
 }
 
 Status local_apply_on_scratch(Handle& h, int spin, int ik, const double2* psi, long ldpsi, int nb, double2* hpsi,
@@ -637,17 +638,17 @@ Status density_accumulate(Handle& h, const double2* psi, long ldpsi, int nb, con
       dim3 grid((g.ncol + g.wz - 1) / g.wz, cnt);
       k_zinv<double><<<grid, block_for(g.wz), 2 * (size_t)g.wz * d2 * sizeof(double2), s>>>(
           psi + (long)c0 * ldpsi, ldpsi, A, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2, div_magic(d2),
-          g.plan[2], g.tw64[2]);
+          g.plan[2], g.tw64[2]); count_launch();
     }
     {
       dim3 grid(g.Xp, (d2 + g.wy - 1) / g.wy, cnt);
       k_y<double, +1><<<grid, block_for(g.wy), 2 * (size_t)g.wy * d1 * sizeof(double2), s>>>(
-          A, B, g.Xp, g.Yp, g.m[1], d1, d2, g.plan[1], g.tw64[1]);
+          A, B, g.Xp, g.Yp, g.m[1], d1, d2, g.plan[1], g.tw64[1]); count_launch();
     }
     {
       dim3 grid(d1, (d2 + g.wx - 1) / g.wx, 1);
       k_x_density<<<grid, block_for(g.wx), 2 * (size_t)g.wx * d0 * sizeof(double2), s>>>(
-          B, fw_dev + c0, cnt, rho, g.Xp, g.m[0], d0, d1, d2, g.plan[0], g.tw64[0]);
+          B, fw_dev + c0, cnt, rho, g.Xp, g.m[0], d0, d1, d2, g.plan[0], g.tw64[0]); count_launch();
     }
   }
   PW_CUDA_TRY(cudaGetLastError());
@@ -684,7 +685,7 @@ Status apply_h_device(Handle& h, int spin, int ik, const double2* psi, long ldps
     mark(tm, 5, s);
     const long tot = (long)h.n_ch * nb;
     k_apply_d<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(h.nl_p, h.nl_q, h.n_ch, nb, h.ch_atom, h.atom_ch_start,
-                                                            h.d_off, h.d_vals);
+                                                            h.d_off, h.d_vals); count_launch();
     mark(tm, 6, s);
     cs = cublasZgemm(h.blas, CUBLAS_OP_N, CUBLAS_OP_N, h.n_pw, nb, h.n_ch, &one, Bm, h.n_pw,
                      reinterpret_cast<const cuDoubleComplex*>(h.nl_q), h.n_ch, &one,

@@ -232,7 +232,7 @@ Status small_geneig_batched(const double2* H, const double2* S, long ld, long st
     configured = true;
   }
   k_small_geneig<<<batch, 256, small_geneig_smem(m), s>>>(H, S, ld, stride, m, nev, evals, C, ldc, cstride,
-                                                          status_dev);
+                                                          status_dev); count_launch();
   PW_CUDA_TRY(cudaGetLastError());
   return kOk;
 }

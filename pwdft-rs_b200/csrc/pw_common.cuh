@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <atomic>
 #include <string>
 
 namespace pwgpu {
@@ -73,6 +74,14 @@ struct Error {
   int code = kOk;
   std::string msg;
 };
+
+// Process-wide count of this library's kernel launches (read through
+// pwgpu_kernel_launches); every launch site is followed by count_launch().
+inline std::atomic<long long>& launch_counter() {
+  static std::atomic<long long> c{0};
+  return c;
+}
+inline void count_launch() { launch_counter().fetch_add(1, std::memory_order_relaxed); }
 
 }  // namespace pwgpu
 

@@ -34,6 +34,7 @@ constexpr double kE2 = 14.399645351950548;
 constexpr double kG2Zero = 1e-12;
 constexpr double kRhoFloor = 1e-30;
 constexpr int kRedBlocks = 512;  // partial sums per reduction (fixed order)
+constexpr double kFp32ResidualFloor = 3e-5;  // eV, eigen-residual floor of the FP32 H|psi> phase
 
 // ---------------------------------------------------------------------------
 // deterministic reductions: partials[blockIdx] then one block sums them
@@ -395,8 +396,8 @@ static Status reduce_host(Handle& h, const double* a, const double* b, long n, i
   ScfState* st = h.scf;
   const cudaStream_t s = h.stream;
   const unsigned nbk = (unsigned)std::min<long>(kRedBlocks, blocks_for(n));
-  k_reduce<<<nbk, 256, 0, s>>>(a, b, n, mode, st->partials);
-  k_final_sum<<<1, 256, 0, s>>>(st->partials, (int)nbk, st->scal);
+  k_reduce<<<nbk, 256, 0, s>>>(a, b, n, mode, st->partials); count_launch();
+  k_final_sum<<<1, 256, 0, s>>>(st->partials, (int)nbk, st->scal); count_launch();
   PW_CUDA_TRY(cudaMemcpyAsync(&out, st->scal, sizeof(double), cudaMemcpyDeviceToHost, s));
   PW_CUDA_TRY(cudaStreamSynchronize(s));
   return kOk;
@@ -404,7 +405,7 @@ static Status reduce_host(Handle& h, const double* a, const double* b, long n, i
 
 static Status final_sum_host(Handle& h, int nparts, double& out, int slot = 0) {
   ScfState* st = h.scf;
-  k_final_sum<<<1, 256, 0, h.stream>>>(st->partials + (long)slot * kRedBlocks, nparts, st->scal + slot);
+  k_final_sum<<<1, 256, 0, h.stream>>>(st->partials + (long)slot * kRedBlocks, nparts, st->scal + slot); count_launch();
   PW_CUDA_TRY(cudaMemcpyAsync(&out, st->scal + slot, sizeof(double), cudaMemcpyDeviceToHost, h.stream));
   PW_CUDA_TRY(cudaStreamSynchronize(h.stream));
   return kOk;
@@ -413,10 +414,10 @@ static Status final_sum_host(Handle& h, int nparts, double& out, int slot = 0) {
 // rho(G) = FFT(rho)/N into st->cg
 static Status density_to_g(Handle& h, const double* rho) {
   const long N = h.g.N;
-  k_real_to_cplx<<<blocks_for(N), 256, 0, h.stream>>>(rho, h.scf->cg, N);
+  k_real_to_cplx<<<blocks_for(N), 256, 0, h.stream>>>(rho, h.scf->cg, N); count_launch();
   Status s = fft3d_full(h, h.scf->cg, -1, h.stream);
   if (s != kOk) return s;
-  k_scale_cplx<<<blocks_for(N), 256, 0, h.stream>>>(h.scf->cg, 1.0 / (double)N, N);
+  k_scale_cplx<<<blocks_for(N), 256, 0, h.stream>>>(h.scf->cg, 1.0 / (double)N, N); count_launch();
   return kOk;
 }
 
@@ -434,11 +435,11 @@ static Status potentials(Handle& h, const double* rho, bool set_hpsi, PotEnergie
   if (r != kOk) return r;
   const double fpe2 = 4.0 * kPi * kE2;
   const unsigned nbk = (unsigned)std::min<long>(kRedBlocks, blocks_for(N));
-  k_hartree<<<nbk, 256, 0, s>>>(st->cg, h.g_squared, N, st->vh, fpe2, st->partials);
+  k_hartree<<<nbk, 256, 0, s>>>(st->cg, h.g_squared, N, st->vh, fpe2, st->partials); count_launch();
   double sh = 0.0;
   if ((r = final_sum_host(h, (int)nbk, sh)) != kOk) return r;
   e.e_hartree = sh * 0.5 * h.omega;
-  k_lda<<<nbk, 256, 0, s>>>(rho, h.rho_core_r, N, st->exc, st->vxc, st->partials, st->partials + kRedBlocks);
+  k_lda<<<nbk, 256, 0, s>>>(rho, h.rho_core_r, N, st->exc, st->vxc, st->partials, st->partials + kRedBlocks); count_launch();
   double sx = 0.0, sv = 0.0;
   if ((r = final_sum_host(h, (int)nbk, sx, 0)) != kOk) return r;
   if ((r = final_sum_host(h, (int)nbk, sv, 1)) != kOk) return r;
@@ -446,14 +447,14 @@ static Status potentials(Handle& h, const double* rho, bool set_hpsi, PotEnergie
   e.e_xc = sx * dv;
   e.e_vxc = sv * dv;
   // V_xc(G) = FFT(vxc)/N, V_eff(G) = V_loc + V_H + V_xc
-  k_real_to_cplx<<<blocks_for(N), 256, 0, s>>>(st->vxc, st->cg2, N);
+  k_real_to_cplx<<<blocks_for(N), 256, 0, s>>>(st->vxc, st->cg2, N); count_launch();
   if ((r = fft3d_full(h, st->cg2, -1, s)) != kOk) return r;
-  k_scale_cplx<<<blocks_for(N), 256, 0, s>>>(st->cg2, 1.0 / (double)N, N);
-  k_veff_g<<<blocks_for(N), 256, 0, s>>>(h.v_local_g, st->vh, st->cg2, st->cg2, N);
+  k_scale_cplx<<<blocks_for(N), 256, 0, s>>>(st->cg2, 1.0 / (double)N, N); count_launch();
+  k_veff_g<<<blocks_for(N), 256, 0, s>>>(h.v_local_g, st->vh, st->cg2, st->cg2, N); count_launch();
   if (set_hpsi) {
     PW_CUDA_TRY(cudaMemcpyAsync(h.tmp_grid, st->cg2, N * sizeof(double2), cudaMemcpyDeviceToDevice, s));
     if ((r = fft3d_full(h, h.tmp_grid, +1, s)) != kOk) return r;
-    k_real_part_both<<<blocks_for(N), 256, 0, s>>>(h.tmp_grid, h.veff_r[0], h.veff_r32[0], N);
+    k_real_part_both<<<blocks_for(N), 256, 0, s>>>(h.tmp_grid, h.veff_r[0], h.veff_r32[0], N); count_launch();
   }
   PW_CUDA_TRY(cudaGetLastError());
   return kOk;
@@ -464,12 +465,12 @@ static Status symmetrize(Handle& h, double* rho) {
   ScfState* st = h.scf;
   const long N = h.g.N;
   const cudaStream_t s = h.stream;
-  k_real_to_cplx<<<blocks_for(N), 256, 0, s>>>(rho, st->cg, N);
+  k_real_to_cplx<<<blocks_for(N), 256, 0, s>>>(rho, st->cg, N); count_launch();
   Status r = fft3d_full(h, st->cg, -1, s);
   if (r != kOk) return r;
-  k_sym_gather<<<blocks_for(N), 256, 0, s>>>(st->cg, h.sym_src, h.sym_arg, h.n_sym, N, st->cg2);
+  k_sym_gather<<<blocks_for(N), 256, 0, s>>>(st->cg, h.sym_src, h.sym_arg, h.n_sym, N, st->cg2); count_launch();
   if ((r = fft3d_full(h, st->cg2, +1, s)) != kOk) return r;
-  k_cplx_real_scaled<<<blocks_for(N), 256, 0, s>>>(st->cg2, rho, 1.0 / (double)N, N);
+  k_cplx_real_scaled<<<blocks_for(N), 256, 0, s>>>(st->cg2, rho, 1.0 / (double)N, N); count_launch();
   PW_CUDA_TRY(cudaGetLastError());
   return kOk;
 }
@@ -565,8 +566,8 @@ static Status davidson(Handle& h, int spin, int ik, double tol, int max_iter, in
   for (;;) {
     PW_CUDA_TRY(cudaMemcpyAsync(st->lam, k.evals.data(), nd * sizeof(double), cudaMemcpyHostToDevice, s));
     k_resid_precond<<<dim3(gx, nd), 256, 0, s>>>(k.V, k.HV, T, n, (int)n, st->lam, h.kp[ik].kinetic, v0,
-                                                 st->partials);
-    k_col_final<<<1, 256, 0, s>>>(st->partials, (int)gx, nd, st->col_sums);
+                                                 st->partials); count_launch();
+    k_col_final<<<1, 256, 0, s>>>(st->partials, (int)gx, nd, st->col_sums); count_launch();
     PW_CUDA_TRY(cudaMemcpyAsync(rn.data(), st->col_sums, nd * sizeof(double), cudaMemcpyDeviceToHost, s));
     PW_CUDA_TRY(cudaStreamSynchronize(s));
     max_res = 0.0;
@@ -576,9 +577,9 @@ static Status davidson(Handle& h, int spin, int ik, double tol, int max_iter, in
     if ((r = zgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, nd, nd, (int)n, k.V, n, T, n, st->Pm, nd)) != kOk) return r;
     if ((r = zgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, nd, nd, k.V, n, st->Pm, nd, T, n, 1.0, -1.0)) != kOk)
       return r;
-    k_col_sumsq<<<dim3(gx, nd), 256, 0, s>>>(T, n, (int)n, st->partials);
-    k_col_final<<<1, 256, 0, s>>>(st->partials, (int)gx, nd, st->col_sums);
-    k_scale_cols_invsqrt<<<dim3(gx, nd), 256, 0, s>>>(T, n, (int)n, st->col_sums);
+    k_col_sumsq<<<dim3(gx, nd), 256, 0, s>>>(T, n, (int)n, st->partials); count_launch();
+    k_col_final<<<1, 256, 0, s>>>(st->partials, (int)gx, nd, st->col_sums); count_launch();
+    k_scale_cols_invsqrt<<<dim3(gx, nd), 256, 0, s>>>(T, n, (int)n, st->col_sums); count_launch();
     if ((r = apply_h_device(h, spin, ik, T, n, nd, HT, n, precision, s)) != kOk) return r;
     happ += nd;
     if ((r = rayleigh_ritz(h, k, 2 * nd, nd)) != kOk) return r;
@@ -701,14 +702,14 @@ static Status mix(Handle& h, const ScfParams& p) {
   }
   const int slot = st->mix_count;
   double* res = st->hres[slot];
-  k_sub<<<blocks_for(N), 256, 0, s>>>(st->rho_out, st->rho_in, res, N);
+  k_sub<<<blocks_for(N), 256, 0, s>>>(st->rho_out, st->rho_in, res, N); count_launch();
   if (st->kerker_w) {
-    k_real_to_cplx<<<blocks_for(N), 256, 0, s>>>(res, st->cg, N);
+    k_real_to_cplx<<<blocks_for(N), 256, 0, s>>>(res, st->cg, N); count_launch();
     Status r = fft3d_full(h, st->cg, -1, s);
     if (r != kOk) return r;
-    k_mul_real_weights<<<blocks_for(N), 256, 0, s>>>(st->cg, st->kerker_w, N);
+    k_mul_real_weights<<<blocks_for(N), 256, 0, s>>>(st->cg, st->kerker_w, N); count_launch();
     if ((r = fft3d_full(h, st->cg, +1, s)) != kOk) return r;
-    k_cplx_real_scaled<<<blocks_for(N), 256, 0, s>>>(st->cg, res, 1.0 / (double)N, N);
+    k_cplx_real_scaled<<<blocks_for(N), 256, 0, s>>>(st->cg, res, 1.0 / (double)N, N); count_launch();
   }
   PW_CUDA_TRY(cudaMemcpyAsync(st->hin[slot], st->rho_in, N * sizeof(double), cudaMemcpyDeviceToDevice, s));
   st->mix_count++;
@@ -722,13 +723,13 @@ static Status mix(Handle& h, const ScfParams& p) {
     std::vector<double> a((size_t)mm * mm), b(mm);
     const unsigned nbk = (unsigned)std::min<long>(kRedBlocks, blocks_for(N));
     for (int i = 0; i < mm; ++i) {
-      k_dr_dot<<<nbk, 256, 0, s>>>(st->hres[i], nullptr, rl, N, st->partials);
+      k_dr_dot<<<nbk, 256, 0, s>>>(st->hres[i], nullptr, rl, N, st->partials); count_launch();
       double v = 0.0;
       Status r = final_sum_host(h, (int)nbk, v);
       if (r != kOk) return r;
       b[i] = -v;
       for (int j = 0; j <= i; ++j) {
-        k_dr_dot<<<nbk, 256, 0, s>>>(st->hres[i], st->hres[j], rl, N, st->partials);
+        k_dr_dot<<<nbk, 256, 0, s>>>(st->hres[i], st->hres[j], rl, N, st->partials); count_launch();
         if ((r = final_sum_host(h, (int)nbk, v)) != kOk) return r;
         a[(size_t)i * mm + j] = v;
         a[(size_t)j * mm + i] = v;
@@ -744,7 +745,7 @@ static Status mix(Handle& h, const ScfParams& p) {
   PW_CUDA_TRY(cudaMemcpyAsync(st->dev_ptrs, ptrs.data(), 2 * m * sizeof(double*), cudaMemcpyHostToDevice, s));
   PW_CUDA_TRY(cudaMemcpyAsync(st->dev_coef, coef.data(), m * sizeof(double), cudaMemcpyHostToDevice, s));
   k_mix_combine<<<blocks_for(N), 256, 0, s>>>(st->dev_ptrs, st->dev_ptrs + m, st->dev_coef, m, p.mixing_beta, N,
-                                             st->rho_in);
+                                             st->rho_in); count_launch();
   PW_CUDA_TRY(cudaStreamSynchronize(s));
   return kOk;
 }
@@ -775,7 +776,10 @@ static Status build_density(Handle& h, const std::vector<std::vector<double>>& o
   Status r = reduce_host(h, rho, nullptr, N, 0, tot);
   if (r != kOk) return r;
   const double integ = tot * (h.omega / (double)N);
-  if (std::fabs(integ) > 1e-15) k_scale_real<<<blocks_for(N), 256, 0, s>>>(rho, h.n_electrons / integ, N);
+  if (std::fabs(integ) > 1e-15) {
+    k_scale_real<<<blocks_for(N), 256, 0, s>>>(rho, h.n_electrons / integ, N);
+    count_launch();
+  }
   return symmetrize(h, rho);
 }
 
@@ -824,7 +828,10 @@ Status scf_run(Handle& h, const ScfParams& p, const double* rho_init, ScfResult&
     PotEnergies ein;
     if ((r = potentials(h, st->rho_in, true, ein)) != kOk) return r;
     const int prec = (p.precision == 1 && !(last_delta < p.fp64_switch)) ? 1 : 0;
-    const double tol = std::max(p.diag_tol, std::min(1e-3, 0.1 * (std::isfinite(last_delta) ? last_delta : 1.0)));
+    double tol = std::max(p.diag_tol, std::min(1e-3, 0.1 * (std::isfinite(last_delta) ? last_delta : 1.0)));
+    // FP32 H|psi> carries ~1e-7 relative noise: residuals below this floor
+    // (eV) are not reachable in that phase and would only burn iterations
+    if (prec == 1) tol = std::max(tol, kFp32ResidualFloor);
     max_res_all = 0.0;
     for (int ik = 0; ik < h.n_k; ++ik) {
       int its = 0;

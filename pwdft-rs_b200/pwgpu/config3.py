@@ -1,0 +1,28 @@
+"""The mixed-precision SCF case: the 64-atom Si cubic supercell (2x2x2
+conventional cells of a = 10.26 bohr, seeded ±0.05 bohr displacements),
+PZ-LDA with the Si UPF, ecutwfc 30 Ry (n_pw 23,847, 72^3 grid), Γ only,
+160 bands (256 electrons), Gaussian smearing 0.01 Ry, Anderson ("Pulay")
+mixing beta 0.4 with Kerker preconditioning (auto q_TF).  The mixed form runs
+the FFT/V_eff product in FP32 and switches H|psi> to FP64 once the density
+rms falls below 1e-6 e/Å³; energies and eigenvalues are compared with the
+FP64 run of the same solve.
+
+The displaced cell keeps only the identity operation, so the density is not
+symmetrised (SymmetryInfo::identity_only, as the reference does for n_ops <= 1).
+"""
+
+from .consts import RY_TO_EV
+from .context import build_system
+from .crystal import gamma_only
+from .symmetry import SymmetryInfo
+from .workloads import si64_crystal
+
+SCF_KW = dict(n_bands=160, max_iter=80, conv_threshold=1e-6, energy_threshold=1e-6, mixing_beta=0.4,
+              mixing_ndim=8, kerker=True, smearing="gaussian", sigma=0.01 * RY_TO_EV)
+
+FP64_SWITCH = 1e-6
+
+
+def config3_system(pp, ecut_ry: float = 30.0, seed=None):
+    cr = si64_crystal() if seed is None else si64_crystal(seed)
+    return build_system(cr, {"Si": pp}, ecut_ry * RY_TO_EV, gamma_only(), SymmetryInfo.identity_only())

@@ -126,6 +126,10 @@ def load_library(path: str = LIB_PATH):
     lib.pwgpu_symmetrize.argtypes = [vp, _f64p]
     lib.pwgpu_potentials.argtypes = [vp, _f64p, _f64p, _f64p]
     lib.pwgpu_small_geneig.argtypes = [ct.c_int32, ct.c_int32, ct.c_int32, _f64p, _f64p, _f64p, _f64p]
+    lib.pwgpu_get_stream.argtypes = [vp, ct.POINTER(vp)]
+    lib.pwgpu_get_stream.restype = ct.c_int32
+    lib.pwgpu_kernel_launches.argtypes = [ct.POINTER(ct.c_int64)]
+    lib.pwgpu_kernel_launches.restype = ct.c_int32
     for name in ("pwgpu_create", "pwgpu_destroy", "pwgpu_set_veff_g", "pwgpu_apply_h", "pwgpu_apply_h_device",
                  "pwgpu_set_precision", "pwgpu_get_dims", "pwgpu_profile_apply_h", "pwgpu_scf_run",
                  "pwgpu_eigensolve", "pwgpu_density", "pwgpu_symmetrize", "pwgpu_potentials",
@@ -231,6 +235,12 @@ class PwGpu:
         except Exception:
             pass
 
+    def stream(self) -> int:
+        """cudaStream_t of the handle (as an integer)."""
+        s = ct.c_void_p()
+        _check(self.lib, self.lib.pwgpu_get_stream(self.h, ct.byref(s)))
+        return s.value or 0
+
     def set_precision(self, precision: int):
         _check(self.lib, self.lib.pwgpu_set_precision(self.h, precision))
 
@@ -322,6 +332,14 @@ class PwGpu:
         _check(self.lib, self.lib.pwgpu_potentials(self.h, _f64(r), vg.view(np.float64).ctypes.data_as(_f64p),
                                                    _f64(en)))
         return vg, {"e_hartree": en[0], "e_xc": en[1], "e_vxc": en[2]}
+
+
+def kernel_launches() -> int:
+    """This library's kernel launches since load (pwgpu_kernel_launches)."""
+    lib = load_library()
+    n = ct.c_int64()
+    _check(lib, lib.pwgpu_kernel_launches(ct.byref(n)))
+    return n.value
 
 
 def small_geneig(H: np.ndarray, S: np.ndarray, nev: int):
