@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -48,6 +49,7 @@ static void release(Handle& h) {
   for (int s = 0; s < 2; ++s) { f(h.veff_r[s]); f(h.veff_r32[s]); }
   f(h.work_a); f(h.work_b); f(h.nl_p); f(h.nl_q); f(h.tmp_grid);
   release_scf(h);
+  release_nl_mixed(h);
   f(h.solver_work); f(h.solver_info);
   if (h.solver) cusolverDnDestroy(h.solver);
   if (h.blas) cublasDestroy(h.blas);
@@ -69,6 +71,7 @@ static Status create(const pwgpu_system* s, const pwgpu_options* o, pwgpu_handle
   if (s->n_sym < 0 || (s->n_sym > 1 && (!s->sym_src || !s->sym_arg)))
     return fail(kInvalid, "pwgpu_create: symmetry map missing");
   h.device = o ? o->device : 0;
+  h.trace = std::getenv("PWGPU_TRACE") != nullptr;
   ph->precision = o ? o->precision : 0;
   PW_CUDA_TRY(cudaSetDevice(h.device));
   h.n_pw = s->n_pw;
@@ -304,7 +307,8 @@ pwgpu_status pwgpu_eigensolve(pwgpu_handle* ph, int32_t spin, int32_t ik, int32_
                               int32_t* iters, double* max_residual) {
   if (!ph || !evals) return fail(kInvalid, "pwgpu_eigensolve: NULL argument");
   PW_CUDA_TRY(cudaSetDevice(ph->h.device));
-  return eigensolve_k(ph->h, spin, ik, n_bands, tol, max_iter, psi_in, evals, psi_out, iters, max_residual);
+  return eigensolve_k(ph->h, spin, ik, n_bands, tol, max_iter, psi_in, evals, psi_out, iters, max_residual,
+                      ph->precision);
 }
 
 pwgpu_status pwgpu_density(pwgpu_handle* ph, int32_t n_bands, const double* occ, const double* psi, double* rho_r) {

@@ -78,6 +78,8 @@ struct Handle {
   size_t solver_work_len = 0;
   int* solver_info = nullptr;
   struct ScfState* scf = nullptr;  // device state of the SCF loop (scf.cu)
+  struct NlMixed* nlm = nullptr;   // split projector operands of the mixed form (nl_mixed.cu)
+  bool trace = false;  // per-iteration eigensolver lines on stderr (PWGPU_TRACE set at create)
   std::string last_error;
 };
 
@@ -89,6 +91,19 @@ struct StageTimer {
   std::vector<cudaEvent_t> events;
   std::vector<int> stage;
 };
+
+// Records a CUDA event for stage `stage` when t is non-null (hpsi.cu).
+void mark(StageTimer* t, int stage, cudaStream_t s);
+
+// Q = D P over the handle's nl_p / nl_q buffers (block-diagonal D).
+Status apply_d_blocks(Handle& h, int nb, cudaStream_t s);
+
+// 3xBF16 tensor-core form of the Kleinman-Bylander term, hpsi += B D B^H psi
+// (nl_mixed.cu); used by the mixed form when nl_mixed_eligible(h).
+bool nl_mixed_eligible(const Handle& h);
+Status nonlocal_mixed(Handle& h, int ik, const double2* psi, long ldpsi, int nb, double2* hpsi, long ldh,
+                      cudaStream_t s, StageTimer* tm = nullptr);
+void release_nl_mixed(Handle& h);
 
 // Grid-map construction and the H|psi> launcher (hpsi.cu).
 Status build_grid_maps(Handle& h, const int* miller_host);

@@ -511,13 +511,22 @@ Status set_veff_from_g(Handle& h, int spin, const double2* veff_g_dev, cudaStrea
 }
 
 // Records an event after each launch when profiling (stage timings).
-static inline void mark(StageTimer* t, int stage, cudaStream_t s) {
+void mark(StageTimer* t, int stage, cudaStream_t s) {
   if (!t) return;
   cudaEvent_t e;
   cudaEventCreate(&e);
   cudaEventRecord(e, s);
   t->events.push_back(e);
   t->stage.push_back(stage);
+}
+
+Status apply_d_blocks(Handle& h, int nb, cudaStream_t s) {
+  const long tot = (long)h.n_ch * nb;
+  k_apply_d<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(h.nl_p, h.nl_q, h.n_ch, nb, h.ch_atom, h.atom_ch_start,
+                                                          h.d_off, h.d_vals);
+  count_launch();
+  PW_CUDA_TRY(cudaGetLastError());
+  return kOk;
 }
 
 template <typename R>
@@ -673,7 +682,9 @@ Status apply_h_device(Handle& h, int spin, int ik, const double2* psi, long ldps
       st = local_chunk<float>(h, spin, ik, psi + (long)c0 * ldpsi, ldpsi, cnt, hpsi + (long)c0 * ldh, ldh, s, tm);
     if (st != kOk) return st;
   }
-  if (h.n_ch > 0) {
+  if (h.n_ch > 0 && precision == 1 && nl_mixed_eligible(h)) {
+    if ((st = nonlocal_mixed(h, ik, psi, ldpsi, nb, hpsi, ldh, s, tm)) != kOk) return st;
+  } else if (h.n_ch > 0) {
     if ((st = ensure_nl_capacity(h, nb)) != kOk) return st;
     cublasSetStream(h.blas, s);
     const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);

@@ -1,0 +1,608 @@
+// Block eigensolver of one (spin, k) Hamiltonian: locally optimal block
+// preconditioned conjugate gradients (LOBPCG) with soft locking, on an
+// explicitly orthonormal basis [X | W | P].
+//
+// Stands in for the dense diagonalisation of the reference's per-k step
+// (pwdft-core/src/eigensolver/dense.rs:50-98, the lowest n_bands pairs of the
+// full n_pw x n_pw Hamiltonian): H is only applied (apply_h_device) and the
+// lowest nd Ritz pairs are refined until the residual norms of the first
+// nconv fall below tol.
+//
+// Numerical design:
+//  * the basis is orthonormal by construction (block Gram-Schmidt against X,
+//    Cholesky-QR inside W and P), so each Rayleigh-Ritz step is a standard
+//    Hermitian problem; an ill-conditioned overlap never enters a solve;
+//  * H is applied to W after it is orthonormalised, so H W is consistent with
+//    W whatever the precision of the product;
+//  * H P follows P through the same linear combinations; P columns whose
+//    component outside span(X, W) is small (which would amplify the error of
+//    the stored H P) are dropped, and the whole P block is dropped when its
+//    Cholesky factor shows near dependence;
+//  * HX is recomputed in FP64 on entry and the X-(W,P) coupling of the
+//    subspace matrix is formed from HX, so reduced-precision products of the
+//    search directions only enter through the (small) correction
+//    coefficients; the residuals the convergence test reads carry no
+//    reduced-precision floor.
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <random>
+#include <vector>
+
+#include "linalg.hpp"
+#include "lobpcg.hpp"
+
+namespace pwgpu {
+
+namespace {
+
+constexpr double kRyToEv = 13.605693122994;
+constexpr int kColBlocks = 64;      // partial sums per column reduction
+constexpr int kSmallSolveMax = 64;  // subspace size up to which the one-CTA solver runs
+// P columns whose component outside span(X, W) is below this fraction of
+// their norm are dropped (FP64 / reduced-precision search directions)
+constexpr double kPDropFp64 = 1e-5;
+constexpr double kPDropMixed = 3e-2;
+
+inline unsigned blocks_for(long n, int t = 256) { return (unsigned)std::max<long>(1, (n + t - 1) / t); }
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  v = 0.0;
+  if (wid == 0) {
+    v = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  }
+  __syncthreads();
+  return v;
+}
+
+// Residual R = HX - lambda X, preconditioned into T with the smooth
+// denominator 0.5 (1 + x + sqrt(1 + (x-1)^2)) in Ry, x = (|k+G|^2 + v0 -
+// lambda)/Ry; per-column partial sums of |R|^2.
+__global__ void k_resid_precond(const double2* __restrict__ X, const double2* __restrict__ HX, double2* __restrict__ T,
+                                long ld, int n, const double* __restrict__ lam, const double* __restrict__ kin,
+                                double v0, double* __restrict__ partials) {
+  __shared__ double sh[32];
+  const int col = blockIdx.y;
+  const double l = lam[col];
+  const double2* x = X + (long)col * ld;
+  const double2* hx = HX + (long)col * ld;
+  double2* t = T + (long)col * ld;
+  double acc = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double2 r = make_double2(hx[i].x - l * x[i].x, hx[i].y - l * x[i].y);
+    acc += r.x * r.x + r.y * r.y;
+    const double xx = (kin[i] + v0 - l) / kRyToEv;
+    const double den = 0.5 * (1.0 + xx + sqrt(1.0 + (xx - 1.0) * (xx - 1.0))) * kRyToEv;
+    t[i] = make_double2(r.x / den, r.y / den);
+  }
+  acc = block_sum(acc, sh);
+  if (threadIdx.x == 0) partials[(long)col * gridDim.x + blockIdx.x] = acc;
+}
+
+__global__ void k_col_sumsq(const double2* __restrict__ X, long ld, int n, double* __restrict__ partials) {
+  __shared__ double sh[32];
+  const int col = blockIdx.y;
+  const double2* x = X + (long)col * ld;
+  double acc = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    acc += x[i].x * x[i].x + x[i].y * x[i].y;
+  acc = block_sum(acc, sh);
+  if (threadIdx.x == 0) partials[(long)col * gridDim.x + blockIdx.x] = acc;
+}
+
+// sums[col] = sum of the nblk partials of each column (fixed order)
+__global__ void k_col_final(const double* __restrict__ partials, int nblk, int ncols, double* __restrict__ sums) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= ncols) return;
+  double acc = 0.0;
+  for (int b = 0; b < nblk; ++b) acc += partials[(long)col * nblk + b];
+  sums[col] = acc;
+}
+
+// X[:, c] /= sqrt(sumsq[c]) (and Y[:, c] with the same factor when Y != null)
+__global__ void k_scale_cols_invsqrt(double2* __restrict__ X, double2* __restrict__ Y, long ld, int n,
+                                     const double* __restrict__ sumsq) {
+  const int col = blockIdx.y;
+  const double s = sumsq[col] > 0.0 ? 1.0 / sqrt(sumsq[col]) : 0.0;
+  double2* x = X + (long)col * ld;
+  double2* y = Y ? Y + (long)col * ld : nullptr;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    x[i] = x[i] * s;
+    if (y) y[i] = y[i] * s;
+  }
+}
+
+// dst[:, c] = src[:, idx[c]] over `rows` rows (src and dst do not overlap)
+__global__ void k_gather_cols(const double2* __restrict__ src, long lds, const int* __restrict__ idx,
+                              double2* __restrict__ dst, long ldd, int rows) {
+  const int c = blockIdx.y;
+  const double2* s = src + (long)idx[c] * lds;
+  double2* d = dst + (long)c * ldd;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) d[i] = s[i];
+}
+
+// Subspace matrix Hs (m x m, ld m) over the basis [X | B], X holding nd Ritz
+// vectors with values lam:  [[diag(lam), Z^H], [Z, (G + G^H)/2]],
+// Z = B^H HX (q x nd, ld q), G = B^H HB (q x q, ld q), q = m - nd.
+__global__ void k_assemble_rr(double2* __restrict__ Hs, int m, int nd, const double* __restrict__ lam,
+                              const double2* __restrict__ Z, const double2* __restrict__ G) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)m * m) return;
+  const int r = (int)(t % m), c = (int)(t / m), q = m - nd;
+  double2 v;
+  if (r < nd && c < nd) {
+    v = make_double2(r == c ? lam[r] : 0.0, 0.0);
+  } else if (c < nd) {
+    v = Z[(r - nd) + (long)c * q];
+  } else if (r < nd) {
+    const double2 z = Z[(c - nd) + (long)r * q];
+    v = make_double2(z.x, -z.y);
+  } else {
+    const double2 a = G[(r - nd) + (long)(c - nd) * q], b = G[(c - nd) + (long)(r - nd) * q];
+    v = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+  }
+  Hs[t] = v;
+}
+
+__global__ void k_set_identity(double2* __restrict__ A, int m) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)m * m) return;
+  A[t] = make_double2((t % m) == (t / m) ? 1.0 : 0.0, 0.0);
+}
+
+// out[i] = Re A[i, i]
+__global__ void k_diag_real(const double2* __restrict__ A, int ld, int m, double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) out[i] = A[i + (long)i * ld].x;
+}
+
+template <typename T> Status walloc(T** p, size_t n) {
+  cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T));
+  if (e != cudaSuccess) return fail(kOom, std::string("cudaMalloc (eigensolver): ") + cudaGetErrorString(e));
+  return kOk;
+}
+
+// ---------------------------------------------------------------------------
+// BLAS / LAPACK steps
+// ---------------------------------------------------------------------------
+
+struct Ctx {
+  Handle& h;
+  EigWork& w;
+  cudaStream_t s;
+  long n;
+  unsigned gx;
+};
+
+Status zgemm(Ctx& c, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k, const double2* A, long lda,
+             const double2* B, long ldb, double2* C, long ldc, double beta_re = 0.0, double alpha_re = 1.0) {
+  if (m == 0 || n == 0) return kOk;
+  const cuDoubleComplex al = make_cuDoubleComplex(alpha_re, 0.0), be = make_cuDoubleComplex(beta_re, 0.0);
+  cublasStatus_t cs = cublasZgemm(c.h.blas, ta, tb, m, n, k, &al, reinterpret_cast<const cuDoubleComplex*>(A),
+                                  (int)lda, reinterpret_cast<const cuDoubleComplex*>(B), (int)ldb, &be,
+                                  reinterpret_cast<cuDoubleComplex*>(C), (int)ldc);
+  if (cs != CUBLAS_STATUS_SUCCESS) return fail(kCuda, "cublasZgemm failed (eigensolver)");
+  return kOk;
+}
+
+Status ensure_solver_work(Ctx& c, size_t lwork) {
+  if (lwork <= c.w.solver_lwork) return kOk;
+  if (c.w.solver_work) cudaFree(c.w.solver_work);
+  c.w.solver_work = nullptr;
+  c.w.solver_lwork = 0;
+  PW_CUDA_TRY(cudaMalloc((void**)&c.w.solver_work, lwork * sizeof(double2)));
+  c.w.solver_lwork = lwork;
+  return kOk;
+}
+
+Status ensure_solver(Ctx& c) {
+  if (!c.h.solver && cusolverDnCreate(&c.h.solver) != CUSOLVER_STATUS_SUCCESS)
+    return fail(kCuda, "cusolverDnCreate failed");
+  cusolverDnSetStream(c.h.solver, c.s);
+  return kOk;
+}
+
+// Column sums of squares of Y (q columns) into w.colsq (device); to the
+// host too when host != null.
+Status col_norms2(Ctx& c, const double2* Y, int q, double* host) {
+  if (q == 0) return kOk;
+  k_col_sumsq<<<dim3(c.gx, q), 256, 0, c.s>>>(Y, c.n, (int)c.n, c.w.partials); count_launch();
+  k_col_final<<<blocks_for(q), 256, 0, c.s>>>(c.w.partials, (int)c.gx, q, c.w.colsq); count_launch();
+  if (host) {
+    PW_CUDA_TRY(cudaMemcpyAsync(host, c.w.colsq, q * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    PW_CUDA_TRY(cudaStreamSynchronize(c.s));
+  }
+  return kOk;
+}
+
+// Y -= A (A^H Y), HY -= HA (A^H Y): Y (q columns) projected out of span(A)
+// (p orthonormal columns).
+Status project_out(Ctx& c, const double2* A, const double2* HA, int p, double2* Y, double2* HY, int q) {
+  if (p == 0 || q == 0) return kOk;
+  Status r;
+  if ((r = zgemm(c, CUBLAS_OP_C, CUBLAS_OP_N, p, q, (int)c.n, A, c.n, Y, c.n, c.w.Z, p)) != kOk) return r;
+  if ((r = zgemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.n, q, p, A, c.n, c.w.Z, p, Y, c.n, 1.0, -1.0)) != kOk) return r;
+  if (HY && (r = zgemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.n, q, p, HA, c.n, c.w.Z, p, HY, c.n, 1.0, -1.0)) != kOk)
+    return r;
+  return kOk;
+}
+
+// One Cholesky-QR pass: G = Y^H Y (+ shift I), G = R^H R, Y <- Y R^-1 (and
+// HY with the same R).  ok = false when the factorisation broke down (Y is
+// left unchanged then).  min_rdiag: smallest diagonal entry of R.
+Status chol_qr(Ctx& c, double2* Y, double2* HY, int q, double shift, bool& ok, double* min_rdiag = nullptr) {
+  ok = true;
+  if (q == 0) return kOk;
+  Status r;
+  if ((r = zgemm(c, CUBLAS_OP_C, CUBLAS_OP_N, q, q, (int)c.n, Y, c.n, Y, c.n, c.w.G, q)) != kOk) return r;
+  if (shift > 0.0) {
+    // add shift to the diagonal through the identity buffer: G += shift I
+    k_set_identity<<<blocks_for((long)q * q), 256, 0, c.s>>>(c.w.Id, q); count_launch();
+    const cuDoubleComplex al = make_cuDoubleComplex(1.0, 0.0), be = make_cuDoubleComplex(shift, 0.0);
+    if (cublasZgeam(c.h.blas, CUBLAS_OP_N, CUBLAS_OP_N, q, q, &al, reinterpret_cast<cuDoubleComplex*>(c.w.G), q, &be,
+                    reinterpret_cast<cuDoubleComplex*>(c.w.Id), q, reinterpret_cast<cuDoubleComplex*>(c.w.G),
+                    q) != CUBLAS_STATUS_SUCCESS)
+      return fail(kCuda, "cublasZgeam failed (eigensolver)");
+  }
+  if ((r = ensure_solver(c)) != kOk) return r;
+  int lwork = 0;
+  if (cusolverDnZpotrf_bufferSize(c.h.solver, CUBLAS_FILL_MODE_UPPER, q, reinterpret_cast<cuDoubleComplex*>(c.w.G), q,
+                                  &lwork) != CUSOLVER_STATUS_SUCCESS)
+    return fail(kCuda, "cusolverDnZpotrf_bufferSize failed");
+  if ((r = ensure_solver_work(c, (size_t)lwork)) != kOk) return r;
+  if (cusolverDnZpotrf(c.h.solver, CUBLAS_FILL_MODE_UPPER, q, reinterpret_cast<cuDoubleComplex*>(c.w.G), q,
+                       reinterpret_cast<cuDoubleComplex*>(c.w.solver_work), lwork,
+                       c.w.info) != CUSOLVER_STATUS_SUCCESS)
+    return fail(kCuda, "cusolverDnZpotrf failed");
+  int info = 0;
+  PW_CUDA_TRY(cudaMemcpyAsync(&info, c.w.info, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+  std::vector<double> dg;
+  if (min_rdiag) {
+    dg.resize(q);
+    k_diag_real<<<blocks_for(q), 256, 0, c.s>>>(c.w.G, q, q, c.w.colsq); count_launch();
+    PW_CUDA_TRY(cudaMemcpyAsync(dg.data(), c.w.colsq, q * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+  }
+  PW_CUDA_TRY(cudaStreamSynchronize(c.s));
+  if (info != 0) {
+    ok = false;
+    return kOk;
+  }
+  if (min_rdiag) {
+    double mn = INFINITY;
+    for (double d : dg) mn = std::min(mn, std::fabs(d));
+    *min_rdiag = mn;
+  }
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
+  for (double2* M : {Y, HY}) {
+    if (!M) continue;
+    if (cublasZtrsm(c.h.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, (int)c.n,
+                    q, &one, reinterpret_cast<const cuDoubleComplex*>(c.w.G), q, reinterpret_cast<cuDoubleComplex*>(M),
+                    (int)c.n) != CUBLAS_STATUS_SUCCESS)
+      return fail(kCuda, "cublasZtrsm failed (eigensolver)");
+  }
+  return kOk;
+}
+
+// Orthonormalise Y (q columns, no H attached): column scaling, then two
+// Cholesky-QR passes; a breakdown of the first pass is retried with a small
+// diagonal shift, which still yields an orthonormal block after the second
+// pass.
+Status orthonormalize(Ctx& c, double2* Y, int q) {
+  if (q == 0) return kOk;
+  Status r;
+  if ((r = col_norms2(c, Y, q, nullptr)) != kOk) return r;
+  k_scale_cols_invsqrt<<<dim3(c.gx, q), 256, 0, c.s>>>(Y, nullptr, c.n, (int)c.n, c.w.colsq); count_launch();
+  bool ok = false;
+  if ((r = chol_qr(c, Y, nullptr, q, 0.0, ok)) != kOk) return r;
+  if (!ok) {
+    if ((r = chol_qr(c, Y, nullptr, q, 1e-10 * q, ok)) != kOk) return r;
+    if (!ok) return fail(kNotConverged, "eigensolver: search block is numerically rank deficient");
+  }
+  if ((r = chol_qr(c, Y, nullptr, q, 0.0, ok)) != kOk) return r;
+  if (!ok) return fail(kNotConverged, "eigensolver: second Cholesky-QR pass broke down");
+  return kOk;
+}
+
+// Lowest nev eigenpairs of the Hermitian subspace matrix w.Hs (m x m):
+// values into w.lam, vectors into *C (ld m).
+Status subspace_eig(Ctx& c, int m, int nev, double2** C) {
+  Status r;
+  if (m <= kSmallSolveMax) {
+    k_set_identity<<<blocks_for((long)m * m), 256, 0, c.s>>>(c.w.Id, m); count_launch();
+    if ((r = small_geneig_batched(c.w.Hs, c.w.Id, m, 0, m, nev, 1, c.w.lam, c.w.Cs, m, 0, c.w.status, c.s)) != kOk)
+      return r;
+    int st = 0;
+    PW_CUDA_TRY(cudaMemcpyAsync(&st, c.w.status, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+    PW_CUDA_TRY(cudaStreamSynchronize(c.s));
+    if (st == 1) return fail(kNotConverged, "eigensolver: subspace solve failed");
+    *C = c.w.Cs;
+    return kOk;
+  }
+  if ((r = ensure_solver(c)) != kOk) return r;
+  int lwork = 0;
+  if (cusolverDnZheevd_bufferSize(c.h.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, m,
+                                  reinterpret_cast<cuDoubleComplex*>(c.w.Hs), m, c.w.lam,
+                                  &lwork) != CUSOLVER_STATUS_SUCCESS)
+    return fail(kCuda, "cusolverDnZheevd_bufferSize failed");
+  if ((r = ensure_solver_work(c, (size_t)lwork)) != kOk) return r;
+  if (cusolverDnZheevd(c.h.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, m,
+                       reinterpret_cast<cuDoubleComplex*>(c.w.Hs), m, c.w.lam,
+                       reinterpret_cast<cuDoubleComplex*>(c.w.solver_work), lwork,
+                       c.w.info) != CUSOLVER_STATUS_SUCCESS)
+    return fail(kCuda, "cusolverDnZheevd failed");
+  int info = 0;
+  PW_CUDA_TRY(cudaMemcpyAsync(&info, c.w.info, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+  PW_CUDA_TRY(cudaStreamSynchronize(c.s));
+  if (info != 0) return fail(kNotConverged, "eigensolver: subspace eigensolver did not converge");
+  *C = c.w.Hs;
+  return kOk;
+}
+
+// Rayleigh-Ritz in span(X) alone (X orthonormal): X <- X C, HX <- HX C.
+Status rr_block(Ctx& c, EigVecs& k, int nd) {
+  Status r;
+  if ((r = zgemm(c, CUBLAS_OP_C, CUBLAS_OP_N, nd, nd, (int)c.n, k.V, c.n, k.HV, c.n, c.w.G, nd)) != kOk) return r;
+  k_assemble_rr<<<blocks_for((long)nd * nd), 256, 0, c.s>>>(c.w.Hs, nd, 0, c.w.lam0, c.w.Z, c.w.G); count_launch();
+  double2* C = nullptr;
+  if ((r = subspace_eig(c, nd, nd, &C)) != kOk) return r;
+  if ((r = zgemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.n, nd, nd, k.V, c.n, C, nd, c.w.T, c.n)) != kOk) return r;
+  if ((r = zgemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.n, nd, nd, k.HV, c.n, C, nd, c.w.HXn, c.n)) != kOk) return r;
+  PW_CUDA_TRY(cudaMemcpyAsync(k.V, c.w.T, c.n * nd * sizeof(double2), cudaMemcpyDeviceToDevice, c.s));
+  PW_CUDA_TRY(cudaMemcpyAsync(k.HV, c.w.HXn, c.n * nd * sizeof(double2), cudaMemcpyDeviceToDevice, c.s));
+  PW_CUDA_TRY(cudaMemcpyAsync(k.evals.data(), c.w.lam, nd * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+  PW_CUDA_TRY(cudaStreamSynchronize(c.s));
+  return kOk;
+}
+
+// Per-phase CUDA-event timing of the block steps (only when the handle's trace
+// flag is set): 0 residual, 1 W, 2 H W, 3 P, 4 subspace matrix, 5 subspace
+// solve, 6 update.
+struct PhaseTimer {
+  static constexpr int kPhases = 7;
+  bool on = false;
+  cudaEvent_t ev[kPhases + 1] = {};
+  double total[kPhases] = {};
+  explicit PhaseTimer(bool enable) : on(enable) {
+    if (on)
+      for (auto& e : ev) cudaEventCreate(&e);
+  }
+  ~PhaseTimer() {
+    if (on)
+      for (auto& e : ev) cudaEventDestroy(e);
+  }
+  void mark(int i, cudaStream_t s) {
+    if (on) cudaEventRecord(ev[i], s);
+  }
+  // after the stream has been synchronised
+  void accumulate() {
+    if (!on) return;
+    for (int i = 0; i < kPhases; ++i) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, ev[i], ev[i + 1]) == cudaSuccess) total[i] += ms;
+    }
+  }
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// allocation
+// ---------------------------------------------------------------------------
+
+Status eig_work_alloc(EigWork& w, long n, int nd) {
+  eig_work_release(w);
+  w.nd = nd;
+  w.n = n;
+  const size_t m = 3 * (size_t)nd;
+  Status r;
+  for (double2** p : {&w.T, &w.HXn, &w.Pn, &w.HPn})
+    if ((r = walloc(p, (size_t)n * nd)) != kOk) return r;
+  for (double2** p : {&w.Hs, &w.Cs, &w.G, &w.Z, &w.Id})
+    if ((r = walloc(p, m * m)) != kOk) return r;
+  if ((r = walloc(&w.lam, m)) != kOk) return r;
+  if ((r = walloc(&w.lam0, m)) != kOk) return r;
+  if ((r = walloc(&w.colsq, m)) != kOk) return r;
+  if ((r = walloc(&w.partials, m * kColBlocks)) != kOk) return r;
+  if ((r = walloc(&w.idx, m)) != kOk) return r;
+  if ((r = walloc(&w.status, 1)) != kOk) return r;
+  if ((r = walloc(&w.info, 1)) != kOk) return r;
+  return kOk;
+}
+
+void eig_work_release(EigWork& w) {
+  auto f = [](void* p) { if (p) cudaFree(p); };
+  f(w.T); f(w.HXn); f(w.Pn); f(w.HPn); f(w.Hs); f(w.Cs); f(w.G); f(w.Z); f(w.Id);
+  f(w.lam); f(w.lam0); f(w.colsq); f(w.partials); f(w.idx); f(w.status); f(w.solver_work); f(w.info);
+  w = EigWork();
+}
+
+Status eig_vecs_alloc(EigVecs& v, long n, int nd) {
+  eig_vecs_release(v);
+  Status r;
+  if ((r = walloc(&v.V, (size_t)n * 3 * nd)) != kOk) return r;
+  if ((r = walloc(&v.HV, (size_t)n * 3 * nd)) != kOk) return r;
+  v.evals.assign(nd, 0.0);
+  v.init = false;
+  return kOk;
+}
+
+void eig_vecs_release(EigVecs& v) {
+  if (v.V) cudaFree(v.V);
+  if (v.HV) cudaFree(v.HV);
+  v = EigVecs();
+}
+
+// ---------------------------------------------------------------------------
+// solver
+// ---------------------------------------------------------------------------
+
+Status lobpcg(Handle& h, EigWork& w, EigVecs& k, int spin, int ik, double v0, double tol, int max_iter, int nconv,
+              int precision, EigStats& out) {
+  const long n = h.n_pw;
+  const int nd = w.nd;
+  if (n != w.n || nd < 1 || nconv < 1 || nconv > nd) return fail(kInvalid, "eigensolver: inconsistent block sizes");
+  const cudaStream_t s = h.stream;
+  cublasSetStream(h.blas, s);
+  Ctx c{h, w, s, n, (unsigned)std::min<long>(kColBlocks, blocks_for(n))};
+  Status r;
+  double2* X = k.V;
+  double2* HX = k.HV;
+  if (!k.init) {
+    // start: unit vectors on the nd lowest |k+G|^2 plus seeded noise
+    std::vector<double> kin(n);
+    PW_CUDA_TRY(cudaMemcpy(kin.data(), h.kp[ik].kinetic, n * sizeof(double), cudaMemcpyDeviceToHost));
+    std::vector<int> order(n);
+    for (long i = 0; i < n; ++i) order[i] = (int)i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return kin[a] < kin[b]; });
+    std::vector<double2> x0((size_t)n * nd);
+    std::mt19937_64 rng(20261203ULL + 7919ULL * (ik + 1) + 104729ULL * spin);
+    std::uniform_real_distribution<double> u(-1.0, 1.0);
+    for (int col = 0; col < nd; ++col)
+      for (long i = 0; i < n; ++i) x0[(size_t)col * n + i] = make_double2(1e-3 * u(rng), 1e-3 * u(rng));
+    for (int col = 0; col < nd && col < n; ++col) x0[(size_t)col * n + order[col]].x += 1.0;
+    PW_CUDA_TRY(cudaMemcpyAsync(X, x0.data(), x0.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
+    k.init = true;
+  }
+  if ((r = orthonormalize(c, X, nd)) != kOk) return r;
+  // HX in FP64: the residuals below refer to the full-precision operator
+  if ((r = apply_h_device(h, spin, ik, X, n, nd, HX, n, 0, s)) != kOk) return r;
+  out.happ += nd;
+  if ((r = rr_block(c, k, nd)) != kOk) return r;
+
+  const double p_drop = precision == 0 ? kPDropFp64 : kPDropMixed;
+  std::vector<double> rn(nd), nu0, nu1;
+  std::vector<int> act, pband, keep, pk;
+  int np = 0;  // columns of Pn / HPn (bands pband)
+  out.iters = 0;
+  PhaseTimer pt(h.trace);
+  for (;;) {
+    const auto t0 = std::chrono::steady_clock::now();
+    pt.mark(0, s);
+    PW_CUDA_TRY(cudaMemcpyAsync(w.lam0, k.evals.data(), nd * sizeof(double), cudaMemcpyHostToDevice, s));
+    k_resid_precond<<<dim3(c.gx, nd), 256, 0, s>>>(X, HX, w.T, n, (int)n, w.lam0, h.kp[ik].kinetic, v0,
+                                                   w.partials); count_launch();
+    k_col_final<<<blocks_for(nd), 256, 0, s>>>(w.partials, (int)c.gx, nd, w.colsq); count_launch();
+    PW_CUDA_TRY(cudaMemcpyAsync(rn.data(), w.colsq, nd * sizeof(double), cudaMemcpyDeviceToHost, s));
+    PW_CUDA_TRY(cudaStreamSynchronize(s));
+    out.max_res = 0.0;
+    for (int b = 0; b < nconv; ++b) out.max_res = std::max(out.max_res, std::sqrt(rn[b]));
+    if (out.max_res < tol || out.iters >= max_iter) break;
+    // active bands: residual above tol (buffer bands: 10 tol)
+    act.clear();
+    for (int b = 0; b < nd; ++b)
+      if (std::sqrt(rn[b]) > (b < nconv ? tol : 10.0 * tol)) act.push_back(b);
+    if ((long)act.size() > n - nd) act.resize((size_t)std::max<long>(0, n - nd));
+    const int na = (int)act.size();
+    if (na == 0) break;
+    double2* W = k.V + n * nd;
+    double2* HW = k.HV + n * nd;
+    pt.mark(1, s);
+    PW_CUDA_TRY(cudaMemcpyAsync(w.idx, act.data(), na * sizeof(int), cudaMemcpyHostToDevice, s));
+    k_gather_cols<<<dim3(c.gx, na), 256, 0, s>>>(w.T, n, w.idx, W, n, (int)n); count_launch();
+    if ((r = project_out(c, X, nullptr, nd, W, nullptr, na)) != kOk) return r;
+    if ((r = project_out(c, X, nullptr, nd, W, nullptr, na)) != kOk) return r;
+    if ((r = orthonormalize(c, W, na)) != kOk) return r;
+    pt.mark(2, s);
+    if ((r = apply_h_device(h, spin, ik, W, n, na, HW, n, precision, s)) != kOk) return r;
+    out.happ += na;
+    pt.mark(3, s);
+    // P: previous directions of the bands still active
+    int npc = 0;
+    pk.clear();
+    for (int j = 0, a = 0; j < np; ++j) {
+      while (a < na && act[a] < pband[j]) ++a;
+      if (a < na && act[a] == pband[j]) pk.push_back(j);
+    }
+    if ((long)pk.size() > n - nd - na) pk.resize((size_t)std::max<long>(0, n - nd - na));
+    double2* P = W + n * na;
+    double2* HP = HW + n * na;
+    if (!pk.empty()) {
+      npc = (int)pk.size();
+      PW_CUDA_TRY(cudaMemcpyAsync(w.idx, pk.data(), npc * sizeof(int), cudaMemcpyHostToDevice, s));
+      k_gather_cols<<<dim3(c.gx, npc), 256, 0, s>>>(w.Pn, n, w.idx, P, n, (int)n); count_launch();
+      k_gather_cols<<<dim3(c.gx, npc), 256, 0, s>>>(w.HPn, n, w.idx, HP, n, (int)n); count_launch();
+      nu0.resize(npc);
+      nu1.resize(npc);
+      if ((r = col_norms2(c, P, npc, nu0.data())) != kOk) return r;
+      if ((r = project_out(c, X, HX, nd, P, HP, npc)) != kOk) return r;
+      if ((r = project_out(c, W, HW, na, P, HP, npc)) != kOk) return r;
+      if ((r = col_norms2(c, P, npc, nu1.data())) != kOk) return r;
+      keep.clear();
+      for (int j = 0; j < npc; ++j)
+        if (nu1[j] > p_drop * p_drop * nu0[j] && nu1[j] > 0.0) keep.push_back(j);
+      if ((int)keep.size() < npc && !keep.empty()) {
+        // compact through Pn / HPn (their old contents were consumed above)
+        const int nk = (int)keep.size();
+        PW_CUDA_TRY(cudaMemcpyAsync(w.idx, keep.data(), nk * sizeof(int), cudaMemcpyHostToDevice, s));
+        k_gather_cols<<<dim3(c.gx, nk), 256, 0, s>>>(P, n, w.idx, w.Pn, n, (int)n); count_launch();
+        k_gather_cols<<<dim3(c.gx, nk), 256, 0, s>>>(HP, n, w.idx, w.HPn, n, (int)n); count_launch();
+        PW_CUDA_TRY(cudaMemcpyAsync(P, w.Pn, n * nk * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+        PW_CUDA_TRY(cudaMemcpyAsync(HP, w.HPn, n * nk * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+      }
+      npc = (int)keep.size();
+      if (npc > 0) {
+        if ((r = col_norms2(c, P, npc, nullptr)) != kOk) return r;
+        k_scale_cols_invsqrt<<<dim3(c.gx, npc), 256, 0, s>>>(P, HP, n, (int)n, w.colsq); count_launch();
+        bool ok = false;
+        double rmin = 0.0;
+        if ((r = chol_qr(c, P, HP, npc, 0.0, ok, &rmin)) != kOk) return r;
+        if (!ok || rmin < p_drop) {
+          npc = 0;  // P block nearly dependent: restart without it
+        } else if ((r = chol_qr(c, P, HP, npc, 0.0, ok)) != kOk) {
+          return r;
+        } else if (!ok) {
+          npc = 0;
+        }
+      }
+    }
+    // Rayleigh-Ritz over [X | W | P]
+    pt.mark(4, s);
+    const int q = na + npc, m = nd + q;
+    if ((r = zgemm(c, CUBLAS_OP_C, CUBLAS_OP_N, q, nd, (int)n, W, n, HX, n, w.Z, q)) != kOk) return r;
+    if ((r = zgemm(c, CUBLAS_OP_C, CUBLAS_OP_N, q, q, (int)n, W, n, HW, n, w.G, q)) != kOk) return r;
+    k_assemble_rr<<<blocks_for((long)m * m), 256, 0, s>>>(w.Hs, m, nd, w.lam0, w.Z, w.G); count_launch();
+    double2* C = nullptr;
+    pt.mark(5, s);
+    if ((r = subspace_eig(c, m, nd, &C)) != kOk) return r;
+    pt.mark(6, s);
+    // new X, HX; new P, HP for the active bands from the (W, P) rows of C
+    if ((r = zgemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, nd, m, k.V, n, C, m, w.T, n)) != kOk) return r;
+    if ((r = zgemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, nd, m, k.HV, n, C, m, w.HXn, n)) != kOk) return r;
+    PW_CUDA_TRY(cudaMemcpyAsync(w.idx, act.data(), na * sizeof(int), cudaMemcpyHostToDevice, s));
+    double2* Ca = C == w.Cs ? w.Z : w.Cs;  // q x na gathered columns, ld q
+    k_gather_cols<<<dim3(1, na), 256, 0, s>>>(C + nd, m, w.idx, Ca, q, q); count_launch();
+    if ((r = zgemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, na, q, W, n, Ca, q, w.Pn, n)) != kOk) return r;
+    if ((r = zgemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, na, q, HW, n, Ca, q, w.HPn, n)) != kOk) return r;
+    PW_CUDA_TRY(cudaMemcpyAsync(X, w.T, n * nd * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+    PW_CUDA_TRY(cudaMemcpyAsync(HX, w.HXn, n * nd * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+    PW_CUDA_TRY(cudaMemcpyAsync(k.evals.data(), w.lam, nd * sizeof(double), cudaMemcpyDeviceToHost, s));
+    pt.mark(7, s);
+    PW_CUDA_TRY(cudaStreamSynchronize(s));
+    pt.accumulate();
+    np = na;
+    pband = act;
+    ++out.iters;
+    if (h.trace) {
+      const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+      std::fprintf(stderr, "pwgpu lobpcg k=%d it=%d res=%.3e na=%d np=%d e0=%.8f e_last=%.8f %.2f ms\n", ik,
+                   out.iters, out.max_res, na, npc, k.evals[0], k.evals[nconv - 1], ms);
+    }
+  }
+  if (pt.on)
+    std::fprintf(stderr,
+                 "pwgpu lobpcg k=%d phases ms: resid %.2f W %.2f HW %.2f P %.2f matrix %.2f solve %.2f update %.2f\n",
+                 ik, pt.total[0], pt.total[1], pt.total[2], pt.total[3], pt.total[4], pt.total[5], pt.total[6]);
+  PW_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
+}  // namespace pwgpu

@@ -1,0 +1,267 @@
+// Kleinman-Bylander term of the mixed form as 3xBF16 tensor-core products.
+//
+// H_NL psi = B D B^H psi (potential/nonlocal.rs:432-450) is two complex
+// GEMMs.  Each is written as one real GEMM through the embedding
+//   P = B^H psi:   [B_r, B_i] (n_ch x 2 n_pw) * [[psi_r, psi_i], [psi_i, -psi_r]]  -> [P_r, P_i]
+//   Y = B Q:       [B_r, B_i] (n_pw x 2 n_ch) * [[Q_r, Q_i], [-Q_i, Q_r]]          -> [Y_r, Y_i]
+// and every real operand x is split x = hi + lo with hi = bf16(x),
+// lo = bf16(x - hi).  The three products hi*hi + hi*lo + lo*hi (lo*lo is
+// dropped, ~2^-16 relative) are summed by one GEMM whose K runs over the
+// concatenation [A_hi | A_hi | A_lo] x [B_hi ; B_lo ; B_hi], accumulated in
+// FP32 on the tensor cores.  The first GEMM (K = 6 n_pw, small M x N) is cut
+// into split-K slices through the GEMM's batch index; the slice partials
+// are summed in FP64 by the epilogue kernel that also forms complex P.  The
+// projector operands are constant per k-point and are split once.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "gemm_bf16.hpp"
+#include "handle.hpp"
+
+namespace pwgpu {
+
+namespace {
+
+inline long round_up(long x, long m) { return (x + m - 1) / m * m; }
+
+__device__ __forceinline__ void split_bf16(double v, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+  const float f = (float)v;
+  hi = __float2bfloat16_rn(f);
+  lo = __float2bfloat16_rn(f - __bfloat162float(hi));
+}
+
+// A1[c][k], c < m1pad, k < k1pad: row c = [hi | hi | lo] of [B_r(:,c), B_i(:,c)]
+__global__ void k_build_a1(const double2* __restrict__ b, int n_pw, int n_ch, long k1pad, int m1pad,
+                           __nv_bfloat16* __restrict__ a1) {
+  const long total = (long)m1pad * k1pad;
+  const long seg_len = 2L * n_pw;
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const long c = t / k1pad, k = t - c * k1pad;
+    __nv_bfloat16 out = __float2bfloat16_rn(0.0f);
+    if (c < n_ch && k < 3 * seg_len) {
+      const int seg = (int)(k / seg_len);
+      const long r = k - seg * seg_len;
+      const double2 z = b[(r < n_pw ? r : r - n_pw) + c * (long)n_pw];
+      __nv_bfloat16 hi, lo;
+      split_bf16(r < n_pw ? z.x : z.y, hi, lo);
+      out = seg < 2 ? hi : lo;
+    }
+    a1[t] = out;
+  }
+}
+
+// A2[G][k], G < m2pad, k < k2pad: row G = [hi | hi | lo] of [B_r(G,:), B_i(G,:)]
+__global__ void k_build_a2(const double2* __restrict__ b, int n_pw, int n_ch, long k2pad, long m2pad,
+                           __nv_bfloat16* __restrict__ a2) {
+  const long total = m2pad * k2pad;
+  const long seg_len = 2L * n_ch;
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const long g = t / k2pad, k = t - g * k2pad;
+    __nv_bfloat16 out = __float2bfloat16_rn(0.0f);
+    if (g < n_pw && k < 3 * seg_len) {
+      const int seg = (int)(k / seg_len);
+      const long r = k - seg * seg_len;
+      const double2 z = b[g + (r < n_ch ? r : r - n_ch) * (long)n_pw];
+      __nv_bfloat16 hi, lo;
+      split_bf16(r < n_ch ? z.x : z.y, hi, lo);
+      out = seg < 2 ? hi : lo;
+    }
+    a2[t] = out;
+  }
+}
+
+// B1[j][k], j < 2 nb, k < k1pad: column j = [hi | lo | hi] of
+// [psi_r; psi_i] (j < nb) or [psi_i; -psi_r] (j >= nb), band j mod nb.
+__global__ void k_split_psi(const double2* __restrict__ psi, long ldpsi, int n_pw, int nb, long k1pad,
+                            __nv_bfloat16* __restrict__ b1) {
+  const long total = 2L * nb * k1pad;
+  const long seg_len = 2L * n_pw;
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const long j = t / k1pad, k = t - j * k1pad;
+    __nv_bfloat16 out = __float2bfloat16_rn(0.0f);
+    if (k < 3 * seg_len) {
+      const int part = j >= nb;
+      const long band = part ? j - nb : j;
+      const int seg = (int)(k / seg_len);
+      const long r = k - seg * seg_len;
+      const double2 z = psi[(r < n_pw ? r : r - n_pw) + band * ldpsi];
+      const double v = part == 0 ? (r < n_pw ? z.x : z.y) : (r < n_pw ? z.y : -z.x);
+      __nv_bfloat16 hi, lo;
+      split_bf16(v, hi, lo);
+      out = seg == 1 ? lo : hi;
+    }
+    b1[t] = out;
+  }
+}
+
+// B2[j][k], j < 2 nb, k < k2pad: column j = [hi | lo | hi] of
+// [Q_r; -Q_i] (j < nb) or [Q_i; Q_r] (j >= nb).
+__global__ void k_split_q(const double2* __restrict__ q, int n_ch, int nb, long k2pad, __nv_bfloat16* __restrict__ b2) {
+  const long total = 2L * nb * k2pad;
+  const long seg_len = 2L * n_ch;
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    const long j = t / k2pad, k = t - j * k2pad;
+    __nv_bfloat16 out = __float2bfloat16_rn(0.0f);
+    if (k < 3 * seg_len) {
+      const int part = j >= nb;
+      const long band = part ? j - nb : j;
+      const int seg = (int)(k / seg_len);
+      const long r = k - seg * seg_len;
+      const double2 z = q[(r < n_ch ? r : r - n_ch) + band * n_ch];
+      const double v = part == 0 ? (r < n_ch ? z.x : -z.y) : (r < n_ch ? z.y : z.x);
+      __nv_bfloat16 hi, lo;
+      split_bf16(v, hi, lo);
+      out = seg == 1 ? lo : hi;
+    }
+    b2[t] = out;
+  }
+}
+
+// P[c + b n_ch] = sum over slices of (D1[c, b], D1[c, nb + b])
+__global__ void k_sum_p(const float* __restrict__ d1, int m1pad, int nb, int slices, long slice_stride, int n_ch,
+                        double2* __restrict__ p) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)n_ch * nb) return;
+  const int c = (int)(t % n_ch);
+  const int b = (int)(t / n_ch);
+  double re = 0.0, im = 0.0;
+  for (int s = 0; s < slices; ++s) {
+    const float* d = d1 + s * slice_stride;
+    re += d[c + (long)b * m1pad];
+    im += d[c + (long)(nb + b) * m1pad];
+  }
+  p[t] = make_double2(re, im);
+}
+
+// hpsi[G, b] += (D2[G, b], D2[G, nb + b])
+__global__ void k_add_nl(const float* __restrict__ d2, long m2pad, int n_pw, int nb, double2* __restrict__ hpsi,
+                         long ldh) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)n_pw * nb) return;
+  const long g = t % n_pw;
+  const long b = t / n_pw;
+  double2 h = hpsi[g + b * ldh];
+  h.x += d2[g + b * m2pad];
+  h.y += d2[g + (nb + b) * m2pad];
+  hpsi[g + b * ldh] = h;
+}
+
+inline unsigned grid_for(long n) { return (unsigned)std::min<long>(148L * 16, std::max<long>(1, (n + 255) / 256)); }
+
+}  // namespace
+
+// Per-k split projector operands and per-call buffers of the mixed form.
+struct NlMixed {
+  long k1pad = 0, k2pad = 0, m2pad = 0;
+  int m1pad = 0;
+  std::vector<__nv_bfloat16*> a1, a2;  // per k
+  __nv_bfloat16 *b1 = nullptr, *b2 = nullptr;
+  float *d1 = nullptr, *d2 = nullptr;
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+  int nb_cap = 0, slices_cap = 0;
+};
+
+void release_nl_mixed(Handle& h) {
+  NlMixed* m = h.nlm;
+  if (!m) return;
+  for (auto p : m->a1) if (p) cudaFree(p);
+  for (auto p : m->a2) if (p) cudaFree(p);
+  if (m->b1) cudaFree(m->b1);
+  if (m->b2) cudaFree(m->b2);
+  if (m->d1) cudaFree(m->d1);
+  if (m->d2) cudaFree(m->d2);
+  if (m->ws) cudaFree(m->ws);
+  delete m;
+  h.nlm = nullptr;
+}
+
+bool nl_mixed_eligible(const Handle& h) { return h.n_ch >= 32 && h.n_pw >= 512; }
+
+static Status nl_alloc(void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 16));
+  if (e != cudaSuccess) return fail(kOom, std::string("cudaMalloc (mixed projectors): ") + cudaGetErrorString(e));
+  return kOk;
+}
+
+Status nonlocal_mixed(Handle& h, int ik, const double2* psi, long ldpsi, int nb, double2* hpsi, long ldh,
+                      cudaStream_t s, StageTimer* tm) {
+  if (!h.nlm) {
+    h.nlm = new NlMixed();
+    h.nlm->a1.assign(h.n_k, nullptr);
+    h.nlm->a2.assign(h.n_k, nullptr);
+    h.nlm->k1pad = round_up(6L * h.n_pw, 64L * 32);
+    h.nlm->k2pad = round_up(6L * h.n_ch, 64);
+    h.nlm->m1pad = (int)round_up(h.n_ch, 8);
+    h.nlm->m2pad = round_up(h.n_pw, 8);
+  }
+  NlMixed& m = *h.nlm;
+  Status st;
+  if (!m.a1[ik]) {
+    if ((st = nl_alloc((void**)&m.a1[ik], (size_t)m.m1pad * m.k1pad * 2)) != kOk) return st;
+    if ((st = nl_alloc((void**)&m.a2[ik], (size_t)m.m2pad * m.k2pad * 2)) != kOk) return st;
+    k_build_a1<<<grid_for((long)m.m1pad * m.k1pad), 256, 0, s>>>(h.kp[ik].b, h.n_pw, h.n_ch, m.k1pad, m.m1pad,
+                                                                m.a1[ik]);
+    count_launch();
+    k_build_a2<<<grid_for(m.m2pad * m.k2pad), 256, 0, s>>>(h.kp[ik].b, h.n_pw, h.n_ch, m.k2pad, m.m2pad, m.a2[ik]);
+    count_launch();
+  }
+  // split-K slices of the first product: about two waves of 128x128 tiles
+  const long tiles = ((m.m1pad + 127) / 128) * ((2L * nb + 127) / 128);
+  int slices = 1;
+  while (slices < 32 && tiles * slices < 2 * 148 && m.k1pad / (slices * 2) >= 2048) slices *= 2;
+  const long ks = m.k1pad / slices;
+  if (nb > m.nb_cap || slices > m.slices_cap) {
+    const int cap = std::max(nb, m.nb_cap);
+    const int scap = std::max(slices, m.slices_cap);
+    if (m.b1) cudaFree(m.b1);
+    if (m.b2) cudaFree(m.b2);
+    if (m.d1) cudaFree(m.d1);
+    if (m.d2) cudaFree(m.d2);
+    if (m.ws) cudaFree(m.ws);
+    m.b1 = m.b2 = nullptr;
+    m.d1 = m.d2 = nullptr;
+    m.ws = nullptr;
+    if ((st = nl_alloc((void**)&m.b1, (size_t)2 * cap * m.k1pad * 2)) != kOk) return st;
+    if ((st = nl_alloc((void**)&m.b2, (size_t)2 * cap * m.k2pad * 2)) != kOk) return st;
+    if ((st = nl_alloc((void**)&m.d1, (size_t)m.m1pad * 2 * cap * scap * 4)) != kOk) return st;
+    if ((st = nl_alloc((void**)&m.d2, (size_t)m.m2pad * 2 * cap * 4)) != kOk) return st;
+    size_t ws = std::max(gemm_bf16_workspace(m.m1pad, 2 * cap, (int)(m.k1pad / scap), scap),
+                         gemm_bf16_workspace((int)m.m2pad, 2 * cap, (int)m.k2pad, 1));
+    for (int sl = 1; sl <= scap; sl *= 2)
+      ws = std::max(ws, gemm_bf16_workspace(m.m1pad, 2 * cap, (int)(m.k1pad / sl), sl));
+    if ((st = nl_alloc(&m.ws, ws)) != kOk) return st;
+    m.ws_bytes = ws;
+    m.nb_cap = cap;
+    m.slices_cap = scap;
+  }
+  if ((st = ensure_nl_capacity(h, nb)) != kOk) return st;
+  const int n2 = 2 * nb;
+  k_split_psi<<<grid_for((long)n2 * m.k1pad), 256, 0, s>>>(psi, ldpsi, h.n_pw, nb, m.k1pad, m.b1);
+  count_launch();
+  const long slice_stride = (long)m.m1pad * n2;
+  if ((st = gemm_bf16_tn_f32(m.a1[ik], m.k1pad, ks, m.b1, m.k1pad, ks, m.d1, m.m1pad, slice_stride, m.m1pad, n2,
+                             (int)ks, slices, m.ws, m.ws_bytes, s)) != kOk)
+    return st;
+  k_sum_p<<<(unsigned)(((long)h.n_ch * nb + 255) / 256), 256, 0, s>>>(m.d1, m.m1pad, nb, slices, slice_stride, h.n_ch,
+                                                                       h.nl_p);
+  count_launch();
+  mark(tm, 5, s);
+  if ((st = apply_d_blocks(h, nb, s)) != kOk) return st;
+  mark(tm, 6, s);
+  k_split_q<<<grid_for((long)n2 * m.k2pad), 256, 0, s>>>(h.nl_q, h.n_ch, nb, m.k2pad, m.b2);
+  count_launch();
+  if ((st = gemm_bf16_tn_f32(m.a2[ik], m.k2pad, 0, m.b2, m.k2pad, 0, m.d2, m.m2pad, 0, (int)m.m2pad, n2,
+                             (int)m.k2pad, 1, m.ws, m.ws_bytes, s)) != kOk)
+    return st;
+  k_add_nl<<<(unsigned)(((long)h.n_pw * nb + 255) / 256), 256, 0, s>>>(m.d2, m.m2pad, h.n_pw, nb, hpsi, ldh);
+  count_launch();
+  mark(tm, 7, s);
+  PW_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
+}  // namespace pwgpu

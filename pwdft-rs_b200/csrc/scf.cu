@@ -2,7 +2,7 @@
 //
 // Replaces the per-iteration body of run_scf_unpolarized
 // (scf/driver.rs:353-735): potentials from rho_in (energy.rs:293-358,
-// xc.rs:129-288), per-k eigensolve (dense.rs:50-98 -> block Davidson here),
+// xc.rs:129-288), per-k eigensolve (dense.rs:50-98 -> LOBPCG here, lobpcg.cu),
 // occupations (smearing.rs:38-252, host FP64), density (density.rs:41-111),
 // G-space symmetrisation (symmetry/density/g_space.rs:147-252), energies
 // (energy.rs:51-235) and Anderson/Kerker mixing (mixing/anderson.rs:158-266,
@@ -19,6 +19,7 @@
 
 #include "handle.hpp"
 #include "linalg.hpp"
+#include "lobpcg.hpp"
 #include "scf.hpp"
 
 namespace pwgpu {
@@ -34,7 +35,6 @@ constexpr double kE2 = 14.399645351950548;
 constexpr double kG2Zero = 1e-12;
 constexpr double kRhoFloor = 1e-30;
 constexpr int kRedBlocks = 512;  // partial sums per reduction (fixed order)
-constexpr double kFp32ResidualFloor = 3e-5;  // eV, eigen-residual floor of the FP32 H|psi> phase
 
 // ---------------------------------------------------------------------------
 // deterministic reductions: partials[blockIdx] then one block sums them
@@ -206,58 +206,6 @@ __global__ void k_sym_gather(const double2* __restrict__ rg, const int* __restri
   out[i] = make_double2(re * inv, im * inv);
 }
 
-// Davidson: residual R = HX - lambda X, preconditioned into T
-// (smooth g_psi denominator 0.5 (1 + x + sqrt(1 + (x-1)^2)) in Ry, x = (h_diag - lambda)/Ry),
-// and per-column partial sums of |R|^2.
-__global__ void k_resid_precond(const double2* __restrict__ X, const double2* __restrict__ HX, double2* __restrict__ T,
-                                long ld, int n, const double* __restrict__ lam, const double* __restrict__ kin,
-                                double v0, double* __restrict__ partials) {
-  __shared__ double sh[32];
-  const int col = blockIdx.y;
-  const double l = lam[col];
-  const double2* x = X + (long)col * ld;
-  const double2* hx = HX + (long)col * ld;
-  double2* t = T + (long)col * ld;
-  double acc = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const double2 r = make_double2(hx[i].x - l * x[i].x, hx[i].y - l * x[i].y);
-    acc += r.x * r.x + r.y * r.y;
-    const double xx = (kin[i] + v0 - l) / kRyToEv;
-    const double den = 0.5 * (1.0 + xx + sqrt(1.0 + (xx - 1.0) * (xx - 1.0))) * kRyToEv;
-    t[i] = make_double2(r.x / den, r.y / den);
-  }
-  acc = block_sum(acc, sh);
-  if (threadIdx.x == 0) partials[(long)col * gridDim.x + blockIdx.x] = acc;
-}
-
-__global__ void k_col_sumsq(const double2* __restrict__ X, long ld, int n, double* __restrict__ partials) {
-  __shared__ double sh[32];
-  const int col = blockIdx.y;
-  const double2* x = X + (long)col * ld;
-  double acc = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    acc += x[i].x * x[i].x + x[i].y * x[i].y;
-  acc = block_sum(acc, sh);
-  if (threadIdx.x == 0) partials[(long)col * gridDim.x + blockIdx.x] = acc;
-}
-
-// sums[col] = sum of the nblk partials of each column (fixed order)
-__global__ void k_col_final(const double* __restrict__ partials, int nblk, int ncols, double* __restrict__ sums) {
-  const int col = blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= ncols) return;
-  double acc = 0.0;
-  for (int b = 0; b < nblk; ++b) acc += partials[(long)col * nblk + b];
-  sums[col] = acc;
-}
-
-__global__ void k_scale_cols_invsqrt(double2* __restrict__ X, long ld, int n, const double* __restrict__ sumsq) {
-  const int col = blockIdx.y;
-  const double s = sumsq[col] > 0.0 ? 1.0 / sqrt(sumsq[col]) : 0.0;
-  double2* x = X + (long)col * ld;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    x[i] = make_double2(x[i].x * s, x[i].y * s);
-}
-
 // Anderson pieces
 __global__ void k_sub(const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out, long n) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -301,19 +249,11 @@ inline unsigned blocks_for(long n, int t = 256) { return (unsigned)std::max<long
 // state
 // ---------------------------------------------------------------------------
 
-struct KState {
-  double2* V = nullptr;   // n_pw x 2 nd: X | T
-  double2* HV = nullptr;  // n_pw x 2 nd: HX | HT
-  std::vector<double> evals;
-  bool init = false;
-};
-
 struct ScfState {
   int nd = 0, nb = 0;
-  std::vector<KState> ks;
-  double2 *Hs = nullptr, *Ss = nullptr, *Cm = nullptr, *Pm = nullptr, *tmp = nullptr;
-  double *lam = nullptr, *col_sums = nullptr, *partials = nullptr, *scal = nullptr, *fw = nullptr;
-  int* status = nullptr;
+  std::vector<EigVecs> ks;  // per (spin, k)
+  EigWork ew;
+  double *partials = nullptr, *scal = nullptr, *fw = nullptr;
   double *rho_in = nullptr, *rho_out = nullptr, *exc = nullptr, *vxc = nullptr, *rtmp = nullptr;
   double2 *cg = nullptr, *cg2 = nullptr, *vh = nullptr;
   double* kerker_w = nullptr;
@@ -333,9 +273,9 @@ void release_scf(Handle& h) {
   ScfState* st = h.scf;
   if (!st) return;
   auto f = [](void* p) { if (p) cudaFree(p); };
-  for (auto& k : st->ks) { f(k.V); f(k.HV); }
-  f(st->Hs); f(st->Ss); f(st->Cm); f(st->Pm); f(st->tmp);
-  f(st->lam); f(st->col_sums); f(st->partials); f(st->scal); f(st->fw); f(st->status);
+  for (auto& k : st->ks) eig_vecs_release(k);
+  eig_work_release(st->ew);
+  f(st->partials); f(st->scal); f(st->fw);
   f(st->rho_in); f(st->rho_out); f(st->exc); f(st->vxc); f(st->rtmp);
   f(st->cg); f(st->cg2); f(st->vh); f(st->kerker_w);
   for (double* p : st->hin) f(p);
@@ -353,25 +293,14 @@ static Status ensure_state(Handle& h, int nb, int nd, int ndim) {
   st->nd = nd;
   st->nb = nb;
   const long n = h.n_pw, N = h.g.N;
-  const int m = 2 * nd;
   Status s;
   st->ks.resize((size_t)h.nspin * h.n_k);
-  for (auto& k : st->ks) {
-    if ((s = salloc(&k.V, (size_t)n * m)) != kOk) return s;
-    if ((s = salloc(&k.HV, (size_t)n * m)) != kOk) return s;
-    k.evals.assign(nd, 0.0);
-  }
-  if ((s = salloc(&st->Hs, (size_t)m * m)) != kOk) return s;
-  if ((s = salloc(&st->Ss, (size_t)m * m)) != kOk) return s;
-  if ((s = salloc(&st->Cm, (size_t)m * m)) != kOk) return s;
-  if ((s = salloc(&st->Pm, (size_t)m * m)) != kOk) return s;
-  if ((s = salloc(&st->tmp, (size_t)n * 2 * nd)) != kOk) return s;
-  if ((s = salloc(&st->lam, (size_t)m)) != kOk) return s;
-  if ((s = salloc(&st->col_sums, (size_t)m)) != kOk) return s;
-  if ((s = salloc(&st->partials, (size_t)std::max<long>(kRedBlocks * 4, (long)m * 64))) != kOk) return s;
+  for (auto& k : st->ks)
+    if ((s = eig_vecs_alloc(k, n, nd)) != kOk) return s;
+  if ((s = eig_work_alloc(st->ew, n, nd)) != kOk) return s;
+  if ((s = salloc(&st->partials, (size_t)kRedBlocks * 4)) != kOk) return s;
   if ((s = salloc(&st->scal, 16)) != kOk) return s;
   if ((s = salloc(&st->fw, (size_t)nd)) != kOk) return s;
-  if ((s = salloc(&st->status, 1)) != kOk) return s;
   if ((s = salloc(&st->rho_in, (size_t)N)) != kOk) return s;
   if ((s = salloc(&st->rho_out, (size_t)N)) != kOk) return s;
   if ((s = salloc(&st->exc, (size_t)N)) != kOk) return s;
@@ -471,120 +400,6 @@ static Status symmetrize(Handle& h, double* rho) {
   k_sym_gather<<<blocks_for(N), 256, 0, s>>>(st->cg, h.sym_src, h.sym_arg, h.n_sym, N, st->cg2); count_launch();
   if ((r = fft3d_full(h, st->cg2, +1, s)) != kOk) return r;
   k_cplx_real_scaled<<<blocks_for(N), 256, 0, s>>>(st->cg2, rho, 1.0 / (double)N, N); count_launch();
-  PW_CUDA_TRY(cudaGetLastError());
-  return kOk;
-}
-
-// ---------------------------------------------------------------------------
-// block Davidson for one (spin, k)
-// ---------------------------------------------------------------------------
-
-static Status zgemm(Handle& h, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k, const double2* A,
-                    long lda, const double2* B, long ldb, double2* C, long ldc, double beta_re = 0.0,
-                    double alpha_re = 1.0) {
-  const cuDoubleComplex al = make_cuDoubleComplex(alpha_re, 0.0), be = make_cuDoubleComplex(beta_re, 0.0);
-  cublasStatus_t cs = cublasZgemm(h.blas, ta, tb, m, n, k, &al, reinterpret_cast<const cuDoubleComplex*>(A), (int)lda,
-                                  reinterpret_cast<const cuDoubleComplex*>(B), (int)ldb, &be,
-                                  reinterpret_cast<cuDoubleComplex*>(C), (int)ldc);
-  if (cs != CUBLAS_STATUS_SUCCESS) return fail(kCuda, "cublasZgemm failed (Davidson)");
-  return kOk;
-}
-
-// Rayleigh-Ritz over the first m columns of V/HV: lowest nd pairs into
-// X/HX (= first nd columns), eigenvalues into st->lam and k.evals.
-static Status rayleigh_ritz(Handle& h, KState& k, int m, int nd) {
-  ScfState* st = h.scf;
-  const long n = h.n_pw;
-  Status r;
-  if ((r = zgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, m, m, (int)n, k.V, n, k.HV, n, st->Hs, m)) != kOk) return r;
-  if ((r = zgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, m, m, (int)n, k.V, n, k.V, n, st->Ss, m)) != kOk) return r;
-  const double2* C;
-  if (m <= 64) {
-    if ((r = small_geneig_batched(st->Hs, st->Ss, m, 0, m, nd, 1, st->lam, st->Cm, m, 0, st->status, h.stream)) != kOk)
-      return r;
-    int status = 0;
-    PW_CUDA_TRY(cudaMemcpyAsync(&status, st->status, sizeof(int), cudaMemcpyDeviceToHost, h.stream));
-    PW_CUDA_TRY(cudaStreamSynchronize(h.stream));
-    if (status == 1) return fail(kNotConverged, "Rayleigh-Ritz overlap matrix is not positive definite");
-    C = st->Cm;
-  } else {
-    if ((r = large_geneig(h, st->Hs, st->Ss, m, st->lam, h.stream)) != kOk) return r;
-    C = st->Hs;
-  }
-  // X = V C, HX = HV C (through tmp, both n x nd)
-  if ((r = zgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, nd, m, k.V, n, C, m, st->tmp, n)) != kOk) return r;
-  if ((r = zgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, nd, m, k.HV, n, C, m, st->tmp + n * nd, n)) != kOk) return r;
-  PW_CUDA_TRY(cudaMemcpyAsync(k.V, st->tmp, n * nd * sizeof(double2), cudaMemcpyDeviceToDevice, h.stream));
-  PW_CUDA_TRY(cudaMemcpyAsync(k.HV, st->tmp + n * nd, n * nd * sizeof(double2), cudaMemcpyDeviceToDevice, h.stream));
-  PW_CUDA_TRY(cudaMemcpyAsync(k.evals.data(), st->lam, nd * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
-  PW_CUDA_TRY(cudaStreamSynchronize(h.stream));
-  return kOk;
-}
-
-static Status davidson(Handle& h, int spin, int ik, double tol, int max_iter, int nconv, int precision,
-                       long& happ, int& iters, double& max_res) {
-  ScfState* st = h.scf;
-  KState& k = st->ks[(size_t)spin * h.n_k + ik];
-  const long n = h.n_pw;
-  const int nd = st->nd;
-  const cudaStream_t s = h.stream;
-  Status r;
-  cublasSetStream(h.blas, s);
-  if (!k.init) {
-    // start: unit vectors on the nd lowest |k+G|^2 plus seeded noise
-    std::vector<double> kin(n);
-    PW_CUDA_TRY(cudaMemcpy(kin.data(), h.kp[ik].kinetic, n * sizeof(double), cudaMemcpyDeviceToHost));
-    std::vector<int> idx(n);
-    for (long i = 0; i < n; ++i) idx[i] = (int)i;
-    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return kin[a] < kin[b]; });
-    std::vector<double2> x0((size_t)n * nd);
-    std::mt19937_64 rng(20261203ULL + 7919ULL * (ik + 1) + 104729ULL * spin);
-    std::uniform_real_distribution<double> u(-1.0, 1.0);
-    for (int c = 0; c < nd; ++c)
-      for (long i = 0; i < n; ++i) x0[(size_t)c * n + i] = make_double2(1e-3 * u(rng), 1e-3 * u(rng));
-    for (int c = 0; c < nd && c < n; ++c) x0[(size_t)c * n + idx[c]].x += 1.0;
-    PW_CUDA_TRY(cudaMemcpyAsync(k.V, x0.data(), x0.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
-    if ((r = apply_h_device(h, spin, ik, k.V, n, nd, k.HV, n, precision, s)) != kOk) return r;
-    happ += nd;
-    if ((r = rayleigh_ritz(h, k, nd, nd)) != kOk) return r;
-    k.init = true;
-  } else {
-    // refresh HX for the current potential, then Rayleigh-Ritz in span(X)
-    if ((r = apply_h_device(h, spin, ik, k.V, n, nd, k.HV, n, precision, s)) != kOk) return r;
-    happ += nd;
-    if ((r = rayleigh_ritz(h, k, nd, nd)) != kOk) return r;
-  }
-  const unsigned gx = (unsigned)std::min<long>(64, blocks_for(n));
-  std::vector<double> rn(nd);
-  double2* T = k.V + n * nd;
-  double2* HT = k.HV + n * nd;
-  // diagonal of H for the preconditioner: |k+G|^2 term + V_eff(G=0) = mean V_eff(r)
-  double vsum = 0.0;
-  if ((r = reduce_host(h, h.veff_r[spin], nullptr, h.g.N, 0, vsum)) != kOk) return r;
-  const double v0 = vsum / (double)h.g.N;
-  iters = 0;
-  for (;;) {
-    PW_CUDA_TRY(cudaMemcpyAsync(st->lam, k.evals.data(), nd * sizeof(double), cudaMemcpyHostToDevice, s));
-    k_resid_precond<<<dim3(gx, nd), 256, 0, s>>>(k.V, k.HV, T, n, (int)n, st->lam, h.kp[ik].kinetic, v0,
-                                                 st->partials); count_launch();
-    k_col_final<<<1, 256, 0, s>>>(st->partials, (int)gx, nd, st->col_sums); count_launch();
-    PW_CUDA_TRY(cudaMemcpyAsync(rn.data(), st->col_sums, nd * sizeof(double), cudaMemcpyDeviceToHost, s));
-    PW_CUDA_TRY(cudaStreamSynchronize(s));
-    max_res = 0.0;
-    for (int c = 0; c < nconv; ++c) max_res = std::max(max_res, std::sqrt(rn[c]));
-    if (max_res < tol || iters >= max_iter) break;
-    // T <- T - X (X^H T), normalise columns
-    if ((r = zgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, nd, nd, (int)n, k.V, n, T, n, st->Pm, nd)) != kOk) return r;
-    if ((r = zgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, nd, nd, k.V, n, st->Pm, nd, T, n, 1.0, -1.0)) != kOk)
-      return r;
-    k_col_sumsq<<<dim3(gx, nd), 256, 0, s>>>(T, n, (int)n, st->partials); count_launch();
-    k_col_final<<<1, 256, 0, s>>>(st->partials, (int)gx, nd, st->col_sums); count_launch();
-    k_scale_cols_invsqrt<<<dim3(gx, nd), 256, 0, s>>>(T, n, (int)n, st->col_sums); count_launch();
-    if ((r = apply_h_device(h, spin, ik, T, n, nd, HT, n, precision, s)) != kOk) return r;
-    happ += nd;
-    if ((r = rayleigh_ritz(h, k, 2 * nd, nd)) != kOk) return r;
-    ++iters;
-  }
   PW_CUDA_TRY(cudaGetLastError());
   return kOk;
 }
@@ -821,25 +636,34 @@ Status scf_run(Handle& h, const ScfParams& p, const double* rho_init, ScfResult&
   for (int k = 0; k < h.n_k; ++k) wk[k] = h.kp[k].weight;
   const double spin_factor = 2.0;
   bool have_prev = false;
+  // mixed form: FP64 H|psi> from the first iteration whose input density rms
+  // is below fp64_switch, or once the reduced-precision phase stops reducing
+  // it (two iterations without a 30 % improvement on the best so far: the
+  // precision floor of the FP32/BF16 operator), for the rest of the solve
+  bool fp64_locked = p.precision != 1;
+  double best_delta = INFINITY;
+  int stalled = 0;
   double e_prev = 0.0, last_delta = INFINITY, max_res_all = 0.0;
   long happ = 0;
   std::vector<std::vector<double>> ev(h.n_k), occ(h.n_k);
   for (int iter = 0; iter < p.max_iter; ++iter) {
     PotEnergies ein;
     if ((r = potentials(h, st->rho_in, true, ein)) != kOk) return r;
-    const int prec = (p.precision == 1 && !(last_delta < p.fp64_switch)) ? 1 : 0;
-    double tol = std::max(p.diag_tol, std::min(1e-3, 0.1 * (std::isfinite(last_delta) ? last_delta : 1.0)));
-    // FP32 H|psi> carries ~1e-7 relative noise: residuals below this floor
-    // (eV) are not reachable in that phase and would only burn iterations
-    if (prec == 1) tol = std::max(tol, kFp32ResidualFloor);
+    if (!fp64_locked && (last_delta < p.fp64_switch || stalled >= 2)) fp64_locked = true;
+    const int prec = fp64_locked ? 0 : 1;
+    const double tol = std::max(p.diag_tol, std::min(1e-3, 0.1 * (std::isfinite(last_delta) ? last_delta : 1.0)));
+    // preconditioner shift: V_eff(G = 0) = mean of V_eff(r)
+    double vsum = 0.0;
+    if ((r = reduce_host(h, h.veff_r[0], nullptr, N, 0, vsum)) != kOk) return r;
+    const double v0 = vsum / (double)N;
     max_res_all = 0.0;
     for (int ik = 0; ik < h.n_k; ++ik) {
-      int its = 0;
-      double mres = 0.0;
-      if ((r = davidson(h, 0, ik, tol, iter == 0 ? 4 * p.diag_max_iter : p.diag_max_iter, nb, prec, happ, its,
-                        mres)) != kOk)
+      EigStats es;
+      if ((r = lobpcg(h, st->ew, st->ks[ik], 0, ik, v0, tol, iter == 0 ? 4 * p.diag_max_iter : p.diag_max_iter, nb,
+                      prec, es)) != kOk)
         return r;
-      max_res_all = std::max(max_res_all, mres);
+      happ += es.happ;
+      max_res_all = std::max(max_res_all, es.max_res);
       ev[ik].assign(st->ks[ik].evals.begin(), st->ks[ik].evals.begin() + nb);
     }
     const double ef = fermi_level(ev, wk, h.n_electrons, p.sigma, p.smearing, spin_factor);
@@ -853,6 +677,14 @@ Status scf_run(Handle& h, const ScfParams& p, const double* rho_init, ScfResult&
     const double dv = h.omega / (double)N;
     const double delta = std::sqrt(dsq * dv / h.omega);
     last_delta = delta;
+    if (!fp64_locked) {
+      if (delta < 0.7 * best_delta) {
+        best_delta = delta;
+        stalled = 0;
+      } else {
+        ++stalled;
+      }
+    }
     PotEnergies eout;
     if ((r = potentials(h, st->rho_out, false, eout)) != kOk) return r;
     double e_band = 0.0;
@@ -919,7 +751,7 @@ Status scf_run(Handle& h, const ScfParams& p, const double* rho_init, ScfResult&
 // ---------------------------------------------------------------------------
 
 Status eigensolve_k(Handle& h, int spin, int ik, int n_bands, double tol, int max_iter, const double* psi_in,
-                    double* evals, double* psi_out, int* iters, double* max_res) {
+                    double* evals, double* psi_out, int* iters, double* max_res, int precision) {
   if (ik < 0 || ik >= h.n_k || spin < 0 || spin >= h.nspin) return fail(kInvalid, "eigensolve: index out of range");
   if (n_bands < 1 || n_bands > h.n_pw) return fail(kInvalid, "eigensolve: n_bands out of range");
   const int extra = std::max(2, n_bands / 8);
@@ -927,23 +759,22 @@ Status eigensolve_k(Handle& h, int spin, int ik, int n_bands, double tol, int ma
   Status r = ensure_state(h, n_bands, nd, 1);
   if (r != kOk) return r;
   ScfState* st = h.scf;
-  KState& k = st->ks[(size_t)spin * h.n_k + ik];
+  EigVecs& k = st->ks[(size_t)spin * h.n_k + ik];
   const long n = h.n_pw;
+  double vsum = 0.0;
+  if ((r = reduce_host(h, h.veff_r[spin], nullptr, h.g.N, 0, vsum)) != kOk) return r;
+  const double v0 = vsum / (double)h.g.N;
+  k.init = false;
   if (psi_in) {
     // warm start: given n_bands columns, remaining columns from the cold-start recipe
-    k.init = false;
-    long happ0 = 0;
-    int it0 = 0;
-    double mr0 = 0.0;
-    if ((r = davidson(h, spin, ik, 1e300, 0, n_bands, 0, happ0, it0, mr0)) != kOk) return r;
+    EigStats e0;
+    if ((r = lobpcg(h, st->ew, k, spin, ik, v0, 1e300, 0, n_bands, precision, e0)) != kOk) return r;
     PW_CUDA_TRY(cudaMemcpyAsync(k.V, psi_in, n * n_bands * sizeof(double2), cudaMemcpyHostToDevice, h.stream));
-  } else {
-    k.init = false;
   }
-  long happ = 0;
-  int its = 0;
-  double mres = 0.0;
-  if ((r = davidson(h, spin, ik, tol, max_iter, n_bands, 0, happ, its, mres)) != kOk) return r;
+  EigStats es;
+  if ((r = lobpcg(h, st->ew, k, spin, ik, v0, tol, max_iter, n_bands, precision, es)) != kOk) return r;
+  const int its = es.iters;
+  const double mres = es.max_res;
   for (int b = 0; b < n_bands; ++b) evals[b] = k.evals[b];
   if (psi_out)
     PW_CUDA_TRY(cudaMemcpyAsync(psi_out, k.V, n * n_bands * sizeof(double2), cudaMemcpyDeviceToHost, h.stream));

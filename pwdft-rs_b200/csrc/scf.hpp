@@ -1,4 +1,4 @@
-// SCF loop on the device: block Davidson eigensolver, density, G-space
+// SCF loop on the device: per-k LOBPCG eigensolver (lobpcg.cu), density, G-space
 // symmetrisation, Hartree + LDA potentials, energies and Anderson/Kerker
 // mixing (scf.cu).
 #pragma once
@@ -46,7 +46,7 @@ Status scf_run(Handle& h, const ScfParams& p, const double* rho_init, ScfResult&
 
 // Pieces exposed through the C-ABI for parity tests.
 Status eigensolve_k(Handle& h, int spin, int ik, int n_bands, double tol, int max_iter, const double* psi_in,
-                    double* evals, double* psi_out, int* iters, double* max_res);
+                    double* evals, double* psi_out, int* iters, double* max_res, int precision);
 Status density_from_host(Handle& h, int n_bands, const double* occ, const double* psi_all, double* rho_out);
 Status symmetrize_host(Handle& h, double* rho);
 Status potentials_host(Handle& h, const double* rho, double* veff_g, double* energies);

@@ -19,14 +19,25 @@ INCLUDE = os.path.join(os.path.dirname(PKG_ROOT), "include")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libpwgpu.so")
 
-SOURCES = ["api.cu", "hpsi.cu", "linalg.cu", "scf.cu", "noalloc.cu"]
+SOURCES = ["api.cu", "hpsi.cu", "linalg.cu", "lobpcg.cu", "scf.cu", "noalloc.cu", "gemm_bf16.cu", "nl_mixed.cu"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
     "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
-    "--expt-relaxed-constexpr",
+    "--expt-relaxed-constexpr", "-diag-suppress", "20012",
 ]
+
+
+def cutlass_root() -> str:
+    """CUTLASS/CuTe header tree vendored with the installed flashinfer wheel."""
+    import sysconfig
+    for base in (sysconfig.get_paths()["purelib"], sysconfig.get_paths()["platlib"]):
+        for rel in ("flashinfer/data/cutlass", "tilelang/3rdparty/cutlass"):
+            p = os.path.join(base, rel)
+            if os.path.isdir(os.path.join(p, "include", "cute")):
+                return p
+    raise RuntimeError("CUTLASS headers not found (flashinfer/data/cutlass)")
 
 
 def nvcc_path() -> str:
@@ -46,7 +57,9 @@ def build(verbose: bool = False, extra_flags=None) -> str:
         deps = [path] + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".hpp"))]
         deps.append(os.path.join(INCLUDE, "pwgpu.h"))
         if not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(d) for d in deps):
-            cmd = [nvcc, *NVCC_FLAGS, *(extra_flags or []), "-I", INCLUDE, "-c", path, "-o", obj]
+            cut = cutlass_root()
+            cmd = [nvcc, *NVCC_FLAGS, *(extra_flags or []), "-I", INCLUDE, "-I", os.path.join(cut, "include"),
+                   "-I", os.path.join(cut, "tools", "util", "include"), "-c", path, "-o", obj]
             if verbose:
                 print(" ".join(cmd))
             subprocess.run(cmd, check=True)
