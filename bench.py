@@ -111,6 +111,17 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
+def max_over_ranks(values, dist, device):
+    """Element-wise maximum of per-rank timings (every rank gets the result);
+    identity without a process group."""
+    if dist is None:
+        return list(values)
+    import torch
+    t = torch.tensor(list(values), device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def scf_kwargs():
     from pwgpu.config3 import FP64_SWITCH, SCF_KW
     kw = dict(SCF_KW)
@@ -160,7 +171,7 @@ def run_reference(args, world, rank):
     from pwgpu.config3 import config3_system
     from pwgpu.upf import load_upf
     sys_ = config3_system(load_upf(SI_UPF))
-    h_apps = 84240  # band applications of the FP64 GPU solve of this cell (measured, bench "fp64" line)
+    h_apps = 22787  # band applications of the FP64 GPU solve of this cell (measured, bench "accuracy" block)
     vals = []
     base = None
     for i in range(args.warmup + args.steps):
@@ -331,7 +342,8 @@ def main():
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(hstream)
         t0 = time.perf_counter()
-        res, ev, rho, _ = dev.scf_run(sys_.rho_init_r, nb, precision=prec, fp64_switch=sw, **kw)
+        res, ev, rho, _ = dev.scf_run(sys_.rho_init_r, nb, precision=prec, fp64_switch=sw,
+                                      raise_on_unconverged=False, **kw)
         t1 = time.perf_counter()
         e1.record(hstream)
         torch.cuda.synchronize()
@@ -350,10 +362,7 @@ def main():
     ms = statistics.mean(r[0] for r in runs)
     wall = statistics.mean(r[1] for r in runs)
     ms64 = statistics.mean(r[0] for r in fp64_runs)
-    if dist:
-        t = torch.tensor([ms, wall, ms64], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, wall, ms64 = t.tolist()
+    ms, wall, ms64 = max_over_ranks([ms, wall, ms64], dist, f"cuda:{local}")
     rm, em = runs[-1][2], runs[-1][3]
     r64, e64 = fp64_runs[-1][2], fp64_runs[-1][3]
     n_at = len(sys_.crystal.atoms)
@@ -363,7 +372,11 @@ def main():
                 "e_total_mixed_ev": rm["total_energy"], "e_total_fp64_ev": r64["total_energy"],
                 "iterations_mixed": rm["n_iterations"], "iterations_fp64": r64["n_iterations"],
                 "h_band_applications_mixed": rm["h_applications"],
-                "h_band_applications_fp64": r64["h_applications"]}
+                "h_band_applications_fp64": r64["h_applications"],
+                "converged_mixed": bool(rm["converged"]), "converged_fp64": bool(r64["converged"])}
+    accuracy["gate_pass"] = bool(accuracy["converged_mixed"] and accuracy["converged_fp64"]
+                                 and accuracy["dE_total_per_atom_ha"] <= 1e-6
+                                 and accuracy["max_eigenvalue_dev_ha"] <= 1e-5)
 
     kb, roofline, kb_cfg = kernel_bench(local, 5, 3, flush, hbm_peak, peak_kind)
 

@@ -88,6 +88,9 @@ typedef struct pwgpu_system {
 typedef struct pwgpu_options {
   int32_t device;     /* CUDA device ordinal */
   int32_t precision;  /* PWGPU_PRECISION_FP64 or PWGPU_PRECISION_MIXED */
+  int32_t lanes;      /* concurrent (spin, k) eigensolves inside pwgpu_scf_run, each on its own
+                         stream (the reference's rayon loop over k, driver_spin.rs:356-384);
+                         0 = min(nspin * n_k, 8), 1 = one block at a time */
 } pwgpu_options;
 
 /* Message of the calling thread's most recent failure ("" if none). */
@@ -142,8 +145,8 @@ pwgpu_status pwgpu_get_stream(const pwgpu_handle* h, void** stream);
 pwgpu_status pwgpu_get_dims(const pwgpu_handle* h, int32_t* n_pw, int64_t* n_grid, int32_t* n_ch);
 
 /* SCF controls: the fields of ScfParams (scf/mod.rs:228-252) that the
- * unpolarised loop reads, plus the eigensolver and precision controls of
- * the matrix-free form. */
+ * unpolarised and spin-polarised loops read, plus the eigensolver and
+ * precision controls of the matrix-free form. */
 typedef struct pwgpu_scf_params {
   int32_t n_bands;
   int32_t max_iter;
@@ -156,11 +159,15 @@ typedef struct pwgpu_scf_params {
   int32_t smearing;         /* 0 Fermi-Dirac, 1 Gaussian, 2 Methfessel-Paxton, 3 cold, 4 fixed */
   double smearing_sigma;    /* eV */
   double diag_tol;          /* eigen-residual floor |H psi - e psi|, eV */
-  int32_t diag_max_iter;    /* Davidson iterations per SCF step */
+  int32_t diag_max_iter;    /* LOBPCG block steps per SCF step */
   int32_t diag_extra_bands; /* < 0: automatic */
   int32_t precision;        /* PWGPU_PRECISION_* for H|psi> */
   double fp64_switch;       /* mixed: FP64 H|psi> once the density rms < this */
   int32_t verbose;          /* per-iteration line on stderr */
+  /* nspin = 2 only (driver_spin.rs:125-167, 400-466): */
+  double starting_magnetization; /* atom average of the per-species fractions; rho splits (1 +- m)/2 */
+  int32_t fixed_magnetization;   /* 1: tot_magnetization fixes N_up - N_down (one Fermi level per spin) */
+  double tot_magnetization;
 } pwgpu_scf_params;
 
 /* ScfResult (scf/mod.rs:269-322) scalars. */
@@ -174,12 +181,15 @@ typedef struct pwgpu_scf_result {
   double max_residual;      /* largest eigen-residual of the last eigensolve */
 } pwgpu_scf_result;
 
-/* Run the SCF loop from rho_init_r (N doubles, e/Å^3).  Replaces
- * run_scf_unpolarized (scf/driver.rs:266-742) with the dense per-k
- * eigensolve replaced by block Davidson on the device.  Outputs may be
- * NULL: eigenvalues n_k x n_bands (eV), rho_r_out N, rho_g_basis_out n_pw
- * complex (rho(G) in basis order, as ScfResult::rho_g).
- * Returns PWGPU_E_NOT_CONVERGED (result filled) if max_iter is reached. */
+/* Run the SCF loop from rho_init_r (N doubles, e/Å^3, the total start
+ * density).  Replaces run_scf_unpolarized (scf/driver.rs:266-742) for
+ * nspin = 1 and run_scf_spin (scf/driver_spin.rs:114-839) for nspin = 2,
+ * with the dense per-k eigensolve replaced by LOBPCG on the device.
+ * Outputs may be NULL: eigenvalues nspin x n_k x n_bands (eV; spin up k-points
+ * first, as ScfResult::eigenvalues), rho_r_out nspin x N (up then down for
+ * nspin = 2), rho_g_basis_out n_pw complex (total rho(G) in basis order, as
+ * ScfResult::rho_g).  Returns PWGPU_E_NOT_CONVERGED (result filled) if
+ * max_iter is reached. */
 pwgpu_status pwgpu_scf_run(pwgpu_handle* h, const pwgpu_scf_params* params, const double* rho_init_r,
                            pwgpu_scf_result* result, double* eigenvalues, double* rho_r_out,
                            double* rho_g_basis_out);
@@ -204,6 +214,18 @@ pwgpu_status pwgpu_symmetrize(pwgpu_handle* h, double* rho_r);
  * and sets it as the H|psi> potential of spin 0; energies[3] = E_H, E_xc,
  * int rho_val v_xc (eV). */
 pwgpu_status pwgpu_potentials(pwgpu_handle* h, const double* rho_r, double* veff_g, double* energies);
+
+/* One density-mixing step (Mixer::mix, scf/mixing/mod.rs:281-287, for the
+ * Plain and Kerker modes: AndersonMixer::mix, mixing/anderson.rs:170-266).
+ * channel 0 or 1 selects one of two independent histories on the handle (the
+ * CCMX total / magnetisation pair of driver_spin.rs:792-826).  rho_in,
+ * rho_out, rho_next: N doubles on the host (rho_next may alias rho_in).
+ * kerker != 0 preconditions the residual with G^2/(G^2 + q_tf^2), q_tf in
+ * Å^-1 (<= 0: Thomas-Fermi estimate, kerker.rs:41-49).  The first call
+ * after pwgpu_mix_reset (or after a change of ndim) starts a new history. */
+pwgpu_status pwgpu_mix(pwgpu_handle* h, int32_t channel, const double* rho_in, const double* rho_out,
+                       double* rho_next, double beta, int32_t ndim, int32_t kerker, double q_tf);
+pwgpu_status pwgpu_mix_reset(pwgpu_handle* h);
 
 /* Local part of H|psi> (kinetic diagonal + V_eff through the FFT pipeline;
  * no Kleinman-Bylander term) on device pointers, allocating nothing.  No

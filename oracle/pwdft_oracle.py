@@ -456,3 +456,120 @@ def run_scf_unpolarized(sys, n_bands, max_iter=100, conv_threshold=1e-6, energy_
         rho = mixer.mix(rho, rho_new)
         rho_g = density_r_to_g(rho, dims)
     raise RuntimeError(f"SCF did not converge in {max_iter} iterations (delta={delta})")
+
+
+# ---------------------------------------------------------------------------
+# Spin-polarised SCF driver (driver_spin.rs:114-839)
+# ---------------------------------------------------------------------------
+
+@dataclass
+class OracleSpinResult:
+    total_energy: float
+    harris_foulkes_energy: float
+    fermi_energy: float
+    eigenvalues: list          # [up k0..k_{n-1}, down k0..k_{n-1}]
+    n_iterations: int
+    final_delta: float
+    rho_up: np.ndarray
+    rho_down: np.ndarray
+    magnetization: float
+    entropy_ts: float = 0.0
+    history: list = field(default_factory=list)
+
+
+def run_scf_spin(sys, n_bands, max_iter=100, conv_threshold=1e-6, energy_threshold=1e-5, mixing_beta=0.3,
+                 mixing_ndim=8, smearing="fermi_dirac", sigma=0.01, kerker=False, q_tf=None,
+                 starting_magnetization=0.0, tot_magnetization=None, verbose=False):
+    """LSDA SCF of driver_spin.rs:114-839 with dense diagonalisation.
+
+    starting_magnetization: the atom average of the per-species fractions
+    (driver_spin.rs:125-167); the start density splits as (1 +- m)/2.
+    Mixing is CCMX: Anderson (+ Kerker when asked) on rho_up + rho_down and
+    plain Anderson on rho_up - rho_down (driver_spin.rs:792-826)."""
+    dims = sys.dims
+    omega = sys.omega
+    weights = list(sys.kpt_weights)
+    n = sys.n_grid
+    dv = omega / n
+    spin_factor = 1.0
+    if sys.symmetry.n_ops > 1:
+        src, arg = gather_map(dims, [(op.rotation, op.translation) for op in sys.symmetry.operations])
+    else:
+        src = arg = np.zeros((1, 0))
+    kw = None
+    if kerker:
+        q2 = q_tf * q_tf if q_tf is not None else auto_q_tf_squared(sys.n_electrons, omega)
+        kw = np.where(sys.g_squared < G2_ZERO_THRESHOLD, 0.0, sys.g_squared / (sys.g_squared + q2))
+    mix_tot = AndersonMixer(mixing_beta, mixing_ndim, dims, kw)
+    mix_mag = AndersonMixer(mixing_beta, mixing_ndim, dims, None)
+    d_dense = [p.d_dense() for p in sys.projectors]
+    core = sys.rho_core_r
+    core_half = core / 2.0 if core.size else core
+    up = sys.rho_init_r * (1.0 + starting_magnetization) / 2.0
+    dn = sys.rho_init_r * (1.0 - starting_magnetization) / 2.0
+    e_prev = None
+    hist = []
+    nk = len(sys.kpoints)
+
+    def diag(veff):
+        ev, ps = [], []
+        for ik in range(nk):
+            h = dense_hamiltonian(sys.basis.miller, sys.kinetic[ik], veff, dims, sys.projectors[ik].b, d_dense[ik])
+            w, v = lowest_eigenpairs(h, n_bands)
+            ev.append(w)
+            ps.append(v)
+        return ev, ps
+
+    for it in range(max_iter):
+        tot = up + dn
+        tot_g = density_r_to_g(tot, dims)
+        vh = hartree(tot_g, sys.g_squared)
+        rxu, rxd = add_core(up, core_half), add_core(dn, core_half)
+        exc_in, vxu_in, vxd_in = lsda_xc(rxu, rxd)
+        ev_up, ps_up = diag(sys.v_local_g + vh + density_r_to_g(vxu_in, dims))
+        ev_dn, ps_dn = diag(sys.v_local_g + vh + density_r_to_g(vxd_in, dims))
+        ev_all = ev_up + ev_dn
+        w_all = weights + weights
+        if tot_magnetization is None:
+            ef = find_fermi_energy(ev_all, w_all, sys.n_electrons, sigma, smearing, spin_factor)
+            ef_up = ef_dn = ef
+        else:
+            n_up_t = 0.5 * (sys.n_electrons + tot_magnetization)
+            n_dn_t = (sys.n_electrons - tot_magnetization) / 2.0
+            ef_up = find_fermi_energy(ev_up, weights, n_up_t, sigma, smearing, spin_factor)
+            ef_dn = find_fermi_energy(ev_dn, weights, n_dn_t, sigma, smearing, spin_factor)
+            ef = 0.5 * (ef_up + ef_dn)
+        occ_up = [spin_factor * occupation01(smearing, e, ef_up, sigma) for e in ev_up]
+        occ_dn = [spin_factor * occupation01(smearing, e, ef_dn, sigma) for e in ev_dn]
+        n_up = float(sum(np.sum(o) * w for o, w in zip(occ_up, weights)))
+        n_dn = float(sum(np.sum(o) * w for o, w in zip(occ_dn, weights)))
+        up_new = compute_density(sys.g_to_fft, dims, ps_up, occ_up, weights, n_up, omega)
+        dn_new = compute_density(sys.g_to_fft, dims, ps_dn, occ_dn, weights, n_dn, omega)
+        if src.shape[0] > 1:
+            up_new = symmetrize_density(up_new, dims, src, arg)
+            dn_new = symmetrize_density(dn_new, dims, src, arg)
+        delta = max(density_diff(up, up_new, omega), density_diff(dn, dn_new, omega))
+        tot_new = up_new + dn_new
+        tot_new_g = density_r_to_g(tot_new, dims)
+        exc_o, vxu_o, vxd_o = lsda_xc(add_core(up_new, core_half), add_core(dn_new, core_half))
+        e_vxc_o = float(np.sum((up_new * vxu_o + dn_new * vxd_o) * dv))
+        e_xc_o = float(np.sum(add_core(tot_new, core) * exc_o * dv))
+        e_band = float(sum(np.sum(o * w * e) for o, w, e in zip(occ_up + occ_dn, w_all, ev_all)))
+        ts = entropy_ts(ev_all, w_all, ef, sigma, smearing, spin_factor)
+        e_tot = e_band - hartree_energy(tot_new_g, sys.g_squared, omega) + (e_xc_o - e_vxc_o) + sys.e_ewald - ts
+        e_xc_i = float(np.sum(add_core(tot, core) * exc_in * dv))
+        e_vxc_i = float(np.sum((up * vxu_in + dn * vxd_in) * dv))
+        e_hf = e_band - hartree_energy(tot_g, sys.g_squared, omega) + (e_xc_i - e_vxc_i) + sys.e_ewald - ts
+        de = None if e_prev is None else abs(e_tot - e_prev)
+        e_prev = e_tot
+        mag = abs(n_up - n_dn)
+        hist.append((it, e_tot, delta, mag))
+        if verbose:
+            print(f"iter {it:3d} E={e_tot:.10f} dE={de} drho={delta:.3e} M={mag:.6f}")
+        if delta < conv_threshold and de is not None and de < energy_threshold:
+            return OracleSpinResult(e_tot, e_hf, ef, ev_all, it + 1, delta, up_new, dn_new, mag, ts, hist)
+        t_mix = mix_tot.mix(tot, tot_new)
+        m_mix = mix_mag.mix(up - dn, up_new - dn_new)
+        up = 0.5 * (t_mix + m_mix)
+        dn = 0.5 * (t_mix - m_mix)
+    raise RuntimeError(f"spin SCF did not converge in {max_iter} iterations (delta={delta})")

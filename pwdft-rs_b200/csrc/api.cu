@@ -26,6 +26,8 @@ Status fail(int code, const std::string& msg) {
   return (Status)code;
 }
 
+std::string last_error_message() { return t_last_error; }
+
 template <typename T> static Status upload(T** dst, const T* src, size_t count) {
   const size_t n = std::max<size_t>(count, 1);
   cudaError_t e = cudaMalloc((void**)dst, n * sizeof(T));
@@ -73,6 +75,8 @@ static Status create(const pwgpu_system* s, const pwgpu_options* o, pwgpu_handle
   h.device = o ? o->device : 0;
   h.trace = std::getenv("PWGPU_TRACE") != nullptr;
   ph->precision = o ? o->precision : 0;
+  h.lanes = o ? o->lanes : 0;
+  if (h.lanes < 0) return fail(kInvalid, "pwgpu_create: lanes must be >= 0");
   PW_CUDA_TRY(cudaSetDevice(h.device));
   h.n_pw = s->n_pw;
   h.n_k = s->n_k;
@@ -277,6 +281,11 @@ pwgpu_status pwgpu_scf_run(pwgpu_handle* ph, const pwgpu_scf_params* p, const do
   q.precision = p->precision;
   q.fp64_switch = p->fp64_switch;
   q.verbose = p->verbose;
+  q.starting_magnetization = p->starting_magnetization;
+  q.fixed_magnetization = p->fixed_magnetization;
+  q.tot_magnetization = p->tot_magnetization;
+  if (q.starting_magnetization < -1.0 || q.starting_magnetization > 1.0)
+    return fail(kInvalid, "pwgpu_scf_run: starting_magnetization must lie in [-1, 1]");
   if (q.smearing < 0 || q.smearing > 4) return fail(kInvalid, "pwgpu_scf_run: unknown smearing scheme");
   if (q.mixing_mode < 0 || q.mixing_mode > 1) return fail(kInvalid, "pwgpu_scf_run: unknown mixing mode");
   ScfResult r;
@@ -309,6 +318,18 @@ pwgpu_status pwgpu_eigensolve(pwgpu_handle* ph, int32_t spin, int32_t ik, int32_
   PW_CUDA_TRY(cudaSetDevice(ph->h.device));
   return eigensolve_k(ph->h, spin, ik, n_bands, tol, max_iter, psi_in, evals, psi_out, iters, max_residual,
                       ph->precision);
+}
+
+pwgpu_status pwgpu_mix(pwgpu_handle* ph, int32_t channel, const double* rho_in, const double* rho_out,
+                       double* rho_next, double beta, int32_t ndim, int32_t kerker, double q_tf) {
+  if (!ph || !rho_in || !rho_out || !rho_next) return fail(kInvalid, "pwgpu_mix: NULL argument");
+  PW_CUDA_TRY(cudaSetDevice(ph->h.device));
+  return mix_host(ph->h, channel, rho_in, rho_out, rho_next, beta, ndim, kerker, q_tf);
+}
+
+pwgpu_status pwgpu_mix_reset(pwgpu_handle* ph) {
+  if (!ph) return fail(kInvalid, "pwgpu_mix_reset: NULL handle");
+  return mix_reset(ph->h);
 }
 
 pwgpu_status pwgpu_density(pwgpu_handle* ph, int32_t n_bands, const double* occ, const double* psi, double* rho_r) {

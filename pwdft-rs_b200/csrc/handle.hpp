@@ -14,6 +14,7 @@
 namespace pwgpu {
 
 Status fail(int code, const std::string& msg);  // records the thread's last error, returns code
+std::string last_error_message();                // the calling thread's last recorded error
 
 // Sphere <-> grid maps and per-axis FFT plans.  Grid flat index is
 // (i0*d1 + i1)*d2 + i2, x slowest, as in the reference's miller_to_idx.
@@ -80,6 +81,7 @@ struct Handle {
   struct ScfState* scf = nullptr;  // device state of the SCF loop (scf.cu)
   struct NlMixed* nlm = nullptr;   // split projector operands of the mixed form (nl_mixed.cu)
   bool trace = false;  // per-iteration eigensolver lines on stderr (PWGPU_TRACE set at create)
+  int lanes = 0;       // concurrent (spin, k) eigensolves in the SCF loop; 0 = automatic
   std::string last_error;
 };
 

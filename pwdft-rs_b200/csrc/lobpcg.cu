@@ -459,7 +459,8 @@ Status lobpcg(Handle& h, EigWork& w, EigVecs& k, int spin, int ik, double v0, do
   if (!k.init) {
     // start: unit vectors on the nd lowest |k+G|^2 plus seeded noise
     std::vector<double> kin(n);
-    PW_CUDA_TRY(cudaMemcpy(kin.data(), h.kp[ik].kinetic, n * sizeof(double), cudaMemcpyDeviceToHost));
+    PW_CUDA_TRY(cudaMemcpyAsync(kin.data(), h.kp[ik].kinetic, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    PW_CUDA_TRY(cudaStreamSynchronize(s));
     std::vector<int> order(n);
     for (long i = 0; i < n; ++i) order[i] = (int)i;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return kin[a] < kin[b]; });

@@ -179,7 +179,11 @@ void release_nl_mixed(Handle& h) {
   h.nlm = nullptr;
 }
 
-bool nl_mixed_eligible(const Handle& h) { return h.n_ch >= 32 && h.n_pw >= 512; }
+// Below a few hundred channels and a few thousand plane waves the projector
+// products are a handful of 128x128 tiles: the split/cast kernels and
+// launches of the 3xBF16 form then cost more than one FP64 ZGEMM (measured on
+// the 8-atom cells: 64-144 channels, 1,045-3,791 plane waves).
+bool nl_mixed_eligible(const Handle& h) { return h.n_ch >= 256 && h.n_pw >= 4096; }
 
 static Status nl_alloc(void** p, size_t bytes) {
   cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 16));

@@ -12,9 +12,12 @@
 #include <cublas_v2.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <memory>
 #include <random>
+#include <thread>
 #include <vector>
 
 #include "handle.hpp"
@@ -28,7 +31,6 @@ namespace {
 
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kHaToEv = 27.211386245988;
-constexpr double kRyToEv = 13.605693122994;
 constexpr double kBohrToAng = 0.529177210903;
 constexpr double kBohr3ToAng3 = kBohrToAng * kBohrToAng * kBohrToAng;
 constexpr double kE2 = 14.399645351950548;
@@ -212,18 +214,109 @@ __global__ void k_sub(const double* __restrict__ a, const double* __restrict__ b
   if (i < n) out[i] = a[i] - b[i];
 }
 
-// dot((r_i - r_l), (r_j - r_l)) partials, or dot(r_i - r_l, r_l) when j < 0
-__global__ void k_dr_dot(const double* __restrict__ ri, const double* __restrict__ rj, const double* __restrict__ rl,
-                         long n, double* __restrict__ partials) {
+// All DIIS inner products of one mixing step in one launch.  With
+// dr_i = res[i] - res[mm] (i < mm), blockIdx.y = i * (mm + 1) + jj:
+// jj = 0 gives dot(dr_i, res[mm]), jj = j + 1 (j <= i) gives dot(dr_i, dr_j);
+// partials[blockIdx.y * gridDim.x + blockIdx.x] (fixed summation order).
+__global__ void k_dr_dots(const double* const* __restrict__ res, int mm, long n, double* __restrict__ partials) {
   __shared__ double sh[32];
+  const int i = blockIdx.y / (mm + 1), jj = blockIdx.y % (mm + 1), j = jj - 1;
+  if (j > i) {
+    if (threadIdx.x == 0) partials[(long)blockIdx.y * gridDim.x + blockIdx.x] = 0.0;
+    return;
+  }
+  const double* ri = res[i];
+  const double* rl = res[mm];
+  const double* rj = j >= 0 ? res[j] : nullptr;
   double acc = 0.0;
-  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-    const double a = ri[i] - rl[i];
-    const double b = rj ? rj[i] - rl[i] : rl[i];
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+    const double a = ri[t] - rl[t];
+    const double b = rj ? rj[t] - rl[t] : rl[t];
     acc += a * b;
   }
   acc = block_sum(acc, sh);
-  if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+  if (threadIdx.x == 0) partials[(long)blockIdx.y * gridDim.x + blockIdx.x] = acc;
+}
+
+// sums[c] = sum of the nblk partials of slot c (fixed order)
+__global__ void k_slot_sums(const double* __restrict__ partials, int nblk, int nslots, double* __restrict__ sums) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nslots) return;
+  double acc = 0.0;
+  for (int b = 0; b < nblk; ++b) acc += partials[(long)c * nblk + b];
+  sums[c] = acc;
+}
+
+// LSDA (xc.rs:374-596): von Barth-Hedin spin interpolation of PZ81 and
+// spin-scaled Slater exchange on rho_sigma + core/2 (add_core_density
+// clamp when a core is present).  Writes V_xc per channel; partial sums of
+// rho_xc_total * exc (rho_xc_total = max(up + down + core, 0)) and of
+// up * v_up + down * v_down (driver_spin.rs:572-610).
+__global__ void k_lsda(const double* __restrict__ up, const double* __restrict__ dn, const double* __restrict__ core,
+                       long n, double* __restrict__ vup_out, double* __restrict__ vdn_out,
+                       double* __restrict__ part_exc, double* __restrict__ part_vxc) {
+  __shared__ double sh[32];
+  double a1 = 0.0, a2 = 0.0;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double u = up[i], d = dn[i];
+    double ru = u, rd = d, rt = u + d;
+    if (core) {
+      const double c = core[i];
+      ru = fmax(u + 0.5 * c, 0.0);
+      rd = fmax(d + 0.5 * c, 0.0);
+      rt = fmax(u + d + c, 0.0);
+    }
+    const double rho = ru + rd;
+    double exc = 0.0, vu = 0.0, vd = 0.0;
+    if (rho >= kRhoFloor) {
+      const double rub = ru * kBohr3ToAng3, rdb = rd * kBohr3ToAng3, rb = rho * kBohr3ToAng3;
+      const double exu = rub > kRhoFloor ? -0.75 * cbrt(6.0 * rub / kPi) : 0.0;
+      const double exd = rdb > kRhoFloor ? -0.75 * cbrt(6.0 * rdb / kPi) : 0.0;
+      const double ex = fma(rub, exu, rdb * exd) / rb;
+      const double rs = cbrt(3.0 / (4.0 * kPi * rb));
+      const double zeta = fmin(fmax((ru - rd) / rho, -1.0), 1.0);
+      double ecu, vcu, ecp, vcp;
+      pz_rs(rs, false, ecu, vcu);
+      pz_rs(rs, true, ecp, vcp);
+      const double fden = fma(cbrt(2.0), 2.0, -2.0);
+      const double op = fmax(1.0 + zeta, 0.0), om = fmax(1.0 - zeta, 0.0);
+      const double cop = cbrt(op), com = cbrt(om);
+      const double fz = (cop * op + com * om - 2.0) / fden;
+      const double dfz = (4.0 / 3.0) * (cop - com) / fden;
+      const double ec = ecu + fz * (ecp - ecu);
+      const double vrs = vcu + fz * (vcp - vcu);
+      const double dz = dfz * (ecp - ecu);
+      exc = (ex + ec) * kHaToEv;
+      vu = ((4.0 / 3.0) * exu + fma(1.0 - zeta, dz, vrs)) * kHaToEv;
+      vd = ((4.0 / 3.0) * exd + fma(1.0 + zeta, -dz, vrs)) * kHaToEv;
+    }
+    vup_out[i] = vu;
+    vdn_out[i] = vd;
+    a1 += rt * exc;
+    a2 += u * vu + d * vd;
+  }
+  a1 = block_sum(a1, sh);
+  a2 = block_sum(a2, sh);
+  if (threadIdx.x == 0) {
+    part_exc[blockIdx.x] = a1;
+    part_vxc[blockIdx.x] = a2;
+  }
+}
+
+// out = a + s * b
+__global__ void k_axpy_to(const double* __restrict__ a, const double* __restrict__ b, double s, double* __restrict__ out,
+                          long n) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = a[i] + s * b[i];
+}
+
+// up = (t + m)/2, dn = (t - m)/2 (driver_spin.rs:817-826)
+__global__ void k_unmix_spin(const double* __restrict__ t, const double* __restrict__ m, double* __restrict__ up,
+                             double* __restrict__ dn, long n) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  up[i] = 0.5 * (t[i] + m[i]);
+  dn[i] = 0.5 * (t[i] - m[i]);
 }
 
 // out = sum_i coef[i] * (hin_i + beta * hres_i)
@@ -249,18 +342,86 @@ inline unsigned blocks_for(long n, int t = 256) { return (unsigned)std::max<long
 // state
 // ---------------------------------------------------------------------------
 
+// Concurrent slot for the per-(spin, k) eigensolves (the reference runs them
+// in parallel over k with rayon, driver_spin.rs:356-384): a shallow view of
+// the handle (shared grid maps, projectors and potentials, all read-only
+// during the eigensolve phase) with its own stream, BLAS/solver handles,
+// H|psi> scratch and eigensolver workspace.
+struct Lane {
+  Handle view;
+  EigWork ew;
+};
+
+constexpr int kMaxLanes = 8;
+
+static void release_lane(Lane& L) {
+  Handle& v = L.view;
+  eig_work_release(L.ew);
+  release_nl_mixed(v);
+  auto f = [](void* p) { if (p) cudaFree(p); };
+  f(v.work_a); f(v.work_b); f(v.nl_p); f(v.nl_q); f(v.solver_work); f(v.solver_info);
+  if (v.solver) cusolverDnDestroy(v.solver);
+  if (v.blas) cublasDestroy(v.blas);
+  if (v.stream) cudaStreamDestroy(v.stream);
+  v.work_a = v.work_b = nullptr;
+  v.nl_p = v.nl_q = nullptr;
+  v.solver_work = nullptr;
+  v.solver_info = nullptr;
+  v.solver = nullptr;
+  v.blas = nullptr;
+  v.stream = nullptr;
+}
+
+static Status create_lane(Handle& h, Lane& L, int nd, int nlanes) {
+  L.view = h;  // pointers to the handle's read-only data; lane-owned members reset below
+  Handle& v = L.view;
+  v.stream = nullptr;
+  v.blas = nullptr;
+  v.solver = nullptr;
+  v.solver_work = nullptr;
+  v.solver_work_len = 0;
+  v.solver_info = nullptr;
+  v.work_a = v.work_b = nullptr;
+  v.nl_p = v.nl_q = nullptr;
+  v.nl_cap = 0;
+  v.nlm = nullptr;
+  v.scf = nullptr;
+  v.tmp_grid = nullptr;
+  // lanes share the L2: each keeps a proportionally smaller band chunk
+  v.chunk = std::max(4, h.chunk / nlanes);
+  PW_CUDA_TRY(cudaStreamCreateWithFlags(&v.stream, cudaStreamNonBlocking));
+  if (cublasCreate(&v.blas) != CUBLAS_STATUS_SUCCESS) return fail(kCuda, "cublasCreate failed (lane)");
+  cublasSetStream(v.blas, v.stream);
+  const GridMaps& g = h.g;
+  cudaError_t e = cudaMalloc(&v.work_a, (size_t)v.chunk * g.ncol * g.d[2] * sizeof(double2));
+  if (e == cudaSuccess) e = cudaMalloc(&v.work_b, (size_t)v.chunk * g.Xp * g.d[1] * g.d[2] * sizeof(double2));
+  if (e != cudaSuccess) return fail(kOom, std::string("cudaMalloc (lane): ") + cudaGetErrorString(e));
+  return eig_work_alloc(L.ew, h.n_pw, nd);
+}
+
+// Anderson history of one mixed channel (anderson.rs:170-266): inputs and
+// (preconditioned) residuals, oldest first.
+struct MixHistory {
+  std::vector<double*> hin, hres;
+  int count = 0;
+  double** dev_ptrs = nullptr;  // 2 * ndim
+  double* dev_coef = nullptr;   // ndim
+};
+
 struct ScfState {
-  int nd = 0, nb = 0;
+  int nd = 0, nb = 0, nspin = 1;
   std::vector<EigVecs> ks;  // per (spin, k)
   EigWork ew;
-  double *partials = nullptr, *scal = nullptr, *fw = nullptr;
+  double *partials = nullptr, *scal = nullptr, *fw = nullptr, *mix_partials = nullptr, *mix_sums = nullptr;
   double *rho_in = nullptr, *rho_out = nullptr, *exc = nullptr, *vxc = nullptr, *rtmp = nullptr;
   double2 *cg = nullptr, *cg2 = nullptr, *vh = nullptr;
   double* kerker_w = nullptr;
-  std::vector<double*> hin, hres;
-  double** dev_ptrs = nullptr;
-  double* dev_coef = nullptr;
-  int mix_count = 0;
+  // nspin = 2: down-channel densities and V_xc, (total, magnetisation) in/out
+  double *rho_in_dn = nullptr, *rho_out_dn = nullptr, *vxc_dn = nullptr;
+  double *t_in = nullptr, *t_out = nullptr, *m_in = nullptr, *m_out = nullptr;
+  MixHistory mixh[2];  // 0: rho (or rho_up + rho_down), 1: rho_up - rho_down
+  int mix_cap = 0;     // history depth mix_partials / mix_sums are sized for
+  std::vector<std::unique_ptr<Lane>> lanes;  // empty: one (spin, k) block at a time
 };
 
 template <typename T> static Status salloc(T** p, size_t n) {
@@ -268,6 +429,8 @@ template <typename T> static Status salloc(T** p, size_t n) {
   if (e != cudaSuccess) return fail(kOom, std::string("cudaMalloc (scf): ") + cudaGetErrorString(e));
   return kOk;
 }
+
+static void release_history(MixHistory& mh);
 
 void release_scf(Handle& h) {
   ScfState* st = h.scf;
@@ -277,21 +440,48 @@ void release_scf(Handle& h) {
   eig_work_release(st->ew);
   f(st->partials); f(st->scal); f(st->fw);
   f(st->rho_in); f(st->rho_out); f(st->exc); f(st->vxc); f(st->rtmp);
-  f(st->cg); f(st->cg2); f(st->vh); f(st->kerker_w);
-  for (double* p : st->hin) f(p);
-  for (double* p : st->hres) f(p);
-  f(st->dev_ptrs); f(st->dev_coef);
+  f(st->cg); f(st->cg2); f(st->vh); f(st->kerker_w); f(st->mix_partials); f(st->mix_sums);
+  f(st->rho_in_dn); f(st->rho_out_dn); f(st->vxc_dn); f(st->t_in); f(st->t_out); f(st->m_in); f(st->m_out);
+  for (auto& mh : st->mixh) release_history(mh);
+  for (auto& L : st->lanes) release_lane(*L);
   delete st;
   h.scf = nullptr;
 }
 
+static void release_history(MixHistory& mh) {
+  auto f = [](void* p) { if (p) cudaFree(p); };
+  for (double* p : mh.hin) f(p);
+  for (double* p : mh.hres) f(p);
+  f(mh.dev_ptrs);
+  f(mh.dev_coef);
+  mh = MixHistory();
+}
+
+static Status alloc_history(MixHistory& mh, long N, int ndim) {
+  release_history(mh);
+  Status s;
+  mh.hin.assign(ndim, nullptr);
+  mh.hres.assign(ndim, nullptr);
+  mh.count = 0;
+  for (int i = 0; i < ndim; ++i) {
+    if ((s = salloc(&mh.hin[i], (size_t)N)) != kOk) return s;
+    if ((s = salloc(&mh.hres[i], (size_t)N)) != kOk) return s;
+  }
+  if ((s = salloc(&mh.dev_ptrs, (size_t)2 * std::max(ndim, 1))) != kOk) return s;
+  if ((s = salloc(&mh.dev_coef, (size_t)std::max(ndim, 1))) != kOk) return s;
+  return kOk;
+}
+
+constexpr int kMixBlocks = 128;  // partial sums per DIIS inner product
+
 static Status ensure_state(Handle& h, int nb, int nd, int ndim) {
-  if (h.scf && h.scf->nd == nd && h.scf->nb == nb && (int)h.scf->hin.size() >= ndim) return kOk;
+  if (h.scf && h.scf->nd == nd && h.scf->nb == nb && (int)h.scf->mixh[0].hin.size() == ndim) return kOk;
   release_scf(h);
   ScfState* st = new ScfState();
   h.scf = st;
   st->nd = nd;
   st->nb = nb;
+  st->nspin = h.nspin;
   const long n = h.n_pw, N = h.g.N;
   Status s;
   st->ks.resize((size_t)h.nspin * h.n_k);
@@ -309,14 +499,24 @@ static Status ensure_state(Handle& h, int nb, int nd, int ndim) {
   if ((s = salloc(&st->cg, (size_t)N)) != kOk) return s;
   if ((s = salloc(&st->cg2, (size_t)N)) != kOk) return s;
   if ((s = salloc(&st->vh, (size_t)N)) != kOk) return s;
-  st->hin.assign(ndim, nullptr);
-  st->hres.assign(ndim, nullptr);
-  for (int i = 0; i < ndim; ++i) {
-    if ((s = salloc(&st->hin[i], (size_t)N)) != kOk) return s;
-    if ((s = salloc(&st->hres[i], (size_t)N)) != kOk) return s;
+  const size_t nslots = (size_t)std::max(ndim, 1) * (std::max(ndim, 1) + 1);
+  if ((s = salloc(&st->mix_partials, nslots * kMixBlocks)) != kOk) return s;
+  if ((s = salloc(&st->mix_sums, nslots)) != kOk) return s;
+  st->mix_cap = std::max(ndim, 1);
+  if ((s = alloc_history(st->mixh[0], N, ndim)) != kOk) return s;
+  if (h.nspin == 2) {
+    for (double** p : {&st->rho_in_dn, &st->rho_out_dn, &st->vxc_dn, &st->t_in, &st->t_out, &st->m_in, &st->m_out})
+      if ((s = salloc(p, (size_t)N)) != kOk) return s;
+    if ((s = alloc_history(st->mixh[1], N, ndim)) != kOk) return s;
   }
-  if ((s = salloc(&st->dev_ptrs, (size_t)2 * std::max(ndim, 1))) != kOk) return s;
-  if ((s = salloc(&st->dev_coef, (size_t)std::max(ndim, 1))) != kOk) return s;
+  const int nitems = h.nspin * h.n_k;
+  const int nl = std::min(nitems, h.lanes > 0 ? h.lanes : kMaxLanes);
+  if (nl > 1) {
+    for (int i = 0; i < nl; ++i) {
+      st->lanes.emplace_back(new Lane());
+      if ((s = create_lane(h, *st->lanes.back(), nd, nl)) != kOk) return s;
+    }
+  }
   return kOk;
 }
 
@@ -503,22 +703,26 @@ static std::vector<double> solve_small(std::vector<double> a, std::vector<double
   return x;
 }
 
-// Anderson/Kerker mixing: rho_in <- mix(rho_in, rho_out) in place.
-static Status mix(Handle& h, const ScfParams& p) {
+// One Anderson step of one channel (anderson.rs:170-266; Kerker residual
+// preconditioning kerker.rs:18-35 when `kerker`): next = sum_i c_i (in_i +
+// beta res_i) over the history, DIIS coefficients from the residual
+// differences (linalg.rs:124-152 solve).  `next` may alias `in`.
+static Status mix_channel(Handle& h, MixHistory& mh, const double* in, const double* out, double* next, double beta,
+                          bool kerker) {
   ScfState* st = h.scf;
   const long N = h.g.N;
   const cudaStream_t s = h.stream;
-  const int ndim = p.mixing_ndim;
+  const int ndim = (int)mh.hin.size();
   // rotate history: slot order oldest .. newest kept in vectors
-  if (st->mix_count == ndim) {
-    std::rotate(st->hin.begin(), st->hin.begin() + 1, st->hin.end());
-    std::rotate(st->hres.begin(), st->hres.begin() + 1, st->hres.end());
-    --st->mix_count;
+  if (mh.count == ndim) {
+    std::rotate(mh.hin.begin(), mh.hin.begin() + 1, mh.hin.end());
+    std::rotate(mh.hres.begin(), mh.hres.begin() + 1, mh.hres.end());
+    --mh.count;
   }
-  const int slot = st->mix_count;
-  double* res = st->hres[slot];
-  k_sub<<<blocks_for(N), 256, 0, s>>>(st->rho_out, st->rho_in, res, N); count_launch();
-  if (st->kerker_w) {
+  const int slot = mh.count;
+  double* res = mh.hres[slot];
+  k_sub<<<blocks_for(N), 256, 0, s>>>(out, in, res, N); count_launch();
+  if (kerker && st->kerker_w) {
     k_real_to_cplx<<<blocks_for(N), 256, 0, s>>>(res, st->cg, N); count_launch();
     Status r = fft3d_full(h, st->cg, -1, s);
     if (r != kOk) return r;
@@ -526,26 +730,29 @@ static Status mix(Handle& h, const ScfParams& p) {
     if ((r = fft3d_full(h, st->cg, +1, s)) != kOk) return r;
     k_cplx_real_scaled<<<blocks_for(N), 256, 0, s>>>(st->cg, res, 1.0 / (double)N, N); count_launch();
   }
-  PW_CUDA_TRY(cudaMemcpyAsync(st->hin[slot], st->rho_in, N * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  st->mix_count++;
-  const int m = st->mix_count;
+  PW_CUDA_TRY(cudaMemcpyAsync(mh.hin[slot], in, N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  mh.count++;
+  const int m = mh.count;
+  std::vector<double*> ptrs(2 * m);
+  for (int j = 0; j < m; ++j) { ptrs[j] = mh.hin[j]; ptrs[m + j] = mh.hres[j]; }
+  PW_CUDA_TRY(cudaMemcpyAsync(mh.dev_ptrs, ptrs.data(), 2 * m * sizeof(double*), cudaMemcpyHostToDevice, s));
   std::vector<double> coef(m, 0.0);
   if (m < 2) {
     coef[0] = 1.0;
   } else {
-    const int mm = m - 1;
-    const double* rl = st->hres[m - 1];
+    // every <dr_i, dr_j> and <dr_i, r_last> in one launch, one host sync
+    const int mm = m - 1, nslots = mm * (mm + 1);
+    const unsigned nbk = (unsigned)std::min<long>(kMixBlocks, blocks_for(N));
+    k_dr_dots<<<dim3(nbk, nslots), 256, 0, s>>>(mh.dev_ptrs + m, mm, N, st->mix_partials); count_launch();
+    k_slot_sums<<<blocks_for(nslots), 256, 0, s>>>(st->mix_partials, (int)nbk, nslots, st->mix_sums); count_launch();
+    std::vector<double> sums(nslots);
+    PW_CUDA_TRY(cudaMemcpyAsync(sums.data(), st->mix_sums, nslots * sizeof(double), cudaMemcpyDeviceToHost, s));
+    PW_CUDA_TRY(cudaStreamSynchronize(s));
     std::vector<double> a((size_t)mm * mm), b(mm);
-    const unsigned nbk = (unsigned)std::min<long>(kRedBlocks, blocks_for(N));
     for (int i = 0; i < mm; ++i) {
-      k_dr_dot<<<nbk, 256, 0, s>>>(st->hres[i], nullptr, rl, N, st->partials); count_launch();
-      double v = 0.0;
-      Status r = final_sum_host(h, (int)nbk, v);
-      if (r != kOk) return r;
-      b[i] = -v;
+      b[i] = -sums[(size_t)i * (mm + 1)];
       for (int j = 0; j <= i; ++j) {
-        k_dr_dot<<<nbk, 256, 0, s>>>(st->hres[i], st->hres[j], rl, N, st->partials); count_launch();
-        if ((r = final_sum_host(h, (int)nbk, v)) != kOk) return r;
+        const double v = sums[(size_t)i * (mm + 1) + j + 1];
         a[(size_t)i * mm + j] = v;
         a[(size_t)j * mm + i] = v;
       }
@@ -555,20 +762,17 @@ static Status mix(Handle& h, const ScfParams& p) {
     for (int i = 0; i < mm; ++i) { coef[i] = al[i]; sum += al[i]; }
     coef[mm] = 1.0 - sum;
   }
-  std::vector<double*> ptrs(2 * m);
-  for (int j = 0; j < m; ++j) { ptrs[j] = st->hin[j]; ptrs[m + j] = st->hres[j]; }
-  PW_CUDA_TRY(cudaMemcpyAsync(st->dev_ptrs, ptrs.data(), 2 * m * sizeof(double*), cudaMemcpyHostToDevice, s));
-  PW_CUDA_TRY(cudaMemcpyAsync(st->dev_coef, coef.data(), m * sizeof(double), cudaMemcpyHostToDevice, s));
-  k_mix_combine<<<blocks_for(N), 256, 0, s>>>(st->dev_ptrs, st->dev_ptrs + m, st->dev_coef, m, p.mixing_beta, N,
-                                             st->rho_in); count_launch();
+  PW_CUDA_TRY(cudaMemcpyAsync(mh.dev_coef, coef.data(), m * sizeof(double), cudaMemcpyHostToDevice, s));
+  k_mix_combine<<<blocks_for(N), 256, 0, s>>>(mh.dev_ptrs, mh.dev_ptrs + m, mh.dev_coef, m, beta, N, next);
+  count_launch();
   PW_CUDA_TRY(cudaStreamSynchronize(s));
   return kOk;
 }
 
-// Density of all k-points (density.rs:41-111): rho_out = renormalised sum,
-// then symmetrised.
+// Density of all k-points of one spin channel (density.rs:41-111): rho =
+// sum renormalised to n_target electrons, then symmetrised.
 static Status build_density(Handle& h, const std::vector<std::vector<double>>& occ, const std::vector<double>& w,
-                            int spin, double* rho) {
+                            int spin, double* rho, double n_target) {
   ScfState* st = h.scf;
   const long N = h.g.N, n = h.n_pw;
   const cudaStream_t s = h.stream;
@@ -582,100 +786,246 @@ static Status build_density(Handle& h, const std::vector<std::vector<double>>& o
       fw.push_back(v);
     }
     if (fw.empty()) continue;
+    // pageable source: the copy has left fw when the call returns, and the
+    // device buffer is reused in stream order
     PW_CUDA_TRY(cudaMemcpyAsync(st->fw, fw.data(), fw.size() * sizeof(double), cudaMemcpyHostToDevice, s));
     Status r = density_accumulate(h, st->ks[(size_t)spin * h.n_k + ik].V, n, (int)fw.size(), st->fw, rho, s);
     if (r != kOk) return r;
-    PW_CUDA_TRY(cudaStreamSynchronize(s));
   }
   double tot = 0.0;
   Status r = reduce_host(h, rho, nullptr, N, 0, tot);
   if (r != kOk) return r;
   const double integ = tot * (h.omega / (double)N);
   if (std::fabs(integ) > 1e-15) {
-    k_scale_real<<<blocks_for(N), 256, 0, s>>>(rho, h.n_electrons / integ, N);
+    k_scale_real<<<blocks_for(N), 256, 0, s>>>(rho, n_target / integ, N);
     count_launch();
   }
   return symmetrize(h, rho);
 }
 
+// Eigensolve of every (spin, k) block for the current potentials.  With
+// lanes, host threads take blocks from a shared counter and run them on
+// their lanes' streams; the potentials on the handle stream are complete
+// before any lane starts.
+static Status eigensolve_all(Handle& h, const double* v0, double tol, int max_it, int nb, int prec,
+                             std::vector<EigStats>& stats) {
+  ScfState* st = h.scf;
+  const int nk = h.n_k, nitems = h.nspin * nk;
+  Status r;
+  if (st->lanes.empty()) {
+    for (int c = 0; c < nitems; ++c)
+      if ((r = lobpcg(h, st->ew, st->ks[c], c / nk, c % nk, v0[c / nk], tol, max_it, nb, prec, stats[c])) != kOk)
+        return r;
+    return kOk;
+  }
+  PW_CUDA_TRY(cudaStreamSynchronize(h.stream));
+  const int nl = (int)st->lanes.size();
+  std::atomic<int> next{0};
+  std::vector<int> codes(nl, kOk);
+  std::vector<std::string> msgs(nl);
+  auto worker = [&](int li) {
+    if (cudaSetDevice(h.device) != cudaSuccess) {
+      codes[li] = kCuda;
+      msgs[li] = "cudaSetDevice failed (lane)";
+      next.store(nitems);
+      return;
+    }
+    Lane& L = *st->lanes[li];
+    for (;;) {
+      const int c = next.fetch_add(1);
+      if (c >= nitems) break;
+      const Status rc = lobpcg(L.view, L.ew, st->ks[c], c / nk, c % nk, v0[c / nk], tol, max_it, nb, prec, stats[c]);
+      if (rc != kOk) {
+        codes[li] = rc;
+        msgs[li] = last_error_message();
+        next.store(nitems);
+        break;
+      }
+    }
+  };
+  std::vector<std::thread> th;
+  th.reserve(nl);
+  for (int li = 0; li < nl; ++li) th.emplace_back(worker, li);
+  for (auto& t : th) t.join();
+  for (int li = 0; li < nl; ++li)
+    if (codes[li] != kOk) return fail(codes[li], msgs[li]);
+  return kOk;
+}
+
+// Kerker weights P(G) = G^2/(G^2 + q^2), P(0) = 0 (kerker.rs:18-49); q_tf
+// <= 0 selects the Thomas-Fermi estimate (auto_q_tf_squared, kerker.rs:41-49).
+static Status set_kerker(Handle& h, bool on, double q_tf) {
+  ScfState* st = h.scf;
+  const long N = h.g.N;
+  if (!on) {
+    if (st->kerker_w) cudaFree(st->kerker_w);
+    st->kerker_w = nullptr;
+    return kOk;
+  }
+  double q2 = q_tf * q_tf;
+  if (q_tf <= 0.0) {
+    const double rb = h.n_electrons / h.omega * kBohr3ToAng3;
+    q2 = 4.0 * std::cbrt(3.0 * kPi * kPi * rb) / kPi / (kBohrToAng * kBohrToAng);
+  }
+  std::vector<double> g2(N), wg(N);
+  PW_CUDA_TRY(cudaMemcpy(g2.data(), h.g_squared, N * sizeof(double), cudaMemcpyDeviceToHost));
+  for (long i = 0; i < N; ++i) wg[i] = g2[i] < kG2Zero ? 0.0 : g2[i] / (g2[i] + q2);
+  Status r;
+  if (!st->kerker_w && (r = salloc(&st->kerker_w, (size_t)N)) != kOk) return r;
+  PW_CUDA_TRY(cudaMemcpy(st->kerker_w, wg.data(), N * sizeof(double), cudaMemcpyHostToDevice));
+  return kOk;
+}
+
+// Potentials of a spin-polarised density (driver_spin.rs:231-328): Hartree
+// from rho_up + rho_down, LSDA V_xc per channel on rho_sigma + core/2,
+// V_eff_sigma(r) into the handle's H|psi> arrays when set_hpsi; energies
+// e_hartree, e_xc = int rho_xc_total eps_xc, e_vxc = int (up v_up + dn v_dn).
+static Status potentials_spin(Handle& h, const double* up, const double* dn, bool set_hpsi, PotEnergies& e) {
+  ScfState* st = h.scf;
+  const long N = h.g.N;
+  const cudaStream_t s = h.stream;
+  k_axpy_to<<<blocks_for(N), 256, 0, s>>>(up, dn, 1.0, st->rtmp, N); count_launch();
+  Status r = density_to_g(h, st->rtmp);
+  if (r != kOk) return r;
+  const double fpe2 = 4.0 * kPi * kE2;
+  const unsigned nbk = (unsigned)std::min<long>(kRedBlocks, blocks_for(N));
+  k_hartree<<<nbk, 256, 0, s>>>(st->cg, h.g_squared, N, st->vh, fpe2, st->partials); count_launch();
+  double sh = 0.0;
+  if ((r = final_sum_host(h, (int)nbk, sh)) != kOk) return r;
+  e.e_hartree = sh * 0.5 * h.omega;
+  k_lsda<<<nbk, 256, 0, s>>>(up, dn, h.rho_core_r, N, st->vxc, st->vxc_dn, st->partials, st->partials + kRedBlocks);
+  count_launch();
+  double sx = 0.0, sv = 0.0;
+  if ((r = final_sum_host(h, (int)nbk, sx, 0)) != kOk) return r;
+  if ((r = final_sum_host(h, (int)nbk, sv, 1)) != kOk) return r;
+  const double dv = h.omega / (double)N;
+  e.e_xc = sx * dv;
+  e.e_vxc = sv * dv;
+  if (!set_hpsi) return kOk;
+  for (int sp = 0; sp < 2; ++sp) {
+    k_real_to_cplx<<<blocks_for(N), 256, 0, s>>>(sp == 0 ? st->vxc : st->vxc_dn, st->cg2, N); count_launch();
+    if ((r = fft3d_full(h, st->cg2, -1, s)) != kOk) return r;
+    k_scale_cplx<<<blocks_for(N), 256, 0, s>>>(st->cg2, 1.0 / (double)N, N); count_launch();
+    k_veff_g<<<blocks_for(N), 256, 0, s>>>(h.v_local_g, st->vh, st->cg2, st->cg2, N); count_launch();
+    PW_CUDA_TRY(cudaMemcpyAsync(h.tmp_grid, st->cg2, N * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+    if ((r = fft3d_full(h, h.tmp_grid, +1, s)) != kOk) return r;
+    k_real_part_both<<<blocks_for(N), 256, 0, s>>>(h.tmp_grid, h.veff_r[sp], h.veff_r32[sp], N); count_launch();
+  }
+  PW_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
+// Whole SCF loop: run_scf_unpolarized (driver.rs:353-735) for nspin = 1,
+// run_scf_spin (driver_spin.rs:114-839) for nspin = 2.  Per iteration:
+// potentials of rho_in, per-(spin, k) eigensolve, Fermi level and
+// occupations, density per channel (renormalised, symmetrised), density
+// change, energies from the output density, Anderson/Kerker mixing (CCMX
+// on total and magnetisation for nspin = 2).
 Status scf_run(Handle& h, const ScfParams& p, const double* rho_init, ScfResult& res, double* evals_out,
                double* rho_out_host, double* rho_g_basis_out) {
-  if (h.nspin != 1) return fail(kNotImplemented, "scf_run: nspin = 2 is not available in this build");
   if (p.n_bands < 1 || p.n_bands > h.n_pw) return fail(kInvalid, "scf_run: n_bands out of range");
   if (p.mixing_ndim < 1 || p.max_iter < 1) return fail(kInvalid, "scf_run: mixing_ndim and max_iter must be >= 1");
   PW_CUDA_TRY(cudaSetDevice(h.device));
-  const int nb = p.n_bands;
+  const int nb = p.n_bands, ns = h.nspin, nk = h.n_k;
   int extra = p.diag_extra_bands >= 0 ? p.diag_extra_bands : std::max(2, nb / 8);
   const int nd = (int)std::min<long>(nb + extra, h.n_pw);
   Status r = ensure_state(h, nb, nd, p.mixing_ndim);
   if (r != kOk) return r;
   ScfState* st = h.scf;
   for (auto& k : st->ks) k.init = false;
-  st->mix_count = 0;
+  for (auto& mh : st->mixh) mh.count = 0;
   const long N = h.g.N;
   const cudaStream_t s = h.stream;
   cublasSetStream(h.blas, s);
-  // Kerker weights P(G) = G^2/(G^2 + q^2), P(0) = 0 (kerker.rs:18-49)
-  if (p.mixing_mode == 1) {
-    double q2 = p.kerker_q_tf * p.kerker_q_tf;
-    if (p.kerker_q_tf <= 0.0) {
-      const double rb = h.n_electrons / h.omega * kBohr3ToAng3;
-      q2 = 4.0 * std::cbrt(3.0 * kPi * kPi * rb) / kPi / (kBohrToAng * kBohrToAng);
+  if ((r = set_kerker(h, p.mixing_mode == 1, p.kerker_q_tf)) != kOk) return r;
+  double* rin[2] = {st->rho_in, st->rho_in_dn};
+  double* rout[2] = {st->rho_out, st->rho_out_dn};
+  if (ns == 1) {
+    PW_CUDA_TRY(cudaMemcpyAsync(st->rho_in, rho_init, N * sizeof(double), cudaMemcpyHostToDevice, s));
+  } else {
+    // split the start density by the atom-averaged starting magnetisation
+    // (driver_spin.rs:160-167)
+    std::vector<double> up(N), dn(N);
+    const double m = p.starting_magnetization;
+    for (long i = 0; i < N; ++i) {
+      up[i] = rho_init[i] * (1.0 + m) / 2.0;
+      dn[i] = rho_init[i] * (1.0 - m) / 2.0;
     }
-    std::vector<double> g2(N), wk(N);
-    PW_CUDA_TRY(cudaMemcpy(g2.data(), h.g_squared, N * sizeof(double), cudaMemcpyDeviceToHost));
-    for (long i = 0; i < N; ++i) wk[i] = g2[i] < kG2Zero ? 0.0 : g2[i] / (g2[i] + q2);
-    if (!st->kerker_w && (r = salloc(&st->kerker_w, (size_t)N)) != kOk) return r;
-    PW_CUDA_TRY(cudaMemcpy(st->kerker_w, wk.data(), N * sizeof(double), cudaMemcpyHostToDevice));
-  } else if (st->kerker_w) {
-    cudaFree(st->kerker_w);
-    st->kerker_w = nullptr;
+    PW_CUDA_TRY(cudaMemcpy(st->rho_in, up.data(), N * sizeof(double), cudaMemcpyHostToDevice));
+    PW_CUDA_TRY(cudaMemcpy(st->rho_in_dn, dn.data(), N * sizeof(double), cudaMemcpyHostToDevice));
   }
-  PW_CUDA_TRY(cudaMemcpyAsync(st->rho_in, rho_init, N * sizeof(double), cudaMemcpyHostToDevice, s));
-  std::vector<double> wk(h.n_k);
-  for (int k = 0; k < h.n_k; ++k) wk[k] = h.kp[k].weight;
-  const double spin_factor = 2.0;
+  std::vector<double> wk(nk), wk_all;
+  for (int k = 0; k < nk; ++k) wk[k] = h.kp[k].weight;
+  for (int sp = 0; sp < ns; ++sp) wk_all.insert(wk_all.end(), wk.begin(), wk.end());
+  const double spin_factor = ns == 1 ? 2.0 : 1.0;
   bool have_prev = false;
   // mixed form: FP64 H|psi> from the first iteration whose input density rms
   // is below fp64_switch, or once the reduced-precision phase stops reducing
-  // it (two iterations without a 30 % improvement on the best so far: the
-  // precision floor of the FP32/BF16 operator), for the rest of the solve
+  // it (two iterations without a 30 % improvement on the best so far), for
+  // the rest of the solve
   bool fp64_locked = p.precision != 1;
   double best_delta = INFINITY;
   int stalled = 0;
   double e_prev = 0.0, last_delta = INFINITY, max_res_all = 0.0;
   long happ = 0;
-  std::vector<std::vector<double>> ev(h.n_k), occ(h.n_k);
+  const double dv = h.omega / (double)N;
+  std::vector<std::vector<double>> ev((size_t)ns * nk), occ((size_t)ns * nk);
   for (int iter = 0; iter < p.max_iter; ++iter) {
     PotEnergies ein;
-    if ((r = potentials(h, st->rho_in, true, ein)) != kOk) return r;
+    if (ns == 1) r = potentials(h, st->rho_in, true, ein);
+    else r = potentials_spin(h, st->rho_in, st->rho_in_dn, true, ein);
+    if (r != kOk) return r;
     if (!fp64_locked && (last_delta < p.fp64_switch || stalled >= 2)) fp64_locked = true;
     const int prec = fp64_locked ? 0 : 1;
     const double tol = std::max(p.diag_tol, std::min(1e-3, 0.1 * (std::isfinite(last_delta) ? last_delta : 1.0)));
     // preconditioner shift: V_eff(G = 0) = mean of V_eff(r)
-    double vsum = 0.0;
-    if ((r = reduce_host(h, h.veff_r[0], nullptr, N, 0, vsum)) != kOk) return r;
-    const double v0 = vsum / (double)N;
+    double v0[2] = {0.0, 0.0};
+    for (int sp = 0; sp < ns; ++sp) {
+      double vsum = 0.0;
+      if ((r = reduce_host(h, h.veff_r[sp], nullptr, N, 0, vsum)) != kOk) return r;
+      v0[sp] = vsum / (double)N;
+    }
+    const int max_it = iter == 0 ? 4 * p.diag_max_iter : p.diag_max_iter;
+    std::vector<EigStats> stats((size_t)ns * nk);
+    if ((r = eigensolve_all(h, v0, tol, max_it, nb, prec, stats)) != kOk) return r;
     max_res_all = 0.0;
-    for (int ik = 0; ik < h.n_k; ++ik) {
-      EigStats es;
-      if ((r = lobpcg(h, st->ew, st->ks[ik], 0, ik, v0, tol, iter == 0 ? 4 * p.diag_max_iter : p.diag_max_iter, nb,
-                      prec, es)) != kOk)
-        return r;
-      happ += es.happ;
-      max_res_all = std::max(max_res_all, es.max_res);
-      ev[ik].assign(st->ks[ik].evals.begin(), st->ks[ik].evals.begin() + nb);
+    for (int c = 0; c < ns * nk; ++c) {
+      happ += stats[c].happ;
+      max_res_all = std::max(max_res_all, stats[c].max_res);
+      ev[c].assign(st->ks[c].evals.begin(), st->ks[c].evals.begin() + nb);
     }
-    const double ef = fermi_level(ev, wk, h.n_electrons, p.sigma, p.smearing, spin_factor);
-    for (int ik = 0; ik < h.n_k; ++ik) {
-      occ[ik].resize(nb);
-      for (int b = 0; b < nb; ++b) occ[ik][b] = occ01(p.smearing, ev[ik][b], ef, p.sigma) * spin_factor;
+    // Fermi level: one over all channels, or one per channel at fixed
+    // magnetisation (driver_spin.rs:400-466); the reported level is their mean
+    double ef_sp[2];
+    double ef;
+    if (ns == 2 && p.fixed_magnetization) {
+      const std::vector<std::vector<double>> ev_up(ev.begin(), ev.begin() + nk), ev_dn(ev.begin() + nk, ev.end());
+      ef_sp[0] = fermi_level(ev_up, wk, 0.5 * (h.n_electrons + p.tot_magnetization), p.sigma, p.smearing, 1.0);
+      ef_sp[1] = fermi_level(ev_dn, wk, (h.n_electrons - p.tot_magnetization) / 2.0, p.sigma, p.smearing, 1.0);
+      ef = 0.5 * (ef_sp[0] + ef_sp[1]);
+    } else {
+      ef = fermi_level(ev, wk_all, h.n_electrons, p.sigma, p.smearing, spin_factor);
+      ef_sp[0] = ef_sp[1] = ef;
     }
-    if ((r = build_density(h, occ, wk, 0, st->rho_out)) != kOk) return r;
-    double dsq = 0.0;
-    if ((r = reduce_host(h, st->rho_in, st->rho_out, N, 2, dsq)) != kOk) return r;
-    const double dv = h.omega / (double)N;
-    const double delta = std::sqrt(dsq * dv / h.omega);
+    double nel_sp[2] = {0.0, 0.0};
+    for (int sp = 0; sp < ns; ++sp)
+      for (int ik = 0; ik < nk; ++ik) {
+        auto& o = occ[(size_t)sp * nk + ik];
+        const auto& e = ev[(size_t)sp * nk + ik];
+        o.resize(nb);
+        for (int b = 0; b < nb; ++b) {
+          o[b] = occ01(p.smearing, e[b], ef_sp[sp], p.sigma) * spin_factor;
+          nel_sp[sp] += o[b] * wk[ik];
+        }
+      }
+    double delta = 0.0;
+    for (int sp = 0; sp < ns; ++sp) {
+      const std::vector<std::vector<double>> oc(occ.begin() + (size_t)sp * nk, occ.begin() + (size_t)(sp + 1) * nk);
+      if ((r = build_density(h, oc, wk, sp, rout[sp], ns == 1 ? h.n_electrons : nel_sp[sp])) != kOk) return r;
+      double dsq = 0.0;
+      if ((r = reduce_host(h, rin[sp], rout[sp], N, 2, dsq)) != kOk) return r;
+      delta = std::max(delta, std::sqrt(dsq * dv / h.omega));
+    }
     last_delta = delta;
     if (!fp64_locked) {
       if (delta < 0.7 * best_delta) {
@@ -686,20 +1036,24 @@ Status scf_run(Handle& h, const ScfParams& p, const double* rho_init, ScfResult&
       }
     }
     PotEnergies eout;
-    if ((r = potentials(h, st->rho_out, false, eout)) != kOk) return r;
+    if (ns == 1) r = potentials(h, st->rho_out, false, eout);
+    else r = potentials_spin(h, st->rho_out, st->rho_out_dn, false, eout);
+    if (r != kOk) return r;
     double e_band = 0.0;
-    for (int ik = 0; ik < h.n_k; ++ik) {
+    for (size_t c = 0; c < ev.size(); ++c) {
       double sk = 0.0;
-      for (int b = 0; b < nb; ++b) sk += occ[ik][b] * wk[ik] * ev[ik][b];
+      for (int b = 0; b < nb; ++b) sk += occ[c][b] * wk_all[c] * ev[c][b];
       e_band += sk;
     }
-    const double ts = entropy_ts(ev, wk, ef, p.sigma, p.smearing, spin_factor);
+    const double ts = entropy_ts(ev, wk_all, ef, p.sigma, p.smearing, spin_factor);
     const double e_tot = e_band - eout.e_hartree + (eout.e_xc - eout.e_vxc) + h.e_ewald - ts;
     const double e_hf = e_band - ein.e_hartree + (ein.e_xc - ein.e_vxc) + h.e_ewald - ts;
     const double de = have_prev ? std::fabs(e_tot - e_prev) : INFINITY;
+    const double mag = ns == 2 ? std::fabs(nel_sp[0] - nel_sp[1]) : 0.0;
     if (p.verbose)
-      std::fprintf(stderr, "pwgpu scf iter %3d E=%.10f dE=%.3e drho=%.3e res=%.2e prec=%d happ=%ld\n", iter, e_tot,
-                   de, delta, max_res_all, prec, happ);
+      std::fprintf(stderr, "pwgpu scf iter %3d E=%.10f dE=%.3e drho=%.3e res=%.2e prec=%d happ=%ld%s", iter, e_tot, de,
+                   delta, max_res_all, prec, happ, ns == 2 ? "" : "\n");
+    if (p.verbose && ns == 2) std::fprintf(stderr, " M=%.6f\n", mag);
     const bool conv = delta < p.conv_threshold && have_prev && de < p.energy_threshold;
     e_prev = e_tot;
     have_prev = true;
@@ -718,16 +1072,23 @@ Status scf_run(Handle& h, const ScfParams& p, const double* rho_init, ScfResult&
       res.e_ewald = h.e_ewald;
       res.n_iterations = iter + 1;
       res.converged = conv ? 1 : 0;
-      res.nspin = 1;
+      res.nspin = ns;
+      res.magnetization = mag;
       res.h_applications = happ;
       res.max_residual = max_res_all;
       if (evals_out)
-        for (int ik = 0; ik < h.n_k; ++ik)
-          for (int b = 0; b < nb; ++b) evals_out[(size_t)ik * nb + b] = ev[ik][b];
-      if (rho_out_host)
-        PW_CUDA_TRY(cudaMemcpyAsync(rho_out_host, st->rho_out, N * sizeof(double), cudaMemcpyDeviceToHost, s));
+        for (size_t c = 0; c < ev.size(); ++c)
+          for (int b = 0; b < nb; ++b) evals_out[c * nb + b] = ev[c][b];
+      for (int sp = 0; sp < ns && rho_out_host; ++sp)
+        PW_CUDA_TRY(cudaMemcpyAsync(rho_out_host + (size_t)sp * N, rout[sp], N * sizeof(double),
+                                    cudaMemcpyDeviceToHost, s));
       if (rho_g_basis_out) {
-        if ((r = density_to_g(h, st->rho_out)) != kOk) return r;
+        const double* tot = st->rho_out;
+        if (ns == 2) {
+          k_axpy_to<<<blocks_for(N), 256, 0, s>>>(st->rho_out, st->rho_out_dn, 1.0, st->rtmp, N); count_launch();
+          tot = st->rtmp;
+        }
+        if ((r = density_to_g(h, tot)) != kOk) return r;
         std::vector<int> gf(h.n_pw);
         std::vector<double2> full(N);
         PW_CUDA_TRY(cudaMemcpyAsync(full.data(), st->cg, N * sizeof(double2), cudaMemcpyDeviceToHost, s));
@@ -741,7 +1102,19 @@ Status scf_run(Handle& h, const ScfParams& p, const double* rho_init, ScfResult&
       PW_CUDA_TRY(cudaStreamSynchronize(s));
       return conv ? kOk : fail(kNotConverged, "SCF did not converge within max_iter");
     }
-    if ((r = mix(h, p)) != kOk) return r;
+    if (ns == 1) {
+      if ((r = mix_channel(h, st->mixh[0], st->rho_in, st->rho_out, st->rho_in, p.mixing_beta, true)) != kOk) return r;
+    } else {
+      // CCMX (driver_spin.rs:792-826): total density with the requested
+      // mode, magnetisation with plain Anderson
+      k_axpy_to<<<blocks_for(N), 256, 0, s>>>(st->rho_in, st->rho_in_dn, 1.0, st->t_in, N); count_launch();
+      k_axpy_to<<<blocks_for(N), 256, 0, s>>>(st->rho_in, st->rho_in_dn, -1.0, st->m_in, N); count_launch();
+      k_axpy_to<<<blocks_for(N), 256, 0, s>>>(st->rho_out, st->rho_out_dn, 1.0, st->t_out, N); count_launch();
+      k_axpy_to<<<blocks_for(N), 256, 0, s>>>(st->rho_out, st->rho_out_dn, -1.0, st->m_out, N); count_launch();
+      if ((r = mix_channel(h, st->mixh[0], st->t_in, st->t_out, st->t_in, p.mixing_beta, true)) != kOk) return r;
+      if ((r = mix_channel(h, st->mixh[1], st->m_in, st->m_out, st->m_in, p.mixing_beta, false)) != kOk) return r;
+      k_unmix_spin<<<blocks_for(N), 256, 0, s>>>(st->t_in, st->m_in, st->rho_in, st->rho_in_dn, N); count_launch();
+    }
   }
   return fail(kNotConverged, "SCF did not converge within max_iter");
 }
@@ -799,7 +1172,7 @@ Status density_from_host(Handle& h, int n_bands, const double* occ, const double
     PW_CUDA_TRY(cudaMemcpyAsync(st->ks[ik].V, psi_all + (size_t)ik * n * n_bands * 2, n * n_bands * sizeof(double2),
                                 cudaMemcpyHostToDevice, h.stream));
   }
-  if ((r = build_density(h, oc, wk, 0, st->rho_out)) != kOk) return r;
+  if ((r = build_density(h, oc, wk, 0, st->rho_out, h.n_electrons)) != kOk) return r;
   PW_CUDA_TRY(cudaMemcpyAsync(rho_out, st->rho_out, h.g.N * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
   PW_CUDA_TRY(cudaStreamSynchronize(h.stream));
   return kOk;
@@ -832,6 +1205,40 @@ Status potentials_host(Handle& h, const double* rho, double* veff_g, double* ene
     energies[1] = e.e_xc;
     energies[2] = e.e_vxc;
   }
+  return kOk;
+}
+
+Status mix_host(Handle& h, int channel, const double* in, const double* out, double* next, double beta, int ndim,
+                int kerker, double q_tf) {
+  if (channel < 0 || channel > 1) return fail(kInvalid, "mix: channel must be 0 or 1");
+  if (ndim < 1) return fail(kInvalid, "mix: ndim must be >= 1");
+  Status r;
+  if (!h.scf && (r = ensure_state(h, 1, 1, ndim)) != kOk) return r;
+  ScfState* st = h.scf;
+  const long N = h.g.N;
+  if (ndim > st->mix_cap) {
+    cudaFree(st->mix_partials);
+    cudaFree(st->mix_sums);
+    st->mix_partials = st->mix_sums = nullptr;
+    const size_t nslots = (size_t)ndim * (ndim + 1);
+    if ((r = salloc(&st->mix_partials, nslots * kMixBlocks)) != kOk) return r;
+    if ((r = salloc(&st->mix_sums, nslots)) != kOk) return r;
+    st->mix_cap = ndim;
+  }
+  MixHistory& mh = st->mixh[channel];
+  if ((int)mh.hin.size() != ndim && (r = alloc_history(mh, N, ndim)) != kOk) return r;
+  if ((r = set_kerker(h, kerker != 0, q_tf)) != kOk) return r;
+  PW_CUDA_TRY(cudaMemcpyAsync(st->rho_in, in, N * sizeof(double), cudaMemcpyHostToDevice, h.stream));
+  PW_CUDA_TRY(cudaMemcpyAsync(st->rho_out, out, N * sizeof(double), cudaMemcpyHostToDevice, h.stream));
+  if ((r = mix_channel(h, mh, st->rho_in, st->rho_out, st->rho_in, beta, kerker != 0)) != kOk) return r;
+  PW_CUDA_TRY(cudaMemcpyAsync(next, st->rho_in, N * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
+  PW_CUDA_TRY(cudaStreamSynchronize(h.stream));
+  return kOk;
+}
+
+Status mix_reset(Handle& h) {
+  if (h.scf)
+    for (auto& mh : h.scf->mixh) mh.count = 0;
   return kOk;
 }
 

@@ -26,6 +26,11 @@ struct ScfParams {
   int precision = 0;                // 0 FP64, 1 mixed
   double fp64_switch = 1e-6;        // mixed: FP64 H|psi> once delta rho < this
   int verbose = 0;
+  // nspin = 2 (driver_spin.rs:125-167): atom average of the per-species
+  // starting_magnetization fractions, and the optional fixed total moment
+  double starting_magnetization = 0.0;
+  int fixed_magnetization = 0;
+  double tot_magnetization = 0.0;
 };
 
 struct ScfResult {
@@ -50,5 +55,9 @@ Status eigensolve_k(Handle& h, int spin, int ik, int n_bands, double tol, int ma
 Status density_from_host(Handle& h, int n_bands, const double* occ, const double* psi_all, double* rho_out);
 Status symmetrize_host(Handle& h, double* rho);
 Status potentials_host(Handle& h, const double* rho, double* veff_g, double* energies);
+// One Anderson/Kerker mixing step on history `channel` (0 or 1), host arrays.
+Status mix_host(Handle& h, int channel, const double* in, const double* out, double* next, double beta, int ndim,
+                int kerker, double q_tf);
+Status mix_reset(Handle& h);
 
 }  // namespace pwgpu

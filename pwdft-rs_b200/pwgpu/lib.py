@@ -64,7 +64,7 @@ class PwgpuSystem(ct.Structure):
 
 
 class PwgpuOptions(ct.Structure):
-    _fields_ = [("device", ct.c_int32), ("precision", ct.c_int32)]
+    _fields_ = [("device", ct.c_int32), ("precision", ct.c_int32), ("lanes", ct.c_int32)]
 
 
 SMEARING = {"fermi_dirac": 0, "gaussian": 1, "methfessel_paxton": 2, "cold": 3, "fixed": 4}
@@ -77,7 +77,8 @@ class PwgpuScfParams(ct.Structure):
         ("mixing_mode", ct.c_int32), ("kerker_q_tf", ct.c_double), ("smearing", ct.c_int32),
         ("smearing_sigma", ct.c_double), ("diag_tol", ct.c_double), ("diag_max_iter", ct.c_int32),
         ("diag_extra_bands", ct.c_int32), ("precision", ct.c_int32), ("fp64_switch", ct.c_double),
-        ("verbose", ct.c_int32),
+        ("verbose", ct.c_int32), ("starting_magnetization", ct.c_double), ("fixed_magnetization", ct.c_int32),
+        ("tot_magnetization", ct.c_double),
     ]
 
 
@@ -125,6 +126,8 @@ def load_library(path: str = LIB_PATH):
     lib.pwgpu_density.argtypes = [vp, ct.c_int32, _f64p, _f64p, _f64p]
     lib.pwgpu_symmetrize.argtypes = [vp, _f64p]
     lib.pwgpu_potentials.argtypes = [vp, _f64p, _f64p, _f64p]
+    lib.pwgpu_mix.argtypes = [vp, ct.c_int32, _f64p, _f64p, _f64p, ct.c_double, ct.c_int32, ct.c_int32, ct.c_double]
+    lib.pwgpu_mix_reset.argtypes = [vp]
     lib.pwgpu_small_geneig.argtypes = [ct.c_int32, ct.c_int32, ct.c_int32, _f64p, _f64p, _f64p, _f64p]
     lib.pwgpu_get_stream.argtypes = [vp, ct.POINTER(vp)]
     lib.pwgpu_get_stream.restype = ct.c_int32
@@ -208,11 +211,11 @@ def pack_system(sys_) -> tuple:
 class PwGpu:
     """One device handle (pwgpu_create .. pwgpu_destroy)."""
 
-    def __init__(self, sys_, precision: int = PRECISION_FP64, device: int = 0):
+    def __init__(self, sys_, precision: int = PRECISION_FP64, device: int = 0, lanes: int = 0):
         self.lib = load_library()
         self.sys = sys_
         st, keep = pack_system(sys_)
-        opt = PwgpuOptions(device, precision)
+        opt = PwgpuOptions(device, precision, lanes)
         h = ct.c_void_p()
         _check(self.lib, self.lib.pwgpu_create(ct.byref(st), ct.byref(opt), ct.byref(h)))
         self.h = h
@@ -277,23 +280,41 @@ class PwGpu:
                 energy_threshold: float = 1e-5, mixing_beta: float = 0.3, mixing_ndim: int = 8, kerker: bool = False,
                 q_tf: float = 0.0, smearing: str = "fermi_dirac", sigma: float = 0.01, diag_tol: float = 1e-8,
                 diag_max_iter: int = 60, diag_extra_bands: int = -1, precision: int = PRECISION_FP64,
-                fp64_switch: float = 1e-6, verbose: bool = False, raise_on_unconverged: bool = True):
-        """run_scf_unpolarized on the device; returns (result dict, eigenvalues [n_k, n_bands],
-        rho_r [N], rho_g in basis order [n_pw])."""
+                fp64_switch: float = 1e-6, verbose: bool = False, raise_on_unconverged: bool = True,
+                starting_magnetization: float = 0.0, tot_magnetization=None):
+        """run_scf_unpolarized / run_scf_spin on the device; returns (result dict, eigenvalues
+        [nspin * n_k, n_bands] (spin up k-points first), rho_r [nspin * N] (up then down),
+        total rho_g in basis order [n_pw])."""
         p = PwgpuScfParams(n_bands, max_iter, conv_threshold, energy_threshold, mixing_beta, mixing_ndim,
                            1 if kerker else 0, q_tf, SMEARING[smearing], sigma, diag_tol, diag_max_iter,
-                           diag_extra_bands, precision, fp64_switch, 1 if verbose else 0)
+                           diag_extra_bands, precision, fp64_switch, 1 if verbose else 0, starting_magnetization,
+                           0 if tot_magnetization is None else 1,
+                           0.0 if tot_magnetization is None else tot_magnetization)
         rho0 = np.ascontiguousarray(rho_init, dtype=np.float64)
         res = PwgpuScfResult()
+        ns = self.sys.nspin
         nk = len(self.sys.kpoints)
-        ev = np.zeros((nk, n_bands))
-        rho = np.zeros(self.sys.n_grid)
+        ev = np.zeros((ns * nk, n_bands))
+        rho = np.zeros(ns * self.sys.n_grid)
         rg = np.zeros(self.n_pw, dtype=np.complex128)
         rc = self.lib.pwgpu_scf_run(self.h, ct.byref(p), _f64(rho0), ct.byref(res), _f64(ev), _f64(rho),
                                     rg.view(np.float64).ctypes.data_as(_f64p))
         if rc != PWGPU_OK and (raise_on_unconverged or rc != -4):
             raise PwGpuError(rc, self.lib.pwgpu_last_error().decode(errors="replace"))
         return res.as_dict(), ev, rho, rg
+
+    def mix(self, rho_in: np.ndarray, rho_out: np.ndarray, beta: float, ndim: int, kerker: bool = False,
+            q_tf: float = 0.0, channel: int = 0) -> np.ndarray:
+        """One Anderson (+ Kerker) step on the device history `channel`; returns the next input density."""
+        a = np.ascontiguousarray(rho_in, dtype=np.float64)
+        b = np.ascontiguousarray(rho_out, dtype=np.float64)
+        out = np.empty_like(a)
+        _check(self.lib, self.lib.pwgpu_mix(self.h, channel, _f64(a), _f64(b), _f64(out), beta, ndim,
+                                            1 if kerker else 0, q_tf))
+        return out
+
+    def mix_reset(self):
+        _check(self.lib, self.lib.pwgpu_mix_reset(self.h))
 
     def eigensolve(self, n_bands: int, ik: int = 0, spin: int = 0, tol: float = 1e-9, max_iter: int = 300,
                    psi_in=None):

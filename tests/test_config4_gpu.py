@@ -1,0 +1,64 @@
+"""Batched-k LSDA case (8-atom cubic diamond cells at 35 Ry, 20 IBZ
+k-points, 24 bands, Fermi-Dirac 0.02 Ry) on the GPU against the committed
+oracle fixtures (tests/golden/make_config4_fixtures.py), and concurrent
+(spin, k) lanes against one-at-a-time execution.
+
+Both loops stop at drho < 1e-8 e/Å^3 and |dE| < 1e-7 eV.  Tolerances: total
+energy 1e-5 eV (first order in drho), Harris-Foulkes energy 1e-6 eV, Fermi
+level and eigenvalues 1e-5 eV, magnetisation 1e-5."""
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from pwgpu.config4 import SCF_KW, config4_system
+from pwgpu.lib import PwGpu
+from pwgpu.upf import load_upf
+
+pytestmark = pytest.mark.gpu
+
+CASES = {"C": ("C", "C.upf", True), "C_nonlcc": ("C", "C.upf", False)}
+TIGHT = dict(conv_threshold=1e-8, energy_threshold=1e-7, max_iter=200)
+
+
+def fixture(name):
+    path = os.path.join(GOLDEN, f"config4_{name}_oracle.json")
+    if not os.path.exists(path):
+        pytest.skip(f"fixture {path} not generated")
+    with open(path) as f:
+        return json.load(f)
+
+
+def run(s, m, lanes=0):
+    kw = dict(SCF_KW)
+    kw.update(TIGHT)
+    nb = kw.pop("n_bands")
+    with PwGpu(s, lanes=lanes) as dev:
+        return dev.scf_run(s.rho_init_r, nb, starting_magnetization=m, **kw)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_config4_cell_matches_oracle(name):
+    ref = fixture(name)
+    species, upf, nlcc = CASES[name]
+    s, m = config4_system(species, load_upf(os.path.join(GOLDEN, "upf", upf)), nlcc=nlcc)
+    assert (s.n_pw, list(s.dims), len(s.kpoints)) == (ref["n_pw"], ref["dims"], ref["n_k"])
+    res, ev, rho, rg = run(s, m)
+    assert res["converged"] == 1
+    assert abs(res["total_energy"] - ref["total_energy"]) < 1e-5
+    assert abs(res["harris_foulkes_energy"] - ref["harris_foulkes_energy"]) < 1e-6
+    assert abs(res["fermi_energy"] - ref["fermi_energy"]) < 1e-5
+    assert abs(res["magnetization"] - ref["magnetization"]) < 1e-5
+    assert np.max(np.abs(ev - np.array(ref["eigenvalues"]))) < 1e-5
+
+
+def test_lanes_match_sequential(c_pp):
+    s, m = config4_system("C", c_pp)
+    r1, ev1, _, _ = run(s, m, lanes=1)
+    r8, ev8, _, _ = run(s, m, lanes=0)
+    assert abs(r1["total_energy"] - r8["total_energy"]) < 1e-5
+    assert abs(r1["harris_foulkes_energy"] - r8["harris_foulkes_energy"]) < 1e-6
+    assert np.max(np.abs(ev1 - ev8)) < 1e-5
