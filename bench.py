@@ -222,6 +222,44 @@ def run_scf_once():
     print("scf once: ok", res["n_iterations"], res["total_energy"])
 
 
+def run_serve(args):
+    """Serving workload: the first --requests requests of the seeded stream
+    (Poisson 50/s; Si/C, 2-64 atoms, strain, displacements, 20-35 Ry, Gamma or
+    2x2x2) replayed in real time through pwgpu_server_* (mixed precision);
+    host setup of each request starts at its arrival on a thread pool.
+    |dE| per atom against FP64 reruns of a seeded 5 % sample."""
+    from pwgpu.lib import PRECISION_FP64, PRECISION_MIXED
+    from pwgpu.serving import Server, request_stream, request_system, run_stream, summarize
+    from pwgpu.upf import load_upf
+    pps = {"Si": load_upf(SI_UPF), "C": load_upf(os.path.join(ROOT, "tests", "golden", "upf", "C.upf"))}
+    reqs = request_stream(args.requests)
+    with Server(workers=4, precision=PRECISION_MIXED, lanes_per_job=2) as srv:
+        recs, wall = run_stream(srv, reqs, pps, precision=PRECISION_MIXED)
+        stats = srv.stats()
+    summ = summarize(recs, wall)
+    rng = np.random.default_rng(20261203)
+    sample = sorted(rng.choice(len(reqs), size=max(1, len(reqs) // 20), replace=False).tolist())
+    de = []
+    with Server(workers=2, precision=PRECISION_FP64, lanes_per_job=2) as srv64:
+        for i in sample:
+            s, kw = request_system(reqs[i], pps)
+            kw = dict(kw)
+            nb = kw.pop("n_bands")
+            jid = srv64.submit(s, nb, precision=PRECISION_FP64, **kw)
+            srv64.wait(jid, 3600.0)
+            res, ev, status, err = srv64.result(jid)
+            srv64.release(jid)
+            de.append(abs(res["total_energy"] - recs[i]["total_energy"]) / reqs[i].n_atoms)
+    line = {"metric": "serving stream: SCF solves/s and latency (mixed precision)", "value": summ["solves_per_s"],
+            "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic (seeded request stream)",
+            "config": {"workload": "serving_stream_poisson50", "requests": len(reqs),
+                       "arrival_rate_per_s": 50.0, "workers": 4, "lanes_per_job": 2},
+            **summ, "server": stats,
+            "accuracy": {"fp64_sample": len(sample), "max_dE_per_atom_ev": max(de) if de else None,
+                         "max_dE_per_atom_ha": (max(de) / HA_TO_EV) if de else None}}
+    print(json.dumps(line), flush=True)
+
+
 def kernel_bench(local, steps, warmup, flush, hbm_peak, peak_kind):
     """H|psi> of the 160-band block (mixed and FP64): device ms per block and
     the per-stage profile; roofline of the dominant own kernel."""
@@ -299,10 +337,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="pwgpu", choices=["pwgpu", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="full", choices=["full", "once", "scf-once"],
-                    help="once: three untimed H|psi> calls per precision; scf-once: one mixed solve")
+    ap.add_argument("--mode", default="full", choices=["full", "once", "scf-once", "serve"],
+                    help="once: three untimed H|psi> calls per precision; scf-once: one mixed solve; "
+                         "serve: the serving stream through pwgpu_server_* (own JSON line)")
+    ap.add_argument("--requests", type=int, default=200, help="serve: requests of the stream replayed")
     args = ap.parse_args()
     world, rank, local = dist_env()
+    if args.mode == "serve":
+        run_serve(args)
+        return
     if args.mode == "once":
         run_once()
         return

@@ -248,6 +248,75 @@ pwgpu_status pwgpu_apply_h_local_noalloc(pwgpu_handle* h, int32_t spin, int32_t 
 pwgpu_status pwgpu_small_geneig(int32_t batch, int32_t m, int32_t nev, const double* H, const double* S,
                                 double* evals, double* C);
 
+/*
+ * Serving: a job queue in front of pwgpu_scf_run.  No counterpart in the
+ * reference (its front door, scf::run_scf at scf/mod.rs:344-402, runs one
+ * solve per call); this is the submit/poll seam a service wraps around it.
+ * Each worker thread owns one job at a time: it builds a handle for the
+ * job's system on the server's device, runs the SCF and releases the
+ * handle.  A job starts only when the estimated device footprint of the
+ * running jobs plus its own fits the HBM budget (first come, first served:
+ * the queue head waits rather than being overtaken); a job larger than the
+ * whole budget is refused at submit with PWGPU_E_OOM.
+ */
+typedef struct pwgpu_server pwgpu_server;
+
+typedef struct pwgpu_server_options {
+  int32_t device;            /* CUDA device ordinal */
+  int32_t workers;           /* jobs in flight at most; 0 = 4 */
+  int32_t precision;         /* pwgpu_options.precision of every job's handle */
+  int32_t lanes_per_job;     /* pwgpu_options.lanes of every job's handle; 0 = 2 */
+  int64_t hbm_budget_bytes;  /* admission budget; 0 = 80 % of the device memory free at create */
+} pwgpu_server_options;
+
+#define PWGPU_JOB_QUEUED 0
+#define PWGPU_JOB_RUNNING 1
+#define PWGPU_JOB_DONE 2
+
+typedef struct pwgpu_job_info {
+  int32_t state;            /* PWGPU_JOB_* */
+  pwgpu_status status;      /* the job's pwgpu_scf_run status once done (PWGPU_E_NOT_CONVERGED: result filled) */
+  double queue_s;           /* submit -> start, seconds (so far, while queued) */
+  double run_s;             /* start -> done, seconds (so far, while running) */
+  int64_t footprint_bytes;  /* admission estimate */
+} pwgpu_job_info;
+
+typedef struct pwgpu_server_stats {
+  int64_t submitted, queued, running, done, failed;
+  int64_t bytes_in_use, peak_bytes, budget_bytes;
+} pwgpu_server_stats;
+
+pwgpu_status pwgpu_server_create(const pwgpu_server_options* opt, pwgpu_server** out);
+
+/* Stops the workers after their running jobs; queued jobs are dropped. */
+pwgpu_status pwgpu_server_destroy(pwgpu_server* s);
+
+/* Queue one SCF: the system, parameters and start density (nspin = the
+ * system's; rho_init_r N doubles) are copied, so the caller's arrays are
+ * free again on return. */
+pwgpu_status pwgpu_server_submit(pwgpu_server* s, const pwgpu_system* sys, const pwgpu_scf_params* params,
+                                 const double* rho_init_r, int64_t* job_id);
+
+pwgpu_status pwgpu_server_poll(pwgpu_server* s, int64_t job_id, pwgpu_job_info* info);
+
+/* Wait until job_id is done (PWGPU_E_TIMEOUT after timeout_s seconds). */
+pwgpu_status pwgpu_server_wait(pwgpu_server* s, int64_t job_id, double timeout_s, pwgpu_job_info* info);
+
+/* Wait until some finished job has not been collected yet and return its
+ * id (each finished job is returned once; PWGPU_E_TIMEOUT after timeout_s). */
+pwgpu_status pwgpu_server_wait_any(pwgpu_server* s, double timeout_s, int64_t* job_id);
+
+/* Result of a finished job: the ScfResult scalars, and (when not NULL) the
+ * eigenvalues nspin x n_k x n_bands and the job's error message (valid
+ * until the job is released). */
+pwgpu_status pwgpu_server_result(pwgpu_server* s, int64_t job_id, pwgpu_scf_result* result, double* eigenvalues,
+                                 const char** error);
+
+/* Forget a finished job. */
+pwgpu_status pwgpu_server_release(pwgpu_server* s, int64_t job_id);
+
+pwgpu_status pwgpu_server_get_stats(pwgpu_server* s, pwgpu_server_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,7 +20,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <numeric>
+#include <set>
 #include <type_traits>
 #include <vector>
 
@@ -356,10 +358,16 @@ template <typename T> Status dalloc(T** p, size_t count) {
   return kOk;
 }
 
-// Opt every FFT kernel into the dynamic shared memory its largest tile needs.
+// Opt every FFT kernel into the dynamic shared memory its largest tile needs
+// (a per-device attribute: done once per device, under a lock, since handles
+// may be created from several host threads).
 Status configure_kernels() {
-  static bool done = false;
-  if (done) return kOk;
+  static std::mutex mu;
+  static std::set<int> done_devices;
+  int dev = 0;
+  PW_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if (done_devices.count(dev)) return kOk;
   const int sm = kMaxDynSmem;
   cudaError_t e = cudaSuccess;
   auto set = [&](const void* f) {
@@ -373,7 +381,7 @@ Status configure_kernels() {
   set((const void*)k_fft_axis<1>); set((const void*)k_fft_axis<-1>);
   set((const void*)k_x_density);
   if (e != cudaSuccess) return fail(kCuda, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
-  done = true;
+  done_devices.insert(dev);
   return kOk;
 }
 

@@ -139,7 +139,8 @@ def build_projectors(crystal: Crystal, basis: BasisSet, k, radial_tables) -> Pro
     for at in crystal.atoms:
         ls, ffun, dij = radial_tables[at.symbol]
         if at.symbol not in ff_cache:
-            ff_cache[at.symbol] = [ffun(i, qn) for i in range(len(ls))]
+            # F_i(|k+G|) on the distinct |k+G| only (bit-identical: same inputs)
+            ff_cache[at.symbol] = [_per_unique(qn, lambda u, i=i: ffun(i, u)) for i in range(len(ls))]
         ffs = ff_cache[at.symbol]
         tau = at.cart(crystal.lattice)
         phase_arg = -((g[:, 0] * tau[0] + g[:, 1] * tau[1]) + g[:, 2] * tau[2])
@@ -262,17 +263,23 @@ def build_system(crystal: Crystal, pps: dict, ecut_ev: float, kpoints, symmetry:
     n = gv.shape[0]
     taus = [a.cart(crystal.lattice) for a in crystal.atoms]
 
+    # per-species structure factors S_s(G) = sum over its atoms of e^{-iG.tau},
+    # shared by the V_loc, core and start-density sums
+    sfac = {}
+    for at, tau in zip(crystal.atoms, taus):
+        ph = -((gv[:, 0] * tau[0] + gv[:, 1] * tau[1]) + gv[:, 2] * tau[2])
+        term = np.cos(ph) + 1j * np.sin(ph)
+        if at.symbol in sfac:
+            sfac[at.symbol] += term
+        else:
+            sfac[at.symbol] = term
+
     def structure_sum(radial_of_species):
         acc = np.zeros(n, dtype=np.complex128)
-        cache = {}
-        for at, tau in zip(crystal.atoms, taus):
-            if at.symbol not in cache:
-                cache[at.symbol] = radial_of_species(at.symbol)
-            rad = cache[at.symbol]
-            if rad is None:
-                continue
-            ph = -((gv[:, 0] * tau[0] + gv[:, 1] * tau[1]) + gv[:, 2] * tau[2])
-            acc += (np.cos(ph) + 1j * np.sin(ph)) * rad
+        for sp in sfac:
+            rad = radial_of_species(sp)
+            if rad is not None:
+                acc += sfac[sp] * rad
         return acc
 
     v_loc = structure_sum(lambda sp: _per_unique(gn, lambda u: v_local_of_g(pps[sp], u, omega)))

@@ -96,6 +96,40 @@ class PwgpuScfResult(ct.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class PwgpuServerOptions(ct.Structure):
+    _fields_ = [("device", ct.c_int32), ("workers", ct.c_int32), ("precision", ct.c_int32),
+                ("lanes_per_job", ct.c_int32), ("hbm_budget_bytes", ct.c_int64)]
+
+
+class PwgpuJobInfo(ct.Structure):
+    _fields_ = [("state", ct.c_int32), ("status", ct.c_int32), ("queue_s", ct.c_double), ("run_s", ct.c_double),
+                ("footprint_bytes", ct.c_int64)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class PwgpuServerStats(ct.Structure):
+    _fields_ = [(name, ct.c_int64) for name in ("submitted", "queued", "running", "done", "failed", "bytes_in_use",
+                                                "peak_bytes", "budget_bytes")]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+def scf_params(n_bands: int, max_iter: int = 100, conv_threshold: float = 1e-6, energy_threshold: float = 1e-5,
+               mixing_beta: float = 0.3, mixing_ndim: int = 8, kerker: bool = False, q_tf: float = 0.0,
+               smearing: str = "fermi_dirac", sigma: float = 0.01, diag_tol: float = 1e-8, diag_max_iter: int = 60,
+               diag_extra_bands: int = -1, precision: int = 0, fp64_switch: float = 1e-6, verbose: bool = False,
+               starting_magnetization: float = 0.0, tot_magnetization=None) -> "PwgpuScfParams":
+    """The pwgpu_scf_params POD (ScfParams fields, reference defaults)."""
+    return PwgpuScfParams(n_bands, max_iter, conv_threshold, energy_threshold, mixing_beta, mixing_ndim,
+                          1 if kerker else 0, q_tf, SMEARING[smearing], sigma, diag_tol, diag_max_iter,
+                          diag_extra_bands, precision, fp64_switch, 1 if verbose else 0, starting_magnetization,
+                          0 if tot_magnetization is None else 1,
+                          0.0 if tot_magnetization is None else tot_magnetization)
+
+
 _lib = None
 
 
@@ -133,10 +167,22 @@ def load_library(path: str = LIB_PATH):
     lib.pwgpu_get_stream.restype = ct.c_int32
     lib.pwgpu_kernel_launches.argtypes = [ct.POINTER(ct.c_int64)]
     lib.pwgpu_kernel_launches.restype = ct.c_int32
+    lib.pwgpu_server_create.argtypes = [ct.POINTER(PwgpuServerOptions), ct.POINTER(vp)]
+    lib.pwgpu_server_destroy.argtypes = [vp]
+    lib.pwgpu_server_submit.argtypes = [vp, ct.POINTER(PwgpuSystem), ct.POINTER(PwgpuScfParams), _f64p,
+                                        ct.POINTER(ct.c_int64)]
+    lib.pwgpu_server_poll.argtypes = [vp, ct.c_int64, ct.POINTER(PwgpuJobInfo)]
+    lib.pwgpu_server_wait.argtypes = [vp, ct.c_int64, ct.c_double, ct.POINTER(PwgpuJobInfo)]
+    lib.pwgpu_server_wait_any.argtypes = [vp, ct.c_double, ct.POINTER(ct.c_int64)]
+    lib.pwgpu_server_result.argtypes = [vp, ct.c_int64, ct.POINTER(PwgpuScfResult), _f64p, ct.POINTER(ct.c_char_p)]
+    lib.pwgpu_server_release.argtypes = [vp, ct.c_int64]
+    lib.pwgpu_server_get_stats.argtypes = [vp, ct.POINTER(PwgpuServerStats)]
     for name in ("pwgpu_create", "pwgpu_destroy", "pwgpu_set_veff_g", "pwgpu_apply_h", "pwgpu_apply_h_device",
                  "pwgpu_set_precision", "pwgpu_get_dims", "pwgpu_profile_apply_h", "pwgpu_scf_run",
                  "pwgpu_eigensolve", "pwgpu_density", "pwgpu_symmetrize", "pwgpu_potentials",
-                 "pwgpu_small_geneig"):
+                 "pwgpu_small_geneig", "pwgpu_mix", "pwgpu_mix_reset", "pwgpu_server_create", "pwgpu_server_destroy",
+                 "pwgpu_server_submit", "pwgpu_server_poll", "pwgpu_server_wait", "pwgpu_server_wait_any",
+                 "pwgpu_server_result", "pwgpu_server_release", "pwgpu_server_get_stats"):
         getattr(lib, name).restype = ct.c_int32
     _lib = lib
     return lib
@@ -285,11 +331,9 @@ class PwGpu:
         """run_scf_unpolarized / run_scf_spin on the device; returns (result dict, eigenvalues
         [nspin * n_k, n_bands] (spin up k-points first), rho_r [nspin * N] (up then down),
         total rho_g in basis order [n_pw])."""
-        p = PwgpuScfParams(n_bands, max_iter, conv_threshold, energy_threshold, mixing_beta, mixing_ndim,
-                           1 if kerker else 0, q_tf, SMEARING[smearing], sigma, diag_tol, diag_max_iter,
-                           diag_extra_bands, precision, fp64_switch, 1 if verbose else 0, starting_magnetization,
-                           0 if tot_magnetization is None else 1,
-                           0.0 if tot_magnetization is None else tot_magnetization)
+        p = scf_params(n_bands, max_iter, conv_threshold, energy_threshold, mixing_beta, mixing_ndim, kerker, q_tf,
+                       smearing, sigma, diag_tol, diag_max_iter, diag_extra_bands, precision, fp64_switch, verbose,
+                       starting_magnetization, tot_magnetization)
         rho0 = np.ascontiguousarray(rho_init, dtype=np.float64)
         res = PwgpuScfResult()
         ns = self.sys.nspin
