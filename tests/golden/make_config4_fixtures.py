@@ -1,9 +1,9 @@
 """Generate the oracle reference values of the batched-k LSDA case (the
 8-atom cubic Si and C diamond cells at 35 Ry, Gamma-centred 6x6x6 mesh
 reduced to 20 IBZ k-points, 24 bands, Fermi-Dirac 0.02 Ry, starting
-magnetisation 0 on Si and 0.125 on C).  The density-rms and energy
-thresholds are tightened to 1e-8 e/Å^3 and 1e-7 eV so that the converged
-energy is path independent to ~1e-6 eV (the deck defaults, 1e-6 and 1e-5,
+magnetisation 0 on Si and 0.125 on C).  The density-rms threshold is
+tightened to 1e-8 e/Å^3 (energy change 1e-6 eV) so that the converged
+energy is path independent to ~1e-5 eV (the deck defaults, 1e-6 and 1e-5,
 leave ~1e-4 eV of first-order error in the total energy).
 
     python tests/golden/make_config4_fixtures.py [C C_nonlcc Si]
@@ -26,7 +26,7 @@ from oracle import pwdft_oracle as O  # noqa: E402
 from pwgpu.config4 import SCF_KW, config4_system  # noqa: E402
 from pwgpu.upf import load_upf  # noqa: E402
 
-TIGHT = dict(conv_threshold=1e-8, energy_threshold=1e-7, max_iter=200)
+TIGHT = dict(conv_threshold=1e-8, energy_threshold=1e-6, max_iter=200)
 CASES = {"C": ("C", "C.upf", True), "C_nonlcc": ("C", "C.upf", False), "Si": ("Si", "Si.upf", True)}
 
 
@@ -39,7 +39,7 @@ def main(names):
         kw.update(TIGHT)
         nb = kw.pop("n_bands")
         r = O.run_scf_spin(s, nb, starting_magnetization=m, smearing=kw.pop("smearing"), sigma=kw.pop("sigma"),
-                           **kw)
+                           verbose=True, **kw)
         out = {"total_energy": r.total_energy, "harris_foulkes_energy": r.harris_foulkes_energy,
                "fermi_energy": r.fermi_energy, "magnetization": r.magnetization, "n_iterations": r.n_iterations,
                "final_delta": r.final_delta, "eigenvalues": [list(map(float, e)) for e in r.eigenvalues],
