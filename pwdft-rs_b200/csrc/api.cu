@@ -40,6 +40,7 @@ template <typename T> static Status upload(T** dst, const T* src, size_t count) 
 }
 
 static void release(Handle& h) {
+  release_gamma(h);
   auto f = [](void* p) { if (p) cudaFree(p); };
   GridMaps& g = h.g;
   for (int a = 0; a < 3; ++a) { f(g.tw64[a]); f(g.tw32[a]); }
@@ -134,6 +135,10 @@ static Status create(const pwgpu_system* s, const pwgpu_options* o, pwgpu_handle
     PW_CUDA_TRY(cudaMemset(h.veff_r[sp], 0, N * sizeof(double)));
     PW_CUDA_TRY(cudaMemset(h.veff_r32[sp], 0, N * sizeof(float)));
   }
+  // Gamma-only systems run with real wavefunctions unless the caller keeps them complex
+  if (!(o && o->gamma_complex) &&
+      (st = build_gamma(h, s->miller, s->kinetic, s->proj_b, s->atom_ch_start, s->d_blocks)) != kOk)
+    return st;
   PW_CUDA_TRY(cudaDeviceSynchronize());
   return kOk;
 }

@@ -46,6 +46,20 @@ struct KPointData {
   double weight = 0.0;
 };
 
+// Gamma-only systems: wavefunctions with psi(-G) = conj(psi(G)) stored as
+// real vectors of n_pw entries, u = [Re psi(0), sqrt2 Re psi(G_p),
+// sqrt2 Im psi(G_p)] over the half sphere G_p > 0 (lexicographic in the
+// Miller indices), so complex inner products are real dot products.
+struct GammaData {
+  bool on = false;
+  int nh = 0;                 // half-sphere points; n_pw = 2 nh + 1
+  int zero = 0;               // basis index of G = 0
+  int* half_idx = nullptr;    // nh: basis index of G_p
+  int* half_neg = nullptr;    // nh: basis index of -G_p
+  double* kin_packed = nullptr;  // n_pw: |G|^2 term in packed order
+  double* b_real = nullptr;      // n_pw x n_ch packed projectors
+};
+
 struct Handle {
   int device = 0;
   int n_pw = 0, n_k = 0, n_ch = 0, n_atoms = 0, nspin = 1, n_sym = 0;
@@ -80,6 +94,14 @@ struct Handle {
   int* solver_info = nullptr;
   struct ScfState* scf = nullptr;  // device state of the SCF loop (scf.cu)
   struct NlMixed* nlm = nullptr;   // split projector operands of the mixed form (nl_mixed.cu)
+  GammaData gam;
+  // per-call scratch of the Gamma path (lane-owned like nl_p / nl_q)
+  double2* gam_c1 = nullptr;
+  double2* gam_c2 = nullptr;
+  long gam_ccap = 0;          // complex pseudo-band columns of gam_c1 / gam_c2
+  double* gam_p = nullptr;
+  double* gam_q = nullptr;
+  int gam_pcap = 0;
   bool trace = false;  // per-iteration eigensolver lines on stderr (PWGPU_TRACE set at create)
   int lanes = 0;       // concurrent (spin, k) eigensolves in the SCF loop; 0 = automatic
   std::string last_error;
@@ -113,6 +135,27 @@ Status apply_h_device(Handle& h, int spin, int ik, const double2* psi, long ldps
                       long ldh, int precision, cudaStream_t stream, StageTimer* timer = nullptr);
 Status set_veff_from_g(Handle& h, int spin, const double2* veff_g_dev, cudaStream_t stream);
 Status ensure_nl_capacity(Handle& h, int nb);
+
+// Local part of H|psi> only (kinetic + V_eff through the FFT pipeline).
+Status apply_local_device(Handle& h, int spin, int ik, const double2* psi, long ldpsi, int nb, double2* hpsi,
+                          long ldh, int precision, cudaStream_t s, StageTimer* tm = nullptr);
+
+// Gamma path (gamma.cu).  build_gamma decides eligibility (one k-point with
+// a kinetic term and projectors symmetric under G -> -G) from host data.
+Status build_gamma(Handle& h, const int* miller_host, const double* kinetic_host, const double* proj_b_host,
+                   const int* atom_ch_start_host, const double* d_blocks_host);
+void release_gamma(Handle& h);
+void release_gamma_scratch(Handle& h);
+// H u for nb packed real bands (local pipeline on pairs of bands packed into
+// one complex vector, then real projector GEMMs).
+Status apply_h_real(Handle& h, int spin, const double* u, long ldu, int nb, double* hu, long ldh, int precision,
+                    cudaStream_t s);
+// rho += sum_b fw[b] |psi_b(r)|^2 for nb packed real bands (fw on the host).
+Status density_accumulate_real(Handle& h, const double* u, long ldu, const std::vector<double>& fw, double* rho,
+                               cudaStream_t s);
+// packed real <-> complex full-sphere coefficients (Gamma-real columns)
+Status gamma_pack(Handle& h, const double2* x, long ldx, int ncols, double* u, long ldu, cudaStream_t s);
+Status gamma_unpack(Handle& h, const double* u, long ldu, int ncols, double2* x, long ldx, cudaStream_t s);
 
 // Local part of H|psi> (kinetic + V_eff, no projectors) with the FFT
 // intermediates in caller-provided device scratch; fails with kInvalid when

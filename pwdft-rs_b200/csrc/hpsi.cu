@@ -672,6 +672,22 @@ Status density_accumulate(Handle& h, const double2* psi, long ldpsi, int nb, con
   return kOk;
 }
 
+Status apply_local_device(Handle& h, int spin, int ik, const double2* psi, long ldpsi, int nb, double2* hpsi,
+                          long ldh, int precision, cudaStream_t s, StageTimer* tm) {
+  // the work buffers are sized for h.chunk FP64 bands; FP32 fits twice as many
+  const int chunk = precision == 0 ? h.chunk : 2 * h.chunk;
+  for (int c0 = 0; c0 < nb; c0 += chunk) {
+    const int cnt = std::min(chunk, nb - c0);
+    Status st;
+    if (precision == 0)
+      st = local_chunk<double>(h, spin, ik, psi + (long)c0 * ldpsi, ldpsi, cnt, hpsi + (long)c0 * ldh, ldh, s, tm);
+    else
+      st = local_chunk<float>(h, spin, ik, psi + (long)c0 * ldpsi, ldpsi, cnt, hpsi + (long)c0 * ldh, ldh, s, tm);
+    if (st != kOk) return st;
+  }
+  return kOk;
+}
+
 Status apply_h_device(Handle& h, int spin, int ik, const double2* psi, long ldpsi, int nb, double2* hpsi, long ldh,
                       int precision, cudaStream_t s, StageTimer* tm) {
   if (ik < 0 || ik >= h.n_k) return fail(kInvalid, "apply_h: k-point index out of range");
@@ -680,16 +696,7 @@ Status apply_h_device(Handle& h, int spin, int ik, const double2* psi, long ldps
   if (ldpsi < h.n_pw || ldh < h.n_pw) return fail(kInvalid, "apply_h: leading dimension smaller than n_pw");
   Status st;
   mark(tm, -1, s);
-  // the work buffers are sized for h.chunk FP64 bands; FP32 fits twice as many
-  const int chunk = precision == 0 ? h.chunk : 2 * h.chunk;
-  for (int c0 = 0; c0 < nb; c0 += chunk) {
-    const int cnt = std::min(chunk, nb - c0);
-    if (precision == 0)
-      st = local_chunk<double>(h, spin, ik, psi + (long)c0 * ldpsi, ldpsi, cnt, hpsi + (long)c0 * ldh, ldh, s, tm);
-    else
-      st = local_chunk<float>(h, spin, ik, psi + (long)c0 * ldpsi, ldpsi, cnt, hpsi + (long)c0 * ldh, ldh, s, tm);
-    if (st != kOk) return st;
-  }
+  if ((st = apply_local_device(h, spin, ik, psi, ldpsi, nb, hpsi, ldh, precision, s, tm)) != kOk) return st;
   if (h.n_ch > 0 && precision == 1 && nl_mixed_eligible(h)) {
     if ((st = nonlocal_mixed(h, ik, psi, ldpsi, nb, hpsi, ldh, s, tm)) != kOk) return st;
   } else if (h.n_ch > 0) {

@@ -4,9 +4,9 @@
 //
 // Stands in for the dense diagonalisation of the reference's per-k step
 // (pwdft-core/src/eigensolver/dense.rs:50-98, the lowest n_bands pairs of the
-// full n_pw x n_pw Hamiltonian): H is only applied (apply_h_device) and the
-// lowest nd Ritz pairs are refined until the residual norms of the first
-// nconv fall below tol.
+// full n_pw x n_pw Hamiltonian): H is only applied (apply_h_device, or
+// apply_h_real for Gamma-only handles) and the lowest nd Ritz pairs are
+// refined until the residual norms of the first nconv fall below tol.
 //
 // Numerical design:
 //  * the basis is orthonormal by construction (block Gram-Schmidt against X,
@@ -23,6 +23,10 @@
 //    search directions only enter through the (small) correction
 //    coefficients; the residuals the convergence test reads carry no
 //    reduced-precision floor.
+//
+// The solver is written once for complex bands (double2) and for the real
+// packed bands of Gamma-only handles (double): the same steps with real
+// GEMMs, Cholesky and symmetric eigensolver.
 #include <cublas_v2.h>
 #include <cusolverDn.h>
 
@@ -31,6 +35,7 @@
 #include <cmath>
 #include <cstdio>
 #include <random>
+#include <type_traits>
 #include <vector>
 
 #include "linalg.hpp"
@@ -50,6 +55,27 @@ constexpr double kPDropMixed = 3e-2;
 
 inline unsigned blocks_for(long n, int t = 256) { return (unsigned)std::max<long>(1, (n + t - 1) / t); }
 
+// scalar helpers for double (Gamma-real) and double2 (complex)
+__host__ __device__ __forceinline__ double abs2(double x) { return x * x; }
+__host__ __device__ __forceinline__ double abs2(double2 x) { return x.x * x.x + x.y * x.y; }
+__host__ __device__ __forceinline__ double scl(double x, double s) { return x * s; }
+__host__ __device__ __forceinline__ double2 scl(double2 x, double s) { return make_double2(x.x * s, x.y * s); }
+__host__ __device__ __forceinline__ double axpy_neg(double hx, double l, double x) { return hx - l * x; }
+__host__ __device__ __forceinline__ double2 axpy_neg(double2 hx, double l, double2 x) {
+  return make_double2(hx.x - l * x.x, hx.y - l * x.y);
+}
+__host__ __device__ __forceinline__ double conj_of(double x) { return x; }
+__host__ __device__ __forceinline__ double2 conj_of(double2 x) { return make_double2(x.x, -x.y); }
+__host__ __device__ __forceinline__ double herm_avg(double a, double b) { return 0.5 * (a + b); }
+__host__ __device__ __forceinline__ double2 herm_avg(double2 a, double2 b) {
+  return make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+}
+template <typename T> __host__ __device__ __forceinline__ T real_scalar(double v);
+template <> __host__ __device__ __forceinline__ double real_scalar<double>(double v) { return v; }
+template <> __host__ __device__ __forceinline__ double2 real_scalar<double2>(double v) { return make_double2(v, 0.0); }
+__host__ __device__ __forceinline__ double real_part(double x) { return x; }
+__host__ __device__ __forceinline__ double real_part(double2 x) { return x.x; }
+
 __device__ __forceinline__ double block_sum(double v, double* sh) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -67,34 +93,35 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
 // Residual R = HX - lambda X, preconditioned into T with the smooth
 // denominator 0.5 (1 + x + sqrt(1 + (x-1)^2)) in Ry, x = (|k+G|^2 + v0 -
 // lambda)/Ry; per-column partial sums of |R|^2.
-__global__ void k_resid_precond(const double2* __restrict__ X, const double2* __restrict__ HX, double2* __restrict__ T,
-                                long ld, int n, const double* __restrict__ lam, const double* __restrict__ kin,
-                                double v0, double* __restrict__ partials) {
+template <typename S>
+__global__ void k_resid_precond(const S* __restrict__ X, const S* __restrict__ HX, S* __restrict__ T, long ld, int n,
+                                const double* __restrict__ lam, const double* __restrict__ kin, double v0,
+                                double* __restrict__ partials) {
   __shared__ double sh[32];
   const int col = blockIdx.y;
   const double l = lam[col];
-  const double2* x = X + (long)col * ld;
-  const double2* hx = HX + (long)col * ld;
-  double2* t = T + (long)col * ld;
+  const S* x = X + (long)col * ld;
+  const S* hx = HX + (long)col * ld;
+  S* t = T + (long)col * ld;
   double acc = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const double2 r = make_double2(hx[i].x - l * x[i].x, hx[i].y - l * x[i].y);
-    acc += r.x * r.x + r.y * r.y;
+    const S r = axpy_neg(hx[i], l, x[i]);
+    acc += abs2(r);
     const double xx = (kin[i] + v0 - l) / kRyToEv;
     const double den = 0.5 * (1.0 + xx + sqrt(1.0 + (xx - 1.0) * (xx - 1.0))) * kRyToEv;
-    t[i] = make_double2(r.x / den, r.y / den);
+    t[i] = scl(r, 1.0 / den);
   }
   acc = block_sum(acc, sh);
   if (threadIdx.x == 0) partials[(long)col * gridDim.x + blockIdx.x] = acc;
 }
 
-__global__ void k_col_sumsq(const double2* __restrict__ X, long ld, int n, double* __restrict__ partials) {
+template <typename S>
+__global__ void k_col_sumsq(const S* __restrict__ X, long ld, int n, double* __restrict__ partials) {
   __shared__ double sh[32];
   const int col = blockIdx.y;
-  const double2* x = X + (long)col * ld;
+  const S* x = X + (long)col * ld;
   double acc = 0.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    acc += x[i].x * x[i].x + x[i].y * x[i].y;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc += abs2(x[i]);
   acc = block_sum(acc, sh);
   if (threadIdx.x == 0) partials[(long)col * gridDim.x + blockIdx.x] = acc;
 }
@@ -109,60 +136,71 @@ __global__ void k_col_final(const double* __restrict__ partials, int nblk, int n
 }
 
 // X[:, c] /= sqrt(sumsq[c]) (and Y[:, c] with the same factor when Y != null)
-__global__ void k_scale_cols_invsqrt(double2* __restrict__ X, double2* __restrict__ Y, long ld, int n,
+template <typename S>
+__global__ void k_scale_cols_invsqrt(S* __restrict__ X, S* __restrict__ Y, long ld, int n,
                                      const double* __restrict__ sumsq) {
   const int col = blockIdx.y;
   const double s = sumsq[col] > 0.0 ? 1.0 / sqrt(sumsq[col]) : 0.0;
-  double2* x = X + (long)col * ld;
-  double2* y = Y ? Y + (long)col * ld : nullptr;
+  S* x = X + (long)col * ld;
+  S* y = Y ? Y + (long)col * ld : nullptr;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    x[i] = x[i] * s;
-    if (y) y[i] = y[i] * s;
+    x[i] = scl(x[i], s);
+    if (y) y[i] = scl(y[i], s);
   }
 }
 
 // dst[:, c] = src[:, idx[c]] over `rows` rows (src and dst do not overlap)
-__global__ void k_gather_cols(const double2* __restrict__ src, long lds, const int* __restrict__ idx,
-                              double2* __restrict__ dst, long ldd, int rows) {
+template <typename S>
+__global__ void k_gather_cols(const S* __restrict__ src, long lds, const int* __restrict__ idx, S* __restrict__ dst,
+                              long ldd, int rows) {
   const int c = blockIdx.y;
-  const double2* s = src + (long)idx[c] * lds;
-  double2* d = dst + (long)c * ldd;
+  const S* s = src + (long)idx[c] * lds;
+  S* d = dst + (long)c * ldd;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) d[i] = s[i];
 }
 
 // Subspace matrix Hs (m x m, ld m) over the basis [X | B], X holding nd Ritz
 // vectors with values lam:  [[diag(lam), Z^H], [Z, (G + G^H)/2]],
 // Z = B^H HX (q x nd, ld q), G = B^H HB (q x q, ld q), q = m - nd.
-__global__ void k_assemble_rr(double2* __restrict__ Hs, int m, int nd, const double* __restrict__ lam,
-                              const double2* __restrict__ Z, const double2* __restrict__ G) {
+template <typename S>
+__global__ void k_assemble_rr(S* __restrict__ Hs, int m, int nd, const double* __restrict__ lam,
+                              const S* __restrict__ Z, const S* __restrict__ G) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long)m * m) return;
   const int r = (int)(t % m), c = (int)(t / m), q = m - nd;
-  double2 v;
+  S v;
   if (r < nd && c < nd) {
-    v = make_double2(r == c ? lam[r] : 0.0, 0.0);
+    v = real_scalar<S>(r == c ? lam[r] : 0.0);
   } else if (c < nd) {
     v = Z[(r - nd) + (long)c * q];
   } else if (r < nd) {
-    const double2 z = Z[(c - nd) + (long)r * q];
-    v = make_double2(z.x, -z.y);
+    v = conj_of(Z[(c - nd) + (long)r * q]);
   } else {
-    const double2 a = G[(r - nd) + (long)(c - nd) * q], b = G[(c - nd) + (long)(r - nd) * q];
-    v = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+    v = herm_avg(G[(r - nd) + (long)(c - nd) * q], G[(c - nd) + (long)(r - nd) * q]);
   }
   Hs[t] = v;
 }
 
-__global__ void k_set_identity(double2* __restrict__ A, int m) {
+template <typename S> __global__ void k_set_identity(S* __restrict__ A, int m) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long)m * m) return;
-  A[t] = make_double2((t % m) == (t / m) ? 1.0 : 0.0, 0.0);
+  A[t] = real_scalar<S>((t % m) == (t / m) ? 1.0 : 0.0);
 }
 
 // out[i] = Re A[i, i]
-__global__ void k_diag_real(const double2* __restrict__ A, int ld, int m, double* __restrict__ out) {
+template <typename S> __global__ void k_diag_real(const S* __restrict__ A, int ld, int m, double* __restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < m) out[i] = A[i + (long)i * ld].x;
+  if (i < m) out[i] = real_part(A[i + (long)i * ld]);
+}
+
+// real m x m <-> complex (zero imaginary part), for the one-CTA complex solver
+__global__ void k_real_to_complex(const double* __restrict__ a, double2* __restrict__ z, long n) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) z[t] = make_double2(a[t], 0.0);
+}
+__global__ void k_complex_to_real(const double2* __restrict__ z, double* __restrict__ a, long n) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) a[t] = z[t].x;
 }
 
 template <typename T> Status walloc(T** p, size_t n) {
@@ -172,7 +210,7 @@ template <typename T> Status walloc(T** p, size_t n) {
 }
 
 // ---------------------------------------------------------------------------
-// BLAS / LAPACK steps
+// BLAS / LAPACK steps, overloaded on the scalar type
 // ---------------------------------------------------------------------------
 
 struct Ctx {
@@ -183,18 +221,60 @@ struct Ctx {
   unsigned gx;
 };
 
-Status zgemm(Ctx& c, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k, const double2* A, long lda,
-             const double2* B, long ldb, double2* C, long ldc, double beta_re = 0.0, double alpha_re = 1.0) {
+Status gemm(Ctx& c, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k, const double2* A, long lda,
+            const double2* B, long ldb, double2* C, long ldc, double beta_re = 0.0, double alpha_re = 1.0) {
   if (m == 0 || n == 0) return kOk;
   const cuDoubleComplex al = make_cuDoubleComplex(alpha_re, 0.0), be = make_cuDoubleComplex(beta_re, 0.0);
-  cublasStatus_t cs = cublasZgemm(c.h.blas, ta, tb, m, n, k, &al, reinterpret_cast<const cuDoubleComplex*>(A),
-                                  (int)lda, reinterpret_cast<const cuDoubleComplex*>(B), (int)ldb, &be,
-                                  reinterpret_cast<cuDoubleComplex*>(C), (int)ldc);
-  if (cs != CUBLAS_STATUS_SUCCESS) return fail(kCuda, "cublasZgemm failed (eigensolver)");
+  if (cublasZgemm(c.h.blas, ta, tb, m, n, k, &al, reinterpret_cast<const cuDoubleComplex*>(A), (int)lda,
+                  reinterpret_cast<const cuDoubleComplex*>(B), (int)ldb, &be, reinterpret_cast<cuDoubleComplex*>(C),
+                  (int)ldc) != CUBLAS_STATUS_SUCCESS)
+    return fail(kCuda, "cublasZgemm failed (eigensolver)");
   return kOk;
 }
 
-Status ensure_solver_work(Ctx& c, size_t lwork) {
+Status gemm(Ctx& c, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k, const double* A, long lda,
+            const double* B, long ldb, double* C, long ldc, double beta = 0.0, double alpha = 1.0) {
+  if (m == 0 || n == 0) return kOk;
+  const cublasOperation_t ra = ta == CUBLAS_OP_C ? CUBLAS_OP_T : ta, rb = tb == CUBLAS_OP_C ? CUBLAS_OP_T : tb;
+  if (cublasDgemm(c.h.blas, ra, rb, m, n, k, &alpha, A, (int)lda, B, (int)ldb, &beta, C, (int)ldc) !=
+      CUBLAS_STATUS_SUCCESS)
+    return fail(kCuda, "cublasDgemm failed (eigensolver)");
+  return kOk;
+}
+
+Status add_shift(Ctx& c, double2* G, double2* Id, int q, double shift) {
+  const cuDoubleComplex al = make_cuDoubleComplex(1.0, 0.0), be = make_cuDoubleComplex(shift, 0.0);
+  if (cublasZgeam(c.h.blas, CUBLAS_OP_N, CUBLAS_OP_N, q, q, &al, reinterpret_cast<cuDoubleComplex*>(G), q, &be,
+                  reinterpret_cast<cuDoubleComplex*>(Id), q, reinterpret_cast<cuDoubleComplex*>(G),
+                  q) != CUBLAS_STATUS_SUCCESS)
+    return fail(kCuda, "cublasZgeam failed (eigensolver)");
+  return kOk;
+}
+Status add_shift(Ctx& c, double* G, double* Id, int q, double shift) {
+  const double al = 1.0;
+  if (cublasDgeam(c.h.blas, CUBLAS_OP_N, CUBLAS_OP_N, q, q, &al, G, q, &shift, Id, q, G, q) != CUBLAS_STATUS_SUCCESS)
+    return fail(kCuda, "cublasDgeam failed (eigensolver)");
+  return kOk;
+}
+
+Status trsm_right_upper(Ctx& c, const double2* R, int q, double2* M) {
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
+  if (cublasZtrsm(c.h.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, (int)c.n, q,
+                  &one, reinterpret_cast<const cuDoubleComplex*>(R), q, reinterpret_cast<cuDoubleComplex*>(M),
+                  (int)c.n) != CUBLAS_STATUS_SUCCESS)
+    return fail(kCuda, "cublasZtrsm failed (eigensolver)");
+  return kOk;
+}
+Status trsm_right_upper(Ctx& c, const double* R, int q, double* M) {
+  const double one = 1.0;
+  if (cublasDtrsm(c.h.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, (int)c.n, q,
+                  &one, R, q, M, (int)c.n) != CUBLAS_STATUS_SUCCESS)
+    return fail(kCuda, "cublasDtrsm failed (eigensolver)");
+  return kOk;
+}
+
+Status ensure_solver_work(Ctx& c, size_t bytes) {
+  const size_t lwork = (bytes + sizeof(double2) - 1) / sizeof(double2);
   if (lwork <= c.w.solver_lwork) return kOk;
   if (c.w.solver_work) cudaFree(c.w.solver_work);
   c.w.solver_work = nullptr;
@@ -211,11 +291,78 @@ Status ensure_solver(Ctx& c) {
   return kOk;
 }
 
+// Cholesky of the q x q Gram (upper); info on the device
+Status potrf(Ctx& c, double2* G, int q) {
+  int lwork = 0;
+  auto* g = reinterpret_cast<cuDoubleComplex*>(G);
+  if (cusolverDnZpotrf_bufferSize(c.h.solver, CUBLAS_FILL_MODE_UPPER, q, g, q, &lwork) != CUSOLVER_STATUS_SUCCESS)
+    return fail(kCuda, "cusolverDnZpotrf_bufferSize failed");
+  Status r;
+  if ((r = ensure_solver_work(c, (size_t)lwork * sizeof(double2))) != kOk) return r;
+  if (cusolverDnZpotrf(c.h.solver, CUBLAS_FILL_MODE_UPPER, q, g, q,
+                       reinterpret_cast<cuDoubleComplex*>(c.w.solver_work), lwork, c.w.info) !=
+      CUSOLVER_STATUS_SUCCESS)
+    return fail(kCuda, "cusolverDnZpotrf failed");
+  return kOk;
+}
+Status potrf(Ctx& c, double* G, int q) {
+  int lwork = 0;
+  if (cusolverDnDpotrf_bufferSize(c.h.solver, CUBLAS_FILL_MODE_UPPER, q, G, q, &lwork) != CUSOLVER_STATUS_SUCCESS)
+    return fail(kCuda, "cusolverDnDpotrf_bufferSize failed");
+  Status r;
+  if ((r = ensure_solver_work(c, (size_t)lwork * sizeof(double))) != kOk) return r;
+  if (cusolverDnDpotrf(c.h.solver, CUBLAS_FILL_MODE_UPPER, q, G, q, reinterpret_cast<double*>(c.w.solver_work),
+                       lwork, c.w.info) != CUSOLVER_STATUS_SUCCESS)
+    return fail(kCuda, "cusolverDnDpotrf failed");
+  return kOk;
+}
+
+// all eigenpairs of the Hermitian / symmetric m x m matrix A (lower), in place
+Status heevd(Ctx& c, double2* A, int m, double* w) {
+  int lwork = 0;
+  auto* a = reinterpret_cast<cuDoubleComplex*>(A);
+  if (cusolverDnZheevd_bufferSize(c.h.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, m, a, m, w, &lwork) !=
+      CUSOLVER_STATUS_SUCCESS)
+    return fail(kCuda, "cusolverDnZheevd_bufferSize failed");
+  Status r;
+  if ((r = ensure_solver_work(c, (size_t)lwork * sizeof(double2))) != kOk) return r;
+  if (cusolverDnZheevd(c.h.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, m, a, m, w,
+                       reinterpret_cast<cuDoubleComplex*>(c.w.solver_work), lwork, c.w.info) !=
+      CUSOLVER_STATUS_SUCCESS)
+    return fail(kCuda, "cusolverDnZheevd failed");
+  return kOk;
+}
+Status heevd(Ctx& c, double* A, int m, double* w) {
+  int lwork = 0;
+  if (cusolverDnDsyevd_bufferSize(c.h.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, m, A, m, w, &lwork) !=
+      CUSOLVER_STATUS_SUCCESS)
+    return fail(kCuda, "cusolverDnDsyevd_bufferSize failed");
+  Status r;
+  if ((r = ensure_solver_work(c, (size_t)lwork * sizeof(double))) != kOk) return r;
+  if (cusolverDnDsyevd(c.h.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, m, A, m, w,
+                       reinterpret_cast<double*>(c.w.solver_work), lwork, c.w.info) != CUSOLVER_STATUS_SUCCESS)
+    return fail(kCuda, "cusolverDnDsyevd failed");
+  return kOk;
+}
+
+// H x for the band type: complex bands through the FFT + projector pipeline,
+// packed real bands through the Gamma path
+Status apply_op(Handle& h, int spin, int ik, const double2* x, long ld, int nb, double2* hx, int precision,
+                cudaStream_t s) {
+  return apply_h_device(h, spin, ik, x, ld, nb, hx, ld, precision, s);
+}
+Status apply_op(Handle& h, int spin, int, const double* x, long ld, int nb, double* hx, int precision,
+                cudaStream_t s) {
+  return apply_h_real(h, spin, x, ld, nb, hx, ld, precision, s);
+}
+
+template <typename T> T* as(double2* p) { return reinterpret_cast<T*>(p); }
+
 // Column sums of squares of Y (q columns) into w.colsq (device); to the
 // host too when host != null.
-Status col_norms2(Ctx& c, const double2* Y, int q, double* host) {
+template <typename T> Status col_norms2(Ctx& c, const T* Y, int q, double* host) {
   if (q == 0) return kOk;
-  k_col_sumsq<<<dim3(c.gx, q), 256, 0, c.s>>>(Y, c.n, (int)c.n, c.w.partials); count_launch();
+  k_col_sumsq<T><<<dim3(c.gx, q), 256, 0, c.s>>>(Y, c.n, (int)c.n, c.w.partials); count_launch();
   k_col_final<<<blocks_for(q), 256, 0, c.s>>>(c.w.partials, (int)c.gx, q, c.w.colsq); count_launch();
   if (host) {
     PW_CUDA_TRY(cudaMemcpyAsync(host, c.w.colsq, q * sizeof(double), cudaMemcpyDeviceToHost, c.s));
@@ -226,12 +373,13 @@ Status col_norms2(Ctx& c, const double2* Y, int q, double* host) {
 
 // Y -= A (A^H Y), HY -= HA (A^H Y): Y (q columns) projected out of span(A)
 // (p orthonormal columns).
-Status project_out(Ctx& c, const double2* A, const double2* HA, int p, double2* Y, double2* HY, int q) {
+template <typename T> Status project_out(Ctx& c, const T* A, const T* HA, int p, T* Y, T* HY, int q) {
   if (p == 0 || q == 0) return kOk;
   Status r;
-  if ((r = zgemm(c, CUBLAS_OP_C, CUBLAS_OP_N, p, q, (int)c.n, A, c.n, Y, c.n, c.w.Z, p)) != kOk) return r;
-  if ((r = zgemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.n, q, p, A, c.n, c.w.Z, p, Y, c.n, 1.0, -1.0)) != kOk) return r;
-  if (HY && (r = zgemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.n, q, p, HA, c.n, c.w.Z, p, HY, c.n, 1.0, -1.0)) != kOk)
+  T* Z = as<T>(c.w.Z);
+  if ((r = gemm(c, CUBLAS_OP_C, CUBLAS_OP_N, p, q, (int)c.n, A, c.n, Y, c.n, Z, p)) != kOk) return r;
+  if ((r = gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.n, q, p, A, c.n, Z, p, Y, c.n, 1.0, -1.0)) != kOk) return r;
+  if (HY && (r = gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.n, q, p, HA, c.n, Z, p, HY, c.n, 1.0, -1.0)) != kOk)
     return r;
   return kOk;
 }
@@ -239,36 +387,26 @@ Status project_out(Ctx& c, const double2* A, const double2* HA, int p, double2* 
 // One Cholesky-QR pass: G = Y^H Y (+ shift I), G = R^H R, Y <- Y R^-1 (and
 // HY with the same R).  ok = false when the factorisation broke down (Y is
 // left unchanged then).  min_rdiag: smallest diagonal entry of R.
-Status chol_qr(Ctx& c, double2* Y, double2* HY, int q, double shift, bool& ok, double* min_rdiag = nullptr) {
+template <typename T>
+Status chol_qr(Ctx& c, T* Y, T* HY, int q, double shift, bool& ok, double* min_rdiag = nullptr) {
   ok = true;
   if (q == 0) return kOk;
   Status r;
-  if ((r = zgemm(c, CUBLAS_OP_C, CUBLAS_OP_N, q, q, (int)c.n, Y, c.n, Y, c.n, c.w.G, q)) != kOk) return r;
+  T* G = as<T>(c.w.G);
+  if ((r = gemm(c, CUBLAS_OP_C, CUBLAS_OP_N, q, q, (int)c.n, Y, c.n, Y, c.n, G, q)) != kOk) return r;
   if (shift > 0.0) {
-    // add shift to the diagonal through the identity buffer: G += shift I
-    k_set_identity<<<blocks_for((long)q * q), 256, 0, c.s>>>(c.w.Id, q); count_launch();
-    const cuDoubleComplex al = make_cuDoubleComplex(1.0, 0.0), be = make_cuDoubleComplex(shift, 0.0);
-    if (cublasZgeam(c.h.blas, CUBLAS_OP_N, CUBLAS_OP_N, q, q, &al, reinterpret_cast<cuDoubleComplex*>(c.w.G), q, &be,
-                    reinterpret_cast<cuDoubleComplex*>(c.w.Id), q, reinterpret_cast<cuDoubleComplex*>(c.w.G),
-                    q) != CUBLAS_STATUS_SUCCESS)
-      return fail(kCuda, "cublasZgeam failed (eigensolver)");
+    T* Id = as<T>(c.w.Id);
+    k_set_identity<T><<<blocks_for((long)q * q), 256, 0, c.s>>>(Id, q); count_launch();
+    if ((r = add_shift(c, G, Id, q, shift)) != kOk) return r;
   }
   if ((r = ensure_solver(c)) != kOk) return r;
-  int lwork = 0;
-  if (cusolverDnZpotrf_bufferSize(c.h.solver, CUBLAS_FILL_MODE_UPPER, q, reinterpret_cast<cuDoubleComplex*>(c.w.G), q,
-                                  &lwork) != CUSOLVER_STATUS_SUCCESS)
-    return fail(kCuda, "cusolverDnZpotrf_bufferSize failed");
-  if ((r = ensure_solver_work(c, (size_t)lwork)) != kOk) return r;
-  if (cusolverDnZpotrf(c.h.solver, CUBLAS_FILL_MODE_UPPER, q, reinterpret_cast<cuDoubleComplex*>(c.w.G), q,
-                       reinterpret_cast<cuDoubleComplex*>(c.w.solver_work), lwork,
-                       c.w.info) != CUSOLVER_STATUS_SUCCESS)
-    return fail(kCuda, "cusolverDnZpotrf failed");
+  if ((r = potrf(c, G, q)) != kOk) return r;
   int info = 0;
   PW_CUDA_TRY(cudaMemcpyAsync(&info, c.w.info, sizeof(int), cudaMemcpyDeviceToHost, c.s));
   std::vector<double> dg;
   if (min_rdiag) {
     dg.resize(q);
-    k_diag_real<<<blocks_for(q), 256, 0, c.s>>>(c.w.G, q, q, c.w.colsq); count_launch();
+    k_diag_real<T><<<blocks_for(q), 256, 0, c.s>>>(G, q, q, c.w.colsq); count_launch();
     PW_CUDA_TRY(cudaMemcpyAsync(dg.data(), c.w.colsq, q * sizeof(double), cudaMemcpyDeviceToHost, c.s));
   }
   PW_CUDA_TRY(cudaStreamSynchronize(c.s));
@@ -281,14 +419,8 @@ Status chol_qr(Ctx& c, double2* Y, double2* HY, int q, double shift, bool& ok, d
     for (double d : dg) mn = std::min(mn, std::fabs(d));
     *min_rdiag = mn;
   }
-  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
-  for (double2* M : {Y, HY}) {
-    if (!M) continue;
-    if (cublasZtrsm(c.h.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, (int)c.n,
-                    q, &one, reinterpret_cast<const cuDoubleComplex*>(c.w.G), q, reinterpret_cast<cuDoubleComplex*>(M),
-                    (int)c.n) != CUBLAS_STATUS_SUCCESS)
-      return fail(kCuda, "cublasZtrsm failed (eigensolver)");
-  }
+  if ((r = trsm_right_upper(c, G, q, Y)) != kOk) return r;
+  if (HY && (r = trsm_right_upper(c, G, q, HY)) != kOk) return r;
   return kOk;
 }
 
@@ -296,68 +428,77 @@ Status chol_qr(Ctx& c, double2* Y, double2* HY, int q, double shift, bool& ok, d
 // Cholesky-QR passes; a breakdown of the first pass is retried with a small
 // diagonal shift, which still yields an orthonormal block after the second
 // pass.
-Status orthonormalize(Ctx& c, double2* Y, int q) {
+template <typename T> Status orthonormalize(Ctx& c, T* Y, int q) {
   if (q == 0) return kOk;
   Status r;
-  if ((r = col_norms2(c, Y, q, nullptr)) != kOk) return r;
-  k_scale_cols_invsqrt<<<dim3(c.gx, q), 256, 0, c.s>>>(Y, nullptr, c.n, (int)c.n, c.w.colsq); count_launch();
+  if ((r = col_norms2(c, (const T*)Y, q, nullptr)) != kOk) return r;
+  k_scale_cols_invsqrt<T><<<dim3(c.gx, q), 256, 0, c.s>>>(Y, nullptr, c.n, (int)c.n, c.w.colsq); count_launch();
   bool ok = false;
-  if ((r = chol_qr(c, Y, nullptr, q, 0.0, ok)) != kOk) return r;
+  if ((r = chol_qr(c, Y, (T*)nullptr, q, 0.0, ok)) != kOk) return r;
   if (!ok) {
-    if ((r = chol_qr(c, Y, nullptr, q, 1e-10 * q, ok)) != kOk) return r;
+    if ((r = chol_qr(c, Y, (T*)nullptr, q, 1e-10 * q, ok)) != kOk) return r;
     if (!ok) return fail(kNotConverged, "eigensolver: search block is numerically rank deficient");
   }
-  if ((r = chol_qr(c, Y, nullptr, q, 0.0, ok)) != kOk) return r;
+  if ((r = chol_qr(c, Y, (T*)nullptr, q, 0.0, ok)) != kOk) return r;
   if (!ok) return fail(kNotConverged, "eigensolver: second Cholesky-QR pass broke down");
   return kOk;
 }
 
-// Lowest nev eigenpairs of the Hermitian subspace matrix w.Hs (m x m):
-// values into w.lam, vectors into *C (ld m).
-Status subspace_eig(Ctx& c, int m, int nev, double2** C) {
+// Lowest nev eigenpairs of the Hermitian subspace matrix Hs (m x m): values
+// into w.lam, vectors into *C (ld m).
+template <typename T> Status subspace_eig(Ctx& c, int m, int nev, T** C) {
   Status r;
+  T* Hs = as<T>(c.w.Hs);
   if (m <= kSmallSolveMax) {
-    k_set_identity<<<blocks_for((long)m * m), 256, 0, c.s>>>(c.w.Id, m); count_launch();
-    if ((r = small_geneig_batched(c.w.Hs, c.w.Id, m, 0, m, nev, 1, c.w.lam, c.w.Cs, m, 0, c.w.status, c.s)) != kOk)
+    // one-CTA Cholesky + Jacobi solver (complex; a real symmetric input stays real)
+    const double2* Hz = c.w.Hs;
+    if (std::is_same<T, double>::value) {
+      k_real_to_complex<<<blocks_for((long)m * m), 256, 0, c.s>>>(reinterpret_cast<const double*>(c.w.Hs), c.w.G,
+                                                                  (long)m * m); count_launch();
+      Hz = c.w.G;
+    }
+    k_set_identity<double2><<<blocks_for((long)m * m), 256, 0, c.s>>>(c.w.Id, m); count_launch();
+    if ((r = small_geneig_batched(Hz, c.w.Id, m, 0, m, nev, 1, c.w.lam, c.w.Cs, m, 0, c.w.status, c.s)) != kOk)
       return r;
     int st = 0;
     PW_CUDA_TRY(cudaMemcpyAsync(&st, c.w.status, sizeof(int), cudaMemcpyDeviceToHost, c.s));
     PW_CUDA_TRY(cudaStreamSynchronize(c.s));
     if (st == 1) return fail(kNotConverged, "eigensolver: subspace solve failed");
-    *C = c.w.Cs;
+    if (std::is_same<T, double>::value) {
+      // real parts into Hs (the complex vectors of a real symmetric matrix are real)
+      k_complex_to_real<<<blocks_for((long)m * nev), 256, 0, c.s>>>(c.w.Cs, reinterpret_cast<double*>(c.w.Hs),
+                                                                    (long)m * nev); count_launch();
+      *C = Hs;
+    } else {
+      *C = as<T>(c.w.Cs);
+    }
     return kOk;
   }
   if ((r = ensure_solver(c)) != kOk) return r;
-  int lwork = 0;
-  if (cusolverDnZheevd_bufferSize(c.h.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, m,
-                                  reinterpret_cast<cuDoubleComplex*>(c.w.Hs), m, c.w.lam,
-                                  &lwork) != CUSOLVER_STATUS_SUCCESS)
-    return fail(kCuda, "cusolverDnZheevd_bufferSize failed");
-  if ((r = ensure_solver_work(c, (size_t)lwork)) != kOk) return r;
-  if (cusolverDnZheevd(c.h.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, m,
-                       reinterpret_cast<cuDoubleComplex*>(c.w.Hs), m, c.w.lam,
-                       reinterpret_cast<cuDoubleComplex*>(c.w.solver_work), lwork,
-                       c.w.info) != CUSOLVER_STATUS_SUCCESS)
-    return fail(kCuda, "cusolverDnZheevd failed");
+  if ((r = heevd(c, Hs, m, c.w.lam)) != kOk) return r;
   int info = 0;
   PW_CUDA_TRY(cudaMemcpyAsync(&info, c.w.info, sizeof(int), cudaMemcpyDeviceToHost, c.s));
   PW_CUDA_TRY(cudaStreamSynchronize(c.s));
   if (info != 0) return fail(kNotConverged, "eigensolver: subspace eigensolver did not converge");
-  *C = c.w.Hs;
+  *C = Hs;
   return kOk;
 }
 
 // Rayleigh-Ritz in span(X) alone (X orthonormal): X <- X C, HX <- HX C.
-Status rr_block(Ctx& c, EigVecs& k, int nd) {
+template <typename T> Status rr_block(Ctx& c, EigVecs& k, int nd) {
   Status r;
-  if ((r = zgemm(c, CUBLAS_OP_C, CUBLAS_OP_N, nd, nd, (int)c.n, k.V, c.n, k.HV, c.n, c.w.G, nd)) != kOk) return r;
-  k_assemble_rr<<<blocks_for((long)nd * nd), 256, 0, c.s>>>(c.w.Hs, nd, 0, c.w.lam0, c.w.Z, c.w.G); count_launch();
-  double2* C = nullptr;
-  if ((r = subspace_eig(c, nd, nd, &C)) != kOk) return r;
-  if ((r = zgemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.n, nd, nd, k.V, c.n, C, nd, c.w.T, c.n)) != kOk) return r;
-  if ((r = zgemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.n, nd, nd, k.HV, c.n, C, nd, c.w.HXn, c.n)) != kOk) return r;
-  PW_CUDA_TRY(cudaMemcpyAsync(k.V, c.w.T, c.n * nd * sizeof(double2), cudaMemcpyDeviceToDevice, c.s));
-  PW_CUDA_TRY(cudaMemcpyAsync(k.HV, c.w.HXn, c.n * nd * sizeof(double2), cudaMemcpyDeviceToDevice, c.s));
+  T* X = as<T>(k.V);
+  T* HX = as<T>(k.HV);
+  T* G = as<T>(c.w.G);
+  if ((r = gemm(c, CUBLAS_OP_C, CUBLAS_OP_N, nd, nd, (int)c.n, X, c.n, HX, c.n, G, nd)) != kOk) return r;
+  k_assemble_rr<T><<<blocks_for((long)nd * nd), 256, 0, c.s>>>(as<T>(c.w.Hs), nd, 0, c.w.lam0, as<T>(c.w.Z), G);
+  count_launch();
+  T* C = nullptr;
+  if ((r = subspace_eig<T>(c, nd, nd, &C)) != kOk) return r;
+  if ((r = gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.n, nd, nd, X, c.n, C, nd, as<T>(c.w.T), c.n)) != kOk) return r;
+  if ((r = gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.n, nd, nd, HX, c.n, C, nd, as<T>(c.w.HXn), c.n)) != kOk) return r;
+  PW_CUDA_TRY(cudaMemcpyAsync(X, c.w.T, c.n * nd * sizeof(T), cudaMemcpyDeviceToDevice, c.s));
+  PW_CUDA_TRY(cudaMemcpyAsync(HX, c.w.HXn, c.n * nd * sizeof(T), cudaMemcpyDeviceToDevice, c.s));
   PW_CUDA_TRY(cudaMemcpyAsync(k.evals.data(), c.w.lam, nd * sizeof(double), cudaMemcpyDeviceToHost, c.s));
   PW_CUDA_TRY(cudaStreamSynchronize(c.s));
   return kOk;
@@ -391,6 +532,180 @@ struct PhaseTimer {
     }
   }
 };
+
+inline void noise(double& x, std::mt19937_64& rng, std::uniform_real_distribution<double>& u) { x = 1e-3 * u(rng); }
+inline void noise(double2& x, std::mt19937_64& rng, std::uniform_real_distribution<double>& u) {
+  const double a = 1e-3 * u(rng);
+  x = make_double2(a, 1e-3 * u(rng));
+}
+inline void add_real(double& x, double v) { x += v; }
+inline void add_real(double2& x, double v) { x.x += v; }
+
+template <typename T>
+Status lobpcg_t(Handle& h, EigWork& w, EigVecs& k, int spin, int ik, double v0, double tol, int max_iter, int nconv,
+                int precision, EigStats& out) {
+  const long n = h.n_pw;
+  const int nd = w.nd;
+  const cudaStream_t s = h.stream;
+  cublasSetStream(h.blas, s);
+  Ctx c{h, w, s, n, (unsigned)std::min<long>(kColBlocks, blocks_for(n))};
+  Status r;
+  T* X = as<T>(k.V);
+  T* HX = as<T>(k.HV);
+  const double* kin = std::is_same<T, double>::value ? h.gam.kin_packed : h.kp[ik].kinetic;
+  if (!k.init) {
+    // start: unit vectors on the nd lowest kinetic entries plus seeded noise
+    std::vector<double> kh(n);
+    PW_CUDA_TRY(cudaMemcpyAsync(kh.data(), kin, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    PW_CUDA_TRY(cudaStreamSynchronize(s));
+    std::vector<int> order(n);
+    for (long i = 0; i < n; ++i) order[i] = (int)i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return kh[a] < kh[b]; });
+    std::vector<T> x0((size_t)n * nd);
+    std::mt19937_64 rng(20261203ULL + 7919ULL * (ik + 1) + 104729ULL * spin);
+    std::uniform_real_distribution<double> u(-1.0, 1.0);
+    for (size_t i = 0; i < x0.size(); ++i) noise(x0[i], rng, u);
+    for (int col = 0; col < nd && col < n; ++col) add_real(x0[(size_t)col * n + order[col]], 1.0);
+    PW_CUDA_TRY(cudaMemcpyAsync(X, x0.data(), x0.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+    PW_CUDA_TRY(cudaStreamSynchronize(s));
+    k.init = true;
+  }
+  if ((r = orthonormalize(c, X, nd)) != kOk) return r;
+  // HX in FP64: the residuals below refer to the full-precision operator
+  if ((r = apply_op(h, spin, ik, X, n, nd, HX, 0, s)) != kOk) return r;
+  out.happ += nd;
+  if ((r = rr_block<T>(c, k, nd)) != kOk) return r;
+
+  const double p_drop = precision == 0 ? kPDropFp64 : kPDropMixed;
+  T* Tb = as<T>(w.T);
+  T* Pn = as<T>(w.Pn);
+  T* HPn = as<T>(w.HPn);
+  std::vector<double> rn(nd), nu0, nu1;
+  std::vector<int> act, pband, keep, pk;
+  int np = 0;  // columns of Pn / HPn (bands pband)
+  out.iters = 0;
+  PhaseTimer pt(h.trace);
+  for (;;) {
+    const auto t0 = std::chrono::steady_clock::now();
+    pt.mark(0, s);
+    PW_CUDA_TRY(cudaMemcpyAsync(w.lam0, k.evals.data(), nd * sizeof(double), cudaMemcpyHostToDevice, s));
+    k_resid_precond<T><<<dim3(c.gx, nd), 256, 0, s>>>(X, HX, Tb, n, (int)n, w.lam0, kin, v0, w.partials);
+    count_launch();
+    k_col_final<<<blocks_for(nd), 256, 0, s>>>(w.partials, (int)c.gx, nd, w.colsq); count_launch();
+    PW_CUDA_TRY(cudaMemcpyAsync(rn.data(), w.colsq, nd * sizeof(double), cudaMemcpyDeviceToHost, s));
+    PW_CUDA_TRY(cudaStreamSynchronize(s));
+    out.max_res = 0.0;
+    for (int b = 0; b < nconv; ++b) out.max_res = std::max(out.max_res, std::sqrt(rn[b]));
+    if (out.max_res < tol || out.iters >= max_iter) break;
+    // active bands: residual above tol (buffer bands: 10 tol)
+    act.clear();
+    for (int b = 0; b < nd; ++b)
+      if (std::sqrt(rn[b]) > (b < nconv ? tol : 10.0 * tol)) act.push_back(b);
+    if ((long)act.size() > n - nd) act.resize((size_t)std::max<long>(0, n - nd));
+    const int na = (int)act.size();
+    if (na == 0) break;
+    T* W = X + n * nd;
+    T* HW = HX + n * nd;
+    pt.mark(1, s);
+    PW_CUDA_TRY(cudaMemcpyAsync(w.idx, act.data(), na * sizeof(int), cudaMemcpyHostToDevice, s));
+    k_gather_cols<T><<<dim3(c.gx, na), 256, 0, s>>>(Tb, n, w.idx, W, n, (int)n); count_launch();
+    if ((r = project_out(c, (const T*)X, (const T*)nullptr, nd, W, (T*)nullptr, na)) != kOk) return r;
+    if ((r = project_out(c, (const T*)X, (const T*)nullptr, nd, W, (T*)nullptr, na)) != kOk) return r;
+    if ((r = orthonormalize(c, W, na)) != kOk) return r;
+    pt.mark(2, s);
+    if ((r = apply_op(h, spin, ik, W, n, na, HW, precision, s)) != kOk) return r;
+    out.happ += na;
+    pt.mark(3, s);
+    // P: previous directions of the bands still active
+    int npc = 0;
+    pk.clear();
+    for (int j = 0, a = 0; j < np; ++j) {
+      while (a < na && act[a] < pband[j]) ++a;
+      if (a < na && act[a] == pband[j]) pk.push_back(j);
+    }
+    if ((long)pk.size() > n - nd - na) pk.resize((size_t)std::max<long>(0, n - nd - na));
+    T* P = W + n * na;
+    T* HP = HW + n * na;
+    if (!pk.empty()) {
+      npc = (int)pk.size();
+      PW_CUDA_TRY(cudaMemcpyAsync(w.idx, pk.data(), npc * sizeof(int), cudaMemcpyHostToDevice, s));
+      k_gather_cols<T><<<dim3(c.gx, npc), 256, 0, s>>>(Pn, n, w.idx, P, n, (int)n); count_launch();
+      k_gather_cols<T><<<dim3(c.gx, npc), 256, 0, s>>>(HPn, n, w.idx, HP, n, (int)n); count_launch();
+      nu0.resize(npc);
+      nu1.resize(npc);
+      if ((r = col_norms2(c, (const T*)P, npc, nu0.data())) != kOk) return r;
+      if ((r = project_out(c, (const T*)X, (const T*)HX, nd, P, HP, npc)) != kOk) return r;
+      if ((r = project_out(c, (const T*)W, (const T*)HW, na, P, HP, npc)) != kOk) return r;
+      if ((r = col_norms2(c, (const T*)P, npc, nu1.data())) != kOk) return r;
+      keep.clear();
+      for (int j = 0; j < npc; ++j)
+        if (nu1[j] > p_drop * p_drop * nu0[j] && nu1[j] > 0.0) keep.push_back(j);
+      if ((int)keep.size() < npc && !keep.empty()) {
+        // compact through Pn / HPn (their old contents were consumed above)
+        const int nk = (int)keep.size();
+        PW_CUDA_TRY(cudaMemcpyAsync(w.idx, keep.data(), nk * sizeof(int), cudaMemcpyHostToDevice, s));
+        k_gather_cols<T><<<dim3(c.gx, nk), 256, 0, s>>>(P, n, w.idx, Pn, n, (int)n); count_launch();
+        k_gather_cols<T><<<dim3(c.gx, nk), 256, 0, s>>>(HP, n, w.idx, HPn, n, (int)n); count_launch();
+        PW_CUDA_TRY(cudaMemcpyAsync(P, Pn, n * nk * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        PW_CUDA_TRY(cudaMemcpyAsync(HP, HPn, n * nk * sizeof(T), cudaMemcpyDeviceToDevice, s));
+      }
+      npc = (int)keep.size();
+      if (npc > 0) {
+        if ((r = col_norms2(c, (const T*)P, npc, nullptr)) != kOk) return r;
+        k_scale_cols_invsqrt<T><<<dim3(c.gx, npc), 256, 0, s>>>(P, HP, n, (int)n, w.colsq); count_launch();
+        bool ok = false;
+        double rmin = 0.0;
+        if ((r = chol_qr(c, P, HP, npc, 0.0, ok, &rmin)) != kOk) return r;
+        if (!ok || rmin < p_drop) {
+          npc = 0;  // P block nearly dependent: restart without it
+        } else if ((r = chol_qr(c, P, HP, npc, 0.0, ok)) != kOk) {
+          return r;
+        } else if (!ok) {
+          npc = 0;
+        }
+      }
+    }
+    // Rayleigh-Ritz over [X | W | P]
+    pt.mark(4, s);
+    const int q = na + npc, m = nd + q;
+    if ((r = gemm(c, CUBLAS_OP_C, CUBLAS_OP_N, q, nd, (int)n, W, n, HX, n, as<T>(w.Z), q)) != kOk) return r;
+    if ((r = gemm(c, CUBLAS_OP_C, CUBLAS_OP_N, q, q, (int)n, W, n, HW, n, as<T>(w.G), q)) != kOk) return r;
+    k_assemble_rr<T><<<blocks_for((long)m * m), 256, 0, s>>>(as<T>(w.Hs), m, nd, w.lam0, as<T>(w.Z), as<T>(w.G));
+    count_launch();
+    T* C = nullptr;
+    pt.mark(5, s);
+    if ((r = subspace_eig<T>(c, m, nd, &C)) != kOk) return r;
+    pt.mark(6, s);
+    // new X, HX; new P, HP for the active bands from the (W, P) rows of C
+    if ((r = gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, nd, m, X, n, C, m, Tb, n)) != kOk) return r;
+    if ((r = gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, nd, m, HX, n, C, m, as<T>(w.HXn), n)) != kOk) return r;
+    PW_CUDA_TRY(cudaMemcpyAsync(w.idx, act.data(), na * sizeof(int), cudaMemcpyHostToDevice, s));
+    T* Ca = C == as<T>(w.Cs) ? as<T>(w.Z) : as<T>(w.Cs);  // q x na gathered columns, ld q
+    k_gather_cols<T><<<dim3(1, na), 256, 0, s>>>(C + nd, m, w.idx, Ca, q, q); count_launch();
+    if ((r = gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, na, q, W, n, Ca, q, Pn, n)) != kOk) return r;
+    if ((r = gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, na, q, HW, n, Ca, q, HPn, n)) != kOk) return r;
+    PW_CUDA_TRY(cudaMemcpyAsync(X, Tb, n * nd * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    PW_CUDA_TRY(cudaMemcpyAsync(HX, w.HXn, n * nd * sizeof(T), cudaMemcpyDeviceToDevice, s));
+    PW_CUDA_TRY(cudaMemcpyAsync(k.evals.data(), w.lam, nd * sizeof(double), cudaMemcpyDeviceToHost, s));
+    pt.mark(7, s);
+    PW_CUDA_TRY(cudaStreamSynchronize(s));
+    pt.accumulate();
+    np = na;
+    pband = act;
+    ++out.iters;
+    if (h.trace) {
+      const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+      std::fprintf(stderr, "pwgpu lobpcg k=%d it=%d res=%.3e na=%d np=%d e0=%.8f e_last=%.8f %.2f ms\n", ik,
+                   out.iters, out.max_res, na, npc, k.evals[0], k.evals[nconv - 1], ms);
+    }
+  }
+  if (pt.on)
+    std::fprintf(stderr,
+                 "pwgpu lobpcg k=%d phases ms: resid %.2f W %.2f HW %.2f P %.2f matrix %.2f solve %.2f update %.2f\n",
+                 ik, pt.total[0], pt.total[1], pt.total[2], pt.total[3], pt.total[4], pt.total[5], pt.total[6]);
+  PW_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
 
 }  // namespace
 
@@ -447,163 +762,10 @@ void eig_vecs_release(EigVecs& v) {
 
 Status lobpcg(Handle& h, EigWork& w, EigVecs& k, int spin, int ik, double v0, double tol, int max_iter, int nconv,
               int precision, EigStats& out) {
-  const long n = h.n_pw;
-  const int nd = w.nd;
-  if (n != w.n || nd < 1 || nconv < 1 || nconv > nd) return fail(kInvalid, "eigensolver: inconsistent block sizes");
-  const cudaStream_t s = h.stream;
-  cublasSetStream(h.blas, s);
-  Ctx c{h, w, s, n, (unsigned)std::min<long>(kColBlocks, blocks_for(n))};
-  Status r;
-  double2* X = k.V;
-  double2* HX = k.HV;
-  if (!k.init) {
-    // start: unit vectors on the nd lowest |k+G|^2 plus seeded noise
-    std::vector<double> kin(n);
-    PW_CUDA_TRY(cudaMemcpyAsync(kin.data(), h.kp[ik].kinetic, n * sizeof(double), cudaMemcpyDeviceToHost, s));
-    PW_CUDA_TRY(cudaStreamSynchronize(s));
-    std::vector<int> order(n);
-    for (long i = 0; i < n; ++i) order[i] = (int)i;
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return kin[a] < kin[b]; });
-    std::vector<double2> x0((size_t)n * nd);
-    std::mt19937_64 rng(20261203ULL + 7919ULL * (ik + 1) + 104729ULL * spin);
-    std::uniform_real_distribution<double> u(-1.0, 1.0);
-    for (int col = 0; col < nd; ++col)
-      for (long i = 0; i < n; ++i) x0[(size_t)col * n + i] = make_double2(1e-3 * u(rng), 1e-3 * u(rng));
-    for (int col = 0; col < nd && col < n; ++col) x0[(size_t)col * n + order[col]].x += 1.0;
-    PW_CUDA_TRY(cudaMemcpyAsync(X, x0.data(), x0.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
-    k.init = true;
-  }
-  if ((r = orthonormalize(c, X, nd)) != kOk) return r;
-  // HX in FP64: the residuals below refer to the full-precision operator
-  if ((r = apply_h_device(h, spin, ik, X, n, nd, HX, n, 0, s)) != kOk) return r;
-  out.happ += nd;
-  if ((r = rr_block(c, k, nd)) != kOk) return r;
-
-  const double p_drop = precision == 0 ? kPDropFp64 : kPDropMixed;
-  std::vector<double> rn(nd), nu0, nu1;
-  std::vector<int> act, pband, keep, pk;
-  int np = 0;  // columns of Pn / HPn (bands pband)
-  out.iters = 0;
-  PhaseTimer pt(h.trace);
-  for (;;) {
-    const auto t0 = std::chrono::steady_clock::now();
-    pt.mark(0, s);
-    PW_CUDA_TRY(cudaMemcpyAsync(w.lam0, k.evals.data(), nd * sizeof(double), cudaMemcpyHostToDevice, s));
-    k_resid_precond<<<dim3(c.gx, nd), 256, 0, s>>>(X, HX, w.T, n, (int)n, w.lam0, h.kp[ik].kinetic, v0,
-                                                   w.partials); count_launch();
-    k_col_final<<<blocks_for(nd), 256, 0, s>>>(w.partials, (int)c.gx, nd, w.colsq); count_launch();
-    PW_CUDA_TRY(cudaMemcpyAsync(rn.data(), w.colsq, nd * sizeof(double), cudaMemcpyDeviceToHost, s));
-    PW_CUDA_TRY(cudaStreamSynchronize(s));
-    out.max_res = 0.0;
-    for (int b = 0; b < nconv; ++b) out.max_res = std::max(out.max_res, std::sqrt(rn[b]));
-    if (out.max_res < tol || out.iters >= max_iter) break;
-    // active bands: residual above tol (buffer bands: 10 tol)
-    act.clear();
-    for (int b = 0; b < nd; ++b)
-      if (std::sqrt(rn[b]) > (b < nconv ? tol : 10.0 * tol)) act.push_back(b);
-    if ((long)act.size() > n - nd) act.resize((size_t)std::max<long>(0, n - nd));
-    const int na = (int)act.size();
-    if (na == 0) break;
-    double2* W = k.V + n * nd;
-    double2* HW = k.HV + n * nd;
-    pt.mark(1, s);
-    PW_CUDA_TRY(cudaMemcpyAsync(w.idx, act.data(), na * sizeof(int), cudaMemcpyHostToDevice, s));
-    k_gather_cols<<<dim3(c.gx, na), 256, 0, s>>>(w.T, n, w.idx, W, n, (int)n); count_launch();
-    if ((r = project_out(c, X, nullptr, nd, W, nullptr, na)) != kOk) return r;
-    if ((r = project_out(c, X, nullptr, nd, W, nullptr, na)) != kOk) return r;
-    if ((r = orthonormalize(c, W, na)) != kOk) return r;
-    pt.mark(2, s);
-    if ((r = apply_h_device(h, spin, ik, W, n, na, HW, n, precision, s)) != kOk) return r;
-    out.happ += na;
-    pt.mark(3, s);
-    // P: previous directions of the bands still active
-    int npc = 0;
-    pk.clear();
-    for (int j = 0, a = 0; j < np; ++j) {
-      while (a < na && act[a] < pband[j]) ++a;
-      if (a < na && act[a] == pband[j]) pk.push_back(j);
-    }
-    if ((long)pk.size() > n - nd - na) pk.resize((size_t)std::max<long>(0, n - nd - na));
-    double2* P = W + n * na;
-    double2* HP = HW + n * na;
-    if (!pk.empty()) {
-      npc = (int)pk.size();
-      PW_CUDA_TRY(cudaMemcpyAsync(w.idx, pk.data(), npc * sizeof(int), cudaMemcpyHostToDevice, s));
-      k_gather_cols<<<dim3(c.gx, npc), 256, 0, s>>>(w.Pn, n, w.idx, P, n, (int)n); count_launch();
-      k_gather_cols<<<dim3(c.gx, npc), 256, 0, s>>>(w.HPn, n, w.idx, HP, n, (int)n); count_launch();
-      nu0.resize(npc);
-      nu1.resize(npc);
-      if ((r = col_norms2(c, P, npc, nu0.data())) != kOk) return r;
-      if ((r = project_out(c, X, HX, nd, P, HP, npc)) != kOk) return r;
-      if ((r = project_out(c, W, HW, na, P, HP, npc)) != kOk) return r;
-      if ((r = col_norms2(c, P, npc, nu1.data())) != kOk) return r;
-      keep.clear();
-      for (int j = 0; j < npc; ++j)
-        if (nu1[j] > p_drop * p_drop * nu0[j] && nu1[j] > 0.0) keep.push_back(j);
-      if ((int)keep.size() < npc && !keep.empty()) {
-        // compact through Pn / HPn (their old contents were consumed above)
-        const int nk = (int)keep.size();
-        PW_CUDA_TRY(cudaMemcpyAsync(w.idx, keep.data(), nk * sizeof(int), cudaMemcpyHostToDevice, s));
-        k_gather_cols<<<dim3(c.gx, nk), 256, 0, s>>>(P, n, w.idx, w.Pn, n, (int)n); count_launch();
-        k_gather_cols<<<dim3(c.gx, nk), 256, 0, s>>>(HP, n, w.idx, w.HPn, n, (int)n); count_launch();
-        PW_CUDA_TRY(cudaMemcpyAsync(P, w.Pn, n * nk * sizeof(double2), cudaMemcpyDeviceToDevice, s));
-        PW_CUDA_TRY(cudaMemcpyAsync(HP, w.HPn, n * nk * sizeof(double2), cudaMemcpyDeviceToDevice, s));
-      }
-      npc = (int)keep.size();
-      if (npc > 0) {
-        if ((r = col_norms2(c, P, npc, nullptr)) != kOk) return r;
-        k_scale_cols_invsqrt<<<dim3(c.gx, npc), 256, 0, s>>>(P, HP, n, (int)n, w.colsq); count_launch();
-        bool ok = false;
-        double rmin = 0.0;
-        if ((r = chol_qr(c, P, HP, npc, 0.0, ok, &rmin)) != kOk) return r;
-        if (!ok || rmin < p_drop) {
-          npc = 0;  // P block nearly dependent: restart without it
-        } else if ((r = chol_qr(c, P, HP, npc, 0.0, ok)) != kOk) {
-          return r;
-        } else if (!ok) {
-          npc = 0;
-        }
-      }
-    }
-    // Rayleigh-Ritz over [X | W | P]
-    pt.mark(4, s);
-    const int q = na + npc, m = nd + q;
-    if ((r = zgemm(c, CUBLAS_OP_C, CUBLAS_OP_N, q, nd, (int)n, W, n, HX, n, w.Z, q)) != kOk) return r;
-    if ((r = zgemm(c, CUBLAS_OP_C, CUBLAS_OP_N, q, q, (int)n, W, n, HW, n, w.G, q)) != kOk) return r;
-    k_assemble_rr<<<blocks_for((long)m * m), 256, 0, s>>>(w.Hs, m, nd, w.lam0, w.Z, w.G); count_launch();
-    double2* C = nullptr;
-    pt.mark(5, s);
-    if ((r = subspace_eig(c, m, nd, &C)) != kOk) return r;
-    pt.mark(6, s);
-    // new X, HX; new P, HP for the active bands from the (W, P) rows of C
-    if ((r = zgemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, nd, m, k.V, n, C, m, w.T, n)) != kOk) return r;
-    if ((r = zgemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, nd, m, k.HV, n, C, m, w.HXn, n)) != kOk) return r;
-    PW_CUDA_TRY(cudaMemcpyAsync(w.idx, act.data(), na * sizeof(int), cudaMemcpyHostToDevice, s));
-    double2* Ca = C == w.Cs ? w.Z : w.Cs;  // q x na gathered columns, ld q
-    k_gather_cols<<<dim3(1, na), 256, 0, s>>>(C + nd, m, w.idx, Ca, q, q); count_launch();
-    if ((r = zgemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, na, q, W, n, Ca, q, w.Pn, n)) != kOk) return r;
-    if ((r = zgemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, na, q, HW, n, Ca, q, w.HPn, n)) != kOk) return r;
-    PW_CUDA_TRY(cudaMemcpyAsync(X, w.T, n * nd * sizeof(double2), cudaMemcpyDeviceToDevice, s));
-    PW_CUDA_TRY(cudaMemcpyAsync(HX, w.HXn, n * nd * sizeof(double2), cudaMemcpyDeviceToDevice, s));
-    PW_CUDA_TRY(cudaMemcpyAsync(k.evals.data(), w.lam, nd * sizeof(double), cudaMemcpyDeviceToHost, s));
-    pt.mark(7, s);
-    PW_CUDA_TRY(cudaStreamSynchronize(s));
-    pt.accumulate();
-    np = na;
-    pband = act;
-    ++out.iters;
-    if (h.trace) {
-      const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-      std::fprintf(stderr, "pwgpu lobpcg k=%d it=%d res=%.3e na=%d np=%d e0=%.8f e_last=%.8f %.2f ms\n", ik,
-                   out.iters, out.max_res, na, npc, k.evals[0], k.evals[nconv - 1], ms);
-    }
-  }
-  if (pt.on)
-    std::fprintf(stderr,
-                 "pwgpu lobpcg k=%d phases ms: resid %.2f W %.2f HW %.2f P %.2f matrix %.2f solve %.2f update %.2f\n",
-                 ik, pt.total[0], pt.total[1], pt.total[2], pt.total[3], pt.total[4], pt.total[5], pt.total[6]);
-  PW_CUDA_TRY(cudaGetLastError());
-  return kOk;
+  if (h.n_pw != w.n || w.nd < 1 || nconv < 1 || nconv > w.nd)
+    return fail(kInvalid, "eigensolver: inconsistent block sizes");
+  if (h.gam.on) return lobpcg_t<double>(h, w, k, spin, ik, v0, tol, max_iter, nconv, precision, out);
+  return lobpcg_t<double2>(h, w, k, spin, ik, v0, tol, max_iter, nconv, precision, out);
 }
 
 }  // namespace pwgpu

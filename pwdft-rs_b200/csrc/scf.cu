@@ -360,6 +360,7 @@ static void release_lane(Lane& L) {
   Handle& v = L.view;
   eig_work_release(L.ew);
   release_nl_mixed(v);
+  release_gamma_scratch(v);
   auto f = [](void* p) { if (p) cudaFree(p); };
   f(v.work_a); f(v.work_b); f(v.nl_p); f(v.nl_q); f(v.solver_work); f(v.solver_info);
   if (v.solver) cusolverDnDestroy(v.solver);
@@ -389,6 +390,10 @@ static Status create_lane(Handle& h, Lane& L, int nd, int nlanes) {
   v.nlm = nullptr;
   v.scf = nullptr;
   v.tmp_grid = nullptr;
+  v.gam_c1 = v.gam_c2 = nullptr;
+  v.gam_ccap = 0;
+  v.gam_p = v.gam_q = nullptr;
+  v.gam_pcap = 0;
   // lanes share the L2: each keeps a proportionally smaller band chunk
   v.chunk = std::max(4, h.chunk / nlanes);
   PW_CUDA_TRY(cudaStreamCreateWithFlags(&v.stream, cudaStreamNonBlocking));
@@ -788,10 +793,16 @@ static Status build_density(Handle& h, const std::vector<std::vector<double>>& o
       fw.push_back(v);
     }
     if (fw.empty()) continue;
-    // pageable source: the copy has left fw when the call returns, and the
-    // device buffer is reused in stream order
-    PW_CUDA_TRY(cudaMemcpyAsync(st->fw, fw.data(), fw.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-    Status r = density_accumulate(h, st->ks[(size_t)spin * h.n_k + ik].V, n, (int)fw.size(), st->fw, rho, s);
+    const double2* v = st->ks[(size_t)spin * h.n_k + ik].V;
+    Status r;
+    if (h.gam.on) {
+      r = density_accumulate_real(h, reinterpret_cast<const double*>(v), n, fw, rho, s);
+    } else {
+      // pageable source: the copy has left fw when the call returns, and the
+      // device buffer is reused in stream order
+      PW_CUDA_TRY(cudaMemcpyAsync(st->fw, fw.data(), fw.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+      r = density_accumulate(h, v, n, (int)fw.size(), st->fw, rho, s);
+    }
     if (r != kOk) return r;
   }
   double tot = 0.0;
@@ -1149,15 +1160,28 @@ Status eigensolve_k(Handle& h, int spin, int ik, int n_bands, double tol, int ma
     // warm start: given n_bands columns, remaining columns from the cold-start recipe
     EigStats e0;
     if ((r = lobpcg(h, st->ew, k, spin, ik, v0, 1e300, 0, n_bands, precision, e0)) != kOk) return r;
-    PW_CUDA_TRY(cudaMemcpyAsync(k.V, psi_in, n * n_bands * sizeof(double2), cudaMemcpyHostToDevice, h.stream));
+    if (h.gam.on) {
+      // complex Gamma-real columns -> packed real bands (through the T scratch)
+      PW_CUDA_TRY(cudaMemcpyAsync(st->ew.T, psi_in, n * n_bands * sizeof(double2), cudaMemcpyHostToDevice, h.stream));
+      if ((r = gamma_pack(h, st->ew.T, n, n_bands, reinterpret_cast<double*>(k.V), n, h.stream)) != kOk) return r;
+    } else {
+      PW_CUDA_TRY(cudaMemcpyAsync(k.V, psi_in, n * n_bands * sizeof(double2), cudaMemcpyHostToDevice, h.stream));
+    }
   }
   EigStats es;
   if ((r = lobpcg(h, st->ew, k, spin, ik, v0, tol, max_iter, n_bands, precision, es)) != kOk) return r;
   const int its = es.iters;
   const double mres = es.max_res;
   for (int b = 0; b < n_bands; ++b) evals[b] = k.evals[b];
-  if (psi_out)
-    PW_CUDA_TRY(cudaMemcpyAsync(psi_out, k.V, n * n_bands * sizeof(double2), cudaMemcpyDeviceToHost, h.stream));
+  if (psi_out) {
+    const double2* src = k.V;
+    if (h.gam.on) {
+      if ((r = gamma_unpack(h, reinterpret_cast<const double*>(k.V), n, n_bands, st->ew.T, n, h.stream)) != kOk)
+        return r;
+      src = st->ew.T;
+    }
+    PW_CUDA_TRY(cudaMemcpyAsync(psi_out, src, n * n_bands * sizeof(double2), cudaMemcpyDeviceToHost, h.stream));
+  }
   PW_CUDA_TRY(cudaStreamSynchronize(h.stream));
   if (iters) *iters = its;
   if (max_res) *max_res = mres;
@@ -1176,8 +1200,15 @@ Status density_from_host(Handle& h, int n_bands, const double* occ, const double
   for (int ik = 0; ik < h.n_k; ++ik) {
     wk[ik] = h.kp[ik].weight;
     oc[ik].assign(occ + (size_t)ik * n_bands, occ + (size_t)(ik + 1) * n_bands);
-    PW_CUDA_TRY(cudaMemcpyAsync(st->ks[ik].V, psi_all + (size_t)ik * n * n_bands * 2, n * n_bands * sizeof(double2),
-                                cudaMemcpyHostToDevice, h.stream));
+    if (h.gam.on) {
+      PW_CUDA_TRY(cudaMemcpyAsync(st->ew.T, psi_all + (size_t)ik * n * n_bands * 2, n * n_bands * sizeof(double2),
+                                  cudaMemcpyHostToDevice, h.stream));
+      if ((r = gamma_pack(h, st->ew.T, n, n_bands, reinterpret_cast<double*>(st->ks[ik].V), n, h.stream)) != kOk)
+        return r;
+    } else {
+      PW_CUDA_TRY(cudaMemcpyAsync(st->ks[ik].V, psi_all + (size_t)ik * n * n_bands * 2,
+                                  n * n_bands * sizeof(double2), cudaMemcpyHostToDevice, h.stream));
+    }
   }
   if ((r = build_density(h, oc, wk, 0, st->rho_out, h.n_electrons)) != kOk) return r;
   PW_CUDA_TRY(cudaMemcpyAsync(rho_out, st->rho_out, h.g.N * sizeof(double), cudaMemcpyDeviceToHost, h.stream));

@@ -172,7 +172,7 @@ struct pwgpu_server {
         job->t_start = Clock::now();
         ++running;
       }
-      pwgpu_options o{opt.device, opt.precision, opt.lanes_per_job > 0 ? opt.lanes_per_job : 2};
+      pwgpu_options o{opt.device, opt.precision, opt.lanes_per_job > 0 ? opt.lanes_per_job : 2, 0};
       pwgpu_handle* h = nullptr;
       pwgpu_status st = pwgpu_create(&job->sys.sys, &o, &h);
       if (st == PWGPU_OK)

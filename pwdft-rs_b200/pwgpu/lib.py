@@ -64,7 +64,7 @@ class PwgpuSystem(ct.Structure):
 
 
 class PwgpuOptions(ct.Structure):
-    _fields_ = [("device", ct.c_int32), ("precision", ct.c_int32), ("lanes", ct.c_int32)]
+    _fields_ = [("device", ct.c_int32), ("precision", ct.c_int32), ("lanes", ct.c_int32), ("gamma_complex", ct.c_int32)]
 
 
 SMEARING = {"fermi_dirac": 0, "gaussian": 1, "methfessel_paxton": 2, "cold": 3, "fixed": 4}
@@ -257,11 +257,12 @@ def pack_system(sys_) -> tuple:
 class PwGpu:
     """One device handle (pwgpu_create .. pwgpu_destroy)."""
 
-    def __init__(self, sys_, precision: int = PRECISION_FP64, device: int = 0, lanes: int = 0):
+    def __init__(self, sys_, precision: int = PRECISION_FP64, device: int = 0, lanes: int = 0,
+                 gamma_complex: bool = False):
         self.lib = load_library()
         self.sys = sys_
         st, keep = pack_system(sys_)
-        opt = PwgpuOptions(device, precision, lanes)
+        opt = PwgpuOptions(device, precision, lanes, 1 if gamma_complex else 0)
         h = ct.c_void_p()
         _check(self.lib, self.lib.pwgpu_create(ct.byref(st), ct.byref(opt), ct.byref(h)))
         self.h = h

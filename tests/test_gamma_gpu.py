@@ -1,0 +1,80 @@
+"""Gamma-only handles store bands as real packed vectors (psi(-G) = conj
+psi(G)); the same system with `gamma_complex=True` keeps complex bands.
+Parity: eigenvalues against the oracle's dense diagonalisation (1e-7 Ha),
+returned eigenvectors Gamma-real and eigenvectors of the dense H (residual
+1e-6 eV), SCF energies of the two forms within the first-order drho error
+(total 1e-5 eV, Harris-Foulkes 1e-6 eV), mixed form too."""
+
+import numpy as np
+import pytest
+
+from oracle import pwdft_oracle as O
+from pwgpu.consts import HA_TO_EV
+from pwgpu.context import build_system
+from pwgpu.crystal import diamond_primitive, diamond_supercell, gamma_only
+from pwgpu.lib import PRECISION_FP64, PRECISION_MIXED, PwGpu
+from pwgpu.symmetry import SymmetryInfo
+
+pytestmark = pytest.mark.gpu
+
+
+def sad_veff(s):
+    rho_g = O.density_r_to_g(s.rho_init_r, s.dims)
+    _, vxc = O.lda_xc(O.add_core(s.rho_init_r, s.rho_core_r))
+    return s.v_local_g + O.hartree(rho_g, s.g_squared) + O.density_r_to_g(vxc, s.dims)
+
+
+def si8(pp):
+    cr = diamond_supercell("Si", 5.431, displacement_ang=0.02, rng=np.random.default_rng(5))
+    return build_system(cr, {"Si": pp}, 120.0, gamma_only(), SymmetryInfo.identity_only())
+
+
+def test_gamma_eigensolve_matches_dense(si_pp):
+    s = si8(si_pp)
+    veff = sad_veff(s)
+    p = s.projectors[0]
+    h = O.dense_hamiltonian(s.basis.miller, s.kinetic[0], veff, s.dims, p.b, p.d_dense())
+    w, _ = np.linalg.eigh(h)
+    nb = 20
+    with PwGpu(s) as dev:
+        dev.set_veff_g(veff)
+        ev, psi, its, res = dev.eigensolve(nb, tol=1e-8, max_iter=300)
+    assert np.max(np.abs(ev - w[:nb])) < 1e-7 * HA_TO_EV
+    # eigenvectors: Gamma-real and H psi = e psi
+    m = s.basis.miller
+    where = {tuple(x): i for i, x in enumerate(m.tolist())}
+    neg = np.array([where[tuple((-x).tolist())] for x in m])
+    assert np.max(np.abs(psi[neg] - psi.conj())) < 1e-12
+    r = h @ psi - psi * ev[None, :]
+    assert np.max(np.linalg.norm(r, axis=0)) < 1e-6
+
+
+@pytest.mark.parametrize("precision", [PRECISION_FP64, PRECISION_MIXED])
+def test_gamma_real_scf_matches_complex(si_pp, precision):
+    s = build_system(diamond_primitive("Si", 5.431), {"Si": si_pp}, 100.0, gamma_only(), fft_grid=(16, 16, 16))
+    kw = dict(n_bands=6, max_iter=100, conv_threshold=1e-8, energy_threshold=1e-7, mixing_beta=0.3,
+              smearing="fermi_dirac", sigma=0.05, precision=precision)
+    with PwGpu(s) as dev:
+        rr, evr, rhor, _ = dev.scf_run(s.rho_init_r, **kw)
+    with PwGpu(s, gamma_complex=True) as dev:
+        rc, evc, rhoc, _ = dev.scf_run(s.rho_init_r, **kw)
+    assert rr["converged"] == 1 and rc["converged"] == 1
+    assert abs(rr["total_energy"] - rc["total_energy"]) < 1e-5
+    assert abs(rr["harris_foulkes_energy"] - rc["harris_foulkes_energy"]) < 1e-6
+    assert np.max(np.abs(evr - evc)) < 1e-5
+    assert abs(rr["total_energy"] - (-213.028339)) < 1e-3  # tests/cpu_scf_baseline.rs:43-44
+
+
+def test_gamma_real_density_matches_oracle(si_pp):
+    """Density of packed real bands (two per FFT, occupations folded into the
+    packing) against the oracle's compute_density."""
+    s = si8(si_pp)
+    veff = sad_veff(s)
+    nb = 18
+    with PwGpu(s) as dev:
+        dev.set_veff_g(veff)
+        ev, psi, _, _ = dev.eigensolve(nb, tol=1e-8, max_iter=300)
+        occ = np.linspace(2.0, 0.1, nb)[None, :]
+        rho = dev.density(occ, [psi])
+    ref = O.compute_density(s.g_to_fft, s.dims, [psi], [occ[0]], s.kpt_weights, s.n_electrons, s.omega)
+    assert np.max(np.abs(rho - ref)) < 1e-10 * np.max(ref)
