@@ -91,6 +91,9 @@ typedef struct pwgpu_options {
   int32_t lanes;      /* concurrent (spin, k) eigensolves inside pwgpu_scf_run, each on its own
                          stream (the reference's rayon loop over k, driver_spin.rs:356-384);
                          0 = min(nspin * n_k, 8), 1 = one block at a time */
+  int32_t gamma_complex;  /* 0: a system with the single k-point Gamma stores its bands as real vectors
+                             (psi(-G) = conj psi(G); real subspace algebra, two bands per FFT);
+                             1: keep complex bands */
 } pwgpu_options;
 
 /* Message of the calling thread's most recent failure ("" if none). */
@@ -154,7 +157,8 @@ typedef struct pwgpu_scf_params {
   double energy_threshold;  /* |E_n - E_{n-1}|, eV */
   double mixing_beta;
   int32_t mixing_ndim;
-  int32_t mixing_mode;      /* 0 plain Anderson, 1 Anderson + Kerker */
+  int32_t mixing_mode;      /* MixingMode (mixing/mod.rs:186-223): 0 Anderson (Plain), 1 Anderson + Kerker,
+                               2 Broyden, 3 Broyden + Kerker, 4 Periodic Pulay, 5 Periodic Pulay + Kerker */
   double kerker_q_tf;       /* Å^-1; <= 0 selects the Thomas-Fermi estimate */
   int32_t smearing;         /* 0 Fermi-Dirac, 1 Gaussian, 2 Methfessel-Paxton, 3 cold, 4 fixed */
   double smearing_sigma;    /* eV */
@@ -168,6 +172,7 @@ typedef struct pwgpu_scf_params {
   double starting_magnetization; /* atom average of the per-species fractions; rho splits (1 +- m)/2 */
   int32_t fixed_magnetization;   /* 1: tot_magnetization fixes N_up - N_down (one Fermi level per spin) */
   double tot_magnetization;
+  int32_t mixing_period;         /* Periodic Pulay: DIIS every period-th step (<= 0: 3) */
 } pwgpu_scf_params;
 
 /* ScfResult (scf/mod.rs:269-322) scalars. */
@@ -215,16 +220,19 @@ pwgpu_status pwgpu_symmetrize(pwgpu_handle* h, double* rho_r);
  * int rho_val v_xc (eV). */
 pwgpu_status pwgpu_potentials(pwgpu_handle* h, const double* rho_r, double* veff_g, double* energies);
 
-/* One density-mixing step (Mixer::mix, scf/mixing/mod.rs:281-287, for the
- * Plain and Kerker modes: AndersonMixer::mix, mixing/anderson.rs:170-266).
+/* One density-mixing step (Mixer::mix, scf/mixing/mod.rs:281-287):
+ * mode as pwgpu_scf_params.mixing_mode (Anderson, mixing/anderson.rs:170-266;
+ * modified Broyden, mixing/broyden.rs:140-245; Periodic Pulay,
+ * mixing/anderson.rs:294-372 with `period`; each with or without Kerker).
  * channel 0 or 1 selects one of two independent histories on the handle (the
  * CCMX total / magnetisation pair of driver_spin.rs:792-826).  rho_in,
  * rho_out, rho_next: N doubles on the host (rho_next may alias rho_in).
- * kerker != 0 preconditions the residual with G^2/(G^2 + q_tf^2), q_tf in
- * Å^-1 (<= 0: Thomas-Fermi estimate, kerker.rs:41-49).  The first call
- * after pwgpu_mix_reset (or after a change of ndim) starts a new history. */
-pwgpu_status pwgpu_mix(pwgpu_handle* h, int32_t channel, const double* rho_in, const double* rho_out,
-                       double* rho_next, double beta, int32_t ndim, int32_t kerker, double q_tf);
+ * Kerker preconditions the residual with G^2/(G^2 + q_tf^2), q_tf in Å^-1
+ * (Anderson: <= 0 selects the Thomas-Fermi estimate, kerker.rs:41-49;
+ * Broyden and Periodic Pulay always use the estimate).  The first call after
+ * pwgpu_mix_reset (or after a change of ndim) starts a new history. */
+pwgpu_status pwgpu_mix(pwgpu_handle* h, int32_t channel, int32_t mode, const double* rho_in, const double* rho_out,
+                       double* rho_next, double beta, int32_t ndim, int32_t period, double q_tf);
 pwgpu_status pwgpu_mix_reset(pwgpu_handle* h);
 
 /* Local part of H|psi> (kinetic diagonal + V_eff through the FFT pipeline;

@@ -368,6 +368,77 @@ class AndersonMixer:
         return out
 
 
+class BroydenMixer:
+    """Modified Broyden (mixing/broyden.rs:26-258): history of input and
+    residual differences, gamma = <df_i|df_j>^-1 <df_i|R>,
+    rho_new = (rho_in - sum gamma dv) + beta (R - sum gamma df)."""
+
+    def __init__(self, beta, ndim, dims, kerker_weights=None):
+        self.beta, self.ndim, self.dims = beta, ndim, dims
+        self.kw = kerker_weights
+        self.dv, self.df = [], []
+        self.prev_in = self.prev_res = None
+
+    def mix(self, rho_in, rho_out):
+        res = rho_out - rho_in
+        if self.kw is not None:
+            rg = fft3(res.astype(np.complex128), self.dims) * self.kw
+            res = (ifft3(rg, self.dims) / res.size).real.copy()
+        if self.prev_in is not None:
+            self.dv.append(rho_in - self.prev_in)
+            self.df.append(res - self.prev_res)
+            if len(self.dv) > self.ndim:
+                self.dv.pop(0)
+                self.df.pop(0)
+        self.prev_in, self.prev_res = rho_in.copy(), res.copy()
+        m = len(self.df)
+        if m == 0:
+            return rho_in + self.beta * res
+        a = np.array([[float(self.df[i] @ self.df[j]) for j in range(m)] for i in range(m)])
+        w = np.array([float(self.df[i] @ res) for i in range(m)])
+        g = solve_small(a, w)
+        cdv = sum(g[i] * self.dv[i] for i in range(m))
+        cdf = sum(g[i] * self.df[i] for i in range(m))
+        return (rho_in - cdv) + self.beta * (res - cdf)
+
+
+class PeriodicPulayMixer(AndersonMixer):
+    """Periodic Pulay (mixing/anderson.rs:294-386): Anderson history every
+    step, a DIIS step every `period`-th step (history >= 2), linear mixing
+    of the last entry otherwise."""
+
+    def __init__(self, beta, ndim, dims, period=3, kerker_weights=None):
+        super().__init__(beta, ndim, dims, kerker_weights)
+        self.period, self.iteration = period, 0
+
+    def mix(self, rho_in, rho_out):
+        self.iteration += 1
+        if self.iteration % self.period == 0:
+            return super().mix(rho_in, rho_out)  # linear while the history is shorter than 2
+        res = rho_out - rho_in
+        if self.kw is not None:
+            rg = fft3(res.astype(np.complex128), self.dims) * self.kw
+            res = (ifft3(rg, self.dims) / res.size).real.copy()
+        self.hin.append(rho_in.copy())
+        self.hres.append(res)
+        if len(self.hin) > self.ndim:
+            self.hin.pop(0)
+            self.hres.pop(0)
+        return self.hin[-1] + self.beta * self.hres[-1]
+
+
+def make_mixer(kind, beta, ndim, dims, kerker_weights=None, period=3):
+    """Mixer::new (mixing/mod.rs:245-276): 'anderson' (Plain / Kerker),
+    'broyden', 'periodic_pulay'."""
+    if kind == "anderson":
+        return AndersonMixer(beta, ndim, dims, kerker_weights)
+    if kind == "broyden":
+        return BroydenMixer(beta, ndim, dims, kerker_weights)
+    if kind == "periodic_pulay":
+        return PeriodicPulayMixer(beta, ndim, dims, period, kerker_weights)
+    raise ValueError(kind)
+
+
 def solve_small(a, b):
     """Partial-pivot LU with the 1e-15 singular-pivot fallback (linalg.rs:124-152)."""
     import scipy.linalg as sl
@@ -399,7 +470,7 @@ class OracleResult:
 
 def run_scf_unpolarized(sys, n_bands, max_iter=100, conv_threshold=1e-6, energy_threshold=1e-5,
                         mixing_beta=0.3, mixing_ndim=8, smearing="fermi_dirac", sigma=0.01,
-                        kerker=False, q_tf=None, verbose=False):
+                        kerker=False, q_tf=None, verbose=False, mixer="anderson", mixing_period=3):
     """Dense-H SCF loop of driver.rs:353-735 on an ScfSystem (pwgpu.context)."""
     dims = sys.dims
     n = sys.n_grid
@@ -412,9 +483,11 @@ def run_scf_unpolarized(sys, n_bands, max_iter=100, conv_threshold=1e-6, energy_
         src = arg = np.zeros((1, 0))
     kw = None
     if kerker:
-        q2 = q_tf * q_tf if q_tf is not None else auto_q_tf_squared(sys.n_electrons, omega)
+        # Broyden and Periodic Pulay always estimate q_TF (mixing/mod.rs:254-275)
+        user_q = q_tf is not None and mixer == "anderson"
+        q2 = q_tf * q_tf if user_q else auto_q_tf_squared(sys.n_electrons, omega)
         kw = np.where(sys.g_squared < G2_ZERO_THRESHOLD, 0.0, sys.g_squared / (sys.g_squared + q2))
-    mixer = AndersonMixer(mixing_beta, mixing_ndim, dims, kw)
+    mixer = make_mixer(mixer, mixing_beta, mixing_ndim, dims, kw, mixing_period)
     d_dense = [p.d_dense() for p in sys.projectors]
     rho = sys.rho_init_r.copy()
     rho_g = density_r_to_g(rho, dims)
@@ -479,7 +552,8 @@ class OracleSpinResult:
 
 def run_scf_spin(sys, n_bands, max_iter=100, conv_threshold=1e-6, energy_threshold=1e-5, mixing_beta=0.3,
                  mixing_ndim=8, smearing="fermi_dirac", sigma=0.01, kerker=False, q_tf=None,
-                 starting_magnetization=0.0, tot_magnetization=None, verbose=False):
+                 starting_magnetization=0.0, tot_magnetization=None, verbose=False, mixer="anderson",
+                 mixing_period=3):
     """LSDA SCF of driver_spin.rs:114-839 with dense diagonalisation.
 
     starting_magnetization: the atom average of the per-species fractions
@@ -498,10 +572,12 @@ def run_scf_spin(sys, n_bands, max_iter=100, conv_threshold=1e-6, energy_thresho
         src = arg = np.zeros((1, 0))
     kw = None
     if kerker:
-        q2 = q_tf * q_tf if q_tf is not None else auto_q_tf_squared(sys.n_electrons, omega)
+        # Broyden and Periodic Pulay always estimate q_TF (mixing/mod.rs:254-275)
+        user_q = q_tf is not None and mixer == "anderson"
+        q2 = q_tf * q_tf if user_q else auto_q_tf_squared(sys.n_electrons, omega)
         kw = np.where(sys.g_squared < G2_ZERO_THRESHOLD, 0.0, sys.g_squared / (sys.g_squared + q2))
-    mix_tot = AndersonMixer(mixing_beta, mixing_ndim, dims, kw)
-    mix_mag = AndersonMixer(mixing_beta, mixing_ndim, dims, None)
+    mix_tot = make_mixer(mixer, mixing_beta, mixing_ndim, dims, kw, mixing_period)
+    mix_mag = make_mixer(mixer, mixing_beta, mixing_ndim, dims, None, mixing_period)
     d_dense = [p.d_dense() for p in sys.projectors]
     core = sys.rho_core_r
     core_half = core / 2.0 if core.size else core

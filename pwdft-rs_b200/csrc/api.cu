@@ -292,7 +292,8 @@ pwgpu_status pwgpu_scf_run(pwgpu_handle* ph, const pwgpu_scf_params* p, const do
   if (q.starting_magnetization < -1.0 || q.starting_magnetization > 1.0)
     return fail(kInvalid, "pwgpu_scf_run: starting_magnetization must lie in [-1, 1]");
   if (q.smearing < 0 || q.smearing > 4) return fail(kInvalid, "pwgpu_scf_run: unknown smearing scheme");
-  if (q.mixing_mode < 0 || q.mixing_mode > 1) return fail(kInvalid, "pwgpu_scf_run: unknown mixing mode");
+  q.mixing_period = p->mixing_period > 0 ? p->mixing_period : 3;
+  if (q.mixing_mode < 0 || q.mixing_mode > 5) return fail(kInvalid, "pwgpu_scf_run: unknown mixing mode");
   ScfResult r;
   Status st = scf_run(ph->h, q, rho_init_r, r, eigenvalues, rho_r_out, rho_g_basis_out);
   result->total_energy = r.total_energy;
@@ -325,11 +326,11 @@ pwgpu_status pwgpu_eigensolve(pwgpu_handle* ph, int32_t spin, int32_t ik, int32_
                       ph->precision);
 }
 
-pwgpu_status pwgpu_mix(pwgpu_handle* ph, int32_t channel, const double* rho_in, const double* rho_out,
-                       double* rho_next, double beta, int32_t ndim, int32_t kerker, double q_tf) {
+pwgpu_status pwgpu_mix(pwgpu_handle* ph, int32_t channel, int32_t mode, const double* rho_in, const double* rho_out,
+                       double* rho_next, double beta, int32_t ndim, int32_t period, double q_tf) {
   if (!ph || !rho_in || !rho_out || !rho_next) return fail(kInvalid, "pwgpu_mix: NULL argument");
   PW_CUDA_TRY(cudaSetDevice(ph->h.device));
-  return mix_host(ph->h, channel, rho_in, rho_out, rho_next, beta, ndim, kerker, q_tf);
+  return mix_host(ph->h, channel, mode, rho_in, rho_out, rho_next, beta, ndim, period, q_tf);
 }
 
 pwgpu_status pwgpu_mix_reset(pwgpu_handle* ph) {

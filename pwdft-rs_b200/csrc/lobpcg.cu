@@ -257,18 +257,19 @@ Status add_shift(Ctx& c, double* G, double* Id, int q, double shift) {
   return kOk;
 }
 
-Status trsm_right_upper(Ctx& c, const double2* R, int q, double2* M) {
+// M (rows x q, ld ldm) <- M R^-1 for the upper-triangular q x q R
+Status trsm_right_upper(Ctx& c, const double2* R, int q, double2* M, int rows, long ldm) {
   const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
-  if (cublasZtrsm(c.h.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, (int)c.n, q,
+  if (cublasZtrsm(c.h.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, rows, q,
                   &one, reinterpret_cast<const cuDoubleComplex*>(R), q, reinterpret_cast<cuDoubleComplex*>(M),
-                  (int)c.n) != CUBLAS_STATUS_SUCCESS)
+                  (int)ldm) != CUBLAS_STATUS_SUCCESS)
     return fail(kCuda, "cublasZtrsm failed (eigensolver)");
   return kOk;
 }
-Status trsm_right_upper(Ctx& c, const double* R, int q, double* M) {
+Status trsm_right_upper(Ctx& c, const double* R, int q, double* M, int rows, long ldm) {
   const double one = 1.0;
-  if (cublasDtrsm(c.h.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, (int)c.n, q,
-                  &one, R, q, M, (int)c.n) != CUBLAS_STATUS_SUCCESS)
+  if (cublasDtrsm(c.h.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, rows, q,
+                  &one, R, q, M, (int)ldm) != CUBLAS_STATUS_SUCCESS)
     return fail(kCuda, "cublasDtrsm failed (eigensolver)");
   return kOk;
 }
@@ -419,8 +420,19 @@ Status chol_qr(Ctx& c, T* Y, T* HY, int q, double shift, bool& ok, double* min_r
     for (double d : dg) mn = std::min(mn, std::fabs(d));
     *min_rdiag = mn;
   }
-  if ((r = trsm_right_upper(c, G, q, Y)) != kOk) return r;
-  if (HY && (r = trsm_right_upper(c, G, q, HY)) != kOk) return r;
+  // Y <- Y R^-1 as one GEMM with the explicit inverse of the small R (a
+  // tall-skinny triangular solve is several times slower than the GEMM);
+  // w.T and w.HXn are free whenever a block is orthonormalised
+  T* Ri = as<T>(c.w.Id);
+  k_set_identity<T><<<blocks_for((long)q * q), 256, 0, c.s>>>(Ri, q); count_launch();
+  if ((r = trsm_right_upper(c, G, q, Ri, q, q)) != kOk) return r;
+  T* tmp[2] = {as<T>(c.w.T), as<T>(c.w.HXn)};
+  T* M[2] = {Y, HY};
+  for (int i = 0; i < 2; ++i) {
+    if (!M[i]) continue;
+    if ((r = gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)c.n, q, q, M[i], c.n, Ri, q, tmp[i], c.n)) != kOk) return r;
+    PW_CUDA_TRY(cudaMemcpyAsync(M[i], tmp[i], c.n * q * sizeof(T), cudaMemcpyDeviceToDevice, c.s));
+  }
   return kOk;
 }
 

@@ -220,7 +220,10 @@ __global__ void k_sub(const double* __restrict__ a, const double* __restrict__ b
 // dr_i = res[i] - res[mm] (i < mm), blockIdx.y = i * (mm + 1) + jj:
 // jj = 0 gives dot(dr_i, res[mm]), jj = j + 1 (j <= i) gives dot(dr_i, dr_j);
 // partials[blockIdx.y * gridDim.x + blockIdx.x] (fixed summation order).
-__global__ void k_dr_dots(const double* const* __restrict__ res, int mm, long n, double* __restrict__ partials) {
+// With diff = 0 the same slots hold plain products: <v_i, v_j> and
+// <v_i, v_mm> (Broyden's <df_i|df_j> and <df_i|R>).
+__global__ void k_dr_dots(const double* const* __restrict__ res, int mm, long n, int diff,
+                          double* __restrict__ partials) {
   __shared__ double sh[32];
   const int i = blockIdx.y / (mm + 1), jj = blockIdx.y % (mm + 1), j = jj - 1;
   if (j > i) {
@@ -232,12 +235,27 @@ __global__ void k_dr_dots(const double* const* __restrict__ res, int mm, long n,
   const double* rj = j >= 0 ? res[j] : nullptr;
   double acc = 0.0;
   for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
-    const double a = ri[t] - rl[t];
-    const double b = rj ? rj[t] - rl[t] : rl[t];
+    const double a = diff ? ri[t] - rl[t] : ri[t];
+    const double b = rj ? (diff ? rj[t] - rl[t] : rj[t]) : rl[t];
     acc += a * b;
   }
   acc = block_sum(acc, sh);
   if (threadIdx.x == 0) partials[(long)blockIdx.y * gridDim.x + blockIdx.x] = acc;
+}
+
+// Broyden update (broyden.rs:228-245): next = (in - sum_k g_k dv_k) +
+// beta (r - sum_k g_k df_k); next may alias in
+__global__ void k_broyden_combine(const double* __restrict__ in, const double* __restrict__ r,
+                                  const double* const* __restrict__ dv, const double* const* __restrict__ df,
+                                  const double* __restrict__ g, int m, double beta, long n, double* next) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double cv = 0.0, cf = 0.0;
+  for (int k = 0; k < m; ++k) {
+    cv += g[k] * dv[k][i];
+    cf += g[k] * df[k][i];
+  }
+  next[i] = fma(beta, r[i] - cf, in[i] - cv);
 }
 
 // sums[c] = sum of the nblk partials of slot c (fixed order)
@@ -408,11 +426,24 @@ static Status create_lane(Handle& h, Lane& L, int nd, int nlanes) {
 
 // Anderson history of one mixed channel (anderson.rs:170-266): inputs and
 // (preconditioned) residuals, oldest first.
+// (Broyden: hin / hres hold the input and residual differences dv, df, and
+// prev_in / prev_res the previous step's input and residual.)
 struct MixHistory {
   std::vector<double*> hin, hres;
   int count = 0;
-  double** dev_ptrs = nullptr;  // 2 * ndim
+  int iteration = 0;            // steps taken (Periodic Pulay's period counter)
+  bool has_prev = false;        // Broyden: prev_in / prev_res hold a step
+  double *prev_in = nullptr, *prev_res = nullptr, *rcur = nullptr;
+  double** dev_ptrs = nullptr;  // 2 * ndim + 2
   double* dev_coef = nullptr;   // ndim
+};
+
+// Mixer::new (mixing/mod.rs:245-276) kinds and options of one channel
+struct MixConfig {
+  int kind = 0;        // 0 Anderson, 1 modified Broyden, 2 Periodic Pulay
+  bool kerker = false;
+  int period = 3;
+  double beta = 0.3;
 };
 
 struct ScfState {
@@ -461,6 +492,9 @@ static void release_history(MixHistory& mh) {
   for (double* p : mh.hres) f(p);
   f(mh.dev_ptrs);
   f(mh.dev_coef);
+  f(mh.prev_in);
+  f(mh.prev_res);
+  f(mh.rcur);
   mh = MixHistory();
 }
 
@@ -474,8 +508,10 @@ static Status alloc_history(MixHistory& mh, long N, int ndim) {
     if ((s = salloc(&mh.hin[i], (size_t)N)) != kOk) return s;
     if ((s = salloc(&mh.hres[i], (size_t)N)) != kOk) return s;
   }
-  if ((s = salloc(&mh.dev_ptrs, (size_t)2 * std::max(ndim, 1))) != kOk) return s;
+  if ((s = salloc(&mh.dev_ptrs, (size_t)2 * std::max(ndim, 1) + 2)) != kOk) return s;
   if ((s = salloc(&mh.dev_coef, (size_t)std::max(ndim, 1))) != kOk) return s;
+  for (double** p : {&mh.prev_in, &mh.prev_res, &mh.rcur})
+    if ((s = salloc(p, (size_t)N)) != kOk) return s;
   return kOk;
 }
 
@@ -710,24 +746,29 @@ static std::vector<double> solve_small(std::vector<double> a, std::vector<double
   return x;
 }
 
-// One Anderson step of one channel (anderson.rs:170-266; Kerker residual
-// preconditioning kerker.rs:18-35 when `kerker`): next = sum_i c_i (in_i +
-// beta res_i) over the history, DIIS coefficients from the residual
-// differences (linalg.rs:124-152 solve).  `next` may alias `in`.
-static Status mix_channel(Handle& h, MixHistory& mh, const double* in, const double* out, double* next, double beta,
-                          bool kerker) {
+// mixing_mode: 0 Anderson, 1 Anderson + Kerker, 2 Broyden, 3 Broyden +
+// Kerker, 4 Periodic Pulay, 5 Periodic Pulay + Kerker (MixingMode,
+// mixing/mod.rs:186-223)
+static MixConfig mix_config(int mode, int period, double beta) {
+  MixConfig c;
+  c.kind = mode / 2;
+  c.kerker = (mode % 2) == 1;
+  c.period = std::max(1, period);
+  c.beta = beta;
+  return c;
+}
+
+static void reset_history(MixHistory& mh) {
+  mh.count = 0;
+  mh.iteration = 0;
+  mh.has_prev = false;
+}
+
+// Kerker-preconditioned residual (kerker.rs:18-35) out - in into res.
+static Status residual_into(Handle& h, const double* in, const double* out, double* res, bool kerker) {
   ScfState* st = h.scf;
   const long N = h.g.N;
   const cudaStream_t s = h.stream;
-  const int ndim = (int)mh.hin.size();
-  // rotate history: slot order oldest .. newest kept in vectors
-  if (mh.count == ndim) {
-    std::rotate(mh.hin.begin(), mh.hin.begin() + 1, mh.hin.end());
-    std::rotate(mh.hres.begin(), mh.hres.begin() + 1, mh.hres.end());
-    --mh.count;
-  }
-  const int slot = mh.count;
-  double* res = mh.hres[slot];
   k_sub<<<blocks_for(N), 256, 0, s>>>(out, in, res, N); count_launch();
   if (kerker && st->kerker_w) {
     k_real_to_cplx<<<blocks_for(N), 256, 0, s>>>(res, st->cg, N); count_launch();
@@ -737,24 +778,61 @@ static Status mix_channel(Handle& h, MixHistory& mh, const double* in, const dou
     if ((r = fft3d_full(h, st->cg, +1, s)) != kOk) return r;
     k_cplx_real_scaled<<<blocks_for(N), 256, 0, s>>>(st->cg, res, 1.0 / (double)N, N); count_launch();
   }
-  PW_CUDA_TRY(cudaMemcpyAsync(mh.hin[slot], in, N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  return kOk;
+}
+
+// All products of one step in one launch and one host sync: slots
+// i * (mm + 1) + jj of st->mix_sums (see k_dr_dots); ptrs = mm + 1 vectors.
+static Status dot_table(Handle& h, double* const* ptrs_dev, int mm, int diff, std::vector<double>& sums) {
+  ScfState* st = h.scf;
+  const long N = h.g.N;
+  const cudaStream_t s = h.stream;
+  const int nslots = mm * (mm + 1);
+  const unsigned nbk = (unsigned)std::min<long>(kMixBlocks, blocks_for(N));
+  k_dr_dots<<<dim3(nbk, nslots), 256, 0, s>>>(ptrs_dev, mm, N, diff, st->mix_partials); count_launch();
+  k_slot_sums<<<blocks_for(nslots), 256, 0, s>>>(st->mix_partials, (int)nbk, nslots, st->mix_sums); count_launch();
+  sums.resize(nslots);
+  PW_CUDA_TRY(cudaMemcpyAsync(sums.data(), st->mix_sums, nslots * sizeof(double), cudaMemcpyDeviceToHost, s));
+  PW_CUDA_TRY(cudaStreamSynchronize(s));
+  return kOk;
+}
+
+// Anderson history push (AndersonMixer::push_history, anderson.rs:170-190)
+static Status push_anderson(Handle& h, MixHistory& mh, const double* in, const double* out, bool kerker) {
+  const long N = h.g.N;
+  const int ndim = (int)mh.hin.size();
+  // rotate history: slot order oldest .. newest kept in vectors
+  if (mh.count == ndim) {
+    std::rotate(mh.hin.begin(), mh.hin.begin() + 1, mh.hin.end());
+    std::rotate(mh.hres.begin(), mh.hres.begin() + 1, mh.hres.end());
+    --mh.count;
+  }
+  const int slot = mh.count;
+  Status r = residual_into(h, in, out, mh.hres[slot], kerker);
+  if (r != kOk) return r;
+  PW_CUDA_TRY(cudaMemcpyAsync(mh.hin[slot], in, N * sizeof(double), cudaMemcpyDeviceToDevice, h.stream));
   mh.count++;
+  return kOk;
+}
+
+// next = sum_i c_i (in_i + beta res_i) over the Anderson history; DIIS
+// coefficients from the residual differences when diis (anderson.rs:192-266),
+// the newest entry alone otherwise.
+static Status combine_anderson(Handle& h, MixHistory& mh, double beta, bool diis, double* next) {
+  const long N = h.g.N;
+  const cudaStream_t s = h.stream;
   const int m = mh.count;
   std::vector<double*> ptrs(2 * m);
   for (int j = 0; j < m; ++j) { ptrs[j] = mh.hin[j]; ptrs[m + j] = mh.hres[j]; }
   PW_CUDA_TRY(cudaMemcpyAsync(mh.dev_ptrs, ptrs.data(), 2 * m * sizeof(double*), cudaMemcpyHostToDevice, s));
   std::vector<double> coef(m, 0.0);
-  if (m < 2) {
-    coef[0] = 1.0;
+  if (m < 2 || !diis) {
+    coef[m - 1] = 1.0;
   } else {
-    // every <dr_i, dr_j> and <dr_i, r_last> in one launch, one host sync
-    const int mm = m - 1, nslots = mm * (mm + 1);
-    const unsigned nbk = (unsigned)std::min<long>(kMixBlocks, blocks_for(N));
-    k_dr_dots<<<dim3(nbk, nslots), 256, 0, s>>>(mh.dev_ptrs + m, mm, N, st->mix_partials); count_launch();
-    k_slot_sums<<<blocks_for(nslots), 256, 0, s>>>(st->mix_partials, (int)nbk, nslots, st->mix_sums); count_launch();
-    std::vector<double> sums(nslots);
-    PW_CUDA_TRY(cudaMemcpyAsync(sums.data(), st->mix_sums, nslots * sizeof(double), cudaMemcpyDeviceToHost, s));
-    PW_CUDA_TRY(cudaStreamSynchronize(s));
+    const int mm = m - 1;
+    std::vector<double> sums;
+    Status r = dot_table(h, mh.dev_ptrs + m, mm, 1, sums);
+    if (r != kOk) return r;
     std::vector<double> a((size_t)mm * mm), b(mm);
     for (int i = 0; i < mm; ++i) {
       b[i] = -sums[(size_t)i * (mm + 1)];
@@ -774,6 +852,72 @@ static Status mix_channel(Handle& h, MixHistory& mh, const double* in, const dou
   count_launch();
   PW_CUDA_TRY(cudaStreamSynchronize(s));
   return kOk;
+}
+
+// Modified Broyden step (BroydenMixer::mix, broyden.rs:140-245).
+static Status mix_broyden(Handle& h, MixHistory& mh, const double* in, const double* out, double* next, double beta,
+                          bool kerker) {
+  const long N = h.g.N;
+  const cudaStream_t s = h.stream;
+  const int ndim = (int)mh.hin.size();
+  Status r = residual_into(h, in, out, mh.rcur, kerker);
+  if (r != kOk) return r;
+  if (mh.has_prev) {
+    if (mh.count == ndim) {
+      std::rotate(mh.hin.begin(), mh.hin.begin() + 1, mh.hin.end());
+      std::rotate(mh.hres.begin(), mh.hres.begin() + 1, mh.hres.end());
+      --mh.count;
+    }
+    const int slot = mh.count++;
+    k_sub<<<blocks_for(N), 256, 0, s>>>(in, mh.prev_in, mh.hin[slot], N); count_launch();      // dv
+    k_sub<<<blocks_for(N), 256, 0, s>>>(mh.rcur, mh.prev_res, mh.hres[slot], N); count_launch();  // df
+  }
+  PW_CUDA_TRY(cudaMemcpyAsync(mh.prev_in, in, N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  PW_CUDA_TRY(cudaMemcpyAsync(mh.prev_res, mh.rcur, N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  mh.has_prev = true;
+  const int m = mh.count;
+  std::vector<double> g(std::max(m, 1), 0.0);
+  // pointers: dv_0..dv_{m-1}, df_0..df_{m-1}, R
+  std::vector<double*> ptrs(2 * m + 1);
+  for (int j = 0; j < m; ++j) { ptrs[j] = mh.hin[j]; ptrs[m + j] = mh.hres[j]; }
+  ptrs[2 * m] = mh.rcur;
+  PW_CUDA_TRY(cudaMemcpyAsync(mh.dev_ptrs, ptrs.data(), ptrs.size() * sizeof(double*), cudaMemcpyHostToDevice, s));
+  if (m > 0) {
+    std::vector<double> sums;
+    if ((r = dot_table(h, mh.dev_ptrs + m, m, 0, sums)) != kOk) return r;
+    std::vector<double> a((size_t)m * m), w(m);
+    for (int i = 0; i < m; ++i) {
+      w[i] = sums[(size_t)i * (m + 1)];
+      for (int j = 0; j <= i; ++j) {
+        const double v = sums[(size_t)i * (m + 1) + j + 1];
+        a[(size_t)i * m + j] = v;
+        a[(size_t)j * m + i] = v;
+      }
+    }
+    g = solve_small(a, w, m);
+  }
+  PW_CUDA_TRY(cudaMemcpyAsync(mh.dev_coef, g.data(), std::max(m, 1) * sizeof(double), cudaMemcpyHostToDevice, s));
+  k_broyden_combine<<<blocks_for(N), 256, 0, s>>>(in, mh.rcur, mh.dev_ptrs, mh.dev_ptrs + m, mh.dev_coef, m, beta, N,
+                                                  next);
+  count_launch();
+  PW_CUDA_TRY(cudaStreamSynchronize(s));
+  return kOk;
+}
+
+// One mixing step of one channel (Mixer::mix, mixing/mod.rs:281-287):
+// Anderson (anderson.rs:170-266), modified Broyden (broyden.rs:140-245) or
+// Periodic Pulay (anderson.rs:353-372: DIIS every period-th step once the
+// history holds two entries, linear mixing of the newest entry otherwise);
+// Kerker residual preconditioning (kerker.rs:18-35) when cfg.kerker.
+// `next` may alias `in`.
+static Status mix_channel(Handle& h, MixHistory& mh, const MixConfig& cfg, const double* in, const double* out,
+                          double* next) {
+  mh.iteration++;
+  if (cfg.kind == 1) return mix_broyden(h, mh, in, out, next, cfg.beta, cfg.kerker);
+  Status r = push_anderson(h, mh, in, out, cfg.kerker);
+  if (r != kOk) return r;
+  const bool diis = cfg.kind == 0 || (mh.iteration % std::max(cfg.period, 1) == 0);
+  return combine_anderson(h, mh, cfg.beta, diis, next);
 }
 
 // Density of all k-points of one spin channel (density.rs:41-111): rho =
@@ -946,11 +1090,15 @@ Status scf_run(Handle& h, const ScfParams& p, const double* rho_init, ScfResult&
   if (r != kOk) return r;
   ScfState* st = h.scf;
   for (auto& k : st->ks) k.init = false;
-  for (auto& mh : st->mixh) mh.count = 0;
+  for (auto& mh : st->mixh) reset_history(mh);
   const long N = h.g.N;
   const cudaStream_t s = h.stream;
   cublasSetStream(h.blas, s);
-  if ((r = set_kerker(h, p.mixing_mode == 1, p.kerker_q_tf)) != kOk) return r;
+  const MixConfig mix_tot = mix_config(p.mixing_mode, p.mixing_period, p.mixing_beta);
+  MixConfig mix_mag = mix_tot;
+  mix_mag.kerker = false;  // Kerker acts on the charge channel only (driver_spin.rs:176-186)
+  // q_TF: the user's value for Anderson + Kerker, the estimate for the others
+  if ((r = set_kerker(h, mix_tot.kerker, mix_tot.kind == 0 ? p.kerker_q_tf : 0.0)) != kOk) return r;
   double* rin[2] = {st->rho_in, st->rho_in_dn};
   double* rout[2] = {st->rho_out, st->rho_out_dn};
   if (ns == 1) {
@@ -1121,7 +1269,7 @@ Status scf_run(Handle& h, const ScfParams& p, const double* rho_init, ScfResult&
       return conv ? kOk : fail(kNotConverged, "SCF did not converge within max_iter");
     }
     if (ns == 1) {
-      if ((r = mix_channel(h, st->mixh[0], st->rho_in, st->rho_out, st->rho_in, p.mixing_beta, true)) != kOk) return r;
+      if ((r = mix_channel(h, st->mixh[0], mix_tot, st->rho_in, st->rho_out, st->rho_in)) != kOk) return r;
     } else {
       // CCMX (driver_spin.rs:792-826): total density with the requested
       // mode, magnetisation with plain Anderson
@@ -1129,8 +1277,8 @@ Status scf_run(Handle& h, const ScfParams& p, const double* rho_init, ScfResult&
       k_axpy_to<<<blocks_for(N), 256, 0, s>>>(st->rho_in, st->rho_in_dn, -1.0, st->m_in, N); count_launch();
       k_axpy_to<<<blocks_for(N), 256, 0, s>>>(st->rho_out, st->rho_out_dn, 1.0, st->t_out, N); count_launch();
       k_axpy_to<<<blocks_for(N), 256, 0, s>>>(st->rho_out, st->rho_out_dn, -1.0, st->m_out, N); count_launch();
-      if ((r = mix_channel(h, st->mixh[0], st->t_in, st->t_out, st->t_in, p.mixing_beta, true)) != kOk) return r;
-      if ((r = mix_channel(h, st->mixh[1], st->m_in, st->m_out, st->m_in, p.mixing_beta, false)) != kOk) return r;
+      if ((r = mix_channel(h, st->mixh[0], mix_tot, st->t_in, st->t_out, st->t_in)) != kOk) return r;
+      if ((r = mix_channel(h, st->mixh[1], mix_mag, st->m_in, st->m_out, st->m_in)) != kOk) return r;
       k_unmix_spin<<<blocks_for(N), 256, 0, s>>>(st->t_in, st->m_in, st->rho_in, st->rho_in_dn, N); count_launch();
     }
   }
@@ -1246,9 +1394,10 @@ Status potentials_host(Handle& h, const double* rho, double* veff_g, double* ene
   return kOk;
 }
 
-Status mix_host(Handle& h, int channel, const double* in, const double* out, double* next, double beta, int ndim,
-                int kerker, double q_tf) {
+Status mix_host(Handle& h, int channel, int mode, const double* in, const double* out, double* next, double beta,
+                int ndim, int period, double q_tf) {
   if (channel < 0 || channel > 1) return fail(kInvalid, "mix: channel must be 0 or 1");
+  if (mode < 0 || mode > 5) return fail(kInvalid, "mix: unknown mixing mode");
   if (ndim < 1) return fail(kInvalid, "mix: ndim must be >= 1");
   Status r;
   if (!h.scf && (r = ensure_state(h, 1, 1, ndim)) != kOk) return r;
@@ -1265,10 +1414,11 @@ Status mix_host(Handle& h, int channel, const double* in, const double* out, dou
   }
   MixHistory& mh = st->mixh[channel];
   if ((int)mh.hin.size() != ndim && (r = alloc_history(mh, N, ndim)) != kOk) return r;
-  if ((r = set_kerker(h, kerker != 0, q_tf)) != kOk) return r;
+  const MixConfig cfg = mix_config(mode, period, beta);
+  if ((r = set_kerker(h, cfg.kerker, cfg.kind == 0 ? q_tf : 0.0)) != kOk) return r;
   PW_CUDA_TRY(cudaMemcpyAsync(st->rho_in, in, N * sizeof(double), cudaMemcpyHostToDevice, h.stream));
   PW_CUDA_TRY(cudaMemcpyAsync(st->rho_out, out, N * sizeof(double), cudaMemcpyHostToDevice, h.stream));
-  if ((r = mix_channel(h, mh, st->rho_in, st->rho_out, st->rho_in, beta, kerker != 0)) != kOk) return r;
+  if ((r = mix_channel(h, mh, cfg, st->rho_in, st->rho_out, st->rho_in)) != kOk) return r;
   PW_CUDA_TRY(cudaMemcpyAsync(next, st->rho_in, N * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
   PW_CUDA_TRY(cudaStreamSynchronize(h.stream));
   return kOk;
@@ -1276,7 +1426,7 @@ Status mix_host(Handle& h, int channel, const double* in, const double* out, dou
 
 Status mix_reset(Handle& h) {
   if (h.scf)
-    for (auto& mh : h.scf->mixh) mh.count = 0;
+    for (auto& mh : h.scf->mixh) reset_history(mh);
   return kOk;
 }
 

