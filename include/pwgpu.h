@@ -83,6 +83,21 @@ typedef struct pwgpu_system {
   double omega;                /* cell volume, Å^3 */
   double e_ewald;              /* eV */
   int32_t nspin;               /* 1 or 2 */
+  /* Projectors built on the device (NonlocalPotential::new, potential/nonlocal.rs:190-382),
+   * used when proj_b is NULL and n_ch > 0: F_i(|k+G|) = 4 pi int [r beta_i] j_l(|k+G| r) r dr
+   * by Simpson on each species' mesh, real Y_lm, e^{-iG.tau}/sqrt(Omega); channels atom by
+   * atom, projector by projector, m = 0, +1, -1, ...  atom_ch_start and d_blocks as above. */
+  const double* g_cart;         /* n_pw x 3 G vectors (Å^-1), basis order */
+  const double* k_cart;         /* n_k x 3 k-points (Å^-1) */
+  const double* atom_tau;       /* n_atoms x 3 Cartesian positions (Å) */
+  const int32_t* atom_species;  /* n_atoms: species index */
+  int32_t n_species;
+  const int32_t* species_mesh;  /* n_species radial mesh sizes */
+  const double* radial_r;       /* concatenated radial meshes r (Å) */
+  const double* radial_rab;     /* concatenated dr/di */
+  const int32_t* species_nbeta; /* n_species projector counts */
+  const int32_t* beta_l;        /* l of each projector, species by species */
+  const double* beta_r;         /* beta_i(r) of each projector on its species' mesh, concatenated */
 } pwgpu_system;
 
 typedef struct pwgpu_options {
@@ -143,6 +158,10 @@ pwgpu_status pwgpu_kernel_launches(int64_t* count);
 /* The CUDA stream (cudaStream_t) a handle runs on, for callers that time or
  * order work against it. */
 pwgpu_status pwgpu_get_stream(const pwgpu_handle* h, void** stream);
+
+/* Copy the device projector matrix B of k-point ik (n_pw x n_ch complex,
+ * column-major) to the host, whether it was uploaded or built on the device. */
+pwgpu_status pwgpu_get_projectors(const pwgpu_handle* h, int32_t ik, double* b);
 
 /* Basis size, grid size and channel count of a handle. */
 pwgpu_status pwgpu_get_dims(const pwgpu_handle* h, int32_t* n_pw, int64_t* n_grid, int32_t* n_ch);

@@ -69,7 +69,7 @@ static Status create(const pwgpu_system* s, const pwgpu_options* o, pwgpu_handle
   if (s->dims[0] > 1024 || s->dims[1] > 1024 || s->dims[2] > 1024)
     return fail(kInvalid, "pwgpu_create: FFT grid dimension exceeds MAX_FFT_DIM=1024");
   if (s->nspin != 1 && s->nspin != 2) return fail(kInvalid, "pwgpu_create: nspin must be 1 or 2");
-  if (s->n_ch < 0 || (s->n_ch > 0 && (!s->proj_b || !s->atom_ch_start || !s->d_blocks || s->n_atoms <= 0)))
+  if (s->n_ch < 0 || (s->n_ch > 0 && (!s->atom_ch_start || !s->d_blocks || s->n_atoms <= 0)))
     return fail(kInvalid, "pwgpu_create: projector arrays missing");
   if (s->n_sym < 0 || (s->n_sym > 1 && (!s->sym_src || !s->sym_arg)))
     return fail(kInvalid, "pwgpu_create: symmetry map missing");
@@ -101,7 +101,9 @@ static Status create(const pwgpu_system* s, const pwgpu_options* o, pwgpu_handle
     kd.weight = s->k_weights[k];
     if ((st = upload(&kd.kinetic, s->kinetic + (long)k * h.n_pw, h.n_pw)) != kOk) return st;
     if (h.n_ch > 0) {
-      const double2* bsrc = reinterpret_cast<const double2*>(s->proj_b) + (long)k * h.n_pw * h.n_ch;
+      // uploaded from the caller, or built on the device below
+      const double2* bsrc =
+          s->proj_b ? reinterpret_cast<const double2*>(s->proj_b) + (long)k * h.n_pw * h.n_ch : nullptr;
       if ((st = upload(&kd.b, bsrc, (size_t)h.n_pw * h.n_ch)) != kOk) return st;
     }
   }
@@ -121,6 +123,21 @@ static Status create(const pwgpu_system* s, const pwgpu_options* o, pwgpu_handle
     if ((st = upload(&h.ch_atom, ch_atom.data(), ch_atom.size())) != kOk) return st;
     if ((st = upload(&h.d_off, d_off.data(), d_off.size())) != kOk) return st;
     if ((st = upload(&h.d_vals, s->d_blocks, (size_t)off)) != kOk) return st;
+    if (!s->proj_b) {
+      ProjectorSource src;
+      src.gvec = s->g_cart;
+      src.kpts = s->k_cart;
+      src.atom_tau = s->atom_tau;
+      src.atom_species = s->atom_species;
+      src.n_species = s->n_species;
+      src.species_mesh = s->species_mesh;
+      src.radial_r = s->radial_r;
+      src.radial_rab = s->radial_rab;
+      src.species_nbeta = s->species_nbeta;
+      src.beta_l = s->beta_l;
+      src.beta_r = s->beta_r;
+      if ((st = build_projectors_device(h, src)) != kOk) return st;
+    }
   }
   if ((st = upload(&h.v_local_g, reinterpret_cast<const double2*>(s->v_local_g), (size_t)N)) != kOk) return st;
   if ((st = upload(&h.g_squared, s->g_squared, (size_t)N)) != kOk) return st;
@@ -137,7 +154,7 @@ static Status create(const pwgpu_system* s, const pwgpu_options* o, pwgpu_handle
   }
   // Gamma-only systems run with real wavefunctions unless the caller keeps them complex
   if (!(o && o->gamma_complex) &&
-      (st = build_gamma(h, s->miller, s->kinetic, s->proj_b, s->atom_ch_start, s->d_blocks)) != kOk)
+      (st = build_gamma(h, s->miller, s->kinetic, s->atom_ch_start, s->d_blocks)) != kOk)
     return st;
   PW_CUDA_TRY(cudaDeviceSynchronize());
   return kOk;
@@ -331,6 +348,16 @@ pwgpu_status pwgpu_mix(pwgpu_handle* ph, int32_t channel, int32_t mode, const do
   if (!ph || !rho_in || !rho_out || !rho_next) return fail(kInvalid, "pwgpu_mix: NULL argument");
   PW_CUDA_TRY(cudaSetDevice(ph->h.device));
   return mix_host(ph->h, channel, mode, rho_in, rho_out, rho_next, beta, ndim, period, q_tf);
+}
+
+pwgpu_status pwgpu_get_projectors(const pwgpu_handle* ph, int32_t ik, double* b) {
+  if (!ph || !b) return fail(kInvalid, "pwgpu_get_projectors: NULL argument");
+  const Handle& h = ph->h;
+  if (ik < 0 || ik >= h.n_k) return fail(kInvalid, "pwgpu_get_projectors: k-point index out of range");
+  if (h.n_ch == 0) return kOk;
+  PW_CUDA_TRY(cudaSetDevice(h.device));
+  PW_CUDA_TRY(cudaMemcpy(b, h.kp[ik].b, (size_t)h.n_pw * h.n_ch * sizeof(double2), cudaMemcpyDeviceToHost));
+  return kOk;
 }
 
 pwgpu_status pwgpu_mix_reset(pwgpu_handle* ph) {

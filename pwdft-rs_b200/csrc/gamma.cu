@@ -143,6 +143,40 @@ __global__ void k_apply_d_real(const double* __restrict__ P, double* __restrict_
   Q[(long)b * n_ch + c] = acc;
 }
 
+// Gamma symmetry of each projector column c (one block per column):
+// out[3c] = max |B(-G) - conj B(G)| with |Im B(0)| (even-l hypothesis),
+// out[3c+1] = max |B(-G) + conj B(G)| with |Re B(0)| (odd-l), out[3c+2] = max |B|.
+__global__ void k_gamma_check(const double2* __restrict__ B, int n, const int* __restrict__ half_idx,
+                              const int* __restrict__ half_neg, int zero, int nh, double* __restrict__ out) {
+  __shared__ double sh[3][256];
+  const double2* col = B + (long)blockIdx.x * n;
+  double de = 0.0, dd = 0.0, bm = 0.0;
+  for (int t = threadIdx.x; t <= nh; t += blockDim.x) {
+    if (t == 0) {
+      const double2 z = col[zero];
+      de = fmax(de, fabs(z.y));
+      dd = fmax(dd, fabs(z.x));
+      bm = fmax(bm, fmax(fabs(z.x), fabs(z.y)));
+      continue;
+    }
+    const double2 x = col[half_idx[t - 1]], y = col[half_neg[t - 1]];
+    de = fmax(de, fmax(fabs(x.x - y.x), fabs(x.y + y.y)));
+    dd = fmax(dd, fmax(fabs(x.x + y.x), fabs(x.y - y.y)));
+    bm = fmax(bm, fmax(fmax(fabs(x.x), fabs(x.y)), fmax(fabs(y.x), fabs(y.y))));
+  }
+  sh[0][threadIdx.x] = de;
+  sh[1][threadIdx.x] = dd;
+  sh[2][threadIdx.x] = bm;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o)
+      for (int q = 0; q < 3; ++q) sh[q][threadIdx.x] = fmax(sh[q][threadIdx.x], sh[q][threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int q = 0; q < 3; ++q) out[3L * blockIdx.x + q] = sh[q][0];
+}
+
 template <typename T> Status galloc(T** p, size_t n) {
   cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T));
   if (e != cudaSuccess) return fail(kOom, std::string("cudaMalloc (gamma): ") + cudaGetErrorString(e));
@@ -170,8 +204,8 @@ Status ensure_pairs(Handle& h, int npairs) {
 
 }  // namespace
 
-Status build_gamma(Handle& h, const int* miller, const double* kinetic, const double* proj_b,
-                   const int* atom_ch_start, const double* d_blocks) {
+Status build_gamma(Handle& h, const int* miller, const double* kinetic, const int* atom_ch_start,
+                   const double* d_blocks) {
   release_gamma(h);
   if (h.n_k != 1) return kOk;
   const int n = h.n_pw;
@@ -204,20 +238,33 @@ Status build_gamma(Handle& h, const int* miller, const double* kinetic, const do
   // are packed as i B, which leaves B D B^H unchanged as long as D couples
   // only columns of the same kind (it couples equal l within an atom).
   std::vector<int> rot(std::max(h.n_ch, 1), 0);
-  if (h.n_ch > 0 && proj_b) {
+  GammaData& g = h.gam;
+  Status r;
+  if ((r = galloc(&g.half_idx, nh)) != kOk) return r;
+  if ((r = galloc(&g.half_neg, nh)) != kOk) return r;
+  PW_CUDA_TRY(cudaMemcpy(g.half_idx, hi.data(), nh * sizeof(int), cudaMemcpyHostToDevice));
+  PW_CUDA_TRY(cudaMemcpy(g.half_neg, hn.data(), nh * sizeof(int), cudaMemcpyHostToDevice));
+  if (h.n_ch > 0) {
+    // symmetry of the device-resident B (uploaded or built on the device)
+    double* dev = nullptr;
+    if ((r = galloc(&dev, 3L * h.n_ch)) != kOk) return r;
+    k_gamma_check<<<h.n_ch, 256, 0, h.stream>>>(h.kp[0].b, n, g.half_idx, g.half_neg, zero, nh, dev);
+    count_launch();
+    std::vector<double> chk(3L * h.n_ch);
+    // h.stream is non-blocking: the legacy-stream copy below would not wait for the check
+    cudaError_t e = cudaStreamSynchronize(h.stream);
+    if (e == cudaSuccess) e = cudaMemcpy(chk.data(), dev, chk.size() * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(dev);
+    if (e != cudaSuccess) return fail(kCuda, std::string("gamma check: ") + cudaGetErrorString(e));
     double bmax = 0.0;
-    for (long t = 0; t < 2L * n * h.n_ch; ++t) bmax = std::max(bmax, std::fabs(proj_b[t]));
+    for (int c = 0; c < h.n_ch; ++c) bmax = std::max(bmax, chk[3L * c + 2]);
     const double tol = 1e-12 * std::max(bmax, 1e-300);
     for (int c = 0; c < h.n_ch; ++c) {
-      const double* col = proj_b + 2L * n * c;
-      bool even = std::fabs(col[2 * zero + 1]) <= tol, odd = std::fabs(col[2 * zero]) <= tol;
-      for (int p = 0; p < nh && (even || odd); ++p) {
-        const double* x = col + 2L * hi[p];
-        const double* y = col + 2L * hn[p];
-        if (std::fabs(x[0] - y[0]) > tol || std::fabs(x[1] + y[1]) > tol) even = false;
-        if (std::fabs(x[0] + y[0]) > tol || std::fabs(x[1] - y[1]) > tol) odd = false;
+      const bool even = chk[3L * c] <= tol, odd = chk[3L * c + 1] <= tol;
+      if (!even && !odd) {
+        release_gamma(h);
+        return kOk;
       }
-      if (!even && !odd) return kOk;
       rot[c] = even ? 0 : 1;
     }
     if (atom_ch_start && d_blocks) {
@@ -226,18 +273,15 @@ Status build_gamma(Handle& h, const int* miller, const double* kinetic, const do
         const int s0 = atom_ch_start[a], nc = atom_ch_start[a + 1] - s0;
         for (int i = 0; i < nc; ++i)
           for (int j = 0; j < nc; ++j)
-            if (d_blocks[off + (long)i * nc + j] != 0.0 && rot[s0 + i] != rot[s0 + j]) return kOk;
+            if (d_blocks[off + (long)i * nc + j] != 0.0 && rot[s0 + i] != rot[s0 + j]) {
+              release_gamma(h);
+              return kOk;
+            }
         off += (long)nc * nc;
       }
     }
   }
-  GammaData& g = h.gam;
-  Status r;
-  if ((r = galloc(&g.half_idx, nh)) != kOk) return r;
-  if ((r = galloc(&g.half_neg, nh)) != kOk) return r;
   if ((r = galloc(&g.kin_packed, n)) != kOk) return r;
-  PW_CUDA_TRY(cudaMemcpy(g.half_idx, hi.data(), nh * sizeof(int), cudaMemcpyHostToDevice));
-  PW_CUDA_TRY(cudaMemcpy(g.half_neg, hn.data(), nh * sizeof(int), cudaMemcpyHostToDevice));
   std::vector<double> kp(n);
   kp[0] = kinetic[zero];
   for (int p = 0; p < nh; ++p) kp[1 + p] = kp[1 + nh + p] = kinetic[hi[p]];

@@ -140,10 +140,28 @@ Status ensure_nl_capacity(Handle& h, int nb);
 Status apply_local_device(Handle& h, int spin, int ik, const double2* psi, long ldpsi, int nb, double2* hpsi,
                           long ldh, int precision, cudaStream_t s, StageTimer* tm = nullptr);
 
+// Radial data for building the projector matrices on the device (setup.cu):
+// G and k vectors, atoms, and per species its radial mesh and projectors.
+struct ProjectorSource {
+  const double* gvec = nullptr;        // n_pw x 3, Å^-1
+  const double* kpts = nullptr;        // n_k x 3, Å^-1
+  const double* atom_tau = nullptr;    // n_atoms x 3, Å
+  const int* atom_species = nullptr;   // n_atoms
+  int n_species = 0;
+  const int* species_mesh = nullptr;   // n_species
+  const double* radial_r = nullptr;    // concatenated meshes
+  const double* radial_rab = nullptr;
+  const int* species_nbeta = nullptr;  // n_species
+  const int* beta_l = nullptr;         // per projector, species by species
+  const double* beta_r = nullptr;      // per projector, on its species' mesh
+};
+// B of every k into h.kp[k].b (allocated by the caller); needs h.atom_ch_start.
+Status build_projectors_device(Handle& h, const ProjectorSource& src);
+
 // Gamma path (gamma.cu).  build_gamma decides eligibility (one k-point with
 // a kinetic term and projectors symmetric under G -> -G) from host data.
-Status build_gamma(Handle& h, const int* miller_host, const double* kinetic_host, const double* proj_b_host,
-                   const int* atom_ch_start_host, const double* d_blocks_host);
+Status build_gamma(Handle& h, const int* miller_host, const double* kinetic_host, const int* atom_ch_start_host,
+                   const double* d_blocks_host);
 void release_gamma(Handle& h);
 void release_gamma_scratch(Handle& h);
 // H u for nb packed real bands (local pipeline on pairs of bands packed into

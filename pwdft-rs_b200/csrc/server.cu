@@ -37,16 +37,21 @@ double seconds_between(Clock::time_point a, Clock::time_point b) {
 // the submit call only).
 struct SystemCopy {
   pwgpu_system sys{};
-  std::vector<int32_t> miller, atom_ch_start, sym_src;
-  std::vector<double> k_weights, kinetic, proj_b, d_blocks, v_local_g, g_squared, rho_core, sym_arg;
+  std::vector<int32_t> miller, atom_ch_start, sym_src, atom_species, species_mesh, species_nbeta, beta_l;
+  std::vector<double> k_weights, kinetic, proj_b, d_blocks, v_local_g, g_squared, rho_core, sym_arg, g_cart, k_cart,
+      atom_tau, radial_r, radial_rab, beta_r;
 
   Status copy_from(const pwgpu_system& s) {
     if (s.n_pw <= 0 || s.n_k <= 0 || s.dims[0] <= 0 || s.dims[1] <= 0 || s.dims[2] <= 0)
       return fail(kInvalid, "pwgpu_server_submit: n_pw, n_k and dims must be positive");
     if (!s.miller || !s.k_weights || !s.kinetic || !s.v_local_g || !s.g_squared)
       return fail(kInvalid, "pwgpu_server_submit: required system array is NULL");
-    if (s.n_ch > 0 && (!s.proj_b || !s.atom_ch_start || !s.d_blocks || s.n_atoms <= 0))
+    if (s.n_ch > 0 && (!s.atom_ch_start || !s.d_blocks || s.n_atoms <= 0))
       return fail(kInvalid, "pwgpu_server_submit: projector arrays missing");
+    if (s.n_ch > 0 && !s.proj_b &&
+        (!s.g_cart || !s.k_cart || !s.atom_tau || !s.atom_species || s.n_species <= 0 || !s.species_mesh ||
+         !s.radial_r || !s.radial_rab || !s.species_nbeta || !s.beta_l || !s.beta_r))
+      return fail(kInvalid, "pwgpu_server_submit: projector radial data missing");
     if (s.n_sym > 1 && (!s.sym_src || !s.sym_arg))
       return fail(kInvalid, "pwgpu_server_submit: symmetry map missing");
     const size_t N = (size_t)s.dims[0] * s.dims[1] * s.dims[2];
@@ -63,7 +68,38 @@ struct SystemCopy {
     sys.v_local_g = v_local_g.data();
     sys.g_squared = g_squared.data();
     if (s.n_ch > 0) {
-      proj_b.assign(s.proj_b, s.proj_b + nk * n * (size_t)s.n_ch * 2);
+      if (s.proj_b) {
+        proj_b.assign(s.proj_b, s.proj_b + nk * n * (size_t)s.n_ch * 2);
+      } else {
+        // radial form of the projectors: G and k vectors, atoms, meshes, betas
+        const int ns = s.n_species;
+        g_cart.assign(s.g_cart, s.g_cart + 3 * n);
+        k_cart.assign(s.k_cart, s.k_cart + 3 * nk);
+        atom_tau.assign(s.atom_tau, s.atom_tau + 3L * s.n_atoms);
+        atom_species.assign(s.atom_species, s.atom_species + s.n_atoms);
+        species_mesh.assign(s.species_mesh, s.species_mesh + ns);
+        species_nbeta.assign(s.species_nbeta, s.species_nbeta + ns);
+        size_t mesh_tot = 0, nbeta = 0, beta_tot = 0;
+        for (int q = 0; q < ns; ++q) {
+          mesh_tot += (size_t)species_mesh[q];
+          nbeta += (size_t)species_nbeta[q];
+          beta_tot += (size_t)species_nbeta[q] * species_mesh[q];
+        }
+        radial_r.assign(s.radial_r, s.radial_r + mesh_tot);
+        radial_rab.assign(s.radial_rab, s.radial_rab + mesh_tot);
+        beta_l.assign(s.beta_l, s.beta_l + nbeta);
+        beta_r.assign(s.beta_r, s.beta_r + beta_tot);
+        sys.g_cart = g_cart.data();
+        sys.k_cart = k_cart.data();
+        sys.atom_tau = atom_tau.data();
+        sys.atom_species = atom_species.data();
+        sys.species_mesh = species_mesh.data();
+        sys.species_nbeta = species_nbeta.data();
+        sys.radial_r = radial_r.data();
+        sys.radial_rab = radial_rab.data();
+        sys.beta_l = beta_l.data();
+        sys.beta_r = beta_r.data();
+      }
       atom_ch_start.assign(s.atom_ch_start, s.atom_ch_start + s.n_atoms + 1);
       size_t nd = 0;
       for (int a = 0; a < s.n_atoms; ++a) {
@@ -72,7 +108,7 @@ struct SystemCopy {
         nd += (size_t)nc * nc;
       }
       d_blocks.assign(s.d_blocks, s.d_blocks + nd);
-      sys.proj_b = proj_b.data();
+      sys.proj_b = s.proj_b ? proj_b.data() : nullptr;
       sys.atom_ch_start = atom_ch_start.data();
       sys.d_blocks = d_blocks.data();
     } else {

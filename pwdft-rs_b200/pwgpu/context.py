@@ -91,7 +91,7 @@ class Projectors:
 
     @property
     def n_ch(self):
-        return self.b.shape[1]
+        return int(self.atom_ch_start[-1]) if self.b is None else self.b.shape[1]
 
     def d_dense(self) -> np.ndarray:
         n = self.n_ch
@@ -154,6 +154,18 @@ def build_projectors(crystal: Crystal, basis: BasisSet, k, radial_tables) -> Pro
         starts.append(starts[-1] + blk.shape[0])
     b = np.stack(cols, axis=1) if cols else np.zeros((len(basis), 0), dtype=np.complex128)
     return Projectors(np.asfortranarray(b), blocks, np.array(starts, dtype=np.int32))
+
+
+def projector_layout(crystal: Crystal, radial_tables) -> Projectors:
+    """D blocks and channel starts of the projectors, without B (b = None):
+    the device builds B from the radial data (pwgpu_system radial fields)."""
+    blocks, starts = [], [0]
+    for at in crystal.atoms:
+        ls, _, dij = radial_tables[at.symbol]
+        blk = _atom_d_block(ls, dij)
+        blocks.append(blk)
+        starts.append(starts[-1] + blk.shape[0])
+    return Projectors(None, blocks, np.array(starts, dtype=np.int32))
 
 
 def upf_radial_table(pp: Upf):
@@ -247,9 +259,10 @@ class ScfSystem:
 
 def build_system(crystal: Crystal, pps: dict, ecut_ev: float, kpoints, symmetry: SymmetryInfo | None = None,
                  ecutrho_ratio: int = 4, fft_grid=None, gaussian_sigma: float = 1.0, nspin: int = 1,
-                 with_initial_density: bool = True) -> ScfSystem:
+                 with_initial_density: bool = True, projectors_on_device: bool = False) -> ScfSystem:
     """ScfContext::new (context.rs:102-231) plus the SAD start density
-    (initial_density.rs:64-143)."""
+    (initial_density.rs:64-143).  projectors_on_device: skip the host B
+    (the GPU builds it from the UPF radial data at pwgpu_create)."""
     basis = BasisSet(crystal.lattice, ecut_ev)
     dims = grid_dims_for(basis, ecutrho_ratio, fft_grid)
     omega = crystal.lattice.volume()
@@ -300,7 +313,11 @@ def build_system(crystal: Crystal, pps: dict, ecut_ev: float, kpoints, symmetry:
 
     tables = {sp: upf_radial_table(pps[sp]) for sp in crystal.species()}
     kin = [basis.kinetic(kp.k) for kp in kpoints]
-    projs = [build_projectors(crystal, basis, kp.k, tables) for kp in kpoints]
+    if projectors_on_device:
+        layout = projector_layout(crystal, tables)
+        projs = [layout for _ in kpoints]
+    else:
+        projs = [build_projectors(crystal, basis, kp.k, tables) for kp in kpoints]
     e_ew = ewald_energy(crystal, [pps[a.symbol].z_valence for a in crystal.atoms])
     sym = symmetry if symmetry is not None else SymmetryInfo.identity_only()
 
@@ -320,5 +337,7 @@ def build_system(crystal: Crystal, pps: dict, ecut_ev: float, kpoints, symmetry:
         if integ > 1e-15:
             rho0 *= nel / integ
 
-    return ScfSystem(crystal, basis, dims, g_to_fft, list(kpoints), kin, projs, v_loc, g2, rho_core_r, nel, omega,
-                     e_ew, sym, rho0, nspin)
+    out = ScfSystem(crystal, basis, dims, g_to_fft, list(kpoints), kin, projs, v_loc, g2, rho_core_r, nel, omega,
+                    e_ew, sym, rho0, nspin)
+    out.extra["pps"] = pps
+    return out

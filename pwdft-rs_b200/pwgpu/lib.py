@@ -60,6 +60,17 @@ class PwgpuSystem(ct.Structure):
         ("omega", ct.c_double),
         ("e_ewald", ct.c_double),
         ("nspin", ct.c_int32),
+        ("g_cart", _f64p),
+        ("k_cart", _f64p),
+        ("atom_tau", _f64p),
+        ("atom_species", _i32p),
+        ("n_species", ct.c_int32),
+        ("species_mesh", _i32p),
+        ("radial_r", _f64p),
+        ("radial_rab", _f64p),
+        ("species_nbeta", _i32p),
+        ("beta_l", _i32p),
+        ("beta_r", _f64p),
     ]
 
 
@@ -172,6 +183,7 @@ def load_library(path: str = LIB_PATH):
     lib.pwgpu_mix.argtypes = [vp, ct.c_int32, ct.c_int32, _f64p, _f64p, _f64p, ct.c_double, ct.c_int32, ct.c_int32,
                               ct.c_double]
     lib.pwgpu_mix_reset.argtypes = [vp]
+    lib.pwgpu_get_projectors.argtypes = [vp, ct.c_int32, _f64p]
     lib.pwgpu_small_geneig.argtypes = [ct.c_int32, ct.c_int32, ct.c_int32, _f64p, _f64p, _f64p, _f64p]
     lib.pwgpu_get_stream.argtypes = [vp, ct.POINTER(vp)]
     lib.pwgpu_get_stream.restype = ct.c_int32
@@ -190,7 +202,7 @@ def load_library(path: str = LIB_PATH):
     for name in ("pwgpu_create", "pwgpu_destroy", "pwgpu_set_veff_g", "pwgpu_apply_h", "pwgpu_apply_h_device",
                  "pwgpu_set_precision", "pwgpu_get_dims", "pwgpu_profile_apply_h", "pwgpu_scf_run",
                  "pwgpu_eigensolve", "pwgpu_density", "pwgpu_symmetrize", "pwgpu_potentials",
-                 "pwgpu_small_geneig", "pwgpu_mix", "pwgpu_mix_reset", "pwgpu_server_create", "pwgpu_server_destroy",
+                 "pwgpu_small_geneig", "pwgpu_mix", "pwgpu_mix_reset", "pwgpu_get_projectors", "pwgpu_server_create", "pwgpu_server_destroy",
                  "pwgpu_server_submit", "pwgpu_server_poll", "pwgpu_server_wait", "pwgpu_server_wait_any",
                  "pwgpu_server_result", "pwgpu_server_release", "pwgpu_server_get_stats"):
         getattr(lib, name).restype = ct.c_int32
@@ -234,13 +246,31 @@ def pack_system(sys_) -> tuple:
     s.kinetic = _f64(kin)
     s.n_ch = n_ch
     if n_ch:
-        b = hold(np.concatenate([np.asfortranarray(p.b).ravel(order="F") for p in projs]).astype(np.complex128))
         starts = hold(np.ascontiguousarray(projs[0].atom_ch_start, dtype=np.int32))
         blocks = hold(np.concatenate([blk.ravel() for blk in projs[0].d_blocks]).astype(np.float64))
-        s.proj_b = b.view(np.float64).ctypes.data_as(_f64p)
         s.n_atoms = len(projs[0].d_blocks)
         s.atom_ch_start = _i32(starts)
         s.d_blocks = _f64(blocks)
+        if projs[0].b is not None:
+            b = hold(np.concatenate([np.asfortranarray(p.b).ravel(order="F") for p in projs]).astype(np.complex128))
+            s.proj_b = b.view(np.float64).ctypes.data_as(_f64p)
+        else:
+            # radial form: the device builds B (NonlocalPotential::new on the GPU)
+            cr, pps = sys_.crystal, sys_.extra["pps"]
+            species = list(dict.fromkeys(a.symbol for a in cr.atoms))
+            s.g_cart = _f64(hold(np.ascontiguousarray(sys_.basis.g, dtype=np.float64)))
+            s.k_cart = _f64(hold(np.ascontiguousarray(np.array([kp.k for kp in sys_.kpoints]), dtype=np.float64)))
+            s.atom_tau = _f64(hold(np.ascontiguousarray(np.array([a.cart(cr.lattice) for a in cr.atoms]),
+                                                        dtype=np.float64)))
+            s.atom_species = _i32(hold(np.array([species.index(a.symbol) for a in cr.atoms], dtype=np.int32)))
+            s.n_species = len(species)
+            s.species_mesh = _i32(hold(np.array([pps[sp].r.size for sp in species], dtype=np.int32)))
+            s.radial_r = _f64(hold(np.concatenate([pps[sp].r for sp in species]).astype(np.float64)))
+            s.radial_rab = _f64(hold(np.concatenate([pps[sp].rab for sp in species]).astype(np.float64)))
+            s.species_nbeta = _i32(hold(np.array([len(pps[sp].beta_l) for sp in species], dtype=np.int32)))
+            s.beta_l = _i32(hold(np.array([l for sp in species for l in pps[sp].beta_l], dtype=np.int32)))
+            betas = [np.asarray(pps[sp].beta[i], dtype=np.float64) for sp in species for i in range(len(pps[sp].beta_l))]
+            s.beta_r = _f64(hold(np.concatenate(betas) if betas else np.zeros(1)))
     vl = hold(np.ascontiguousarray(sys_.v_local_g, dtype=np.complex128))
     s.v_local_g = vl.view(np.float64).ctypes.data_as(_f64p)
     g2 = hold(np.ascontiguousarray(sys_.g_squared, dtype=np.float64))
@@ -368,6 +398,14 @@ class PwGpu:
         out = np.empty_like(a)
         _check(self.lib, self.lib.pwgpu_mix(self.h, channel, mixing_mode(mixer, kerker), _f64(a), _f64(b),
                                             _f64(out), beta, ndim, period, q_tf))
+        return out
+
+    def projectors(self, ik: int = 0) -> np.ndarray:
+        """The device copy of B at k-point ik (n_pw x n_ch complex)."""
+        n_ch = self.sys.projectors[ik].n_ch
+        out = np.zeros((self.n_pw, n_ch), dtype=np.complex128, order="F")
+        _check(self.lib, self.lib.pwgpu_get_projectors(self.h, ik,
+                                                       out.ravel(order="F").view(np.float64).ctypes.data_as(_f64p)))
         return out
 
     def mix_reset(self):

@@ -9,6 +9,9 @@ displacements U(-0.05, 0.05) bohr per component, ecutwfc uniform in
 {20, 25, 30, 35} Ry, a Gamma-only or Gamma-centred 2x2x2 mesh (50/50,
 reduced by the cell's symmetry), PZ-LDA, unpolarised, mixed precision.
 
+The projector matrices of a request are built on the device from the UPF
+radial data (pwgpu_create), not on the host.
+
 SCF controls of a request: bands = N_el/2 + max(4, N_el/20); Gaussian
 smearing 0.01 Ry; Anderson beta 0.4 + Kerker, 8 slots (the settings of the
 64-atom benchmark solve, which converge the wide-gap C cells too); density
@@ -171,7 +174,7 @@ def request_system(req: Request, pps: dict):
     cr = request_crystal(req)
     sym = SymmetryInfo.from_crystal(cr, 1e-5)
     kp = reduce_kpoints(req.kgrid, "gamma", sym, cr.lattice)
-    s = build_system(cr, {req.species: pps[req.species]}, req.ecut_ry * RY_TO_EV, kp, sym)
+    s = build_system(cr, {req.species: pps[req.species]}, req.ecut_ry * RY_TO_EV, kp, sym, projectors_on_device=True)
     nel = int(round(s.n_electrons))
     nb = nel // 2 + max(4, nel // 20)
     return s, dict(SERVE_KW, n_bands=nb)

@@ -82,18 +82,26 @@ def test_wait_times_out_then_completes(si_pp, c_pp):
 
 
 def test_stream_requests_build_and_solve(si_pp, c_pp):
-    """The first small requests of the serving stream run through the queue."""
+    """Small requests of the serving stream (device-built projectors, Gamma
+    and 2x2x2 meshes, Si and C) run four at a time through the queue and
+    give the energies of the same requests solved one by one."""
     pps = {"Si": si_pp, "C": c_pp}
-    reqs = [r for r in request_stream(30) if r.n_atoms == 2][:4]
-    with Server(workers=2) as srv:
-        ids = []
-        for r in reqs:
-            s, kw = request_system(r, pps)
-            kw = dict(kw)
-            nb = kw.pop("n_bands")
-            ids.append(srv.submit(s, nb, **kw))
+    reqs = [r for r in request_stream(40) if r.n_atoms <= 8][:8]
+    built = []
+    for r in reqs:
+        s, kw = request_system(r, pps)
+        kw = dict(kw)
+        built.append((r, s, kw.pop("n_bands"), kw))
+    with Server(workers=4) as srv:
+        ids = [srv.submit(s, nb, **kw) for _, s, nb, kw in built]
+        got = []
         for jid in ids:
             info = srv.wait(jid, 300.0)
             assert info["status"] == 0
             res, ev, status, err = srv.result(jid)
             assert res["converged"] == 1 and np.all(np.isfinite(ev))
+            got.append(res["total_energy"])
+    for (r, s, nb, kw), e in zip(built, got):
+        with PwGpu(s, lanes=2) as dev:
+            res, _, _, _ = dev.scf_run(s.rho_init_r, nb, **kw)
+        assert abs(res["total_energy"] - e) / r.n_atoms < 1e-4, (r, res["total_energy"], e)
