@@ -203,6 +203,10 @@ typedef struct pwgpu_scf_result {
   double magnetization;
   int64_t h_applications;   /* band applications of H over the run */
   double max_residual;      /* largest eigen-residual of the last eigensolve */
+  /* EnergyComponents (scf/energy.rs:597-670) of the final iteration, eV:
+   * sum f w <psi|T|psi>, int rho V_loc dV (V_loc(G = 0) included), sum f w <psi|V_NL|psi>;
+   * with e_hartree, e_xc, e_ewald and -entropy_ts they sum to total_energy at self-consistency */
+  double e_kinetic, e_local, e_nonlocal;
 } pwgpu_scf_result;
 
 /* Run the SCF loop from rho_init_r (N doubles, e/Å^3, the total start

@@ -320,6 +320,35 @@ def xc_energy_corrected(rho_xc, rho_val, exc, vxc, omega):
     return float(np.sum(rho_xc * exc * dv)) - float(np.sum(rho_val * vxc * dv))
 
 
+def kinetic_expectation(kinetic, psis, occs, weights):
+    """Σ_k w_k Σ_b f_b Σ_G |c_b(G)|² (ħ²/2m)|k+G|² (kinetic_expectation, energy.rs:382-421)."""
+    e = 0.0
+    for kin, v, o, w in zip(kinetic, psis, occs, weights):
+        t = np.sum(np.abs(v) ** 2 * kin[:, None], axis=0)
+        e += w * float(np.sum(np.where(o == 0.0, 0.0, o * t)))
+    return e
+
+
+def nonlocal_expectation(bs, d_dense, psis, occs, weights):
+    """Σ_k w_k Σ_b f_b Re ψ_b^H H_NL ψ_b with the dense H_NL = B D B^H of each k
+    (nonlocal_expectation, energy.rs:467-516)."""
+    e = 0.0
+    for b, d, v, o, w in zip(bs, d_dense, psis, occs, weights):
+        if b.shape[1] == 0:
+            continue
+        h_nl = b @ (d @ b.conj().T)
+        t = np.real(np.sum(v.conj() * (h_nl @ v), axis=0))
+        e += w * float(np.sum(np.where(o == 0.0, 0.0, o * t)))
+    return e
+
+
+def local_pp_energy(rho_r, v_local_g, dims, omega):
+    """∫ρ V_loc dV with V_loc(r) the unnormalised inverse FFT of V_loc(G), G = 0
+    kept (driver.rs:664-668, local_pp_energy_grid energy.rs:439-445)."""
+    v_r = ifft3(v_local_g, dims).real
+    return float(np.sum(rho_r * v_r)) * omega / rho_r.size
+
+
 def density_diff(a, b, omega):
     n = a.size
     dv = omega / n
@@ -466,6 +495,7 @@ class OracleResult:
     rho_r: np.ndarray
     entropy_ts: float = 0.0
     history: list = field(default_factory=list)
+    components: dict = None    # EnergyComponents (energy.rs:597-670) of the final iteration
 
 
 def run_scf_unpolarized(sys, n_bands, max_iter=100, conv_threshold=1e-6, energy_threshold=1e-5,
@@ -525,7 +555,15 @@ def run_scf_unpolarized(sys, n_bands, max_iter=100, conv_threshold=1e-6, energy_
         if verbose:
             print(f"iter {it:3d} E={e_tot:.10f} dE={de} drho={delta:.3e}")
         if delta < conv_threshold and de is not None and de < energy_threshold:
-            return OracleResult(e_tot, e_hf, ef, evals, it + 1, delta, rho_new, ts, hist)
+            dv = omega / n
+            comp = dict(e_band=e_band,
+                        e_kinetic=kinetic_expectation(sys.kinetic, psis, occs, weights),
+                        e_local=local_pp_energy(rho_new, sys.v_local_g, dims, omega),
+                        e_nonlocal=nonlocal_expectation([p.b for p in sys.projectors], d_dense, psis, occs, weights),
+                        e_hartree=hartree_energy(rho_g_new, sys.g_squared, omega),
+                        e_xc=float(np.sum(rxc_new * exc_o * dv)), e_vxc=float(np.sum(rho_new * vxc_o * dv)),
+                        e_ewald=sys.e_ewald, e_smearing=-ts)
+            return OracleResult(e_tot, e_hf, ef, evals, it + 1, delta, rho_new, ts, hist, comp)
         rho = mixer.mix(rho, rho_new)
         rho_g = density_r_to_g(rho, dims)
     raise RuntimeError(f"SCF did not converge in {max_iter} iterations (delta={delta})")
@@ -548,6 +586,7 @@ class OracleSpinResult:
     magnetization: float
     entropy_ts: float = 0.0
     history: list = field(default_factory=list)
+    components: dict = None    # EnergyComponents (driver_spin.rs:715-780) of the final iteration
 
 
 def run_scf_spin(sys, n_bands, max_iter=100, conv_threshold=1e-6, energy_threshold=1e-5, mixing_beta=0.3,
@@ -643,7 +682,16 @@ def run_scf_spin(sys, n_bands, max_iter=100, conv_threshold=1e-6, energy_thresho
         if verbose:
             print(f"iter {it:3d} E={e_tot:.10f} dE={de} drho={delta:.3e} M={mag:.6f}")
         if delta < conv_threshold and de is not None and de < energy_threshold:
-            return OracleSpinResult(e_tot, e_hf, ef, ev_all, it + 1, delta, up_new, dn_new, mag, ts, hist)
+            bs = [p.b for p in sys.projectors]
+            comp = dict(e_band=e_band,
+                        e_kinetic=(kinetic_expectation(sys.kinetic, ps_up, occ_up, weights)
+                                   + kinetic_expectation(sys.kinetic, ps_dn, occ_dn, weights)),
+                        e_local=local_pp_energy(tot_new, sys.v_local_g, dims, omega),
+                        e_nonlocal=(nonlocal_expectation(bs, d_dense, ps_up, occ_up, weights)
+                                    + nonlocal_expectation(bs, d_dense, ps_dn, occ_dn, weights)),
+                        e_hartree=hartree_energy(tot_new_g, sys.g_squared, omega), e_xc=e_xc_o, e_vxc=e_vxc_o,
+                        e_ewald=sys.e_ewald, e_smearing=-ts)
+            return OracleSpinResult(e_tot, e_hf, ef, ev_all, it + 1, delta, up_new, dn_new, mag, ts, hist, comp)
         t_mix = mix_tot.mix(tot, tot_new)
         m_mix = mix_mag.mix(up - dn, up_new - dn_new)
         up = 0.5 * (t_mix + m_mix)

@@ -331,6 +331,9 @@ pwgpu_status pwgpu_scf_run(pwgpu_handle* ph, const pwgpu_scf_params* p, const do
   result->magnetization = r.magnetization;
   result->h_applications = r.h_applications;
   result->max_residual = r.max_residual;
+  result->e_kinetic = r.e_kinetic;
+  result->e_local = r.e_local;
+  result->e_nonlocal = r.e_nonlocal;
   return st;
 }
 

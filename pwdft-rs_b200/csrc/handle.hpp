@@ -129,12 +129,20 @@ Status nonlocal_mixed(Handle& h, int ik, const double2* psi, long ldpsi, int nb,
                       cudaStream_t s, StageTimer* tm = nullptr);
 void release_nl_mixed(Handle& h);
 
+// Per-band kinetic and nonlocal expectations of nb columns of V at k-point ik
+// (packed real on Gamma handles), into host t_kin and t_nl (components.cu).
+Status band_energy_terms(Handle& h, int ik, const double2* V, long ldv, int nb, double* t_kin, double* t_nl,
+                         cudaStream_t s);
+
 // Grid-map construction and the H|psi> launcher (hpsi.cu).
 Status build_grid_maps(Handle& h, const int* miller_host);
 Status apply_h_device(Handle& h, int spin, int ik, const double2* psi, long ldpsi, int nb, double2* hpsi,
                       long ldh, int precision, cudaStream_t stream, StageTimer* timer = nullptr);
 Status set_veff_from_g(Handle& h, int spin, const double2* veff_g_dev, cudaStream_t stream);
 Status ensure_nl_capacity(Handle& h, int nb);
+// P = B^H psi into h.nl_p and Q = D P into h.nl_q (FP64), nb columns.
+Status nonlocal_pq(Handle& h, int ik, const double2* psi, long ldpsi, int nb, cudaStream_t s,
+                   StageTimer* tm = nullptr);
 
 // Local part of H|psi> only (kinetic + V_eff through the FFT pipeline).
 Status apply_local_device(Handle& h, int spin, int ik, const double2* psi, long ldpsi, int nb, double2* hpsi,
@@ -168,6 +176,8 @@ void release_gamma_scratch(Handle& h);
 // one complex vector, then real projector GEMMs).
 Status apply_h_real(Handle& h, int spin, const double* u, long ldu, int nb, double* hu, long ldh, int precision,
                     cudaStream_t s);
+// P = B_r^T u into h.gam_p and Q = D P into h.gam_q for nb packed real bands.
+Status nonlocal_pq_real(Handle& h, const double* u, long ldu, int nb, cudaStream_t s);
 // rho += sum_b fw[b] |psi_b(r)|^2 for nb packed real bands (fw on the host).
 Status density_accumulate_real(Handle& h, const double* u, long ldu, const std::vector<double>& fw, double* rho,
                                cudaStream_t s);

@@ -688,6 +688,26 @@ Status apply_local_device(Handle& h, int spin, int ik, const double2* psi, long 
   return kOk;
 }
 
+Status nonlocal_pq(Handle& h, int ik, const double2* psi, long ldpsi, int nb, cudaStream_t s, StageTimer* tm) {
+  if (h.n_ch <= 0 || nb <= 0) return kOk;
+  Status st;
+  if ((st = ensure_nl_capacity(h, nb)) != kOk) return st;
+  cublasSetStream(h.blas, s);
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+  const cuDoubleComplex* Bm = reinterpret_cast<const cuDoubleComplex*>(h.kp[ik].b);
+  cublasStatus_t cs = cublasZgemm(h.blas, CUBLAS_OP_C, CUBLAS_OP_N, h.n_ch, nb, h.n_pw, &one, Bm, h.n_pw,
+                                  reinterpret_cast<const cuDoubleComplex*>(psi), (int)ldpsi, &zero,
+                                  reinterpret_cast<cuDoubleComplex*>(h.nl_p), h.n_ch);
+  if (cs != CUBLAS_STATUS_SUCCESS) return fail(kCuda, "cublasZgemm (B^H psi) failed");
+  mark(tm, 5, s);
+  const long tot = (long)h.n_ch * nb;
+  k_apply_d<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(h.nl_p, h.nl_q, h.n_ch, nb, h.ch_atom, h.atom_ch_start,
+                                                          h.d_off, h.d_vals); count_launch();
+  mark(tm, 6, s);
+  PW_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
 Status apply_h_device(Handle& h, int spin, int ik, const double2* psi, long ldpsi, int nb, double2* hpsi, long ldh,
                       int precision, cudaStream_t s, StageTimer* tm) {
   if (ik < 0 || ik >= h.n_k) return fail(kInvalid, "apply_h: k-point index out of range");
@@ -700,20 +720,10 @@ Status apply_h_device(Handle& h, int spin, int ik, const double2* psi, long ldps
   if (h.n_ch > 0 && precision == 1 && nl_mixed_eligible(h)) {
     if ((st = nonlocal_mixed(h, ik, psi, ldpsi, nb, hpsi, ldh, s, tm)) != kOk) return st;
   } else if (h.n_ch > 0) {
-    if ((st = ensure_nl_capacity(h, nb)) != kOk) return st;
-    cublasSetStream(h.blas, s);
-    const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+    if ((st = nonlocal_pq(h, ik, psi, ldpsi, nb, s, tm)) != kOk) return st;
+    const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
     const cuDoubleComplex* Bm = reinterpret_cast<const cuDoubleComplex*>(h.kp[ik].b);
-    cublasStatus_t cs = cublasZgemm(h.blas, CUBLAS_OP_C, CUBLAS_OP_N, h.n_ch, nb, h.n_pw, &one, Bm, h.n_pw,
-                                    reinterpret_cast<const cuDoubleComplex*>(psi), (int)ldpsi, &zero,
-                                    reinterpret_cast<cuDoubleComplex*>(h.nl_p), h.n_ch);
-    if (cs != CUBLAS_STATUS_SUCCESS) return fail(kCuda, "cublasZgemm (B^H psi) failed");
-    mark(tm, 5, s);
-    const long tot = (long)h.n_ch * nb;
-    k_apply_d<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(h.nl_p, h.nl_q, h.n_ch, nb, h.ch_atom, h.atom_ch_start,
-                                                            h.d_off, h.d_vals); count_launch();
-    mark(tm, 6, s);
-    cs = cublasZgemm(h.blas, CUBLAS_OP_N, CUBLAS_OP_N, h.n_pw, nb, h.n_ch, &one, Bm, h.n_pw,
+    cublasStatus_t cs = cublasZgemm(h.blas, CUBLAS_OP_N, CUBLAS_OP_N, h.n_pw, nb, h.n_ch, &one, Bm, h.n_pw,
                      reinterpret_cast<const cuDoubleComplex*>(h.nl_q), h.n_ch, &one,
                      reinterpret_cast<cuDoubleComplex*>(hpsi), (int)ldh);
     if (cs != CUBLAS_STATUS_SUCCESS) return fail(kCuda, "cublasZgemm (B Q) failed");

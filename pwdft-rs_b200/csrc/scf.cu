@@ -183,6 +183,11 @@ __global__ void k_veff_g(const double2* __restrict__ vloc, const double2* __rest
   }
 }
 
+__global__ void k_real_part(const double2* __restrict__ c, double* __restrict__ r, long n) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) r[i] = c[i].x;
+}
+
 __global__ void k_real_part_both(const double2* __restrict__ c, double* __restrict__ r64, float* __restrict__ r32,
                                  long n) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -629,6 +634,27 @@ static Status potentials(Handle& h, const double* rho, bool set_hpsi, PotEnergie
     k_real_part_both<<<blocks_for(N), 256, 0, s>>>(h.tmp_grid, h.veff_r[0], h.veff_r32[0], N); count_launch();
   }
   PW_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
+// E_local = int rho V_loc dV over the given density channels, V_loc(r) the
+// unnormalised inverse FFT of V_loc(G) with its G = 0 term (driver.rs:664-668,
+// local_pp_energy_grid energy.rs:439-445); uses cg2 and rtmp as scratch.
+static Status local_energy(Handle& h, double* const* rho, int nrho, double& e) {
+  ScfState* st = h.scf;
+  const long N = h.g.N;
+  const cudaStream_t s = h.stream;
+  PW_CUDA_TRY(cudaMemcpyAsync(st->cg2, h.v_local_g, N * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+  Status r = fft3d_full(h, st->cg2, +1, s);
+  if (r != kOk) return r;
+  k_real_part<<<blocks_for(N), 256, 0, s>>>(st->cg2, st->rtmp, N); count_launch();
+  e = 0.0;
+  for (int c = 0; c < nrho; ++c) {
+    double part = 0.0;
+    if ((r = reduce_host(h, rho[c], st->rtmp, N, 1, part)) != kOk) return r;
+    e += part;
+  }
+  e *= h.omega / (double)N;
   return kOk;
 }
 
@@ -1242,6 +1268,26 @@ Status scf_run(Handle& h, const ScfParams& p, const double* rho_init, ScfResult&
       res.magnetization = mag;
       res.h_applications = happ;
       res.max_residual = max_res_all;
+      // energy decomposition of the final iteration (driver.rs:652-710,
+      // driver_spin.rs:715-780): band terms from the last eigenvectors and
+      // occupations, the local term from the output density
+      {
+        std::vector<double> tk(nb), tn(nb);
+        double ekin = 0.0, enl = 0.0;
+        for (int c = 0; c < ns * nk; ++c) {
+          if ((r = band_energy_terms(h, c % nk, st->ks[c].V, h.n_pw, nb, tk.data(), tn.data(), s)) != kOk) return r;
+          for (int b = 0; b < nb; ++b) {
+            if (occ[c][b] == 0.0) continue;
+            ekin += occ[c][b] * wk_all[c] * tk[b];
+            enl += occ[c][b] * wk_all[c] * tn[b];
+          }
+        }
+        double eloc = 0.0;
+        if ((r = local_energy(h, rout, ns, eloc)) != kOk) return r;
+        res.e_kinetic = ekin;
+        res.e_local = eloc;
+        res.e_nonlocal = enl;
+      }
       if (evals_out)
         for (size_t c = 0; c < ev.size(); ++c)
           for (int b = 0; b < nb; ++b) evals_out[c * nb + b] = ev[c][b];

@@ -42,6 +42,7 @@ struct ScfResult {
   double magnetization = 0;
   long h_applications = 0;
   double max_residual = 0;
+  double e_kinetic = 0, e_local = 0, e_nonlocal = 0;  // EnergyComponents of the final iteration
 };
 
 // Whole SCF (driver.rs:266-742 for nspin = 1).  rho_init: N doubles on the

@@ -100,7 +100,8 @@ class PwgpuScfResult(ct.Structure):
         ("final_delta", ct.c_double), ("e_band", ct.c_double), ("e_hartree", ct.c_double), ("e_xc", ct.c_double),
         ("e_vxc", ct.c_double), ("e_ewald", ct.c_double), ("n_iterations", ct.c_int32), ("converged", ct.c_int32),
         ("nspin", ct.c_int32), ("magnetization", ct.c_double), ("h_applications", ct.c_int64),
-        ("max_residual", ct.c_double),
+        ("max_residual", ct.c_double), ("e_kinetic", ct.c_double), ("e_local", ct.c_double),
+        ("e_nonlocal", ct.c_double),
     ]
 
     def as_dict(self):

@@ -103,3 +103,30 @@ def test_cpu_scf_baseline_golden(si_pp):
     assert r.n_iterations < 40
     assert abs(r.total_energy - (-213.028339)) < 1e-3
     assert abs(r.fermi_energy - 8.052064) < 1e-3
+
+
+def test_energy_components_match_reference_pins(si_pp):
+    """EnergyComponents of the Si diamond 15 Ry, shifted 4x4x4 MP, 8 bands,
+    Fermi-Dirac 0.01 Ry case against the reference's regression pins
+    (tests/vgc5_per_component_si.rs:238-331: per term, 0.05 eV there; the
+    pins carry four decimals and the oracle lands within 1e-3 eV of each),
+    the direct-sum identity (< 1e-5 eV, :325-331) and the band-sum identity
+    E_band = E_kin + E_loc + E_nl + 2 E_H + E_vxc (< 1e-7 eV, :509-540)."""
+    from pwgpu.symmetry import reduce_kpoints
+    cr = diamond_primitive("Si", 5.431)
+    sym = SymmetryInfo.from_crystal(cr, 1e-5)
+    kp = reduce_kpoints((4, 4, 4), "mp1976", sym, cr.lattice)
+    s = build_system(cr, {"Si": si_pp}, 15.0 * RY_TO_EV, kp, sym)
+    r = O.run_scf_unpolarized(s, 8, max_iter=80, conv_threshold=1e-8, energy_threshold=1e-6, mixing_beta=0.3,
+                              mixing_ndim=8, smearing="fermi_dirac", sigma=0.01 * RY_TO_EV)
+    c = r.components
+    pins = {"e_band": 7.7748, "e_kinetic": 83.4120, "e_local": -52.9772, "e_nonlocal": 35.7641,
+            "e_hartree": 14.8249, "e_xc": -84.3474, "e_ewald": -228.5192}
+    for name, want in pins.items():
+        assert abs(c[name] - want) < 1e-3, (name, c[name], want)
+    assert abs(r.total_energy - (-231.8429)) < 0.05
+    direct = (c["e_kinetic"] + c["e_local"] + c["e_nonlocal"] + c["e_hartree"] + c["e_xc"] + c["e_ewald"]
+              + c["e_smearing"])
+    assert abs(direct - r.total_energy) < 1e-5
+    band = c["e_kinetic"] + c["e_local"] + c["e_nonlocal"] + 2.0 * c["e_hartree"] + c["e_vxc"]
+    assert abs(band - c["e_band"]) < 1e-7
