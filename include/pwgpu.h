@@ -222,6 +222,22 @@ pwgpu_status pwgpu_scf_run(pwgpu_handle* h, const pwgpu_scf_params* params, cons
                            pwgpu_scf_result* result, double* eigenvalues, double* rho_r_out,
                            double* rho_g_basis_out);
 
+/* Exactly one SCF iteration seeded from a density given as rho(G) on the full
+ * FFT grid (N complex, rho(G) = (1/N) sum_r rho(r) e^{-iG.r}, grid order of
+ * g_vector_at_dims): replaces run_scf_iter1_from_rho_g_fft
+ * (scf/transplant.rs:114-376).  rho_in(r) is the unnormalised inverse
+ * transform of the input; V_eff from rho_in, eigenpairs to params->diag_tol
+ * from a cold start, occupations, output density, energies and components
+ * on the output density; result->final_delta is drho_rms(in, out) and
+ * result->converged 0.  nspin = 1 only (PWGPU_E_INVALID otherwise), as the
+ * reference.  Outputs may be NULL: eigenvalues n_k x n_bands, rho_r_out N,
+ * rho_g_fft_out N complex (the output density on the same grid: a restart
+ * point), rho_r_in N (the input density re-materialised). */
+pwgpu_status pwgpu_scf_iter1_from_rho_g(pwgpu_handle* h, const pwgpu_scf_params* params,
+                                        const double* rho_g_fft_in, pwgpu_scf_result* result,
+                                        double* eigenvalues, double* rho_r_out, double* rho_g_fft_out,
+                                        double* rho_r_in);
+
 /* Lowest n_bands eigenpairs of H at (spin, ik) for the current V_eff
  * (diagonalize_dispatch, scf/driver.rs:125-184, lowest-n contract of
  * eigensolver/dense.rs:87-98).  psi_in: optional warm start (n_pw x n_bands

@@ -569,6 +569,73 @@ def run_scf_unpolarized(sys, n_bands, max_iter=100, conv_threshold=1e-6, energy_
     raise RuntimeError(f"SCF did not converge in {max_iter} iterations (delta={delta})")
 
 
+@dataclass
+class OracleIter1Result:
+    total_energy: float
+    harris_foulkes_energy: float
+    fermi_energy: float
+    entropy_ts: float
+    eigenvalues: list
+    components: dict
+    rho_r_out: np.ndarray
+    rho_g_out: np.ndarray
+    rho_r_in: np.ndarray
+    delta_rho: float
+
+
+def run_scf_iter1_from_rho_g(sys, n_bands, rho_g_fft, smearing="fermi_dirac", sigma=0.01):
+    """One SCF iteration from a transplanted full-grid rho(G)
+    (run_scf_iter1_from_rho_g_fft, scf/transplant.rs:114-376): rho_in(r) =
+    Re N·IFFT(rho_g), rho(G) re-derived from it, then the first iteration of
+    the unpolarised driver with cold dense diagonalisation; energies and
+    components on the output density."""
+    dims = sys.dims
+    n = sys.n_grid
+    omega = sys.omega
+    weights = sys.kpt_weights
+    spin_factor = 2.0
+    if len(rho_g_fft) != n:
+        raise ValueError(f"transplanted rho_g_fft has {len(rho_g_fft)} entries; expected n_grid={n}")
+    rho = ifft3(np.asarray(rho_g_fft, dtype=np.complex128), dims).real.copy()
+    rho_g = density_r_to_g(rho, dims)
+    vh = hartree(rho_g, sys.g_squared)
+    rxc = add_core(rho, sys.rho_core_r)
+    exc_in, vxc_in = lda_xc(rxc)
+    veff = sys.v_local_g + vh + density_r_to_g(vxc_in, dims)
+    d_dense = [p.d_dense() for p in sys.projectors]
+    evals, psis = [], []
+    for ik in range(len(sys.kpoints)):
+        h = dense_hamiltonian(sys.basis.miller, sys.kinetic[ik], veff, dims, sys.projectors[ik].b, d_dense[ik])
+        w, v = lowest_eigenpairs(h, n_bands)
+        evals.append(w)
+        psis.append(v)
+    ef = find_fermi_energy(evals, weights, sys.n_electrons, sigma, smearing, spin_factor)
+    occs = [spin_factor * occupation01(smearing, e, ef, sigma) for e in evals]
+    rho_new = compute_density(sys.g_to_fft, dims, psis, occs, weights, sys.n_electrons, omega)
+    if sys.symmetry.n_ops > 1:
+        src, arg = gather_map(dims, [(op.rotation, op.translation) for op in sys.symmetry.operations])
+        rho_new = symmetrize_density(rho_new, dims, src, arg)
+    delta = density_diff(rho, rho_new, omega)
+    rho_g_new = density_r_to_g(rho_new, dims)
+    rxc_new = add_core(rho_new, sys.rho_core_r)
+    exc_o, vxc_o = lda_xc(rxc_new)
+    e_band = float(sum(np.sum(o * w * e) for o, w, e in zip(occs, weights, evals)))
+    ts = entropy_ts(evals, weights, ef, sigma, smearing, spin_factor)
+    e_tot = (e_band - hartree_energy(rho_g_new, sys.g_squared, omega)
+             + xc_energy_corrected(rxc_new, rho_new, exc_o, vxc_o, omega) + sys.e_ewald - ts)
+    e_hf = (e_band - hartree_energy(rho_g, sys.g_squared, omega)
+            + xc_energy_corrected(rxc, rho, exc_in, vxc_in, omega) + sys.e_ewald - ts)
+    dv = omega / n
+    comp = dict(e_band=e_band,
+                e_kinetic=kinetic_expectation(sys.kinetic, psis, occs, weights),
+                e_local=local_pp_energy(rho_new, sys.v_local_g, dims, omega),
+                e_nonlocal=nonlocal_expectation([p.b for p in sys.projectors], d_dense, psis, occs, weights),
+                e_hartree=hartree_energy(rho_g_new, sys.g_squared, omega),
+                e_xc=float(np.sum(rxc_new * exc_o * dv)), e_vxc=float(np.sum(rho_new * vxc_o * dv)),
+                e_ewald=sys.e_ewald, e_smearing=-ts)
+    return OracleIter1Result(e_tot, e_hf, ef, ts, evals, comp, rho_new, rho_g_new, rho, delta)
+
+
 # ---------------------------------------------------------------------------
 # Spin-polarised SCF driver (driver_spin.rs:114-839)
 # ---------------------------------------------------------------------------

@@ -282,11 +282,7 @@ pwgpu_status pwgpu_set_precision(pwgpu_handle* ph, int32_t precision) {
   return kOk;
 }
 
-pwgpu_status pwgpu_scf_run(pwgpu_handle* ph, const pwgpu_scf_params* p, const double* rho_init_r,
-                           pwgpu_scf_result* result, double* eigenvalues, double* rho_r_out,
-                           double* rho_g_basis_out) {
-  if (!ph || !p || !rho_init_r || !result) return fail(kInvalid, "pwgpu_scf_run: NULL argument");
-  ScfParams q;
+static Status convert_params(const pwgpu_scf_params* p, ScfParams& q) {
   q.n_bands = p->n_bands;
   q.max_iter = p->max_iter;
   q.conv_threshold = p->conv_threshold;
@@ -307,12 +303,14 @@ pwgpu_status pwgpu_scf_run(pwgpu_handle* ph, const pwgpu_scf_params* p, const do
   q.fixed_magnetization = p->fixed_magnetization;
   q.tot_magnetization = p->tot_magnetization;
   if (q.starting_magnetization < -1.0 || q.starting_magnetization > 1.0)
-    return fail(kInvalid, "pwgpu_scf_run: starting_magnetization must lie in [-1, 1]");
-  if (q.smearing < 0 || q.smearing > 4) return fail(kInvalid, "pwgpu_scf_run: unknown smearing scheme");
+    return fail(kInvalid, "scf params: starting_magnetization must lie in [-1, 1]");
+  if (q.smearing < 0 || q.smearing > 4) return fail(kInvalid, "scf params: unknown smearing scheme");
   q.mixing_period = p->mixing_period > 0 ? p->mixing_period : 3;
-  if (q.mixing_mode < 0 || q.mixing_mode > 5) return fail(kInvalid, "pwgpu_scf_run: unknown mixing mode");
-  ScfResult r;
-  Status st = scf_run(ph->h, q, rho_init_r, r, eigenvalues, rho_r_out, rho_g_basis_out);
+  if (q.mixing_mode < 0 || q.mixing_mode > 5) return fail(kInvalid, "scf params: unknown mixing mode");
+  return kOk;
+}
+
+static void copy_result(const ScfResult& r, pwgpu_scf_result* result) {
   result->total_energy = r.total_energy;
   result->harris_foulkes_energy = r.harris_foulkes_energy;
   result->free_energy = r.free_energy;
@@ -334,6 +332,31 @@ pwgpu_status pwgpu_scf_run(pwgpu_handle* ph, const pwgpu_scf_params* p, const do
   result->e_kinetic = r.e_kinetic;
   result->e_local = r.e_local;
   result->e_nonlocal = r.e_nonlocal;
+}
+
+pwgpu_status pwgpu_scf_run(pwgpu_handle* ph, const pwgpu_scf_params* p, const double* rho_init_r,
+                           pwgpu_scf_result* result, double* eigenvalues, double* rho_r_out,
+                           double* rho_g_basis_out) {
+  if (!ph || !p || !rho_init_r || !result) return fail(kInvalid, "pwgpu_scf_run: NULL argument");
+  ScfParams q;
+  Status st = convert_params(p, q);
+  if (st != kOk) return st;
+  ScfResult r;
+  st = scf_run(ph->h, q, rho_init_r, r, eigenvalues, rho_r_out, rho_g_basis_out);
+  copy_result(r, result);
+  return st;
+}
+
+pwgpu_status pwgpu_scf_iter1_from_rho_g(pwgpu_handle* ph, const pwgpu_scf_params* p, const double* rho_g_fft_in,
+                                        pwgpu_scf_result* result, double* eigenvalues, double* rho_r_out,
+                                        double* rho_g_fft_out, double* rho_r_in) {
+  if (!ph || !p || !rho_g_fft_in || !result) return fail(kInvalid, "pwgpu_scf_iter1_from_rho_g: NULL argument");
+  ScfParams q;
+  Status st = convert_params(p, q);
+  if (st != kOk) return st;
+  ScfResult r;
+  st = scf_iter1_from_rho_g(ph->h, q, rho_g_fft_in, r, eigenvalues, rho_r_out, rho_g_fft_out, rho_r_in);
+  copy_result(r, result);
   return st;
 }
 

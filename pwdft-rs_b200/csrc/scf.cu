@@ -1168,8 +1168,9 @@ Status scf_run(Handle& h, const ScfParams& p, const double* rho_init, ScfResult&
     // below the SCF's own delta rho until the last iterations (measured on
     // the 64-atom cell: 0.1 drho capped at 1e-3 eV took 2.8 s, 3 drho capped
     // at 3e-2 eV 1.4 s, same converged energy within 3e-5 eV)
-    const double tol = std::max(p.diag_tol, std::min(kDiagTolCap,
-                                                     kDiagTolPerDrho * (std::isfinite(last_delta) ? last_delta : 1.0)));
+    const double tol = p.single_step ? p.diag_tol
+                                     : std::max(p.diag_tol, std::min(kDiagTolCap, kDiagTolPerDrho *
+                                                (std::isfinite(last_delta) ? last_delta : 1.0)));
     // preconditioner shift: V_eff(G = 0) = mean of V_eff(r)
     double v0[2] = {0.0, 0.0};
     for (int sp = 0; sp < ns; ++sp) {
@@ -1177,7 +1178,7 @@ Status scf_run(Handle& h, const ScfParams& p, const double* rho_init, ScfResult&
       if ((r = reduce_host(h, h.veff_r[sp], nullptr, N, 0, vsum)) != kOk) return r;
       v0[sp] = vsum / (double)N;
     }
-    const int max_it = iter == 0 ? 4 * p.diag_max_iter : p.diag_max_iter;
+    const int max_it = (iter == 0 || p.single_step) ? 4 * p.diag_max_iter : p.diag_max_iter;
     std::vector<EigStats> stats((size_t)ns * nk);
     if ((r = eigensolve_all(h, v0, tol, max_it, nb, prec, stats)) != kOk) return r;
     max_res_all = 0.0;
@@ -1249,7 +1250,7 @@ Status scf_run(Handle& h, const ScfParams& p, const double* rho_init, ScfResult&
     const bool conv = delta < p.conv_threshold && have_prev && de < p.energy_threshold;
     e_prev = e_tot;
     have_prev = true;
-    if (conv || iter == p.max_iter - 1) {
+    if (conv || iter == p.max_iter - 1 || p.single_step) {
       res.total_energy = e_tot;
       res.harris_foulkes_energy = e_hf;
       res.free_energy = e_tot;
@@ -1312,7 +1313,7 @@ Status scf_run(Handle& h, const ScfParams& p, const double* rho_init, ScfResult&
         }
       }
       PW_CUDA_TRY(cudaStreamSynchronize(s));
-      return conv ? kOk : fail(kNotConverged, "SCF did not converge within max_iter");
+      return (conv || p.single_step) ? kOk : fail(kNotConverged, "SCF did not converge within max_iter");
     }
     if (ns == 1) {
       if ((r = mix_channel(h, st->mixh[0], mix_tot, st->rho_in, st->rho_out, st->rho_in)) != kOk) return r;
@@ -1436,6 +1437,38 @@ Status potentials_host(Handle& h, const double* rho, double* veff_g, double* ene
     energies[0] = e.e_hartree;
     energies[1] = e.e_xc;
     energies[2] = e.e_vxc;
+  }
+  return kOk;
+}
+
+Status scf_iter1_from_rho_g(Handle& h, const ScfParams& p, const double* rho_g_fft_in, ScfResult& res,
+                            double* evals_out, double* rho_out_host, double* rho_g_fft_out, double* rho_in_host) {
+  if (h.nspin != 1)
+    return fail(kInvalid, "transplanted iteration: nspin = 1 only (transplant.rs:128-133)");
+  if (!rho_g_fft_in) return fail(kInvalid, "transplanted iteration: rho_g_fft_in is NULL");
+  PW_CUDA_TRY(cudaSetDevice(h.device));
+  const long N = h.g.N;
+  const cudaStream_t s = h.stream;
+  // rho_in(r) = Re sum_G rho(G) e^{iG.r}: the unnormalised inverse transform
+  // (transplant.rs:140-148); the iteration re-derives rho(G) from it
+  std::vector<double2> grid(N);
+  PW_CUDA_TRY(cudaMemcpyAsync(h.tmp_grid, rho_g_fft_in, N * sizeof(double2), cudaMemcpyHostToDevice, s));
+  Status r = fft3d_full(h, h.tmp_grid, +1, s);
+  if (r != kOk) return r;
+  PW_CUDA_TRY(cudaMemcpyAsync(grid.data(), h.tmp_grid, N * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  PW_CUDA_TRY(cudaStreamSynchronize(s));
+  std::vector<double> rin(N);
+  for (long i = 0; i < N; ++i) rin[i] = grid[i].x;
+  if (rho_in_host) std::copy(rin.begin(), rin.end(), rho_in_host);
+  ScfParams q = p;
+  q.max_iter = 1;
+  q.single_step = 1;
+  if ((r = scf_run(h, q, rin.data(), res, evals_out, rho_out_host, nullptr)) != kOk) return r;
+  res.converged = 0;
+  if (rho_g_fft_out) {
+    if ((r = density_to_g(h, h.scf->rho_out)) != kOk) return r;
+    PW_CUDA_TRY(cudaMemcpyAsync(rho_g_fft_out, h.scf->cg, N * sizeof(double2), cudaMemcpyDeviceToHost, s));
+    PW_CUDA_TRY(cudaStreamSynchronize(s));
   }
   return kOk;
 }

@@ -32,6 +32,9 @@ struct ScfParams {
   double starting_magnetization = 0.0;
   int fixed_magnetization = 0;
   double tot_magnetization = 0.0;
+  // one iteration only, eigenpairs to diag_tol from a cold start, reported
+  // as a completed run (the transplanted iteration, transplant.rs:114-376)
+  int single_step = 0;
 };
 
 struct ScfResult {
@@ -50,6 +53,13 @@ struct ScfResult {
 // (may be null); rho_g_basis_out: n_pw complex (may be null).
 Status scf_run(Handle& h, const ScfParams& p, const double* rho_init, ScfResult& res, double* evals_out,
                double* rho_out, double* rho_g_basis_out);
+
+// One SCF iteration seeded from rho(G) on the full FFT grid (N complex,
+// rho(G) = (1/N) sum_r rho(r) e^{-iG.r}): run_scf_iter1_from_rho_g_fft,
+// scf/transplant.rs:114-376.  nspin = 1.  rho_in_host (N, the input density
+// re-materialised), rho_g_fft_out (N complex, the output density) may be null.
+Status scf_iter1_from_rho_g(Handle& h, const ScfParams& p, const double* rho_g_fft_in, ScfResult& res,
+                            double* evals_out, double* rho_out_host, double* rho_g_fft_out, double* rho_in_host);
 
 // Pieces exposed through the C-ABI for parity tests.
 Status eigensolve_k(Handle& h, int spin, int ik, int n_bands, double tol, int max_iter, const double* psi_in,

@@ -192,6 +192,8 @@ def load_library(path: str = LIB_PATH):
     lib.pwgpu_kernel_launches.restype = ct.c_int32
     lib.pwgpu_server_create.argtypes = [ct.POINTER(PwgpuServerOptions), ct.POINTER(vp)]
     lib.pwgpu_server_destroy.argtypes = [vp]
+    lib.pwgpu_scf_iter1_from_rho_g.argtypes = [vp, ct.POINTER(PwgpuScfParams), _f64p, ct.POINTER(PwgpuScfResult),
+                                               _f64p, _f64p, _f64p, _f64p]
     lib.pwgpu_server_submit.argtypes = [vp, ct.POINTER(PwgpuSystem), ct.POINTER(PwgpuScfParams), _f64p,
                                         ct.POINTER(ct.c_int64)]
     lib.pwgpu_server_poll.argtypes = [vp, ct.c_int64, ct.POINTER(PwgpuJobInfo)]
@@ -201,7 +203,7 @@ def load_library(path: str = LIB_PATH):
     lib.pwgpu_server_release.argtypes = [vp, ct.c_int64]
     lib.pwgpu_server_get_stats.argtypes = [vp, ct.POINTER(PwgpuServerStats)]
     for name in ("pwgpu_create", "pwgpu_destroy", "pwgpu_set_veff_g", "pwgpu_apply_h", "pwgpu_apply_h_device",
-                 "pwgpu_set_precision", "pwgpu_get_dims", "pwgpu_profile_apply_h", "pwgpu_scf_run",
+                 "pwgpu_set_precision", "pwgpu_get_dims", "pwgpu_profile_apply_h", "pwgpu_scf_run", "pwgpu_scf_iter1_from_rho_g",
                  "pwgpu_eigensolve", "pwgpu_density", "pwgpu_symmetrize", "pwgpu_potentials",
                  "pwgpu_small_geneig", "pwgpu_mix", "pwgpu_mix_reset", "pwgpu_get_projectors", "pwgpu_server_create", "pwgpu_server_destroy",
                  "pwgpu_server_submit", "pwgpu_server_poll", "pwgpu_server_wait", "pwgpu_server_wait_any",
@@ -389,6 +391,28 @@ class PwGpu:
         if rc != PWGPU_OK and (raise_on_unconverged or rc != -4):
             raise PwGpuError(rc, self.lib.pwgpu_last_error().decode(errors="replace"))
         return res.as_dict(), ev, rho, rg
+
+    def scf_iter1_from_rho_g(self, rho_g_fft: np.ndarray, n_bands: int, smearing: str = "fermi_dirac",
+                             sigma: float = 0.01, diag_tol: float = 1e-10, diag_max_iter: int = 60,
+                             diag_extra_bands: int = -1, precision: int = PRECISION_FP64):
+        """One SCF iteration seeded from rho(G) on the full FFT grid (run_scf_iter1_from_rho_g_fft,
+        scf/transplant.rs:114-376); returns (result dict, eigenvalues [n_k, n_bands], rho_r_out [N],
+        rho_g_fft_out [N] complex, rho_r_in [N])."""
+        p = scf_params(n_bands, 1, 0.0, 0.0, 0.3, 1, False, 0.0, smearing, sigma, diag_tol, diag_max_iter,
+                       diag_extra_bands, precision, 1e-6, False)
+        rg = np.ascontiguousarray(rho_g_fft, dtype=np.complex128).ravel()
+        n = self.sys.n_grid
+        if rg.size != n:
+            raise ValueError(f"rho_g_fft has {rg.size} entries; the FFT grid has {n}")
+        res = PwgpuScfResult()
+        ev = np.zeros((len(self.sys.kpoints), n_bands))
+        rho = np.zeros(n)
+        rg_out = np.zeros(n, dtype=np.complex128)
+        rho_in = np.zeros(n)
+        _check(self.lib, self.lib.pwgpu_scf_iter1_from_rho_g(
+            self.h, ct.byref(p), rg.view(np.float64).ctypes.data_as(_f64p), ct.byref(res), _f64(ev), _f64(rho),
+            rg_out.view(np.float64).ctypes.data_as(_f64p), _f64(rho_in)))
+        return res.as_dict(), ev, rho, rg_out, rho_in
 
     def mix(self, rho_in: np.ndarray, rho_out: np.ndarray, beta: float, ndim: int, kerker: bool = False,
             q_tf: float = 0.0, channel: int = 0, mixer: str = "anderson", period: int = 3) -> np.ndarray:

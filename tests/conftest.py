@@ -12,6 +12,14 @@ for p in (PKG, ROOT):
     if p not in sys.path:
         sys.path.insert(0, p)
 
+# The oracle's dense eigensolves use BLAS threads; more threads than free
+# cores (other jobs on the host) makes spinning BLAS workers crawl.
+try:
+    from threadpoolctl import threadpool_limits
+    threadpool_limits(limits=max(1, min(4, os.cpu_count() or 1)), user_api="blas")
+except ImportError:
+    pass
+
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 UPF_DIR = os.path.join(GOLDEN, "upf")
 

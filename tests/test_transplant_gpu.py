@@ -1,0 +1,85 @@
+"""One SCF iteration seeded from a full-grid rho(G)
+(pwgpu_scf_iter1_from_rho_g; run_scf_iter1_from_rho_g_fft,
+scf/transplant.rs:114-376) on the GPU against the oracle's restatement,
+complex bands over k-points and Gamma-real bands, and the restart of a
+converged run from its density checkpoint.
+
+Both sides diagonalise from a cold start (dense on the oracle side, LOBPCG
+to a 1e-10 eV residual on the device), so the results agree to the
+eigen-residual: energies and components 1e-7 eV, eigenvalues 1e-8 eV,
+densities 1e-8 of their maximum.  Fermi-Dirac smearing keeps the Fermi
+level of these gapped cells determined (a Gaussian tail is flat to 1e-12
+inside the gap, where bisection stops wherever rounding sends it)."""
+
+import numpy as np
+import pytest
+
+from oracle import pwdft_oracle as O
+from pwgpu.context import build_system
+from pwgpu.crystal import KPoint, diamond_primitive, diamond_supercell, gamma_only
+from pwgpu.lib import PwGpu, PwGpuError
+from pwgpu.output import read_density, restart_rho_g, write_density
+from pwgpu.symmetry import SymmetryInfo
+
+pytestmark = pytest.mark.gpu
+
+KW = dict(smearing="fermi_dirac", sigma=0.1)
+
+
+def cases(pp):
+    return {
+        "si2_k": (build_system(diamond_primitive("Si", 5.431), {"Si": pp}, 120.0,
+                               [KPoint(np.array([0.11, -0.23, 0.31]), 0.5), KPoint(np.array([0.0, 0.2, 0.1]), 0.5)],
+                               SymmetryInfo.identity_only()), 6),
+        "si8_gamma": (build_system(diamond_supercell("Si", 5.431, displacement_ang=0.02,
+                                                     rng=np.random.default_rng(5)), {"Si": pp}, 120.0, gamma_only(),
+                                   SymmetryInfo.identity_only()), 20),
+    }
+
+
+@pytest.mark.parametrize("name", ["si2_k", "si8_gamma"])
+def test_transplanted_iteration_matches_oracle(si_pp, name):
+    s, nb = cases(si_pp)[name]
+    rho_g = O.density_r_to_g(s.rho_init_r, s.dims)
+    ref = O.run_scf_iter1_from_rho_g(s, nb, rho_g, **KW)
+    with PwGpu(s) as dev:
+        res, ev, rho, rg_out, rho_in = dev.scf_iter1_from_rho_g(rho_g, nb, diag_tol=1e-10, **KW)
+    scale = np.max(ref.rho_r_out)
+    assert np.max(np.abs(rho_in - ref.rho_r_in)) < 1e-12 * scale
+    assert abs(res["total_energy"] - ref.total_energy) < 1e-7
+    assert abs(res["harris_foulkes_energy"] - ref.harris_foulkes_energy) < 1e-7
+    assert abs(res["fermi_energy"] - ref.fermi_energy) < 1e-7
+    assert abs(res["final_delta"] - ref.delta_rho) < 1e-9
+    assert res["n_iterations"] == 1 and res["converged"] == 0
+    assert np.max(np.abs(ev - np.array(ref.eigenvalues))) < 1e-8
+    assert np.max(np.abs(rho - ref.rho_r_out)) < 1e-8 * scale
+    assert np.max(np.abs(rg_out - ref.rho_g_out)) < 1e-8 * scale
+    for k in ("e_kinetic", "e_local", "e_nonlocal", "e_hartree", "e_xc", "e_vxc"):
+        assert abs(res[k] - ref.components[k]) < 1e-7, k
+
+
+def test_restart_from_density_checkpoint(tmp_path, si_pp):
+    s, nb = cases(si_pp)["si2_k"]
+    with PwGpu(s) as dev:
+        res, ev, rho, rg = dev.scf_run(s.rho_init_r, nb, max_iter=80, conv_threshold=1e-9, energy_threshold=1e-8,
+                                       mixing_beta=0.3, diag_tol=1e-10, **KW)
+        assert res["converged"] == 1
+        path = str(tmp_path / "rho.npz")
+        write_density(path, s, rho, rg)
+        ck = read_density(path)
+        r1, ev1, rho1, _, _ = dev.scf_iter1_from_rho_g(restart_rho_g(s, ck), nb, diag_tol=1e-10, **KW)
+    # the restarted iteration stays at the fixed point
+    assert r1["final_delta"] < 1e-8
+    assert abs(r1["total_energy"] - res["total_energy"]) < 1e-6
+    assert np.max(np.abs(ev1 - ev)) < 1e-6
+
+
+def test_transplant_rejects_spin_and_bad_sizes(si_pp):
+    s = build_system(diamond_primitive("Si", 5.431), {"Si": si_pp}, 100.0, gamma_only(), fft_grid=(16, 16, 16),
+                     nspin=2)
+    with PwGpu(s) as dev:
+        with pytest.raises(PwGpuError) as e:
+            dev.scf_iter1_from_rho_g(O.density_r_to_g(s.rho_init_r, s.dims), 4)
+        assert e.value.code == -1
+        with pytest.raises(ValueError):
+            dev.scf_iter1_from_rho_g(np.zeros(10, dtype=complex), 4)
