@@ -80,14 +80,13 @@ __global__ void k_band_pq_real(const double* __restrict__ P, const double* __res
 
 }  // namespace
 
-Status band_energy_terms(Handle& h, int ik, const double2* V, long ldv, int nb, double* t_kin, double* t_nl,
-                         cudaStream_t s) {
+Status band_energy_terms(Handle& h, int ik, const double2* V, long ldv, int nb, double* d_out, double* t_kin,
+                         double* t_nl, cudaStream_t s) {
   if (ik < 0 || ik >= h.n_k) return fail(kInvalid, "band_energy_terms: k-point index out of range");
   if (nb <= 0) return kOk;
   if (ldv < h.n_pw) return fail(kInvalid, "band_energy_terms: leading dimension smaller than n_pw");
+  if (!d_out) return fail(kInvalid, "band_energy_terms: no scratch");
   const int n = h.n_pw;
-  double* d_out = nullptr;
-  PW_CUDA_TRY(cudaMalloc((void**)&d_out, 2 * (size_t)nb * sizeof(double)));
   Status r = kOk;
   if (h.gam.on) {
     const double* u = reinterpret_cast<const double*>(V);
@@ -116,8 +115,6 @@ Status band_energy_terms(Handle& h, int ik, const double2* V, long ldv, int nb, 
       std::copy(host.begin() + nb, host.end(), t_nl);
     }
   }
-  cudaStreamSynchronize(s);
-  cudaFree(d_out);
   return r;
 }
 

@@ -131,8 +131,9 @@ void release_nl_mixed(Handle& h);
 
 // Per-band kinetic and nonlocal expectations of nb columns of V at k-point ik
 // (packed real on Gamma handles), into host t_kin and t_nl (components.cu).
-Status band_energy_terms(Handle& h, int ik, const double2* V, long ldv, int nb, double* t_kin, double* t_nl,
-                         cudaStream_t s);
+// d_out: device scratch of 2 nb doubles.
+Status band_energy_terms(Handle& h, int ik, const double2* V, long ldv, int nb, double* d_out, double* t_kin,
+                         double* t_nl, cudaStream_t s);
 
 // Grid-map construction and the H|psi> launcher (hpsi.cu).
 Status build_grid_maps(Handle& h, const int* miller_host);

@@ -159,6 +159,15 @@ __global__ void k_gather_cols(const S* __restrict__ src, long lds, const int* __
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) d[i] = s[i];
 }
 
+template <typename S>
+__global__ void k_scatter_cols(const S* __restrict__ src, long lds, const int* __restrict__ idx, S* __restrict__ dst,
+                               long ldd, int rows) {
+  const int c = blockIdx.y;
+  const S* s = src + (long)c * lds;
+  S* d = dst + (long)idx[c] * ldd;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) d[i] = s[i];
+}
+
 // Subspace matrix Hs (m x m, ld m) over the basis [X | B], X holding nd Ritz
 // vectors with values lam:  [[diag(lam), Z^H], [Z, (G + G^H)/2]],
 // Z = B^H HX (q x nd, ld q), G = B^H HB (q x q, ld q), q = m - nd.
@@ -458,10 +467,10 @@ template <typename T> Status orthonormalize(Ctx& c, T* Y, int q) {
 
 // Lowest nev eigenpairs of the Hermitian subspace matrix Hs (m x m): values
 // into w.lam, vectors into *C (ld m).
-template <typename T> Status subspace_eig(Ctx& c, int m, int nev, T** C) {
+template <typename T> Status subspace_eig(Ctx& c, int m, int nev, T** C, bool allow_small = true) {
   Status r;
   T* Hs = as<T>(c.w.Hs);
-  if (m <= kSmallSolveMax) {
+  if (allow_small && m <= kSmallSolveMax) {
     // one-CTA Cholesky + Jacobi solver (complex; a real symmetric input stays real)
     const double2* Hz = c.w.Hs;
     if (std::is_same<T, double>::value) {
@@ -677,9 +686,90 @@ Status lobpcg_t(Handle& h, EigWork& w, EigVecs& k, int spin, int ik, double v0, 
         }
       }
     }
+    const int q = na + npc;
+    if (4 * na <= nd) {
+      // few active bands: hard locking.  W and P are orthogonal to every
+      // column of X, so [X_a | W | P] (X_a the active Ritz vectors) is an
+      // orthonormal basis orthogonal to the converged ones; Rayleigh-Ritz in
+      // it alone leaves the converged pairs as they are (their coupling to W
+      // and P is their residual, below tol) at a third of the subspace size
+      pt.mark(4, s);
+      const int ms = na + q;
+      T* Bx = Tb;                      // [X_a | W | P], n x ms
+      T* Bh = as<T>(w.HXn);            // [HX_a | HW | HP]
+      PW_CUDA_TRY(cudaMemcpyAsync(w.idx, act.data(), na * sizeof(int), cudaMemcpyHostToDevice, s));
+      k_gather_cols<T><<<dim3(c.gx, na), 256, 0, s>>>(X, n, w.idx, Bx, n, (int)n); count_launch();
+      k_gather_cols<T><<<dim3(c.gx, na), 256, 0, s>>>(HX, n, w.idx, Bh, n, (int)n); count_launch();
+      PW_CUDA_TRY(cudaMemcpyAsync(Bx + n * na, W, n * q * sizeof(T), cudaMemcpyDeviceToDevice, s));
+      PW_CUDA_TRY(cudaMemcpyAsync(Bh + n * na, HW, n * q * sizeof(T), cudaMemcpyDeviceToDevice, s));
+      std::vector<double> lam_a(na);
+      for (int j = 0; j < na; ++j) lam_a[j] = k.evals[act[j]];
+      PW_CUDA_TRY(cudaMemcpyAsync(w.lam0, lam_a.data(), na * sizeof(double), cudaMemcpyHostToDevice, s));
+      if ((r = gemm(c, CUBLAS_OP_C, CUBLAS_OP_N, q, na, (int)n, W, n, Bh, n, as<T>(w.Z), q)) != kOk) return r;
+      if ((r = gemm(c, CUBLAS_OP_C, CUBLAS_OP_N, q, q, (int)n, W, n, HW, n, as<T>(w.G), q)) != kOk) return r;
+      k_assemble_rr<T><<<blocks_for((long)ms * ms), 256, 0, s>>>(as<T>(w.Hs), ms, na, w.lam0, as<T>(w.Z),
+                                                                  as<T>(w.G));
+      count_launch();
+      T* C = nullptr;
+      pt.mark(5, s);
+      if ((r = subspace_eig<T>(c, ms, na, &C, false)) != kOk) return r;
+      pt.mark(6, s);
+      // new active X, HX into the W, HW columns; new P, HP from the (W, P) rows
+      if ((r = gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, na, ms, Bx, n, C, ms, W, n)) != kOk) return r;
+      if ((r = gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, na, ms, Bh, n, C, ms, HW, n)) != kOk) return r;
+      if ((r = gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, na, q, Bx + n * na, n, C + na, ms, Pn, n)) != kOk) return r;
+      if ((r = gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, na, q, Bh + n * na, n, C + na, ms, HPn, n)) != kOk)
+        return r;
+      k_scatter_cols<T><<<dim3(c.gx, na), 256, 0, s>>>(W, n, w.idx, X, n, (int)n); count_launch();
+      k_scatter_cols<T><<<dim3(c.gx, na), 256, 0, s>>>(HW, n, w.idx, HX, n, (int)n); count_launch();
+      PW_CUDA_TRY(cudaMemcpyAsync(lam_a.data(), w.lam, na * sizeof(double), cudaMemcpyDeviceToHost, s));
+      PW_CUDA_TRY(cudaStreamSynchronize(s));
+      for (int j = 0; j < na; ++j) k.evals[act[j]] = lam_a[j];
+      // keep the bands in ascending order (a new active value may pass a converged one)
+      std::vector<int> order(nd);
+      for (int b = 0; b < nd; ++b) order[b] = b;
+      std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return k.evals[a] < k.evals[b]; });
+      bool sorted = true;
+      for (int b = 0; b < nd; ++b) sorted = sorted && order[b] == b;
+      pband = act;
+      if (!sorted) {
+        std::vector<int> inv(nd);
+        for (int b = 0; b < nd; ++b) inv[order[b]] = b;
+        PW_CUDA_TRY(cudaMemcpyAsync(w.idx, order.data(), nd * sizeof(int), cudaMemcpyHostToDevice, s));
+        k_gather_cols<T><<<dim3(c.gx, nd), 256, 0, s>>>(X, n, w.idx, Tb, n, (int)n); count_launch();
+        k_gather_cols<T><<<dim3(c.gx, nd), 256, 0, s>>>(HX, n, w.idx, as<T>(w.HXn), n, (int)n); count_launch();
+        PW_CUDA_TRY(cudaMemcpyAsync(X, Tb, n * nd * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        PW_CUDA_TRY(cudaMemcpyAsync(HX, w.HXn, n * nd * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        std::vector<double> ev(nd);
+        for (int b = 0; b < nd; ++b) ev[b] = k.evals[order[b]];
+        std::copy(ev.begin(), ev.end(), k.evals.begin());
+        // P columns follow their bands: new band numbers, in ascending order
+        std::vector<int> pj(na);
+        for (int j = 0; j < na; ++j) pj[j] = j;
+        std::sort(pj.begin(), pj.end(), [&](int a, int b) { return inv[act[a]] < inv[act[b]]; });
+        for (int j = 0; j < na; ++j) pband[j] = inv[act[pj[j]]];
+        PW_CUDA_TRY(cudaMemcpyAsync(w.idx, pj.data(), na * sizeof(int), cudaMemcpyHostToDevice, s));
+        k_gather_cols<T><<<dim3(c.gx, na), 256, 0, s>>>(Pn, n, w.idx, Tb, n, (int)n); count_launch();
+        k_gather_cols<T><<<dim3(c.gx, na), 256, 0, s>>>(HPn, n, w.idx, as<T>(w.HXn), n, (int)n); count_launch();
+        PW_CUDA_TRY(cudaMemcpyAsync(Pn, Tb, n * na * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        PW_CUDA_TRY(cudaMemcpyAsync(HPn, w.HXn, n * na * sizeof(T), cudaMemcpyDeviceToDevice, s));
+      }
+      pt.mark(7, s);
+      PW_CUDA_TRY(cudaStreamSynchronize(s));
+      pt.accumulate();
+      np = na;
+      ++out.iters;
+      if (h.trace) {
+        const double ms_it =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        std::fprintf(stderr, "pwgpu lobpcg k=%d it=%d res=%.3e na=%d np=%d hard e0=%.8f e_last=%.8f %.2f ms\n", ik,
+                     out.iters, out.max_res, na, npc, k.evals[0], k.evals[nconv - 1], ms_it);
+      }
+      continue;
+    }
     // Rayleigh-Ritz over [X | W | P]
     pt.mark(4, s);
-    const int q = na + npc, m = nd + q;
+    const int m = nd + q;
     if ((r = gemm(c, CUBLAS_OP_C, CUBLAS_OP_N, q, nd, (int)n, W, n, HX, n, as<T>(w.Z), q)) != kOk) return r;
     if ((r = gemm(c, CUBLAS_OP_C, CUBLAS_OP_N, q, q, (int)n, W, n, HW, n, as<T>(w.G), q)) != kOk) return r;
     k_assemble_rr<T><<<blocks_for((long)m * m), 256, 0, s>>>(as<T>(w.Hs), m, nd, w.lam0, as<T>(w.Z), as<T>(w.G));

@@ -183,6 +183,13 @@ __global__ void k_veff_g(const double2* __restrict__ vloc, const double2* __rest
   }
 }
 
+// Kerker weights P(G) = G^2 / (G^2 + q^2), P = 0 at G^2 < g2_zero (kerker.rs:18-35)
+__global__ void k_kerker_weights(const double* __restrict__ g2, long n, double q2, double g2_zero,
+                                 double* __restrict__ w) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) w[i] = g2[i] < g2_zero ? 0.0 : g2[i] / (g2[i] + q2);
+}
+
 __global__ void k_real_part(const double2* __restrict__ c, double* __restrict__ r, long n) {
   const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) r[i] = c[i].x;
@@ -456,6 +463,7 @@ struct ScfState {
   std::vector<EigVecs> ks;  // per (spin, k)
   EigWork ew;
   double *partials = nullptr, *scal = nullptr, *fw = nullptr, *mix_partials = nullptr, *mix_sums = nullptr;
+  double* band_terms = nullptr;  // 2 nd: per-band kinetic and nonlocal expectations
   double *rho_in = nullptr, *rho_out = nullptr, *exc = nullptr, *vxc = nullptr, *rtmp = nullptr;
   double2 *cg = nullptr, *cg2 = nullptr, *vh = nullptr;
   double* kerker_w = nullptr;
@@ -481,7 +489,7 @@ void release_scf(Handle& h) {
   auto f = [](void* p) { if (p) cudaFree(p); };
   for (auto& k : st->ks) eig_vecs_release(k);
   eig_work_release(st->ew);
-  f(st->partials); f(st->scal); f(st->fw);
+  f(st->partials); f(st->scal); f(st->fw); f(st->band_terms);
   f(st->rho_in); f(st->rho_out); f(st->exc); f(st->vxc); f(st->rtmp);
   f(st->cg); f(st->cg2); f(st->vh); f(st->kerker_w); f(st->mix_partials); f(st->mix_sums);
   f(st->rho_in_dn); f(st->rho_out_dn); f(st->vxc_dn); f(st->t_in); f(st->t_out); f(st->m_in); f(st->m_out);
@@ -539,6 +547,7 @@ static Status ensure_state(Handle& h, int nb, int nd, int ndim) {
   if ((s = salloc(&st->partials, (size_t)kRedBlocks * 4)) != kOk) return s;
   if ((s = salloc(&st->scal, 16)) != kOk) return s;
   if ((s = salloc(&st->fw, (size_t)nd)) != kOk) return s;
+  if ((s = salloc(&st->band_terms, 2 * (size_t)nd)) != kOk) return s;
   if ((s = salloc(&st->rho_in, (size_t)N)) != kOk) return s;
   if ((s = salloc(&st->rho_out, (size_t)N)) != kOk) return s;
   if ((s = salloc(&st->exc, (size_t)N)) != kOk) return s;
@@ -1050,12 +1059,10 @@ static Status set_kerker(Handle& h, bool on, double q_tf) {
     const double rb = h.n_electrons / h.omega * kBohr3ToAng3;
     q2 = 4.0 * std::cbrt(3.0 * kPi * kPi * rb) / kPi / (kBohrToAng * kBohrToAng);
   }
-  std::vector<double> g2(N), wg(N);
-  PW_CUDA_TRY(cudaMemcpy(g2.data(), h.g_squared, N * sizeof(double), cudaMemcpyDeviceToHost));
-  for (long i = 0; i < N; ++i) wg[i] = g2[i] < kG2Zero ? 0.0 : g2[i] / (g2[i] + q2);
   Status r;
   if (!st->kerker_w && (r = salloc(&st->kerker_w, (size_t)N)) != kOk) return r;
-  PW_CUDA_TRY(cudaMemcpy(st->kerker_w, wg.data(), N * sizeof(double), cudaMemcpyHostToDevice));
+  k_kerker_weights<<<blocks_for(N), 256, 0, h.stream>>>(h.g_squared, N, q2, kG2Zero, st->kerker_w); count_launch();
+  PW_CUDA_TRY(cudaGetLastError());
   return kOk;
 }
 
@@ -1276,7 +1283,9 @@ Status scf_run(Handle& h, const ScfParams& p, const double* rho_init, ScfResult&
         std::vector<double> tk(nb), tn(nb);
         double ekin = 0.0, enl = 0.0;
         for (int c = 0; c < ns * nk; ++c) {
-          if ((r = band_energy_terms(h, c % nk, st->ks[c].V, h.n_pw, nb, tk.data(), tn.data(), s)) != kOk) return r;
+          if ((r = band_energy_terms(h, c % nk, st->ks[c].V, h.n_pw, nb, st->band_terms, tk.data(), tn.data(), s)) !=
+              kOk)
+            return r;
           for (int b = 0; b < nb; ++b) {
             if (occ[c][b] == 0.0) continue;
             ekin += occ[c][b] * wk_all[c] * tk[b];
