@@ -98,6 +98,18 @@ typedef struct pwgpu_system {
   const int32_t* species_nbeta; /* n_species projector counts */
   const int32_t* beta_l;        /* l of each projector, species by species */
   const double* beta_r;         /* beta_i(r) of each projector on its species' mesh, concatenated */
+  /* Local pseudopotential, NLCC core density and start density built on the device
+   * (ScfContext::new, scf/context.rs:102-231, with potentials.rs:18-115 and
+   * generate_initial_density, scf/initial_density.rs:64-166), used when v_local_g is NULL
+   * (rho_core_r must then be NULL too): atom_tau, atom_species, n_species, species_mesh,
+   * radial_r and radial_rab as above, for all n_atoms atoms, plus: */
+  const double* recip;          /* 3 x 3 reciprocal vectors b1, b2, b3 as rows (Å^-1, 2 pi included) */
+  const double* species_zval;   /* n_species valence charges */
+  const double* vloc_r;         /* V_loc(r) of each species on its mesh (eV), concatenated */
+  const double* core_r;         /* NLCC core charge on the meshes (e/Å^3), concatenated, or NULL */
+  const double* rho_atom_r;     /* PP_RHOATOM on the meshes (e/Å), concatenated, or NULL */
+  const int32_t* species_flags; /* n_species: bit 0 core charge given, bit 1 rho_atom given */
+  double gaussian_sigma;        /* Å: start-density width of species without rho_atom */
 } pwgpu_system;
 
 typedef struct pwgpu_options {
@@ -208,6 +220,16 @@ typedef struct pwgpu_scf_result {
    * with e_hartree, e_xc, e_ewald and -entropy_ts they sum to total_energy at self-consistency */
   double e_kinetic, e_local, e_nonlocal;
 } pwgpu_scf_result;
+
+/* The start density of a handle created with v_local_g NULL (N doubles, e/Å^3):
+ * the superposition of atomic densities of generate_initial_density
+ * (scf/initial_density.rs:64-166), built on the device at pwgpu_create.
+ * PWGPU_E_STATE for a handle whose local potential came from the caller. */
+pwgpu_status pwgpu_initial_density(const pwgpu_handle* h, double* rho_r);
+
+/* Read-back of the device V_loc(G) (N complex) and NLCC core density (N; zeros
+ * without one); either pointer may be NULL.  For checking a device build. */
+pwgpu_status pwgpu_get_local_potential(const pwgpu_handle* h, double* v_local_g, double* rho_core_r);
 
 /* Run the SCF loop from rho_init_r (N doubles, e/Å^3, the total start
  * density).  Replaces run_scf_unpolarized (scf/driver.rs:266-742) for

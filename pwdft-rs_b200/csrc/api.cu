@@ -48,7 +48,7 @@ static void release(Handle& h) {
   for (auto& k : h.kp) { f(k.kinetic); f(k.b); f(k.b32); }
   h.kp.clear();
   f(h.ch_atom); f(h.atom_ch_start); f(h.d_off); f(h.d_vals);
-  f(h.v_local_g); f(h.g_squared); f(h.rho_core_r); f(h.sym_src); f(h.sym_arg);
+  f(h.v_local_g); f(h.g_squared); f(h.rho_core_r); f(h.rho_sad); f(h.sym_src); f(h.sym_arg);
   for (int s = 0; s < 2; ++s) { f(h.veff_r[s]); f(h.veff_r32[s]); }
   f(h.work_a); f(h.work_b); f(h.nl_p); f(h.nl_q); f(h.tmp_grid);
   release_scf(h);
@@ -62,7 +62,7 @@ static void release(Handle& h) {
 
 static Status create(const pwgpu_system* s, const pwgpu_options* o, pwgpu_handle* ph) {
   Handle& h = ph->h;
-  if (!s || !s->miller || !s->kinetic || !s->k_weights || !s->v_local_g || !s->g_squared)
+  if (!s || !s->miller || !s->kinetic || !s->k_weights || !s->g_squared)
     return fail(kInvalid, "pwgpu_create: required system array is NULL");
   if (s->n_pw <= 0 || s->n_k <= 0 || s->dims[0] <= 0 || s->dims[1] <= 0 || s->dims[2] <= 0)
     return fail(kInvalid, "pwgpu_create: n_pw, n_k and dims must be positive");
@@ -139,9 +139,31 @@ static Status create(const pwgpu_system* s, const pwgpu_options* o, pwgpu_handle
       if ((st = build_projectors_device(h, src)) != kOk) return st;
     }
   }
-  if ((st = upload(&h.v_local_g, reinterpret_cast<const double2*>(s->v_local_g), (size_t)N)) != kOk) return st;
   if ((st = upload(&h.g_squared, s->g_squared, (size_t)N)) != kOk) return st;
-  if (s->rho_core_r && (st = upload(&h.rho_core_r, s->rho_core_r, (size_t)N)) != kOk) return st;
+  if (s->v_local_g) {
+    if ((st = upload(&h.v_local_g, reinterpret_cast<const double2*>(s->v_local_g), (size_t)N)) != kOk) return st;
+    if (s->rho_core_r && (st = upload(&h.rho_core_r, s->rho_core_r, (size_t)N)) != kOk) return st;
+  } else {
+    // V_loc(G), the core density and the start density from the radial data
+    if (s->rho_core_r) return fail(kInvalid, "pwgpu_create: rho_core_r must be NULL when v_local_g is");
+    if ((st = upload<double2>(&h.v_local_g, nullptr, (size_t)N)) != kOk) return st;
+    LocalSource ls;
+    ls.recip = s->recip;
+    ls.atom_tau = s->atom_tau;
+    ls.atom_species = s->atom_species;
+    ls.n_atoms = s->n_atoms;
+    ls.n_species = s->n_species;
+    ls.species_mesh = s->species_mesh;
+    ls.radial_r = s->radial_r;
+    ls.radial_rab = s->radial_rab;
+    ls.species_zval = s->species_zval;
+    ls.vloc_r = s->vloc_r;
+    ls.species_flags = s->species_flags;
+    ls.core_r = s->core_r;
+    ls.rho_atom_r = s->rho_atom_r;
+    ls.gaussian_sigma = s->gaussian_sigma;
+    if ((st = build_local_device(h, ls, h.v_local_g, &h.rho_core_r, &h.rho_sad)) != kOk) return st;
+  }
   if (h.n_sym > 1) {
     if ((st = upload(&h.sym_src, s->sym_src, (size_t)h.n_sym * N)) != kOk) return st;
     if ((st = upload(&h.sym_arg, s->sym_arg, (size_t)h.n_sym * N)) != kOk) return st;
@@ -383,6 +405,30 @@ pwgpu_status pwgpu_get_projectors(const pwgpu_handle* ph, int32_t ik, double* b)
   if (h.n_ch == 0) return kOk;
   PW_CUDA_TRY(cudaSetDevice(h.device));
   PW_CUDA_TRY(cudaMemcpy(b, h.kp[ik].b, (size_t)h.n_pw * h.n_ch * sizeof(double2), cudaMemcpyDeviceToHost));
+  return kOk;
+}
+
+pwgpu_status pwgpu_initial_density(const pwgpu_handle* ph, double* rho_r) {
+  if (!ph || !rho_r) return fail(kInvalid, "pwgpu_initial_density: NULL argument");
+  const Handle& h = ph->h;
+  if (!h.rho_sad) return fail(kState, "pwgpu_initial_density: the system was created with v_local_g given");
+  PW_CUDA_TRY(cudaSetDevice(h.device));
+  PW_CUDA_TRY(cudaMemcpy(rho_r, h.rho_sad, (size_t)h.g.N * sizeof(double), cudaMemcpyDeviceToHost));
+  return kOk;
+}
+
+pwgpu_status pwgpu_get_local_potential(const pwgpu_handle* ph, double* v_local_g, double* rho_core_r) {
+  if (!ph) return fail(kInvalid, "pwgpu_get_local_potential: NULL handle");
+  const Handle& h = ph->h;
+  PW_CUDA_TRY(cudaSetDevice(h.device));
+  if (v_local_g)
+    PW_CUDA_TRY(cudaMemcpy(v_local_g, h.v_local_g, (size_t)h.g.N * sizeof(double2), cudaMemcpyDeviceToHost));
+  if (rho_core_r) {
+    if (h.rho_core_r)
+      PW_CUDA_TRY(cudaMemcpy(rho_core_r, h.rho_core_r, (size_t)h.g.N * sizeof(double), cudaMemcpyDeviceToHost));
+    else
+      std::fill(rho_core_r, rho_core_r + h.g.N, 0.0);
+  }
   return kOk;
 }
 

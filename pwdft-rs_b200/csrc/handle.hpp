@@ -73,6 +73,7 @@ struct Handle {
   double2* v_local_g = nullptr;    // N
   double* g_squared = nullptr;     // N
   double* rho_core_r = nullptr;    // N or null
+  double* rho_sad = nullptr;       // N: start density built on the device, or null
   int* sym_src = nullptr;          // n_sym x N
   double* sym_arg = nullptr;       // n_sym x N
   // effective potential per spin in real space
@@ -166,6 +167,30 @@ struct ProjectorSource {
 };
 // B of every k into h.kp[k].b (allocated by the caller); needs h.atom_ch_start.
 Status build_projectors_device(Handle& h, const ProjectorSource& src);
+
+// Radial data for the local pseudopotential, the NLCC core density and the
+// start density on the full grid (setup.cu); meshes as in ProjectorSource.
+struct LocalSource {
+  const double* recip = nullptr;        // 3 x 3: rows b1, b2, b3 (Å^-1)
+  const double* atom_tau = nullptr;     // n_atoms x 3, Å
+  const int* atom_species = nullptr;    // n_atoms
+  int n_atoms = 0;
+  int n_species = 0;
+  const int* species_mesh = nullptr;
+  const double* radial_r = nullptr;
+  const double* radial_rab = nullptr;
+  const double* species_zval = nullptr;  // n_species
+  const double* vloc_r = nullptr;        // concatenated V_loc(r), eV
+  const int* species_flags = nullptr;    // bit 0: core charge, bit 1: rho_atom
+  const double* core_r = nullptr;        // concatenated, or null
+  const double* rho_atom_r = nullptr;    // concatenated, or null
+  double gaussian_sigma = 1.0;           // Å
+};
+// V_loc(G) into v_local_g (N complex, allocated), rho_core(r) into *rho_core_r
+// (allocated here when null and a species has a core charge), the start
+// density into *rho_start when rho_start is given.  Needs the grid maps.
+Status build_local_device(Handle& h, const LocalSource& src, double2* v_local_g, double** rho_core_r,
+                          double** rho_start);
 
 // Gamma path (gamma.cu).  build_gamma decides eligibility (one k-point with
 // a kinetic term and projectors symmetric under G -> -G) from host data.

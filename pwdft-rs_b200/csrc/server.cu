@@ -37,15 +37,19 @@ double seconds_between(Clock::time_point a, Clock::time_point b) {
 // the submit call only).
 struct SystemCopy {
   pwgpu_system sys{};
-  std::vector<int32_t> miller, atom_ch_start, sym_src, atom_species, species_mesh, species_nbeta, beta_l;
+  std::vector<int32_t> miller, atom_ch_start, sym_src, atom_species, species_mesh, species_nbeta, beta_l, species_flags;
   std::vector<double> k_weights, kinetic, proj_b, d_blocks, v_local_g, g_squared, rho_core, sym_arg, g_cart, k_cart,
-      atom_tau, radial_r, radial_rab, beta_r;
+      atom_tau, radial_r, radial_rab, beta_r, recip, species_zval, vloc_r, core_r, rho_atom_r;
 
   Status copy_from(const pwgpu_system& s) {
     if (s.n_pw <= 0 || s.n_k <= 0 || s.dims[0] <= 0 || s.dims[1] <= 0 || s.dims[2] <= 0)
       return fail(kInvalid, "pwgpu_server_submit: n_pw, n_k and dims must be positive");
-    if (!s.miller || !s.k_weights || !s.kinetic || !s.v_local_g || !s.g_squared)
+    if (!s.miller || !s.k_weights || !s.kinetic || !s.g_squared)
       return fail(kInvalid, "pwgpu_server_submit: required system array is NULL");
+    if (!s.v_local_g && (!s.recip || !s.species_zval || !s.vloc_r || !s.species_flags || !s.atom_tau ||
+                         !s.atom_species || s.n_species <= 0 || !s.species_mesh || !s.radial_r || !s.radial_rab ||
+                         s.n_atoms <= 0))
+      return fail(kInvalid, "pwgpu_server_submit: local radial data missing");
     if (s.n_ch > 0 && (!s.atom_ch_start || !s.d_blocks || s.n_atoms <= 0))
       return fail(kInvalid, "pwgpu_server_submit: projector arrays missing");
     if (s.n_ch > 0 && !s.proj_b &&
@@ -60,43 +64,73 @@ struct SystemCopy {
     miller.assign(s.miller, s.miller + 3 * n);
     k_weights.assign(s.k_weights, s.k_weights + nk);
     kinetic.assign(s.kinetic, s.kinetic + nk * n);
-    v_local_g.assign(s.v_local_g, s.v_local_g + 2 * N);
     g_squared.assign(s.g_squared, s.g_squared + N);
     sys.miller = miller.data();
     sys.k_weights = k_weights.data();
     sys.kinetic = kinetic.data();
-    sys.v_local_g = v_local_g.data();
     sys.g_squared = g_squared.data();
+    // atoms and species meshes: shared by the projector and local radial forms
+    const bool radial = (s.n_ch > 0 && !s.proj_b) || !s.v_local_g;
+    size_t mesh_tot = 0;
+    if (radial) {
+      const int ns = s.n_species;
+      atom_tau.assign(s.atom_tau, s.atom_tau + 3L * s.n_atoms);
+      atom_species.assign(s.atom_species, s.atom_species + s.n_atoms);
+      species_mesh.assign(s.species_mesh, s.species_mesh + ns);
+      for (int q = 0; q < ns; ++q) mesh_tot += (size_t)species_mesh[q];
+      radial_r.assign(s.radial_r, s.radial_r + mesh_tot);
+      radial_rab.assign(s.radial_rab, s.radial_rab + mesh_tot);
+      sys.atom_tau = atom_tau.data();
+      sys.atom_species = atom_species.data();
+      sys.species_mesh = species_mesh.data();
+      sys.radial_r = radial_r.data();
+      sys.radial_rab = radial_rab.data();
+    }
+    if (s.v_local_g) {
+      v_local_g.assign(s.v_local_g, s.v_local_g + 2 * N);
+      sys.v_local_g = v_local_g.data();
+    } else {
+      const int ns = s.n_species;
+      recip.assign(s.recip, s.recip + 9);
+      species_zval.assign(s.species_zval, s.species_zval + ns);
+      species_flags.assign(s.species_flags, s.species_flags + ns);
+      vloc_r.assign(s.vloc_r, s.vloc_r + mesh_tot);
+      bool any_core = false, any_atom = false;
+      for (int q = 0; q < ns; ++q) {
+        any_core = any_core || (species_flags[q] & 1);
+        any_atom = any_atom || (species_flags[q] & 2);
+      }
+      if ((any_core && !s.core_r) || (any_atom && !s.rho_atom_r))
+        return fail(kInvalid, "pwgpu_server_submit: flagged core or atomic density missing");
+      if (any_core) core_r.assign(s.core_r, s.core_r + mesh_tot);
+      if (any_atom) rho_atom_r.assign(s.rho_atom_r, s.rho_atom_r + mesh_tot);
+      sys.recip = recip.data();
+      sys.species_zval = species_zval.data();
+      sys.species_flags = species_flags.data();
+      sys.vloc_r = vloc_r.data();
+      sys.core_r = any_core ? core_r.data() : nullptr;
+      sys.rho_atom_r = any_atom ? rho_atom_r.data() : nullptr;
+    }
     if (s.n_ch > 0) {
       if (s.proj_b) {
         proj_b.assign(s.proj_b, s.proj_b + nk * n * (size_t)s.n_ch * 2);
       } else {
-        // radial form of the projectors: G and k vectors, atoms, meshes, betas
+        // radial form of the projectors: G and k vectors and betas (atoms and
+        // meshes are copied above)
         const int ns = s.n_species;
         g_cart.assign(s.g_cart, s.g_cart + 3 * n);
         k_cart.assign(s.k_cart, s.k_cart + 3 * nk);
-        atom_tau.assign(s.atom_tau, s.atom_tau + 3L * s.n_atoms);
-        atom_species.assign(s.atom_species, s.atom_species + s.n_atoms);
-        species_mesh.assign(s.species_mesh, s.species_mesh + ns);
         species_nbeta.assign(s.species_nbeta, s.species_nbeta + ns);
-        size_t mesh_tot = 0, nbeta = 0, beta_tot = 0;
+        size_t nbeta = 0, beta_tot = 0;
         for (int q = 0; q < ns; ++q) {
-          mesh_tot += (size_t)species_mesh[q];
           nbeta += (size_t)species_nbeta[q];
           beta_tot += (size_t)species_nbeta[q] * species_mesh[q];
         }
-        radial_r.assign(s.radial_r, s.radial_r + mesh_tot);
-        radial_rab.assign(s.radial_rab, s.radial_rab + mesh_tot);
         beta_l.assign(s.beta_l, s.beta_l + nbeta);
         beta_r.assign(s.beta_r, s.beta_r + beta_tot);
         sys.g_cart = g_cart.data();
         sys.k_cart = k_cart.data();
-        sys.atom_tau = atom_tau.data();
-        sys.atom_species = atom_species.data();
-        sys.species_mesh = species_mesh.data();
         sys.species_nbeta = species_nbeta.data();
-        sys.radial_r = radial_r.data();
-        sys.radial_rab = radial_rab.data();
         sys.beta_l = beta_l.data();
         sys.beta_r = beta_r.data();
       }
@@ -211,6 +245,11 @@ struct pwgpu_server {
       pwgpu_options o{opt.device, opt.precision, opt.lanes_per_job > 0 ? opt.lanes_per_job : 2, 0};
       pwgpu_handle* h = nullptr;
       pwgpu_status st = pwgpu_create(&job->sys.sys, &o, &h);
+      if (st == PWGPU_OK && job->rho_init.empty()) {
+        // start density built on the device with the local potential
+        job->rho_init.resize((size_t)job->sys.sys.dims[0] * job->sys.sys.dims[1] * job->sys.sys.dims[2]);
+        st = pwgpu_initial_density(h, job->rho_init.data());
+      }
       if (st == PWGPU_OK)
         st = pwgpu_scf_run(h, &job->params, job->rho_init.data(), &job->result, job->evals.data(), nullptr, nullptr);
       const std::string err = st == PWGPU_OK ? std::string() : std::string(pwgpu_last_error());
@@ -288,7 +327,9 @@ pwgpu_status pwgpu_server_destroy(pwgpu_server* s) {
 
 pwgpu_status pwgpu_server_submit(pwgpu_server* s, const pwgpu_system* sys, const pwgpu_scf_params* params,
                                  const double* rho_init_r, int64_t* job_id) {
-  if (!s || !sys || !params || !rho_init_r || !job_id) return fail(kInvalid, "pwgpu_server_submit: NULL argument");
+  if (!s || !sys || !params || !job_id) return fail(kInvalid, "pwgpu_server_submit: NULL argument");
+  if (!rho_init_r && sys->v_local_g)
+    return fail(kInvalid, "pwgpu_server_submit: rho_init_r may be NULL only when the local part is built on the device");
   if (sys->nspin != 1 && sys->nspin != 2) return fail(kInvalid, "pwgpu_server_submit: nspin must be 1 or 2");
   if (params->n_bands < 1 || params->n_bands > sys->n_pw)
     return fail(kInvalid, "pwgpu_server_submit: n_bands out of range");
@@ -297,7 +338,7 @@ pwgpu_status pwgpu_server_submit(pwgpu_server* s, const pwgpu_system* sys, const
   if (st != kOk) return st;
   const size_t N = (size_t)sys->dims[0] * sys->dims[1] * sys->dims[2];
   job->params = *params;
-  job->rho_init.assign(rho_init_r, rho_init_r + N);
+  if (rho_init_r) job->rho_init.assign(rho_init_r, rho_init_r + N);
   job->evals.assign((size_t)sys->nspin * sys->n_k * params->n_bands, 0.0);
   job->bytes = footprint(*sys, *params, s->opt.lanes_per_job > 0 ? s->opt.lanes_per_job : 2);
   if (job->bytes > s->budget)

@@ -10,6 +10,21 @@
 // by atom, projector by projector, m by m.  Every |k+G| is evaluated
 // directly (no interpolation table), so B equals the host construction to
 // rounding.
+//
+// The local part of ScfContext::new on the full FFT grid, from the same
+// radial meshes (build_local_device):
+//
+//   V_loc(G) = sum_s S_s(G) v_s(|G|),  S_s(G) = sum_{a in s} e^{-iG.tau_a}
+//   v_s(G)   = (4 pi/Omega) int r^2 [V(r) + Z e^2 erf(r)/r] sinc(Gr) dr
+//              - 4 pi Z e^2 e^{-G^2/4} / (Omega G^2)               (G != 0)
+//   v_s(0)   = (4 pi/Omega) int r^2 [V(r) + Z e^2 / r] dr           (upf/mod.rs:166-213)
+//   rho_core(G) = sum_s S_s(G) (4 pi/Omega) int r^2 rho_c(r) j0(Gr) dr  (potentials.rs:99-115)
+//   rho_0(G)    = sum_s S_s(G) (1/Omega) int rho_atom(r) j0(Gr) dr, or
+//                 Z e^{-G^2 sigma^2/2} / Omega without PP_RHOATOM  (initial_density.rs:64-166)
+//
+// rho_core(r) and rho_0(r) are unnormalised inverse transforms (real part);
+// rho_0 is clipped at zero and scaled to the electron count.  Each |G| is
+// evaluated directly, one warp per grid point.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -152,6 +167,163 @@ __global__ void k_assemble_b(const double* __restrict__ gvec, int n_pw, const do
   }
 }
 
+// G of flat grid index t with the host's operation order (grid_g_vectors:
+// signed Miller index i > n/2 -> i - n; g_c = (f1 b1_c + f2 b2_c) + f3 b3_c)
+__device__ __forceinline__ void grid_g(long t, int d0, int d1, int d2, const double* __restrict__ rec, double* g) {
+  const int i2 = (int)(t % d2), i1 = (int)((t / d2) % d1), i0 = (int)(t / ((long)d1 * d2));
+  const double f1 = i0 > d0 / 2 ? i0 - d0 : i0, f2 = i1 > d1 / 2 ? i1 - d1 : i1, f3 = i2 > d2 / 2 ? i2 - d2 : i2;
+  for (int c = 0; c < 3; ++c)
+    g[c] = __dadd_rn(__dadd_rn(__dmul_rn(f1, rec[c]), __dmul_rn(f2, rec[3 + c])), __dmul_rn(f3, rec[6 + c]));
+}
+
+__device__ __forceinline__ double norm3(const double* g) {
+  return sqrt(__dadd_rn(__dadd_rn(__dmul_rn(g[0], g[0]), __dmul_rn(g[1], g[1])), __dmul_rn(g[2], g[2])));
+}
+
+// sin(x)/x with the host's small-argument form 1 - x^2/6 below 1e-10
+__device__ __forceinline__ double sinc_host(double x) {
+  if (x < 1e-10) return 1.0 - x * x / 6.0;
+  return sin(x) / x;
+}
+
+enum LocalKind { kVloc = 0, kCore = 1, kAtom = 2, kGauss = 3 };
+
+constexpr double kE2 = 14.399645351950548;  // e^2 in eV Angstrom
+constexpr double kGZero = 1e-12;             // |G| below which G = 0
+
+// rad[t] = radial transform of one species at |G_t|, one warp per grid point
+__global__ void k_local_radial(int kind, long N, int d0, int d1, int d2, const double* __restrict__ rec,
+                               const double* __restrict__ r, const double* __restrict__ rab, int mesh,
+                               const double* __restrict__ f, double z, double omega, double sigma,
+                               double* __restrict__ rad) {
+  const long t = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (t >= N) return;
+  double g[3];
+  grid_g(t, d0, d1, d2, rec, g);
+  const double gn = norm3(g);
+  const double fpi = 4.0 * kPi;
+  if (kind == kGauss) {
+    if (lane == 0) {
+      const double g2 = __dadd_rn(__dadd_rn(__dmul_rn(g[0], g[0]), __dmul_rn(g[1], g[1])), __dmul_rn(g[2], g[2]));
+      rad[t] = z * exp(-0.5 * g2 * sigma * sigma) / omega;
+    }
+    return;
+  }
+  double acc = 0.0;
+  const bool g0 = gn < kGZero;
+  for (int i = lane; i < mesh; i += 32) {
+    const double ri = r[i];
+    double v;
+    if (kind == kVloc) {
+      double eor;
+      if (g0) eor = 1.0 / fmax(ri, 1e-20);
+      else eor = ri < 1e-20 ? 2.0 / sqrt(kPi) : erf(ri) / ri;
+      const double vs = f[i] + z * kE2 * eor;
+      v = ri * ri * vs * (g0 ? 1.0 : sinc_host(gn * ri));
+    } else if (kind == kCore) {
+      v = f[i] * (ri * ri) * sinc_host(gn * ri);
+    } else {
+      v = f[i] * sinc_host(gn * ri);
+    }
+    acc += simpson_w(i, mesh) * (v * rab[i]);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if (lane != 0) return;
+  const double sint = acc / 3.0;
+  double out;
+  if (kind == kVloc) {
+    out = fpi / omega * sint;
+    if (!g0) {
+      const double g2 = gn * gn;
+      out -= fpi * z * kE2 * exp(-g2 / 4.0) / (omega * g2);
+    }
+  } else if (kind == kCore) {
+    out = fpi * sint / omega;
+  } else {
+    out = sint / omega;
+  }
+  rad[t] = out;
+}
+
+// out[t] = sum_a e^{-iG_t.tau_a} rad[species(a)][t] (species with rad_used 0 skipped)
+__global__ void k_structure_sum(long N, int d0, int d1, int d2, const double* __restrict__ rec,
+                                const double* __restrict__ tau, const int* __restrict__ atom_species, int n_atoms,
+                                const double* __restrict__ rad, const int* __restrict__ used,
+                                double2* __restrict__ out) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= N) return;
+  double g[3];
+  grid_g(t, d0, d1, d2, rec, g);
+  double re = 0.0, im = 0.0;
+  for (int a = 0; a < n_atoms; ++a) {
+    const int sp = atom_species[a];
+    if (!used[sp]) continue;
+    const double* ta = tau + 3L * a;
+    const double ph = -__dadd_rn(__dadd_rn(__dmul_rn(g[0], ta[0]), __dmul_rn(g[1], ta[1])), __dmul_rn(g[2], ta[2]));
+    double sn, cs;
+    sincos(ph, &sn, &cs);
+    const double v = rad[(long)sp * N + t];
+    re += cs * v;
+    im += sn * v;
+  }
+  out[t] = make_double2(re, im);
+}
+
+__global__ void k_real_clip(const double2* __restrict__ c, double* __restrict__ r, long n, int clip) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) r[i] = (clip && c[i].x < 0.0) ? 0.0 : c[i].x;
+}
+
+constexpr int kSumBlocks = 512;
+
+__global__ void k_sum_partials(const double* __restrict__ a, long n, double* __restrict__ partials) {
+  __shared__ double sh[256];
+  double acc = 0.0;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) acc += a[i];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partials[blockIdx.x] = sh[0];
+}
+
+__global__ void k_sum_final(double* __restrict__ partials, int n) {
+  __shared__ double sh[256];
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc += partials[i];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partials[kSumBlocks] = sh[0];
+}
+
+__global__ void k_scale_vec(double* __restrict__ a, long n, double f) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] *= f;
+}
+
+// sum of a[0..n) (fixed block count: the same order on every call); red
+// holds kSumBlocks + 1 doubles
+Status device_sum(Handle& h, const double* a, long n, double* red, double& out) {
+  k_sum_partials<<<kSumBlocks, 256, 0, h.stream>>>(a, n, red); count_launch();
+  k_sum_final<<<1, 256, 0, h.stream>>>(red, kSumBlocks); count_launch();
+  PW_CUDA_TRY(cudaMemcpyAsync(&out, red + kSumBlocks, sizeof(double), cudaMemcpyDeviceToHost, h.stream));
+  PW_CUDA_TRY(cudaStreamSynchronize(h.stream));
+  return kOk;
+}
+
+Status device_scale(Handle& h, double* a, long n, double f) {
+  k_scale_vec<<<(unsigned)((n + 255) / 256), 256, 0, h.stream>>>(a, n, f); count_launch();
+  PW_CUDA_TRY(cudaGetLastError());
+  return kOk;
+}
+
 template <typename T> Status sup_upload(T** dst, const T* src, size_t n) {
   cudaError_t e = cudaMalloc((void**)dst, std::max<size_t>(n, 1) * sizeof(T));
   if (e != cudaSuccess) return fail(kOom, std::string("cudaMalloc (projector build): ") + cudaGetErrorString(e));
@@ -242,6 +414,107 @@ Status build_projectors_device(Handle& h, const ProjectorSource& src) {
   cleanup();
   if (e != cudaSuccess) return fail(kCuda, std::string("projector build: ") + cudaGetErrorString(e));
   return kOk;
+}
+
+Status build_local_device(Handle& h, const LocalSource& src, double2* v_local_g, double** rho_core_r,
+                          double** rho_start) {
+  if (src.n_species <= 0 || !src.species_mesh || !src.radial_r || !src.radial_rab || !src.species_zval ||
+      !src.vloc_r || !src.species_flags || !src.atom_tau || !src.atom_species || src.n_atoms <= 0 || !src.recip)
+    return fail(kInvalid, "pwgpu_create: v_local_g is NULL and the local radial data is incomplete");
+  if (!(src.gaussian_sigma > 0.0) || !std::isfinite(src.gaussian_sigma))
+    return fail(kInvalid, "pwgpu_create: gaussian_sigma must be positive and finite");
+  const int ns = src.n_species;
+  const long N = h.g.N;
+  std::vector<long> off(ns + 1, 0);
+  bool any_core = false, any_atom = false;
+  for (int q = 0; q < ns; ++q) {
+    if (src.species_mesh[q] < 1) return fail(kInvalid, "pwgpu_create: species radial mesh out of range");
+    off[q + 1] = off[q] + src.species_mesh[q];
+    any_core = any_core || (src.species_flags[q] & 1);
+    any_atom = any_atom || (src.species_flags[q] & 2);
+  }
+  if (any_core && !src.core_r) return fail(kInvalid, "pwgpu_create: core charge flagged but core_r is NULL");
+  if (any_atom && !src.rho_atom_r) return fail(kInvalid, "pwgpu_create: rho_atom flagged but rho_atom_r is NULL");
+  for (int a = 0; a < src.n_atoms; ++a)
+    if (src.atom_species[a] < 0 || src.atom_species[a] >= ns)
+      return fail(kInvalid, "pwgpu_create: atom species index out of range");
+  std::vector<void*> owned;
+  Status r = kOk;
+  auto up = [&](auto** dst, const auto* srcp, size_t cnt) {
+    if (r != kOk) return;
+    r = sup_upload(dst, srcp, cnt);
+    if (r == kOk) owned.push_back((void*)*dst);
+  };
+  double *rec = nullptr, *rr = nullptr, *rab = nullptr, *vl = nullptr, *cr = nullptr, *ra = nullptr, *tau = nullptr,
+         *rad = nullptr, *red = nullptr;
+  int *sp = nullptr, *used = nullptr;
+  up(&rec, src.recip, 9);
+  up(&rr, src.radial_r, (size_t)off[ns]);
+  up(&rab, src.radial_rab, (size_t)off[ns]);
+  up(&vl, src.vloc_r, (size_t)off[ns]);
+  if (any_core) up(&cr, src.core_r, (size_t)off[ns]);
+  if (any_atom) up(&ra, src.rho_atom_r, (size_t)off[ns]);
+  up(&tau, src.atom_tau, 3L * src.n_atoms);
+  up(&sp, src.atom_species, (size_t)src.n_atoms);
+  up(&rad, (const double*)nullptr, (size_t)ns * N);
+  up(&used, (const int*)nullptr, (size_t)ns);
+  up(&red, (const double*)nullptr, 1024);
+  auto done = [&](Status st) {
+    cudaStreamSynchronize(h.stream);
+    for (void* p : owned) cudaFree(p);
+    return st;
+  };
+  if (r != kOk) return done(r);
+  const int d0 = h.g.d[0], d1 = h.g.d[1], d2 = h.g.d[2];
+  const cudaStream_t s = h.stream;
+  const unsigned wblocks = (unsigned)((N * 32 + 255) / 256), tblocks = (unsigned)((N + 255) / 256);
+  std::vector<int> use(ns);
+  // one structure sum for the given per-species kinds into out
+  auto structure = [&](auto kind_of, double2* out) -> Status {
+    for (int q = 0; q < ns; ++q) {
+      const int kind = kind_of(q);
+      use[q] = kind >= 0;
+      if (kind < 0) continue;
+      const double* f = kind == kVloc ? vl + off[q] : (kind == kCore ? cr + off[q] : (kind == kAtom ? ra + off[q]
+                                                                                                   : nullptr));
+      k_local_radial<<<wblocks, 256, 0, s>>>(kind, N, d0, d1, d2, rec, rr + off[q], rab + off[q],
+                                             src.species_mesh[q], f, src.species_zval[q], h.omega,
+                                             src.gaussian_sigma, rad + (long)q * N);
+      count_launch();
+    }
+    PW_CUDA_TRY(cudaMemcpyAsync(used, use.data(), ns * sizeof(int), cudaMemcpyHostToDevice, s));
+    k_structure_sum<<<tblocks, 256, 0, s>>>(N, d0, d1, d2, rec, tau, sp, src.n_atoms, rad, used, out);
+    count_launch();
+    PW_CUDA_TRY(cudaStreamSynchronize(s));  // use[] is reused by the next sum
+    return kOk;
+  };
+  Status st = structure([](int) { return (int)kVloc; }, v_local_g);
+  if (st != kOk) return done(st);
+  if (any_core) {
+    st = structure([&](int q) { return (src.species_flags[q] & 1) ? (int)kCore : -1; }, h.tmp_grid);
+    if (st == kOk) st = fft3d_full(h, h.tmp_grid, +1, s);
+    if (st == kOk && !*rho_core_r) st = sup_upload(rho_core_r, (const double*)nullptr, (size_t)N);
+    if (st != kOk) return done(st);
+    k_real_clip<<<tblocks, 256, 0, s>>>(h.tmp_grid, *rho_core_r, N, 0); count_launch();
+  }
+  if (rho_start) {
+    st = structure([&](int q) { return (src.species_flags[q] & 2) ? (int)kAtom : (int)kGauss; }, h.tmp_grid);
+    if (st == kOk) st = fft3d_full(h, h.tmp_grid, +1, s);
+    if (st == kOk && !*rho_start) st = sup_upload(rho_start, (const double*)nullptr, (size_t)N);
+    if (st != kOk) return done(st);
+    k_real_clip<<<tblocks, 256, 0, s>>>(h.tmp_grid, *rho_start, N, 1); count_launch();
+    // scale to the electron count: int rho dV = N_el (initial_density.rs:128-143)
+    double sum = 0.0;
+    if ((st = device_sum(h, *rho_start, N, red, sum)) != kOk) return done(st);
+    const double integ = sum * (h.omega / (double)N);
+    if (integ > 1e-15) {
+      if ((st = device_scale(h, *rho_start, N, h.n_electrons / integ)) != kOk) return done(st);
+    }
+  }
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return done(fail(kCuda, std::string("local potential build: ") + cudaGetErrorString(e)));
+  return done(kOk);
 }
 
 }  // namespace pwgpu

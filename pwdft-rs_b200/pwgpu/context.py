@@ -259,10 +259,14 @@ class ScfSystem:
 
 def build_system(crystal: Crystal, pps: dict, ecut_ev: float, kpoints, symmetry: SymmetryInfo | None = None,
                  ecutrho_ratio: int = 4, fft_grid=None, gaussian_sigma: float = 1.0, nspin: int = 1,
-                 with_initial_density: bool = True, projectors_on_device: bool = False) -> ScfSystem:
+                 with_initial_density: bool = True, projectors_on_device: bool = False,
+                 local_on_device: bool = False) -> ScfSystem:
     """ScfContext::new (context.rs:102-231) plus the SAD start density
     (initial_density.rs:64-143).  projectors_on_device: skip the host B
-    (the GPU builds it from the UPF radial data at pwgpu_create)."""
+    (the GPU builds it from the UPF radial data at pwgpu_create).
+    local_on_device: skip the host V_loc(G), core density and start density
+    (v_local_g and rho_init_r are None; the GPU builds them at pwgpu_create,
+    PwGpu.initial_density() returns the start density)."""
     basis = BasisSet(crystal.lattice, ecut_ev)
     dims = grid_dims_for(basis, ecutrho_ratio, fft_grid)
     omega = crystal.lattice.volume()
@@ -276,40 +280,42 @@ def build_system(crystal: Crystal, pps: dict, ecut_ev: float, kpoints, symmetry:
     n = gv.shape[0]
     taus = [a.cart(crystal.lattice) for a in crystal.atoms]
 
-    # per-species structure factors S_s(G) = sum over its atoms of e^{-iG.tau},
-    # shared by the V_loc, core and start-density sums
-    sfac = {}
-    for at, tau in zip(crystal.atoms, taus):
-        ph = -((gv[:, 0] * tau[0] + gv[:, 1] * tau[1]) + gv[:, 2] * tau[2])
-        term = np.cos(ph) + 1j * np.sin(ph)
-        if at.symbol in sfac:
-            sfac[at.symbol] += term
+    v_loc, rho_core_r = None, np.zeros(0)
+    if not local_on_device:
+        # per-species structure factors S_s(G) = sum over its atoms of e^{-iG.tau},
+        # shared by the V_loc, core and start-density sums
+        sfac = {}
+        for at, tau in zip(crystal.atoms, taus):
+            ph = -((gv[:, 0] * tau[0] + gv[:, 1] * tau[1]) + gv[:, 2] * tau[2])
+            term = np.cos(ph) + 1j * np.sin(ph)
+            if at.symbol in sfac:
+                sfac[at.symbol] += term
+            else:
+                sfac[at.symbol] = term
+
+        def structure_sum(radial_of_species):
+            acc = np.zeros(n, dtype=np.complex128)
+            for sp in sfac:
+                rad = radial_of_species(sp)
+                if rad is not None:
+                    acc += sfac[sp] * rad
+            return acc
+
+        v_loc = structure_sum(lambda sp: _per_unique(gn, lambda u: v_local_of_g(pps[sp], u, omega)))
+
+        if any(pps[s].has_nlcc() for s in crystal.species()):
+            four_pi = 4.0 * math.pi
+
+            def core_rad(sp):
+                pp = pps[sp]
+                if not pp.has_nlcc():
+                    return None
+                return _per_unique(gn, lambda u: four_pi * sinc_transform(pp, pp.core_charge, True, u) / omega)
+
+            rho_core_g = structure_sum(core_rad)
+            rho_core_r = inverse_fft_unnormalized(rho_core_g, dims).real.copy()
         else:
-            sfac[at.symbol] = term
-
-    def structure_sum(radial_of_species):
-        acc = np.zeros(n, dtype=np.complex128)
-        for sp in sfac:
-            rad = radial_of_species(sp)
-            if rad is not None:
-                acc += sfac[sp] * rad
-        return acc
-
-    v_loc = structure_sum(lambda sp: _per_unique(gn, lambda u: v_local_of_g(pps[sp], u, omega)))
-
-    if any(pps[s].has_nlcc() for s in crystal.species()):
-        four_pi = 4.0 * math.pi
-
-        def core_rad(sp):
-            pp = pps[sp]
-            if not pp.has_nlcc():
-                return None
-            return _per_unique(gn, lambda u: four_pi * sinc_transform(pp, pp.core_charge, True, u) / omega)
-
-        rho_core_g = structure_sum(core_rad)
-        rho_core_r = inverse_fft_unnormalized(rho_core_g, dims).real.copy()
-    else:
-        rho_core_r = np.zeros(0)
+            rho_core_r = np.zeros(0)
 
     tables = {sp: upf_radial_table(pps[sp]) for sp in crystal.species()}
     kin = [basis.kinetic(kp.k) for kp in kpoints]
@@ -321,8 +327,8 @@ def build_system(crystal: Crystal, pps: dict, ecut_ev: float, kpoints, symmetry:
     e_ew = ewald_energy(crystal, [pps[a.symbol].z_valence for a in crystal.atoms])
     sym = symmetry if symmetry is not None else SymmetryInfo.identity_only()
 
-    rho0 = np.zeros(0)
-    if with_initial_density:
+    rho0 = None if local_on_device else np.zeros(0)
+    if with_initial_density and not local_on_device:
         def sad_rad(sp):
             pp = pps[sp]
             if pp.has_rho_atom():
@@ -340,4 +346,5 @@ def build_system(crystal: Crystal, pps: dict, ecut_ev: float, kpoints, symmetry:
     out = ScfSystem(crystal, basis, dims, g_to_fft, list(kpoints), kin, projs, v_loc, g2, rho_core_r, nel, omega,
                     e_ew, sym, rho0, nspin)
     out.extra["pps"] = pps
+    out.extra["gaussian_sigma"] = float(gaussian_sigma)
     return out

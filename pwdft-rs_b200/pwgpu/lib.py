@@ -71,6 +71,8 @@ class PwgpuSystem(ct.Structure):
         ("species_nbeta", _i32p),
         ("beta_l", _i32p),
         ("beta_r", _f64p),
+        ("recip", _f64p), ("species_zval", _f64p), ("vloc_r", _f64p), ("core_r", _f64p),
+        ("rho_atom_r", _f64p), ("species_flags", _i32p), ("gaussian_sigma", ct.c_double),
     ]
 
 
@@ -185,6 +187,8 @@ def load_library(path: str = LIB_PATH):
                               ct.c_double]
     lib.pwgpu_mix_reset.argtypes = [vp]
     lib.pwgpu_get_projectors.argtypes = [vp, ct.c_int32, _f64p]
+    lib.pwgpu_initial_density.argtypes = [vp, _f64p]
+    lib.pwgpu_get_local_potential.argtypes = [vp, _f64p, _f64p]
     lib.pwgpu_small_geneig.argtypes = [ct.c_int32, ct.c_int32, ct.c_int32, _f64p, _f64p, _f64p, _f64p]
     lib.pwgpu_get_stream.argtypes = [vp, ct.POINTER(vp)]
     lib.pwgpu_get_stream.restype = ct.c_int32
@@ -205,7 +209,8 @@ def load_library(path: str = LIB_PATH):
     for name in ("pwgpu_create", "pwgpu_destroy", "pwgpu_set_veff_g", "pwgpu_apply_h", "pwgpu_apply_h_device",
                  "pwgpu_set_precision", "pwgpu_get_dims", "pwgpu_profile_apply_h", "pwgpu_scf_run", "pwgpu_scf_iter1_from_rho_g",
                  "pwgpu_eigensolve", "pwgpu_density", "pwgpu_symmetrize", "pwgpu_potentials",
-                 "pwgpu_small_geneig", "pwgpu_mix", "pwgpu_mix_reset", "pwgpu_get_projectors", "pwgpu_server_create", "pwgpu_server_destroy",
+                 "pwgpu_small_geneig", "pwgpu_mix", "pwgpu_mix_reset", "pwgpu_get_projectors", "pwgpu_initial_density",
+                 "pwgpu_get_local_potential", "pwgpu_server_create", "pwgpu_server_destroy",
                  "pwgpu_server_submit", "pwgpu_server_poll", "pwgpu_server_wait", "pwgpu_server_wait_any",
                  "pwgpu_server_result", "pwgpu_server_release", "pwgpu_server_get_stats"):
         getattr(lib, name).restype = ct.c_int32
@@ -248,6 +253,23 @@ def pack_system(sys_) -> tuple:
     s.k_weights = _f64(kw)
     s.kinetic = _f64(kin)
     s.n_ch = n_ch
+    packed = []
+
+    def species_radial():
+        """Atoms and species meshes shared by the device builds (packed once)."""
+        cr, pps = sys_.crystal, sys_.extra["pps"]
+        species = list(dict.fromkeys(a.symbol for a in cr.atoms))
+        if not packed:
+            s.atom_tau = _f64(hold(np.ascontiguousarray(np.array([a.cart(cr.lattice) for a in cr.atoms]),
+                                                        dtype=np.float64)))
+            s.atom_species = _i32(hold(np.array([species.index(a.symbol) for a in cr.atoms], dtype=np.int32)))
+            s.n_species = len(species)
+            s.species_mesh = _i32(hold(np.array([pps[sp].r.size for sp in species], dtype=np.int32)))
+            s.radial_r = _f64(hold(np.concatenate([pps[sp].r for sp in species]).astype(np.float64)))
+            s.radial_rab = _f64(hold(np.concatenate([pps[sp].rab for sp in species]).astype(np.float64)))
+            packed.append(True)
+        return species
+
     if n_ch:
         starts = hold(np.ascontiguousarray(projs[0].atom_ch_start, dtype=np.int32))
         blocks = hold(np.concatenate([blk.ravel() for blk in projs[0].d_blocks]).astype(np.float64))
@@ -259,28 +281,42 @@ def pack_system(sys_) -> tuple:
             s.proj_b = b.view(np.float64).ctypes.data_as(_f64p)
         else:
             # radial form: the device builds B (NonlocalPotential::new on the GPU)
-            cr, pps = sys_.crystal, sys_.extra["pps"]
-            species = list(dict.fromkeys(a.symbol for a in cr.atoms))
+            pps = sys_.extra["pps"]
+            species = species_radial()
             s.g_cart = _f64(hold(np.ascontiguousarray(sys_.basis.g, dtype=np.float64)))
             s.k_cart = _f64(hold(np.ascontiguousarray(np.array([kp.k for kp in sys_.kpoints]), dtype=np.float64)))
-            s.atom_tau = _f64(hold(np.ascontiguousarray(np.array([a.cart(cr.lattice) for a in cr.atoms]),
-                                                        dtype=np.float64)))
-            s.atom_species = _i32(hold(np.array([species.index(a.symbol) for a in cr.atoms], dtype=np.int32)))
-            s.n_species = len(species)
-            s.species_mesh = _i32(hold(np.array([pps[sp].r.size for sp in species], dtype=np.int32)))
-            s.radial_r = _f64(hold(np.concatenate([pps[sp].r for sp in species]).astype(np.float64)))
-            s.radial_rab = _f64(hold(np.concatenate([pps[sp].rab for sp in species]).astype(np.float64)))
             s.species_nbeta = _i32(hold(np.array([len(pps[sp].beta_l) for sp in species], dtype=np.int32)))
             s.beta_l = _i32(hold(np.array([l for sp in species for l in pps[sp].beta_l], dtype=np.int32)))
             betas = [np.asarray(pps[sp].beta[i], dtype=np.float64) for sp in species for i in range(len(pps[sp].beta_l))]
             s.beta_r = _f64(hold(np.concatenate(betas) if betas else np.zeros(1)))
-    vl = hold(np.ascontiguousarray(sys_.v_local_g, dtype=np.complex128))
-    s.v_local_g = vl.view(np.float64).ctypes.data_as(_f64p)
+    if sys_.v_local_g is not None:
+        vl = hold(np.ascontiguousarray(sys_.v_local_g, dtype=np.complex128))
+        s.v_local_g = vl.view(np.float64).ctypes.data_as(_f64p)
+        if sys_.rho_core_r.size:
+            rc = hold(np.ascontiguousarray(sys_.rho_core_r, dtype=np.float64))
+            s.rho_core_r = _f64(rc)
+    else:
+        # radial form: the device builds V_loc(G), the core density and the start density
+        pps = sys_.extra["pps"]
+        species = species_radial()
+        s.n_atoms = len(sys_.crystal.atoms)
+        rec = sys_.crystal.lattice.reciprocal()
+        s.recip = _f64(hold(np.ascontiguousarray(np.array([rec.a, rec.b, rec.c]), dtype=np.float64)))
+        s.species_zval = _f64(hold(np.array([pps[sp].z_valence for sp in species], dtype=np.float64)))
+        s.vloc_r = _f64(hold(np.concatenate([pps[sp].v_local for sp in species]).astype(np.float64)))
+        flags = np.array([(1 if pps[sp].has_nlcc() else 0) | (2 if pps[sp].has_rho_atom() else 0)
+                          for sp in species], dtype=np.int32)
+        s.species_flags = _i32(hold(flags))
+        if np.any(flags & 1):
+            s.core_r = _f64(hold(np.concatenate([pps[sp].core_charge if pps[sp].has_nlcc() else np.zeros(pps[sp].r.size)
+                                                 for sp in species]).astype(np.float64)))
+        if np.any(flags & 2):
+            s.rho_atom_r = _f64(hold(np.concatenate([pps[sp].rho_atom if pps[sp].has_rho_atom()
+                                                     else np.zeros(pps[sp].r.size) for sp in species])
+                                     .astype(np.float64)))
+        s.gaussian_sigma = sys_.extra["gaussian_sigma"]
     g2 = hold(np.ascontiguousarray(sys_.g_squared, dtype=np.float64))
     s.g_squared = _f64(g2)
-    if sys_.rho_core_r.size:
-        rc = hold(np.ascontiguousarray(sys_.rho_core_r, dtype=np.float64))
-        s.rho_core_r = _f64(rc)
     n_sym = sys_.symmetry.n_ops
     s.n_sym = n_sym
     if n_sym > 1:
@@ -424,6 +460,21 @@ class PwGpu:
         _check(self.lib, self.lib.pwgpu_mix(self.h, channel, mixing_mode(mixer, kerker), _f64(a), _f64(b),
                                             _f64(out), beta, ndim, period, q_tf))
         return out
+
+    def initial_density(self) -> np.ndarray:
+        """The device-built start density (N,) of a system whose local part is built on the device."""
+        out = np.zeros(self.sys.n_grid)
+        _check(self.lib, self.lib.pwgpu_initial_density(self.h, _f64(out)))
+        return out
+
+    def local_potential(self):
+        """(V_loc(G) (N,) complex, rho_core(r) (N,)) as held on the device."""
+        n = self.sys.n_grid
+        v = np.zeros(n, dtype=np.complex128)
+        rc = np.zeros(n)
+        _check(self.lib, self.lib.pwgpu_get_local_potential(self.h, v.view(np.float64).ctypes.data_as(_f64p),
+                                                           _f64(rc)))
+        return v, rc
 
     def projectors(self, ik: int = 0) -> np.ndarray:
         """The device copy of B at k-point ik (n_pw x n_ch complex)."""

@@ -9,8 +9,9 @@ displacements U(-0.05, 0.05) bohr per component, ecutwfc uniform in
 {20, 25, 30, 35} Ry, a Gamma-only or Gamma-centred 2x2x2 mesh (50/50,
 reduced by the cell's symmetry), PZ-LDA, unpolarised, mixed precision.
 
-The projector matrices of a request are built on the device from the UPF
-radial data (pwgpu_create), not on the host.
+The projector matrices, the local potential, the core density and the
+start density of a request are built on the device from the UPF radial
+data (pwgpu_create), not on the host.
 
 SCF controls of a request: bands = N_el/2 + max(4, N_el/20); Gaussian
 smearing 0.01 Ry; Anderson beta 0.4 + Kerker, 8 slots (the settings of the
@@ -72,9 +73,12 @@ class Server:
     def submit(self, sys_, n_bands: int, rho_init=None, **kw) -> int:
         st, keep = pack_system(sys_)
         p = scf_params(n_bands, **kw)
-        rho = np.ascontiguousarray(sys_.rho_init_r if rho_init is None else rho_init, dtype=np.float64)
+        rho0 = sys_.rho_init_r if rho_init is None else rho_init
+        # None: the start density is built on the device with the local potential
+        rho = None if rho0 is None else np.ascontiguousarray(rho0, dtype=np.float64)
         jid = ct.c_int64()
-        _check(self.lib, self.lib.pwgpu_server_submit(self.h, ct.byref(st), ct.byref(p), _f64(rho), ct.byref(jid)))
+        _check(self.lib, self.lib.pwgpu_server_submit(self.h, ct.byref(st), ct.byref(p),
+                                                      None if rho is None else _f64(rho), ct.byref(jid)))
         with self._lock:
             self.shapes[jid.value] = (sys_.nspin * len(sys_.kpoints), n_bands)
         return jid.value
@@ -174,7 +178,8 @@ def request_system(req: Request, pps: dict):
     cr = request_crystal(req)
     sym = SymmetryInfo.from_crystal(cr, 1e-5)
     kp = reduce_kpoints(req.kgrid, "gamma", sym, cr.lattice)
-    s = build_system(cr, {req.species: pps[req.species]}, req.ecut_ry * RY_TO_EV, kp, sym, projectors_on_device=True)
+    s = build_system(cr, {req.species: pps[req.species]}, req.ecut_ry * RY_TO_EV, kp, sym, projectors_on_device=True,
+                     local_on_device=True)
     nel = int(round(s.n_electrons))
     nb = nel // 2 + max(4, nel // 20)
     return s, dict(SERVE_KW, n_bands=nb)

@@ -82,9 +82,10 @@ def test_wait_times_out_then_completes(si_pp, c_pp):
 
 
 def test_stream_requests_build_and_solve(si_pp, c_pp):
-    """Small requests of the serving stream (device-built projectors, Gamma
-    and 2x2x2 meshes, Si and C) run four at a time through the queue and
-    give the energies of the same requests solved one by one."""
+    """Small requests of the serving stream (projectors, local potential and
+    start density built on the device; Gamma and 2x2x2 meshes, Si and C) run
+    four at a time through the queue and give the energies of the same
+    requests solved one by one."""
     pps = {"Si": si_pp, "C": c_pp}
     reqs = [r for r in request_stream(40) if r.n_atoms <= 8][:8]
     built = []
@@ -103,5 +104,5 @@ def test_stream_requests_build_and_solve(si_pp, c_pp):
             got.append(res["total_energy"])
     for (r, s, nb, kw), e in zip(built, got):
         with PwGpu(s, lanes=2) as dev:
-            res, _, _, _ = dev.scf_run(s.rho_init_r, nb, **kw)
+            res, _, _, _ = dev.scf_run(dev.initial_density(), nb, **kw)
         assert abs(res["total_energy"] - e) / r.n_atoms < 1e-4, (r, res["total_energy"], e)
