@@ -157,11 +157,68 @@ __device__ __forceinline__ void fft_stage(const C* __restrict__ src, C* __restri
   __syncthreads();
 }
 
+// The same stage with the radix, the stride Ns and the length known at
+// compile time: constant index arithmetic and twiddle steps.
+template <int R_, int Ns, int L, int S, typename C>
+__device__ __forceinline__ void fft_stage_ct(const C* __restrict__ src, C* __restrict__ dst, int W,
+                                             const C* __restrict__ tw) {
+  constexpr int LR = L / R_;
+  constexpr int twstep = L / (Ns * R_);
+  const int line = threadIdx.x;
+  for (int j = threadIdx.y; j < LR; j += blockDim.y) {
+    const int jq = j / Ns;
+    const int k = j - jq * Ns;
+    C v[R_];
+#pragma unroll
+    for (int r = 0; r < R_; ++r) {
+      C x = src[(j + r * LR) * W + line];
+      if (r > 0 && Ns > 1) {
+        const C w = tw[k * r * twstep];
+        x = (S < 0) ? cmul(x, w) : cmulc(x, w);
+      }
+      v[r] = x;
+    }
+    dft<R_, S>(v);
+    const int ob = (jq * Ns * R_ + k) * W + line;
+#pragma unroll
+    for (int q = 0; q < R_; ++q) dst[ob + q * Ns * W] = v[q];
+  }
+  __syncthreads();
+}
+
+// Two-stage lengths R0 * R1 (plan order: radix R0 first, stride 1; then R1,
+// stride R0); the result ends in `a`.
+template <int S, int R0, int R1, typename C>
+__device__ __forceinline__ C* fft_lines_2(C* a, C* b, int W, const C* __restrict__ tw) {
+  fft_stage_ct<R0, 1, R0 * R1, S>(a, b, W, tw);
+  fft_stage_ct<R1, R0, R0 * R1, S>(b, a, W, tw);
+  return a;
+}
+
 // Full 1-D transform of the W interleaved lines of a tile (S = -1 forward,
 // +1 inverse).  The data starts in `a`; `b` is scratch of the same size.
 // Returns the buffer holding the result (by the parity of the stage count).
+// Common two-stage lengths take a compile-time path; the rest the plan's.
 template <int S, typename C>
 __device__ __forceinline__ C* fft_lines(C* a, C* b, const FftPlan& p, int W, const C* __restrict__ tw) {
+  if (p.nstages == 2) {
+    switch (p.radix[0] * 16 + p.radix[1]) {
+      case 8 * 16 + 9: return fft_lines_2<S, 8, 9>(a, b, W, tw);   // 72
+      case 8 * 16 + 5: return fft_lines_2<S, 8, 5>(a, b, W, tw);   // 40
+      case 8 * 16 + 8: return fft_lines_2<S, 8, 8>(a, b, W, tw);   // 64
+      case 8 * 16 + 4: return fft_lines_2<S, 8, 4>(a, b, W, tw);   // 32
+      case 8 * 16 + 3: return fft_lines_2<S, 8, 3>(a, b, W, tw);   // 24
+      case 8 * 16 + 2: return fft_lines_2<S, 8, 2>(a, b, W, tw);   // 16
+      case 9 * 16 + 9: return fft_lines_2<S, 9, 9>(a, b, W, tw);   // 81
+      case 9 * 16 + 5: return fft_lines_2<S, 9, 5>(a, b, W, tw);   // 45
+      case 9 * 16 + 4: return fft_lines_2<S, 9, 4>(a, b, W, tw);   // 36
+      case 9 * 16 + 3: return fft_lines_2<S, 9, 3>(a, b, W, tw);   // 27
+      case 9 * 16 + 2: return fft_lines_2<S, 9, 2>(a, b, W, tw);   // 18
+      case 5 * 16 + 5: return fft_lines_2<S, 5, 5>(a, b, W, tw);   // 25
+      case 4 * 16 + 5: return fft_lines_2<S, 4, 5>(a, b, W, tw);   // 20
+      default: break;
+    }
+  }
   C* src = a;
   C* dst = b;
   // Unrolled over the stage slots so every plan field is read at a fixed
