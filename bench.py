@@ -176,7 +176,7 @@ def run_reference(args, world, rank):
     from pwgpu.config3 import config3_system
     from pwgpu.upf import load_upf
     sys_ = config3_system(load_upf(SI_UPF))
-    h_apps = 22787  # band applications of the FP64 GPU solve of this cell (measured, bench "accuracy" block)
+    h_apps = 12574  # band applications of the FP64 GPU solve of this cell (measured, bench "accuracy" block)
     vals = []
     base = None
     for i in range(args.warmup + args.steps):
