@@ -238,7 +238,7 @@ def run_serve(args):
     from pwgpu.upf import load_upf
     pps = {"Si": load_upf(SI_UPF), "C": load_upf(os.path.join(ROOT, "tests", "golden", "upf", "C.upf"))}
     reqs = request_stream(args.requests)
-    with Server(workers=4, precision=PRECISION_MIXED, lanes_per_job=2) as srv:
+    with Server(workers=args.workers, precision=PRECISION_MIXED, lanes_per_job=2) as srv:
         recs, wall = run_stream(srv, reqs, pps, precision=PRECISION_MIXED)
         stats = srv.stats()
     summ = summarize(recs, wall)
@@ -258,7 +258,7 @@ def run_serve(args):
     line = {"metric": "serving stream: SCF solves/s and latency (mixed precision)", "value": summ["solves_per_s"],
             "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic (seeded request stream)",
             "config": {"workload": "serving_stream_poisson50", "requests": len(reqs),
-                       "arrival_rate_per_s": 50.0, "workers": 4, "lanes_per_job": 2},
+                       "arrival_rate_per_s": 50.0, "workers": args.workers, "lanes_per_job": 2},
             **summ, "server": stats,
             "accuracy": {"fp64_sample": len(sample), "max_dE_per_atom_ev": max(de) if de else None,
                          "max_dE_per_atom_ha": (max(de) / HA_TO_EV) if de else None}}
@@ -346,6 +346,7 @@ def main():
                     help="once: three untimed H|psi> calls per precision; scf-once: one mixed solve; "
                          "serve: the serving stream through pwgpu_server_* (own JSON line)")
     ap.add_argument("--requests", type=int, default=200, help="serve: requests of the stream replayed")
+    ap.add_argument("--workers", type=int, default=4, help="serve: concurrent jobs on the device")
     args = ap.parse_args()
     world, rank, local = dist_env()
     if args.mode == "serve":

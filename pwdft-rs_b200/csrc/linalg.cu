@@ -13,6 +13,8 @@
 #include <cusolverDn.h>
 
 #include <algorithm>
+#include <mutex>
+#include <set>
 #include <cmath>
 #include <vector>
 
@@ -225,11 +227,19 @@ size_t small_geneig_smem(int m) {
 Status small_geneig_batched(const double2* H, const double2* S, long ld, long stride, int m, int nev, int batch,
                             double* evals, double2* C, long ldc, long cstride, int* status_dev, cudaStream_t s) {
   if (m < 1 || m > kSmallMax || nev < 1 || nev > m) return fail(kInvalid, "small_geneig: size out of range");
-  static bool configured = false;
-  if (!configured) {
-    PW_CUDA_TRY(cudaFuncSetAttribute((const void*)k_small_geneig, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)small_geneig_smem(kSmallMax)));
-    configured = true;
+  // the shared-memory opt-in is a per-device attribute; set it once per device
+  // (lanes and server workers call this from several host threads)
+  {
+    static std::mutex mu;
+    static std::set<int> done;
+    int dev = 0;
+    PW_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    if (!done.count(dev)) {
+      PW_CUDA_TRY(cudaFuncSetAttribute((const void*)k_small_geneig, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)small_geneig_smem(kSmallMax)));
+      done.insert(dev);
+    }
   }
   k_small_geneig<<<batch, 256, small_geneig_smem(m), s>>>(H, S, ld, stride, m, nev, evals, C, ldc, cstride,
                                                           status_dev); count_launch();
