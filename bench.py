@@ -48,6 +48,7 @@ HA_TO_EV = 27.211386245988
 SI_UPF = os.path.join(ROOT, "tests", "golden", "upf", "Si.upf")
 SEED = 20261203
 BATCH = 4  # Si64 cells solved concurrently in one step
+XV_TRAFFIC_BYTES = 33504000 + 5120  # k_xv<float>, one 20-band launch: dram__bytes_read.sum + dram__bytes_write.sum
 
 
 def load_peaks():
@@ -328,7 +329,11 @@ def kernel_bench(local, steps, warmup, flush, hbm_peak, peak_kind):
     ms_launch = own[dom] / nl
     achieved = alg / (ms_launch * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "traffic": None, "peak_kind": peak_kind,
+                "frac": achieved / hbm_peak,
+                # DRAM bytes read + written by one 20-band launch of the mixed x-pass kernel in one
+                # ncu capture (profiles/hpsi_fft_kernels_si64.md); the output stays in L2
+                "traffic": XV_TRAFFIC_BYTES if (dom == "fft_x_inv_v_fwd" and nb // nl == 20) else None,
+                "traffic_unit": "bytes per launch", "peak_kind": peak_kind,
                 "alg_bytes_per_launch": alg, "ms_per_launch": ms_launch,
                 "note": "dominant own kernel of H|psi> (the inner operator of every SCF step); "
                         "alg bytes = compact-grid read+write per band x bands per launch, V(r) FP32 read"}
