@@ -37,6 +37,7 @@ struct GridMaps {
   int* g_to_fft = nullptr;   // n_pw (basis order): flat grid index
   // tile widths chosen for the FFT kernels (lines per block)
   int wz = 1, wy = 1, wx = 1;
+  int wz32 = 1, wy32 = 1, wx32 = 1;  // FP32 tiles: measured at handle creation
 };
 
 struct KPointData {

@@ -19,7 +19,10 @@
 #include <cublas_v2.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
+#include <map>
+#include <tuple>
 #include <mutex>
 #include <numeric>
 #include <set>
@@ -387,6 +390,101 @@ Status configure_kernels() {
 
 }  // namespace
 
+// FP32 tile widths by measurement.  For each axis the candidate widths W
+// that fit the shared memory of an FP64 tile (2 W L 16 bytes <= kMaxDynSmem)
+// -- and, on the x axis, the density kernel's 16 rows per thread -- are timed
+// on this grid with the FP32 kernel of the axis (z-inverse, y-inverse, x pass)
+// over the handle's scratch, the fastest kept.  The kernels compute each line
+// the same way whatever the tile holds, so the choice changes speed only.
+// FP64 tiles keep the heuristic widths (twice the bytes per tile: wider ones
+// cost resident blocks).  Results are cached per device and grid shape (a
+// server builds a handle per job); a failed timing keeps the heuristic.
+static Status autotune_tiles(Handle& h) {
+  GridMaps& g = h.g;
+  const int d0 = g.d[0], d1 = g.d[1], d2 = g.d[2];
+  int dev = 0;
+  PW_CUDA_TRY(cudaGetDevice(&dev));
+  struct Key {
+    int dev, d0, d1, d2, Xp, Yp, ncol;
+    bool operator<(const Key& o) const {
+      return std::tie(dev, d0, d1, d2, Xp, Yp, ncol) < std::tie(o.dev, o.d0, o.d1, o.d2, o.Xp, o.Yp, o.ncol);
+    }
+  };
+  static std::mutex mu;
+  static std::map<Key, std::array<int, 3>> cache;
+  const Key key{dev, d0, d1, d2, g.Xp, g.Yp, g.ncol};
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+      g.wx32 = it->second[0];
+      g.wy32 = it->second[1];
+      g.wz32 = it->second[2];
+      return kOk;
+    }
+  }
+  const int nb = (int)std::max<long>(1, std::min<long>(h.chunk, g.N / std::max(1, h.n_pw)));
+  float2* A = reinterpret_cast<float2*>(h.work_a);
+  float2* B = reinterpret_cast<float2*>(h.work_b);
+  const double2* psi = h.tmp_grid;                               // nb x n_pw <= N entries
+  const float* vr = reinterpret_cast<const float*>(h.tmp_grid);  // N entries
+  const cudaStream_t s = h.stream;
+  cudaEvent_t e0, e1;
+  PW_CUDA_TRY(cudaEventCreate(&e0));
+  PW_CUDA_TRY(cudaEventCreate(&e1));
+  auto fits = [&](int W, int L) { return W >= 1 && W <= kThreads && 2L * W * L * 16 <= kMaxDynSmem; };
+  auto best = [&](const std::vector<int>& cands, int L, int fallback, auto launch) -> int {
+    int arg = fallback;
+    float tbest = 1e30f;
+    for (int W : cands) {
+      if (!fits(W, L)) continue;
+      launch(W);  // warm-up
+      cudaEventRecord(e0, s);
+      for (int r = 0; r < 3; ++r) launch(W);
+      cudaEventRecord(e1, s);
+      if (cudaEventSynchronize(e1) != cudaSuccess) return fallback;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (cudaGetLastError() != cudaSuccess) return fallback;
+      if (ms < tbest) {
+        tbest = ms;
+        arg = W;
+      }
+    }
+    return arg;
+  };
+  const std::vector<int> even = {8, 12, 16, 18, 20, 24, 28, 32, 36, 40, 48};
+  const std::vector<int> odd = {7, 9, 11, 15, 17, 21, 25, 31, 33, 41, 63};
+  std::vector<int> cx;
+  for (int W : even)
+    if (d0 <= 16 * (kThreads / W)) cx.push_back(W);
+  const int wz = best(odd, d2, g.wz, [&](int W) {
+    k_zinv<float><<<dim3((g.ncol + W - 1) / W, nb), block_for(W), 2 * (size_t)W * d2 * sizeof(float2), s>>>(
+        psi, h.n_pw, A, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2, div_magic(d2), g.plan[2], g.tw32[2]);
+  });
+  const int wy = best(even, d1, g.wy, [&](int W) {
+    k_y<float, +1><<<dim3(g.Xp, (d2 + W - 1) / W, nb), block_for(W), 2 * (size_t)W * d1 * sizeof(float2), s>>>(
+        A, B, g.Xp, g.Yp, g.m[1], d1, d2, g.plan[1], g.tw32[1]);
+  });
+  const int wx = best(cx, d0, g.wx, [&](int W) {
+    k_xv<float><<<dim3(d1, (d2 + W - 1) / W, nb), block_for(W), 2 * (size_t)W * d0 * sizeof(float2), s>>>(
+        B, vr, g.Xp, g.m[0], d0, d1, d2, g.plan[0], g.tw32[0]);
+  });
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  PW_CUDA_TRY(cudaStreamSynchronize(s));
+  PW_CUDA_TRY(cudaGetLastError());
+  if (h.trace)
+    std::fprintf(stderr, "pwgpu FP32 tiles %dx%dx%d: x %d y %d z %d (heuristic %d %d %d)\n", d0, d1, d2, wx, wy, wz,
+                 g.wx, g.wy, g.wz);
+  g.wx32 = wx;
+  g.wy32 = wy;
+  g.wz32 = wz;
+  std::lock_guard<std::mutex> lock(mu);
+  cache[key] = {wx, wy, wz};
+  return kOk;
+}
+
 Status build_grid_maps(Handle& h, const int* miller) {
   GridMaps& g = h.g;
   for (int a = 0; a < 3; ++a) {
@@ -456,6 +554,9 @@ Status build_grid_maps(Handle& h, const int* miller) {
   g.wz = odd_w(balance_w(g.ncol, pick_w(g.plan[2], 64)));
   g.wy = balance_w(g.d[2], pick_w(g.plan[1], 32));
   g.wx = balance_w(g.d[2], pick_w(g.plan[0], 32));
+  g.wx32 = g.wx;
+  g.wy32 = g.wy;
+  g.wz32 = g.wz;
   if (Status st0 = configure_kernels(); st0 != kOk) return st0;
   // band chunk: keep A + B of one chunk within ~48 MB (FP64) of L2
   const double per_band = 16.0 * ((double)g.ncol * g.d[2] + (double)g.Xp * g.d[1] * g.d[2]);
@@ -463,7 +564,7 @@ Status build_grid_maps(Handle& h, const int* miller) {
   if ((st = dalloc((double2**)&h.work_a, (size_t)h.chunk * g.ncol * g.d[2])) != kOk) return st;
   if ((st = dalloc((double2**)&h.work_b, (size_t)h.chunk * g.Xp * g.d[1] * g.d[2])) != kOk) return st;
   if ((st = dalloc(&h.tmp_grid, (size_t)g.N)) != kOk) return st;
-  return kOk;
+  return autotune_tiles(h);
 }
 
 Status ensure_nl_capacity(Handle& h, int nb) {
@@ -543,6 +644,9 @@ static Status local_chunk(Handle& h, int spin, int ik, const double2* psi, long 
   using C = cplx<R>;
   GridMaps& g = h.g;
   const int d0 = g.d[0], d1 = g.d[1], d2 = g.d[2];
+  // FP32 tiles use the measured widths, FP64 ones the heuristic widths
+  const bool f32 = std::is_same<R, float>::value;
+  const int wx = f32 ? g.wx32 : g.wx, wy = f32 ? g.wy32 : g.wy, wz = f32 ? g.wz32 : g.wz;
   C* A = reinterpret_cast<C*>(h.work_a);
   C* B = reinterpret_cast<C*>(h.work_b);
   const C* tw0 = std::is_same<R, double>::value ? (const C*)g.tw64[0] : (const C*)g.tw32[0];
@@ -551,32 +655,32 @@ static Status local_chunk(Handle& h, int spin, int ik, const double2* psi, long 
   const R* vr = std::is_same<R, double>::value ? (const R*)h.veff_r[spin] : (const R*)h.veff_r32[spin];
   const double scale = 1.0 / (double)g.N;
   {
-    dim3 grid((g.ncol + g.wz - 1) / g.wz, nb);
-    k_zinv<R><<<grid, block_for(g.wz), 2 * (size_t)g.wz * d2 * sizeof(C), s>>>(
+    dim3 grid((g.ncol + wz - 1) / wz, nb);
+    k_zinv<R><<<grid, block_for(wz), 2 * (size_t)wz * d2 * sizeof(C), s>>>(
         psi, ldpsi, A, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2, div_magic(d2), g.plan[2], tw2); count_launch();
     mark(tm, 0, s);
   }
   {
-    dim3 grid(g.Xp, (d2 + g.wy - 1) / g.wy, nb);
-    k_y<R, +1><<<grid, block_for(g.wy), 2 * (size_t)g.wy * d1 * sizeof(C), s>>>(A, B, g.Xp, g.Yp, g.m[1], d1, d2,
+    dim3 grid(g.Xp, (d2 + wy - 1) / wy, nb);
+    k_y<R, +1><<<grid, block_for(wy), 2 * (size_t)wy * d1 * sizeof(C), s>>>(A, B, g.Xp, g.Yp, g.m[1], d1, d2,
                                                                               g.plan[1], tw1); count_launch();
     mark(tm, 1, s);
   }
   {
-    dim3 grid(d1, (d2 + g.wx - 1) / g.wx, nb);
-    k_xv<R><<<grid, block_for(g.wx), 2 * (size_t)g.wx * d0 * sizeof(C), s>>>(B, vr, g.Xp, g.m[0], d0, d1, d2,
+    dim3 grid(d1, (d2 + wx - 1) / wx, nb);
+    k_xv<R><<<grid, block_for(wx), 2 * (size_t)wx * d0 * sizeof(C), s>>>(B, vr, g.Xp, g.m[0], d0, d1, d2,
                                                                            g.plan[0], tw0); count_launch();
     mark(tm, 2, s);
   }
   {
-    dim3 grid(g.Xp, (d2 + g.wy - 1) / g.wy, nb);
-    k_y<R, -1><<<grid, block_for(g.wy), 2 * (size_t)g.wy * d1 * sizeof(C), s>>>(A, B, g.Xp, g.Yp, g.m[1], d1, d2,
+    dim3 grid(g.Xp, (d2 + wy - 1) / wy, nb);
+    k_y<R, -1><<<grid, block_for(wy), 2 * (size_t)wy * d1 * sizeof(C), s>>>(A, B, g.Xp, g.Yp, g.m[1], d1, d2,
                                                                               g.plan[1], tw1); count_launch();
     mark(tm, 3, s);
   }
   {
-    dim3 grid((g.ncol + g.wz - 1) / g.wz, nb);
-    k_zfwd<R><<<grid, block_for(g.wz), 2 * (size_t)g.wz * d2 * sizeof(C), s>>>(
+    dim3 grid((g.ncol + wz - 1) / wz, nb);
+    k_zfwd<R><<<grid, block_for(wz), 2 * (size_t)wz * d2 * sizeof(C), s>>>(
         A, psi, ldpsi, hpsi, ldh, h.kp[ik].kinetic, scale, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2,
         div_magic(d2), g.plan[2], tw2); count_launch();
     mark(tm, 4, s);
@@ -593,20 +697,23 @@ static void local_chunk_on(Handle& h, int spin, int ik, const double2* psi, long
   using C = cplx<R>;
   GridMaps& g = h.g;
   const int d0 = g.d[0], d1 = g.d[1], d2 = g.d[2];
+  // FP32 tiles use the measured widths, FP64 ones the heuristic widths
+  const bool f32 = std::is_same<R, float>::value;
+  const int wx = f32 ? g.wx32 : g.wx, wy = f32 ? g.wy32 : g.wy, wz = f32 ? g.wz32 : g.wz;
   const bool dbl = std::is_same<R, double>::value;
   const C* tw0 = dbl ? (const C*)g.tw64[0] : (const C*)g.tw32[0];
   const C* tw1 = dbl ? (const C*)g.tw64[1] : (const C*)g.tw32[1];
   const C* tw2 = dbl ? (const C*)g.tw64[2] : (const C*)g.tw32[2];
   const R* vr = dbl ? (const R*)h.veff_r[spin] : (const R*)h.veff_r32[spin];
-  k_zinv<R><<<dim3((g.ncol + g.wz - 1) / g.wz, nb), block_for(g.wz), 2 * (size_t)g.wz * d2 * sizeof(C), s>>>(
+  k_zinv<R><<<dim3((g.ncol + wz - 1) / wz, nb), block_for(wz), 2 * (size_t)wz * d2 * sizeof(C), s>>>(
       psi, ldpsi, A, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2, div_magic(d2), g.plan[2], tw2); count_launch();
-  k_y<R, +1><<<dim3(g.Xp, (d2 + g.wy - 1) / g.wy, nb), block_for(g.wy), 2 * (size_t)g.wy * d1 * sizeof(C), s>>>(
+  k_y<R, +1><<<dim3(g.Xp, (d2 + wy - 1) / wy, nb), block_for(wy), 2 * (size_t)wy * d1 * sizeof(C), s>>>(
       A, B, g.Xp, g.Yp, g.m[1], d1, d2, g.plan[1], tw1); count_launch();
-  k_xv<R><<<dim3(d1, (d2 + g.wx - 1) / g.wx, nb), block_for(g.wx), 2 * (size_t)g.wx * d0 * sizeof(C), s>>>(
+  k_xv<R><<<dim3(d1, (d2 + wx - 1) / wx, nb), block_for(wx), 2 * (size_t)wx * d0 * sizeof(C), s>>>(
       B, vr, g.Xp, g.m[0], d0, d1, d2, g.plan[0], tw0); count_launch();
-  k_y<R, -1><<<dim3(g.Xp, (d2 + g.wy - 1) / g.wy, nb), block_for(g.wy), 2 * (size_t)g.wy * d1 * sizeof(C), s>>>(
+  k_y<R, -1><<<dim3(g.Xp, (d2 + wy - 1) / wy, nb), block_for(wy), 2 * (size_t)wy * d1 * sizeof(C), s>>>(
       A, B, g.Xp, g.Yp, g.m[1], d1, d2, g.plan[1], tw1); count_launch();
-  k_zfwd<R><<<dim3((g.ncol + g.wz - 1) / g.wz, nb), block_for(g.wz), 2 * (size_t)g.wz * d2 * sizeof(C), s>>>(
+  k_zfwd<R><<<dim3((g.ncol + wz - 1) / wz, nb), block_for(wz), 2 * (size_t)wz * d2 * sizeof(C), s>>>(
       A, psi, ldpsi, hpsi, ldh, h.kp[ik].kinetic, 1.0 / (double)g.N, g.col_start, g.pt_ig, g.pt_col, g.pt_z,
       g.ncol, d2, div_magic(d2), g.plan[2], tw2); count_launch();
 }
