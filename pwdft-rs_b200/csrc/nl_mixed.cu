@@ -75,48 +75,51 @@ __global__ void k_build_a2(const double2* __restrict__ b, int n_pw, int n_ch, lo
 
 // B1[j][k], j < 2 nb, k < k1pad: column j = [hi | lo | hi] of
 // [psi_r; psi_i] (j < nb) or [psi_i; -psi_r] (j >= nb), band j mod nb.
+// One grid row per column j (blockIdx.y), threads along k.
 __global__ void k_split_psi(const double2* __restrict__ psi, long ldpsi, int n_pw, int nb, long k1pad,
                             __nv_bfloat16* __restrict__ b1) {
-  const long total = 2L * nb * k1pad;
+  const int j = blockIdx.y;
+  const int part = j >= nb;
+  const long band = part ? j - nb : j;
   const long seg_len = 2L * n_pw;
-  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
-    const long j = t / k1pad, k = t - j * k1pad;
-    __nv_bfloat16 out = __float2bfloat16_rn(0.0f);
+  const double2* col = psi + band * ldpsi;
+  __nv_bfloat16* out = b1 + (long)j * k1pad;
+  for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < k1pad; k += (long)gridDim.x * blockDim.x) {
+    __nv_bfloat16 o = __float2bfloat16_rn(0.0f);
     if (k < 3 * seg_len) {
-      const int part = j >= nb;
-      const long band = part ? j - nb : j;
-      const int seg = (int)(k / seg_len);
+      const int seg = k >= 2 * seg_len ? 2 : (k >= seg_len ? 1 : 0);
       const long r = k - seg * seg_len;
-      const double2 z = psi[(r < n_pw ? r : r - n_pw) + band * ldpsi];
+      const double2 z = col[r < n_pw ? r : r - n_pw];
       const double v = part == 0 ? (r < n_pw ? z.x : z.y) : (r < n_pw ? z.y : -z.x);
       __nv_bfloat16 hi, lo;
       split_bf16(v, hi, lo);
-      out = seg == 1 ? lo : hi;
+      o = seg == 1 ? lo : hi;
     }
-    b1[t] = out;
+    out[k] = o;
   }
 }
 
 // B2[j][k], j < 2 nb, k < k2pad: column j = [hi | lo | hi] of
-// [Q_r; -Q_i] (j < nb) or [Q_i; Q_r] (j >= nb).
+// [Q_r; -Q_i] (j < nb) or [Q_i; Q_r] (j >= nb).  One grid row per column.
 __global__ void k_split_q(const double2* __restrict__ q, int n_ch, int nb, long k2pad, __nv_bfloat16* __restrict__ b2) {
-  const long total = 2L * nb * k2pad;
+  const int j = blockIdx.y;
+  const int part = j >= nb;
+  const long band = part ? j - nb : j;
   const long seg_len = 2L * n_ch;
-  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
-    const long j = t / k2pad, k = t - j * k2pad;
-    __nv_bfloat16 out = __float2bfloat16_rn(0.0f);
+  const double2* col = q + band * n_ch;
+  __nv_bfloat16* out = b2 + (long)j * k2pad;
+  for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < k2pad; k += (long)gridDim.x * blockDim.x) {
+    __nv_bfloat16 o = __float2bfloat16_rn(0.0f);
     if (k < 3 * seg_len) {
-      const int part = j >= nb;
-      const long band = part ? j - nb : j;
-      const int seg = (int)(k / seg_len);
+      const int seg = k >= 2 * seg_len ? 2 : (k >= seg_len ? 1 : 0);
       const long r = k - seg * seg_len;
-      const double2 z = q[(r < n_ch ? r : r - n_ch) + band * n_ch];
+      const double2 z = col[r < n_ch ? r : r - n_ch];
       const double v = part == 0 ? (r < n_ch ? z.x : -z.y) : (r < n_ch ? z.y : z.x);
       __nv_bfloat16 hi, lo;
       split_bf16(v, hi, lo);
-      out = seg == 1 ? lo : hi;
+      o = seg == 1 ? lo : hi;
     }
-    b2[t] = out;
+    out[k] = o;
   }
 }
 
@@ -244,7 +247,8 @@ Status nonlocal_mixed(Handle& h, int ik, const double2* psi, long ldpsi, int nb,
   }
   if ((st = ensure_nl_capacity(h, nb)) != kOk) return st;
   const int n2 = 2 * nb;
-  k_split_psi<<<grid_for((long)n2 * m.k1pad), 256, 0, s>>>(psi, ldpsi, h.n_pw, nb, m.k1pad, m.b1);
+  k_split_psi<<<dim3((unsigned)std::min<long>(64, (m.k1pad + 255) / 256), n2), 256, 0, s>>>(psi, ldpsi, h.n_pw, nb,
+                                                                                          m.k1pad, m.b1);
   count_launch();
   const long slice_stride = (long)m.m1pad * n2;
   if ((st = gemm_bf16_tn_f32(m.a1[ik], m.k1pad, ks, m.b1, m.k1pad, ks, m.d1, m.m1pad, slice_stride, m.m1pad, n2,
@@ -256,7 +260,8 @@ Status nonlocal_mixed(Handle& h, int ik, const double2* psi, long ldpsi, int nb,
   mark(tm, 5, s);
   if ((st = apply_d_blocks(h, nb, s)) != kOk) return st;
   mark(tm, 6, s);
-  k_split_q<<<grid_for((long)n2 * m.k2pad), 256, 0, s>>>(h.nl_q, h.n_ch, nb, m.k2pad, m.b2);
+  k_split_q<<<dim3((unsigned)std::min<long>(64, (m.k2pad + 255) / 256), n2), 256, 0, s>>>(h.nl_q, h.n_ch, nb,
+                                                                                        m.k2pad, m.b2);
   count_launch();
   if ((st = gemm_bf16_tn_f32(m.a2[ik], m.k2pad, 0, m.b2, m.k2pad, 0, m.d2, m.m2pad, 0, (int)m.m2pad, n2,
                              (int)m.k2pad, 1, m.ws, m.ws_bytes, s)) != kOk)
