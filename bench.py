@@ -272,7 +272,7 @@ def kernel_bench(local, steps, warmup, flush, hbm_peak, peak_kind):
     import torch
 
     from pwgpu.lib import PRECISION_FP64, PRECISION_MIXED, PwGpu
-    from pwgpu.workloads import hpsi_system, si64_crystal
+    from pwgpu.workloads import hpsi_algorithmic_bytes, hpsi_system, si64_crystal
     sys_, veff_g, psi = hpsi_system(si64_crystal())
     nb = psi.shape[1]
     n_pw, N = sys_.n_pw, sys_.n_grid
@@ -337,6 +337,17 @@ def kernel_bench(local, steps, warmup, flush, hbm_peak, peak_kind):
                 "alg_bytes_per_launch": alg, "ms_per_launch": ms_launch,
                 "note": "dominant own kernel of H|psi> (the inner operator of every SCF step); "
                         "alg bytes = compact-grid read+write per band x bands per launch, V(r) FP32 read"}
+    # the whole local H|psi> (the five FFT kernels) against its per-band algorithmic bytes
+    # 2c n_pw + 4c N + (c/2) N, c = 8 B (FP32 complex)
+    pipe_bytes = hpsi_algorithmic_bytes(n_pw, N, 8) * nb
+    fft_stages = ("fft_z_inv_scatter", "fft_y_inv", "fft_x_inv_v_fwd", "fft_y_fwd", "fft_z_fwd_gather")
+    pipe_ms = sum(p["stage_ms"][k] for k in fft_stages)
+    pipe_gbs = pipe_bytes / (pipe_ms * 1e-3) / 1e9
+    roofline["local_hpsi"] = {"bound": "hbm", "achieved": pipe_gbs, "peak": hbm_peak, "unit": "GB/s",
+                              "frac": pipe_gbs / hbm_peak, "alg_bytes_per_block": pipe_bytes, "ms_per_block": pipe_ms,
+                              "bands": nb,
+                              "note": "five FFT kernels of one mixed H|psi> block, per-band bytes "
+                                      "2c n_pw + 4c N + (c/2) N with c = 8 B"}
     return out, roofline, {"n_pw": n_pw, "grid": [d0, d1, d2], "n_bands": nb, "n_ch": 256}
 
 
