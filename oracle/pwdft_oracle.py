@@ -225,6 +225,25 @@ def symmetrize_density(rho_r, dims, src, arg):
     return (ifft3(acc, dims) / rg.size).real.copy()
 
 
+def symmetrize_real_space(rho_r, dims, symmetry):
+    """Real-space symmetrisation on the grid points, the reference's test
+    helper `symmetrize_real_ref` (symmetry/density/g_space.rs:278-323):
+    rho_sym(r) = (1/N_ops) sum_S rho(S^-1 r), S^-1 = (R^-1, -R^-1 tau) on
+    fractional coordinates, each image rounded to its nearest grid point.
+    Equal to the G-space form only where every image lands on a grid point
+    (Si Fd-3m: grid sizes divisible by 4)."""
+    d = np.array(dims, dtype=np.int64)
+    idx = np.indices(tuple(dims)).reshape(3, -1).T.astype(np.float64)
+    f = idx / d
+    out = np.zeros(rho_r.size)
+    for op in symmetry.operations:
+        rinv = np.rint(np.linalg.inv(np.array(op.rotation, dtype=np.float64)))
+        tinv = -rinv @ np.array(op.translation, dtype=np.float64)
+        j = np.rint((f @ rinv.T + tinv) * d).astype(np.int64) % d
+        out += rho_r[(j[:, 0] * d[1] + j[:, 1]) * d[2] + j[:, 2]]
+    return out / symmetry.n_ops
+
+
 # ---------------------------------------------------------------------------
 # Potentials and XC (energy.rs:293-358, xc.rs:129-596)
 # ---------------------------------------------------------------------------

@@ -130,3 +130,38 @@ def test_energy_components_match_reference_pins(si_pp):
     assert abs(direct - r.total_energy) < 1e-5
     band = c["e_kinetic"] + c["e_local"] + c["e_nonlocal"] + 2.0 * c["e_hartree"] + c["e_vxc"]
     assert abs(band - c["e_band"]) < 1e-7
+
+
+def test_qe_validation_si_full_mesh(si_pp):
+    """Si diamond, 15 Ry, full 4x4x4 Gamma-centred mesh (64 points, as the
+    reference's QE comparison passes it), 8 bands, Fermi-Dirac 0.01 Ry,
+    beta 0.3, ndim 8 (tests/qe_validation.rs:146-250, 376-510): the total
+    energy pin -231.6544 eV to 1 meV (:460-510), E_F 6.3449 eV to 30 meV,
+    QE's -17.02299344 Ry to 60 meV and its one-electron sum 4.86744632 Ry
+    to 80 meV (:393-458)."""
+    from pwgpu.crystal import monkhorst_pack
+    cr = diamond_primitive("Si", 5.431)
+    sym = SymmetryInfo.from_crystal(cr, 1e-5)
+    s = build_system(cr, {"Si": si_pp}, 15.0 * RY_TO_EV, monkhorst_pack((4, 4, 4), "gamma", cr.lattice), sym)
+    r = O.run_scf_unpolarized(s, 8, max_iter=80, conv_threshold=1e-8, energy_threshold=1e-6, mixing_beta=0.3,
+                              mixing_ndim=8, smearing="fermi_dirac", sigma=0.01 * RY_TO_EV)
+    assert r.n_iterations < 80
+    assert abs(r.total_energy - (-231.6544)) < 1e-3
+    assert abs(r.fermi_energy - 6.3449) < 0.030
+    assert abs(r.total_energy - (-17.02299344 * RY_TO_EV)) < 0.060
+    c = r.components
+    assert abs(c["e_kinetic"] + c["e_local"] + c["e_nonlocal"] - 4.86744632 * RY_TO_EV) < 0.080
+
+
+def test_symmetrizers_agree_on_compatible_grid():
+    """The oracle's G-space symmetrisation equals its restatement of the
+    reference's real-space helper on a 12^3 grid, where Si's tau = (1/4,
+    1/4, 1/4) lands on grid points (symmetry/density/g_space.rs:457-486)."""
+    cr = diamond_primitive("Si", 5.431)
+    sym = SymmetryInfo.from_crystal(cr, 1e-5)
+    dims = (12, 12, 12)
+    rho0 = np.abs(np.sin(np.arange(12 ** 3) * 0.23)) + 0.05
+    src, arg = O.gather_map(dims, [(op.rotation, op.translation) for op in sym.operations])
+    got = O.symmetrize_density(rho0, dims, src, arg)
+    want = O.symmetrize_real_space(rho0, dims, sym)
+    assert np.max(np.abs(got - want)) < 1e-10 * max(np.max(want), 1.0)

@@ -1,0 +1,144 @@
+"""Analytic and property checks of the device path, after the reference's
+own tests on the same quantities:
+
+* free-electron bands (tests/free_electron_bands.rs:90-140): with V = 0
+  and no projectors the eigenvalues are the sorted (hbar^2/2m)|k+G|^2 at
+  the fcc high-symmetry points, relative 1e-8;
+* the FFT round trip inside H|psi> (fft.rs:285-339): a constant potential
+  c gives H psi = (T + c) psi, so the zero-padded inverse, the forward
+  transform, 1/N and the sphere gather compose to the identity;
+* G-space symmetrisation (symmetry/density/g_space.rs:340-553):
+  idempotent on a band-limited 18^3 density, equal to the real-space form
+  on the compatible 12^3 grid, a fixed point on a pre-symmetrised density,
+  the integral and a uniform density preserved, identity-only a bit-exact
+  no-op;
+* the Si 4x4x4 Gamma-centred QE-validation case (tests/qe_validation.rs:
+  376-510) on the full 64-point mesh: -231.6544 eV to 1 meV, E_F 6.3449 eV
+  to 30 meV, QE's -17.02299344 Ry to 60 meV, and the oracle's energy."""
+
+import numpy as np
+import pytest
+
+from conftest import rng
+from oracle import pwdft_oracle as O
+from pwgpu.consts import RY_TO_EV
+from pwgpu.context import Projectors, build_system
+from pwgpu.crystal import KPoint, diamond_primitive, gamma_only, monkhorst_pack
+from pwgpu.lib import PRECISION_FP64, PRECISION_MIXED, PwGpu
+from pwgpu.symmetry import SymmetryInfo
+
+pytestmark = pytest.mark.gpu
+
+HIGH_SYM = {"G": (0.0, 0.0, 0.0), "X": (0.5, 0.0, 0.5), "L": (0.5, 0.5, 0.5), "W": (0.5, 0.25, 0.75),
+            "K": (0.375, 0.375, 0.75), "U": (0.625, 0.25, 0.625)}
+
+
+def without_nonlocal(s):
+    """The same system with every KB coupling D set to zero."""
+    s.projectors = [Projectors(p.b, [np.zeros_like(blk) for blk in p.d_blocks], p.atom_ch_start)
+                    for p in s.projectors]
+    return s
+
+
+def test_free_electron_eigenvalues_match_analytic(si_pp):
+    cr = diamond_primitive("Si", 5.431)
+    rec = cr.lattice.reciprocal()
+    kps = [KPoint(f[0] * rec.a + f[1] * rec.b + f[2] * rec.c, 1.0 / len(HIGH_SYM)) for f in HIGH_SYM.values()]
+    s = without_nonlocal(build_system(cr, {"Si": si_pp}, 100.0, kps, SymmetryInfo.identity_only()))
+    with PwGpu(s) as dev:
+        dev.set_veff_g(np.zeros(s.n_grid, dtype=np.complex128))
+        for ik, label in enumerate(HIGH_SYM):
+            ev, psi, _, _ = dev.eigensolve(15, ik=ik, tol=1e-9)
+            want = np.sort(s.kinetic[ik])[:15]
+            assert np.all(np.abs(ev - want) <= 1e-8 * np.maximum(np.abs(want), 1.0)), (label, ev, want)
+            assert np.max(np.abs(psi.conj().T @ psi - np.eye(15))) < 1e-10
+
+
+@pytest.mark.parametrize("precision,tol", [(PRECISION_FP64, 1e-12), (PRECISION_MIXED, 1e-5)])
+def test_constant_potential_gives_kinetic_plus_constant(si_pp, precision, tol):
+    s = without_nonlocal(build_system(diamond_primitive("Si", 5.431), {"Si": si_pp}, 150.0,
+                                      [KPoint(np.array([0.1, -0.2, 0.15]), 1.0)], SymmetryInfo.identity_only()))
+    c = -3.7
+    veff = np.zeros(s.n_grid, dtype=np.complex128)
+    veff[0] = c  # V(r) = sum_G V(G) e^{iGr} = c
+    g = rng(21)
+    psi = g.standard_normal((s.n_pw, 12)) + 1j * g.standard_normal((s.n_pw, 12))
+    psi /= np.linalg.norm(psi, axis=0)
+    with PwGpu(s, precision=precision) as dev:
+        dev.set_veff_g(veff)
+        hpsi = dev.apply_h(psi)
+    want = (s.kinetic[0] + c)[:, None] * psi
+    assert np.max(np.abs(hpsi - want)) < tol * np.max(np.abs(want))
+
+
+def band_limited_density(dims):
+    """Real density with Fourier support |m_i| <= 2 (cosine modes)."""
+    modes = [((0, 0, 0), 1.0), ((1, 0, 0), 0.17), ((0, 1, 0), 0.11), ((0, 0, 1), 0.13), ((1, 1, 0), 0.07),
+             ((1, 0, 1), 0.05), ((1, 1, 1), 0.04), ((2, 0, 0), 0.03)]
+    f = [np.arange(n) / n for n in dims]
+    fx, fy, fz = np.meshgrid(*f, indexing="ij")
+    s = sum(a * np.cos(2 * np.pi * (m[0] * fx + m[1] * fy + m[2] * fz)) for m, a in modes)
+    return (np.abs(s) + 0.5).ravel()
+
+
+def si_fd3m(si_pp, dims):
+    cr = diamond_primitive("Si", 5.431)
+    sym = SymmetryInfo.from_crystal(cr, 1e-5)
+    assert sym.n_ops == 48
+    return build_system(cr, {"Si": si_pp}, 20.0, gamma_only(), sym, fft_grid=dims), sym
+
+
+def test_symmetrize_idempotent_band_limited_18(si_pp):
+    s, _ = si_fd3m(si_pp, (18, 18, 18))
+    rho = band_limited_density(s.dims)
+    with PwGpu(s) as dev:
+        once = dev.symmetrize(rho)
+        twice = dev.symmetrize(once)
+    assert np.max(np.abs(twice - once)) < 1e-12 * max(np.max(once), 1.0)
+
+
+def test_symmetrize_matches_real_space_on_compatible_grid(si_pp):
+    s, sym = si_fd3m(si_pp, (12, 12, 12))
+    rho0 = np.abs(np.sin(np.arange(s.n_grid) * 0.23)) + 0.05
+    want = O.symmetrize_real_space(rho0, s.dims, sym)
+    pre = O.symmetrize_real_space(np.abs(np.sin(np.arange(s.n_grid) * 0.17)) + 0.01, s.dims, sym)
+    with PwGpu(s) as dev:
+        got = dev.symmetrize(rho0)
+        fixed = dev.symmetrize(pre)
+    assert np.max(np.abs(got - want)) < 1e-10 * max(np.max(want), 1.0)
+    assert np.max(np.abs(fixed - pre)) < 1e-10 * max(np.max(pre), 1.0)
+
+
+def test_symmetrize_preserves_integral_and_uniform(si_pp):
+    s, _ = si_fd3m(si_pp, (18, 18, 18))
+    rho = np.abs(np.sin(np.arange(s.n_grid) * 0.37)) + 0.1
+    with PwGpu(s) as dev:
+        got = dev.symmetrize(rho)
+        uni = dev.symmetrize(np.ones(s.n_grid))
+    assert abs(got.sum() - rho.sum()) <= 1e-9 * abs(rho.sum())
+    assert np.max(np.abs(uni - 1.0)) < 1e-12
+
+
+def test_symmetrize_identity_only_is_bit_exact_noop(si_pp):
+    s = build_system(diamond_primitive("Si", 5.431), {"Si": si_pp}, 20.0, gamma_only(),
+                     SymmetryInfo.identity_only(), fft_grid=(8, 8, 8))
+    rho = np.sin(np.arange(s.n_grid) * 0.13) + 1.0
+    with PwGpu(s) as dev:
+        got = dev.symmetrize(rho)
+    assert np.array_equal(got.view(np.uint64), rho.view(np.uint64))
+
+
+def test_qe_validation_si_full_mesh(si_pp):
+    cr = diamond_primitive("Si", 5.431)
+    sym = SymmetryInfo.from_crystal(cr, 1e-5)
+    s = build_system(cr, {"Si": si_pp}, 15.0 * RY_TO_EV, monkhorst_pack((4, 4, 4), "gamma", cr.lattice), sym)
+    kw = dict(max_iter=80, conv_threshold=1e-8, energy_threshold=1e-6, mixing_beta=0.3, mixing_ndim=8,
+              smearing="fermi_dirac", sigma=0.01 * RY_TO_EV)
+    ref = O.run_scf_unpolarized(s, 8, **kw)
+    with PwGpu(s, lanes=8) as dev:
+        res, _, _, _ = dev.scf_run(s.rho_init_r, 8, diag_tol=1e-10, **kw)
+    assert res["converged"] == 1
+    assert abs(res["total_energy"] - (-231.6544)) < 1e-3
+    assert abs(res["fermi_energy"] - 6.3449) < 0.030
+    assert abs(res["total_energy"] - (-17.02299344 * RY_TO_EV)) < 0.060
+    assert abs(res["total_energy"] - ref.total_energy) < 1e-5
