@@ -165,3 +165,29 @@ def test_symmetrizers_agree_on_compatible_grid():
     got = O.symmetrize_density(rho0, dims, src, arg)
     want = O.symmetrize_real_space(rho0, dims, sym)
     assert np.max(np.abs(got - want)) < 1e-10 * max(np.max(want), 1.0)
+
+
+def test_real_ylm_addition_theorem():
+    """sum_m Y_lm(q1) Y_lm(q2) = (2l+1)/(4 pi) P_l(q1.q2) for l <= 5 on the
+    reference's q-vector set (potential/nonlocal.rs:964-1002), 1e-12."""
+    from numpy.polynomial import legendre
+    from pwgpu.context import real_sph_harmonics
+    qs = np.array([[0.3, 0.7, -0.5], [-1.1, 0.2, 0.4], [0.0, 0.0, 1.0], [1.0, 0.0, 0.0]])
+    y = real_sph_harmonics(qs, 5)
+    for i in range(len(qs)):
+        for j in range(len(qs)):
+            cos_t = qs[i] @ qs[j] / (np.linalg.norm(qs[i]) * np.linalg.norm(qs[j]))
+            for l in range(6):
+                lhs = y[i, l * l:(l + 1) ** 2] @ y[j, l * l:(l + 1) ** 2]
+                rhs = (2 * l + 1) / (4 * math.pi) * legendre.legval(cos_t, [0.0] * l + [1.0])
+                assert abs(lhs - rhs) < 1e-12, (l, lhs, rhs)
+
+
+def test_nlcc_double_counting_sign_probe():
+    """Two-point synthetic probe of the NLCC double counting (scf/energy.rs:
+    870-918): E_xc integrates eps_xc over rho_val + rho_core, the subtraction
+    over rho_val only; -1.7 eV to 1e-12."""
+    rho_val = np.array([0.5, 1.5])
+    rho_core = np.array([0.1, 0.3])
+    got = O.xc_energy_corrected(rho_val + rho_core, rho_val, np.array([-1.0, -2.0]), np.array([-0.5, -1.5]), 2.0)
+    assert abs(got - (-1.7)) < 1e-12

@@ -142,3 +142,38 @@ def test_qe_validation_si_full_mesh(si_pp):
     assert abs(res["fermi_energy"] - 6.3449) < 0.030
     assert abs(res["total_energy"] - (-17.02299344 * RY_TO_EV)) < 0.060
     assert abs(res["total_energy"] - ref.total_energy) < 1e-5
+
+
+@pytest.mark.parametrize("on_device", [False, True])
+def test_single_l2_channel_matrix_element(si_pp, on_device):
+    """Si ONCV with every D_ij zero except the first l = 2 projector's D_44,
+    one atom at the origin of a cubic cell a = 2 pi (b_i = e_i), Gamma, 50 eV
+    (potential/nonlocal.rs:870-962): H_NL[(1,0,1), (2,0,1)] =
+    D_44 / Omega F_4(sqrt 2) F_4(sqrt 5) 17 / (16 pi), to 1e-10; read from
+    H applied to a unit vector with V = 0 (T is diagonal), for the host-
+    and the device-built projectors."""
+    import dataclasses
+    import math
+    from pwgpu.crystal import Atom, Crystal, Lattice
+    from pwgpu.upf import beta_form_factor
+    assert si_pp.beta_l[4] == 2
+    d44 = si_pp.dij.reshape(6, 6)[4, 4]
+    dij = np.zeros(36)
+    dij[4 * 6 + 4] = d44
+    pp = dataclasses.replace(si_pp, dij=dij)
+    a = 2.0 * math.pi
+    cr = Crystal(Lattice(np.array([a, 0.0, 0.0]), np.array([0.0, a, 0.0]), np.array([0.0, 0.0, a])),
+                 [Atom("Si", (0.0, 0.0, 0.0))])
+    s = build_system(cr, {"Si": pp}, 50.0, [KPoint(np.zeros(3), 1.0)], SymmetryInfo.identity_only(),
+                     projectors_on_device=on_device)
+    mil = np.asarray(s.basis.miller)
+    i1 = int(np.flatnonzero((mil == (1, 0, 1)).all(axis=1))[0])
+    i2 = int(np.flatnonzero((mil == (2, 0, 1)).all(axis=1))[0])
+    e2 = np.zeros((s.n_pw, 1), dtype=np.complex128)
+    e2[i2, 0] = 1.0
+    with PwGpu(s, precision=PRECISION_FP64) as dev:
+        dev.set_veff_g(np.zeros(s.n_grid, dtype=np.complex128))
+        col = dev.apply_h(e2)[:, 0]
+    f = beta_form_factor(pp, 4, np.array([math.sqrt(2.0), math.sqrt(5.0)]))
+    want = d44 / cr.lattice.volume() * f[0] * f[1] * 17.0 / (16.0 * math.pi)
+    assert abs(col[i1] - want) < 1e-10 * max(abs(want), 1.0), (col[i1], want)
