@@ -135,16 +135,20 @@ __global__ void __launch_bounds__(kThreads) k_y(cplx<R>* __restrict__ A, cplx<R>
   const long ncol = (long)Xp * Yp;
   C* a_base = A + ((long)b * ncol + (long)p * Yp) * d2 + z0 + w;
   C* b_base = B + (((long)b * Xp + p) * d1) * d2 + z0 + w;
+  // rows copied asynchronously (all in flight at once), missing rows zero-filled
   if (S > 0) {
     // row y holds compact row q = y + m1 (y <= m1) or y - d1 + m1 (y >= d1 - m1), else zero
     for (int y = threadIdx.y; y < d1; y += blockDim.y) {
       const int q = y <= m1 ? y + m1 : (y >= d1 - m1 ? y - d1 + m1 : -1);
-      buf[y * W + w] = (live && q >= 0) ? a_base[(long)q * d2] : cmake<C>(0.0, 0.0);
+      const bool ok = live && q >= 0;
+      cp_async_zfill<sizeof(C)>(&buf[y * W + w], ok ? (const void*)(a_base + (long)q * d2) : (const void*)A, ok);
     }
   } else {
     for (int y = threadIdx.y; y < d1; y += blockDim.y)
-      buf[y * W + w] = live ? b_base[(long)y * d2] : cmake<C>(0.0, 0.0);
+      cp_async_zfill<sizeof(C)>(&buf[y * W + w], live ? (const void*)(b_base + (long)y * d2) : (const void*)B, live);
   }
+  cp_async_commit();
+  cp_async_wait<0>();
   __syncthreads();
   const C* res = fft_lines<S>(buf, scr, py, W, twy);
   if (!live) return;
@@ -161,30 +165,55 @@ template <typename R>
 __global__ void __launch_bounds__(kThreads) k_xv(cplx<R>* __restrict__ B, const R* __restrict__ vr, int Xp, int m0,
                                                 int d0, int d1, int d2, FftPlan px, const cplx<R>* __restrict__ twx) {
   using C = cplx<R>;
+  // FP32 tiles also stage their V(r) rows in shared memory (xv_smem)
+  constexpr bool kStageV = std::is_same<R, float>::value;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int W = blockDim.x;
   const int w = threadIdx.x;
   C* buf = reinterpret_cast<C*>(smem_raw);
   C* scr = buf + d0 * W;
+  R* vt = reinterpret_cast<R*>(scr + d0 * W);
   const int y = blockIdx.x;
   const int z0 = blockIdx.y * W;
   const int b = blockIdx.z;
   const bool live = w < d2 - z0;
   const long plane = (long)d1 * d2;
   C* base = B + (long)b * Xp * plane + (long)y * d2 + z0 + w;
+  const R* vb = vr + (long)y * d2 + z0 + w;
+  // every row of the tile in flight at once: asynchronous copies, rows
+  // outside the compact x range (and columns past d2) zero-filled
   for (int x = threadIdx.y; x < d0; x += blockDim.y) {
     const int q = x <= m0 ? x + m0 : (x >= d0 - m0 ? x - d0 + m0 : -1);
-    buf[x * W + w] = (live && q >= 0) ? base[(long)q * plane] : cmake<C>(0.0, 0.0);
+    const bool ok = live && q >= 0;
+    cp_async_zfill<sizeof(C)>(&buf[x * W + w], ok ? (const void*)(base + (long)q * plane) : (const void*)B, ok);
+  }
+  cp_async_commit();
+  if constexpr (kStageV) {
+    for (int x = threadIdx.y; x < d0; x += blockDim.y)
+      cp_async_zfill<sizeof(R)>(&vt[x * W + w], live ? (const void*)(vb + (long)x * plane) : (const void*)vr, live);
+    cp_async_commit();
+    cp_async_wait<1>();  // the tile; the V rows may still be arriving
+  } else {
+    cp_async_wait<0>();
   }
   __syncthreads();
   C* r1 = fft_lines<+1>(buf, scr, px, W, twx);
-  const R* vb = vr + (long)y * d2 + z0 + w;
+  if constexpr (kStageV) {
+    cp_async_wait<0>();
+    __syncthreads();
+  }
   for (int x = threadIdx.y; x < d0; x += blockDim.y)
-    if (live) r1[x * W + w] = r1[x * W + w] * vb[(long)x * plane];
+    if (live) r1[x * W + w] = r1[x * W + w] * (kStageV ? vt[x * W + w] : vb[(long)x * plane]);
   __syncthreads();
   const C* r2 = fft_lines<-1>(r1, r1 == buf ? scr : buf, px, W, twx);
   if (!live) return;
   for (int q = threadIdx.y; q < Xp; q += blockDim.y) base[(long)q * plane] = r2[wrap_idx(q - m0, d0) * W + w];
+}
+
+// Shared memory of a k_xv tile: two W x d0 line buffers, plus the V(r) rows
+// for FP32 tiles
+template <typename R> inline size_t xv_smem(int W, int d0) {
+  return 2 * (size_t)W * d0 * sizeof(cplx<R>) + (std::is_same<R, float>::value ? (size_t)W * d0 * sizeof(float) : 0);
 }
 
 // Density: for each band of the chunk, compact x rows of B -> x-inverse ->
@@ -467,7 +496,7 @@ static Status autotune_tiles(Handle& h) {
         A, B, g.Xp, g.Yp, g.m[1], d1, d2, g.plan[1], g.tw32[1]);
   });
   const int wx = best(cx, d0, g.wx, [&](int W) {
-    k_xv<float><<<dim3(d1, (d2 + W - 1) / W, nb), block_for(W), 2 * (size_t)W * d0 * sizeof(float2), s>>>(
+    k_xv<float><<<dim3(d1, (d2 + W - 1) / W, nb), block_for(W), xv_smem<float>(W, d0), s>>>(
         B, vr, g.Xp, g.m[0], d0, d1, d2, g.plan[0], g.tw32[0]);
   });
   cudaEventDestroy(e0);
@@ -668,7 +697,7 @@ static Status local_chunk(Handle& h, int spin, int ik, const double2* psi, long 
   }
   {
     dim3 grid(d1, (d2 + wx - 1) / wx, nb);
-    k_xv<R><<<grid, block_for(wx), 2 * (size_t)wx * d0 * sizeof(C), s>>>(B, vr, g.Xp, g.m[0], d0, d1, d2,
+    k_xv<R><<<grid, block_for(wx), xv_smem<R>(wx, d0), s>>>(B, vr, g.Xp, g.m[0], d0, d1, d2,
                                                                            g.plan[0], tw0); count_launch();
     mark(tm, 2, s);
   }
@@ -709,7 +738,7 @@ static void local_chunk_on(Handle& h, int spin, int ik, const double2* psi, long
       psi, ldpsi, A, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2, div_magic(d2), g.plan[2], tw2); count_launch();
   k_y<R, +1><<<dim3(g.Xp, (d2 + wy - 1) / wy, nb), block_for(wy), 2 * (size_t)wy * d1 * sizeof(C), s>>>(
       A, B, g.Xp, g.Yp, g.m[1], d1, d2, g.plan[1], tw1); count_launch();
-  k_xv<R><<<dim3(d1, (d2 + wx - 1) / wx, nb), block_for(wx), 2 * (size_t)wx * d0 * sizeof(C), s>>>(
+  k_xv<R><<<dim3(d1, (d2 + wx - 1) / wx, nb), block_for(wx), xv_smem<R>(wx, d0), s>>>(
       B, vr, g.Xp, g.m[0], d0, d1, d2, g.plan[0], tw0); count_launch();
   k_y<R, -1><<<dim3(g.Xp, (d2 + wy - 1) / wy, nb), block_for(wy), 2 * (size_t)wy * d1 * sizeof(C), s>>>(
       A, B, g.Xp, g.Yp, g.m[1], d1, d2, g.plan[1], tw1); count_launch();

@@ -39,6 +39,24 @@ template <int S, typename C> __host__ __device__ __forceinline__ C mul_si(C a) {
   return c;
 }
 
+// Asynchronous global -> shared copy of one element of Bytes (4, 8 or 16)
+// bytes (cp.async, no register staging); with valid false nothing is read
+// and the destination is zero-filled.  Both addresses aligned to Bytes.
+template <int Bytes>
+__device__ __forceinline__ void cp_async_zfill(void* smem_dst, const void* gmem_src, bool valid) {
+  static_assert(Bytes == 4 || Bytes == 8 || Bytes == 16, "cp.async copies 4, 8 or 16 bytes");
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
+  const int src_bytes = valid ? Bytes : 0;
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(dst), "l"(gmem_src), "n"(Bytes),
+               "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// wait until at most N of this thread's committed copy groups are pending
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // Maximum number of radix stages per 1-D length (2,3,5-smooth lengths up to
 // 1024 need at most 5 with radices 2,3,4,5,8,9).
 constexpr int kMaxStages = 6;
