@@ -452,7 +452,10 @@ static Status autotune_tiles(Handle& h) {
       return kOk;
     }
   }
-  const int nb = (int)std::max<long>(1, std::min<long>(h.chunk, g.N / std::max(1, h.n_pw)));
+  // FP32 launches carry 2 chunk bands (the scratch is sized for FP64
+  // chunks); the z kernel reads its psi rows from tmp_grid (N entries)
+  const int nb = 2 * h.chunk;
+  const int nb_in = (int)std::max<long>(1, std::min<long>(nb, g.N / std::max(1, h.n_pw)));
   float2* A = reinterpret_cast<float2*>(h.work_a);
   float2* B = reinterpret_cast<float2*>(h.work_b);
   const double2* psi = h.tmp_grid;                               // nb x n_pw <= N entries
@@ -469,7 +472,7 @@ static Status autotune_tiles(Handle& h) {
       if (!fits(W, L)) continue;
       launch(W);  // warm-up
       cudaEventRecord(e0, s);
-      for (int r = 0; r < 3; ++r) launch(W);
+      for (int r = 0; r < 5; ++r) launch(W);
       cudaEventRecord(e1, s);
       if (cudaEventSynchronize(e1) != cudaSuccess) return fallback;
       float ms = 0.f;
@@ -488,7 +491,7 @@ static Status autotune_tiles(Handle& h) {
   for (int W : even)
     if (d0 <= 16 * (kThreads / W)) cx.push_back(W);
   const int wz = best(odd, d2, g.wz, [&](int W) {
-    k_zinv<float><<<dim3((g.ncol + W - 1) / W, nb), block_for(W), 2 * (size_t)W * d2 * sizeof(float2), s>>>(
+    k_zinv<float><<<dim3((g.ncol + W - 1) / W, nb_in), block_for(W), 2 * (size_t)W * d2 * sizeof(float2), s>>>(
         psi, h.n_pw, A, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2, div_magic(d2), g.plan[2], g.tw32[2]);
   });
   const int wy = best(even, d1, g.wy, [&](int W) {
