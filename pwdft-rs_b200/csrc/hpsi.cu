@@ -98,10 +98,13 @@ __global__ void __launch_bounds__(kThreads) k_zfwd(const cplx<R>* __restrict__ A
   const int tid = threadIdx.y * W + threadIdx.x;
   const int T = W * blockDim.y;
   const C* in = A + ((long)b * ncol + c0) * d2;
+  // asynchronous copies, columns past the last one zero-filled
   for (int i = tid; i < W * d2; i += T) {
     const int c = fast_div(i, d2, md2), e = i - c * d2;
-    buf[e * W + c] = (c < nl) ? in[i] : cmake<C>(0.0, 0.0);
+    cp_async_zfill<sizeof(C)>(&buf[e * W + c], c < nl ? (const void*)(in + i) : (const void*)A, c < nl);
   }
+  cp_async_commit();
+  cp_async_wait<0>();
   __syncthreads();
   const C* res = fft_lines<-1>(buf, scr, pz, W, twz);
   const double2* ps = psi + (long)b * ldpsi;
@@ -240,8 +243,11 @@ __global__ void __launch_bounds__(kThreads) k_x_density(const double2* __restric
     const double2* base = B + (long)b * Xp * plane + (long)y * d2 + z0 + w;
     for (int x = threadIdx.y; x < d0; x += blockDim.y) {
       const int q = x <= m0 ? x + m0 : (x >= d0 - m0 ? x - d0 + m0 : -1);
-      buf[x * W + w] = (live && q >= 0) ? base[(long)q * plane] : make_double2(0.0, 0.0);
+      const bool ok = live && q >= 0;
+      cp_async_zfill<16>(&buf[x * W + w], ok ? (const void*)(base + (long)q * plane) : (const void*)B, ok);
     }
+    cp_async_commit();
+    cp_async_wait<0>();
     __syncthreads();
     const double2* res = fft_lines<+1>(buf, scr, px, W, twx);
     const double f = fw[b];
