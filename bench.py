@@ -48,7 +48,11 @@ HA_TO_EV = 27.211386245988
 SI_UPF = os.path.join(ROOT, "tests", "golden", "upf", "Si.upf")
 SEED = 20261203
 BATCH = 4  # Si64 cells solved concurrently in one step
-XV_TRAFFIC_BYTES = 33504000 + 5120  # k_xv<float>, one 20-band launch: dram__bytes_read.sum + dram__bytes_write.sum
+# k_xv<float> on the 72^3 grid, one 22-band launch in one ncu capture:
+# dram__bytes_read.sum + dram__bytes_write.sum.  It is the compact input of
+# each band plus one FP32 V(r) read (the output stays in L2), so it is scaled
+# to a launch's band count as (capture - V) / 22 per band + V.
+XV_TRAFFIC_CAPTURE = (33503744 + 3072, 22)
 
 
 def load_peaks():
@@ -328,12 +332,17 @@ def kernel_bench(local, steps, warmup, flush, hbm_peak, peak_kind):
     alg = per_band * nb / nl
     ms_launch = own[dom] / nl
     achieved = alg / (ms_launch * 1e-3) / 1e9
+    traffic = None
+    if dom == "fft_x_inv_v_fwd" and (d0, d1, d2) == (72, 72, 72):
+        cap, cap_bands = XV_TRAFFIC_CAPTURE
+        v_bytes = 4.0 * N
+        traffic = (cap - v_bytes) / cap_bands * (nb / nl) + v_bytes
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved / hbm_peak,
-                # DRAM bytes read + written by one 20-band launch of the mixed x-pass kernel in one
-                # ncu capture (profiles/hpsi_fft_kernels_si64.md); the output stays in L2
-                "traffic": XV_TRAFFIC_BYTES if (dom == "fft_x_inv_v_fwd" and nb // nl == 20) else None,
-                "traffic_unit": "bytes per launch", "peak_kind": peak_kind,
+                # DRAM bytes of the mixed x-pass kernel from one ncu capture of a 22-band launch
+                # (profiles/hpsi_fft_kernels_si64.md), scaled to this launch's average band count
+                "traffic": traffic, "traffic_unit": "bytes per launch (ncu capture of 22 bands, scaled by bands)",
+                "peak_kind": peak_kind,
                 "alg_bytes_per_launch": alg, "ms_per_launch": ms_launch,
                 "note": "dominant own kernel of H|psi> (the inner operator of every SCF step); "
                         "alg bytes = compact-grid read+write per band x bands per launch, V(r) FP32 read"}
