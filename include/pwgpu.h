@@ -296,6 +296,17 @@ pwgpu_status pwgpu_mix(pwgpu_handle* h, int32_t channel, int32_t mode, const dou
                        double* rho_next, double beta, int32_t ndim, int32_t period, double q_tf);
 pwgpu_status pwgpu_mix_reset(pwgpu_handle* h);
 
+/* Occupations of a set of eigenvalues, host FP64, no device work:
+ * find_fermi_energy / occupation / entropy_ts (scf/smearing.rs:38-252).
+ * ev: n_sets x nb (one row per (spin, k) set), weights: n_sets (k weights);
+ * smearing as pwgpu_scf_params.smearing; spin_factor 2 (nspin 1) or 1.
+ * find_fermi != 0: *fermi_energy receives the level that holds n_electrons;
+ * otherwise *fermi_energy is the given level.  occ (n_sets x nb, may be
+ * NULL) = spin_factor * f(e); *entropy_ts (may be NULL) = TS, eV. */
+pwgpu_status pwgpu_occupations(int32_t n_sets, int32_t nb, const double* ev, const double* weights,
+                               double n_electrons, double sigma, int32_t smearing, double spin_factor,
+                               int32_t find_fermi, double* fermi_energy, double* occ, double* entropy_ts);
+
 /* Local part of H|psi> (kinetic diagonal + V_eff through the FFT pipeline;
  * no Kleinman-Bylander term) on device pointers, allocating nothing.  No
  * counterpart in the reference.  For callers that cannot call cudaMalloc:

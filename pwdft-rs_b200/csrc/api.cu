@@ -455,6 +455,17 @@ pwgpu_status pwgpu_potentials(pwgpu_handle* ph, const double* rho_r, double* vef
   return potentials_host(ph->h, rho_r, veff_g, energies);
 }
 
+pwgpu_status pwgpu_occupations(int32_t n_sets, int32_t nb, const double* ev, const double* weights,
+                               double n_electrons, double sigma, int32_t smearing, double spin_factor,
+                               int32_t find_fermi, double* fermi_energy, double* occ, double* entropy_ts) {
+  if (!ev || !weights || !fermi_energy || n_sets < 1 || nb < 1)
+    return fail(kInvalid, "pwgpu_occupations: bad argument");
+  if (smearing < 0 || smearing > 4 || !(sigma >= 0.0) || !(spin_factor > 0.0))
+    return fail(kInvalid, "pwgpu_occupations: smearing, sigma or spin_factor out of range");
+  return occupations_host(n_sets, nb, ev, weights, n_electrons, sigma, smearing, spin_factor, find_fermi != 0,
+                          fermi_energy, occ, entropy_ts);
+}
+
 pwgpu_status pwgpu_small_geneig(int32_t batch, int32_t m, int32_t nev, const double* H, const double* S,
                                 double* evals, double* C) {
   if (!H || !S || !evals || !C || batch < 1) return fail(kInvalid, "pwgpu_small_geneig: bad argument");

@@ -753,6 +753,21 @@ static double entropy_ts(const std::vector<std::vector<double>>& ev, const std::
   return s * sigma * spin_factor;
 }
 
+Status occupations_host(int n_sets, int nb, const double* ev, const double* w, double n_electrons, double sigma,
+                        int scheme, double spin_factor, bool find_fermi, double* fermi_energy, double* occ,
+                        double* ts) {
+  std::vector<std::vector<double>> e((size_t)n_sets);
+  std::vector<double> wk(w, w + n_sets);
+  for (int s = 0; s < n_sets; ++s) e[s].assign(ev + (size_t)s * nb, ev + (size_t)(s + 1) * nb);
+  const double ef = find_fermi ? fermi_level(e, wk, n_electrons, sigma, scheme, spin_factor) : *fermi_energy;
+  if (occ)
+    for (int s = 0; s < n_sets; ++s)
+      for (int b = 0; b < nb; ++b) occ[(size_t)s * nb + b] = spin_factor * occ01(scheme, e[s][b], ef, sigma);
+  if (ts) *ts = entropy_ts(e, wk, ef, sigma, scheme, spin_factor);
+  *fermi_energy = ef;
+  return kOk;
+}
+
 // partial-pivot LU solve with the 1e-15 singular-pivot fallback (linalg.rs:124-152)
 static std::vector<double> solve_small(std::vector<double> a, std::vector<double> b, int n) {
   std::vector<int> piv(n);

@@ -71,5 +71,10 @@ Status potentials_host(Handle& h, const double* rho, double* veff_g, double* ene
 Status mix_host(Handle& h, int channel, int mode, const double* in, const double* out, double* next, double beta,
                 int ndim, int period, double q_tf);
 Status mix_reset(Handle& h);
+// Fermi level (bisection, or *fermi_energy as given), occupations
+// spin_factor * f(e) per state and TS, host FP64 (smearing.rs:38-252).
+Status occupations_host(int n_sets, int nb, const double* ev, const double* w, double n_electrons, double sigma,
+                        int scheme, double spin_factor, bool find_fermi, double* fermi_energy, double* occ,
+                        double* ts);
 
 }  // namespace pwgpu

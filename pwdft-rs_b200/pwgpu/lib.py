@@ -190,6 +190,8 @@ def load_library(path: str = LIB_PATH):
     lib.pwgpu_initial_density.argtypes = [vp, _f64p]
     lib.pwgpu_get_local_potential.argtypes = [vp, _f64p, _f64p]
     lib.pwgpu_small_geneig.argtypes = [ct.c_int32, ct.c_int32, ct.c_int32, _f64p, _f64p, _f64p, _f64p]
+    lib.pwgpu_occupations.argtypes = [ct.c_int32, ct.c_int32, _f64p, _f64p, ct.c_double, ct.c_double, ct.c_int32,
+                                      ct.c_double, ct.c_int32, _f64p, _f64p, _f64p]
     lib.pwgpu_get_stream.argtypes = [vp, ct.POINTER(vp)]
     lib.pwgpu_get_stream.restype = ct.c_int32
     lib.pwgpu_kernel_launches.argtypes = [ct.POINTER(ct.c_int64)]
@@ -209,7 +211,7 @@ def load_library(path: str = LIB_PATH):
     for name in ("pwgpu_create", "pwgpu_destroy", "pwgpu_set_veff_g", "pwgpu_apply_h", "pwgpu_apply_h_device",
                  "pwgpu_set_precision", "pwgpu_get_dims", "pwgpu_profile_apply_h", "pwgpu_scf_run", "pwgpu_scf_iter1_from_rho_g",
                  "pwgpu_eigensolve", "pwgpu_density", "pwgpu_symmetrize", "pwgpu_potentials",
-                 "pwgpu_small_geneig", "pwgpu_mix", "pwgpu_mix_reset", "pwgpu_get_projectors", "pwgpu_initial_density",
+                 "pwgpu_small_geneig", "pwgpu_occupations", "pwgpu_mix", "pwgpu_mix_reset", "pwgpu_get_projectors", "pwgpu_initial_density",
                  "pwgpu_get_local_potential", "pwgpu_server_create", "pwgpu_server_destroy",
                  "pwgpu_server_submit", "pwgpu_server_poll", "pwgpu_server_wait", "pwgpu_server_wait_any",
                  "pwgpu_server_result", "pwgpu_server_release", "pwgpu_server_get_stats"):
@@ -532,6 +534,25 @@ def kernel_launches() -> int:
     n = ct.c_int64()
     _check(lib, lib.pwgpu_kernel_launches(ct.byref(n)))
     return n.value
+
+
+def occupations(eigenvalues, weights, n_electrons: float, sigma: float, smearing: str = "fermi_dirac",
+                spin_factor: float = 2.0, fermi_energy: float | None = None):
+    """Fermi level, occupations and TS through the library's host code
+    (pwgpu_occupations; find_fermi_energy / occupation / entropy_ts,
+    scf/smearing.rs:38-252).  eigenvalues: (n_sets, nb); weights: (n_sets,).
+    fermi_energy None: searched for n_electrons; else used as given.
+    Returns (fermi_energy, occ [n_sets, nb] = spin_factor f, TS)."""
+    lib = load_library()
+    ev = np.ascontiguousarray(np.atleast_2d(eigenvalues), dtype=np.float64)
+    w = np.ascontiguousarray(weights, dtype=np.float64)
+    ef = np.array([0.0 if fermi_energy is None else float(fermi_energy)])
+    occ = np.zeros_like(ev)
+    ts = np.zeros(1)
+    _check(lib, lib.pwgpu_occupations(ev.shape[0], ev.shape[1], _f64(ev), _f64(w), float(n_electrons), float(sigma),
+                                      SMEARING[smearing], float(spin_factor), 1 if fermi_energy is None else 0,
+                                      _f64(ef), _f64(occ), _f64(ts)))
+    return float(ef[0]), occ, float(ts[0])
 
 
 def small_geneig(H: np.ndarray, S: np.ndarray, nev: int):
