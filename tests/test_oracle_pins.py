@@ -191,3 +191,14 @@ def test_nlcc_double_counting_sign_probe():
     rho_core = np.array([0.1, 0.3])
     got = O.xc_energy_corrected(rho_val + rho_core, rho_val, np.array([-1.0, -2.0]), np.array([-0.5, -1.5]), 2.0)
     assert abs(got - (-1.7)) < 1e-12
+
+
+def test_ewald_fe_bcc_vs_qe():
+    """Ewald energy of BCC Fe (a = 2.87 A, Z_val 16) against QE's
+    -171.77906580 Ry to 0.01 eV (tests/qe_validation.rs:1089-1117)."""
+    from pwgpu.context import ewald_energy
+    from pwgpu.crystal import Atom, Crystal, Lattice
+    a = 2.87
+    cr = Crystal(Lattice(a / 2 * np.array([-1.0, 1.0, 1.0]), a / 2 * np.array([1.0, -1.0, 1.0]),
+                         a / 2 * np.array([1.0, 1.0, -1.0])), [Atom("Fe", (0.0, 0.0, 0.0))])
+    assert abs(ewald_energy(cr, [16.0]) - (-171.77906580 * RY_TO_EV)) < 0.01
