@@ -6,8 +6,10 @@ Run once in a checkout that has the reference tree available:
 
 Copied verbatim (data files, not source):
   * pseudopotentials/nc/lda/{Si,Si_hgh,C}.upf   -> tests/golden/upf/
-  * data/csv/{vloc_g_si,beta_q_si,dij_si,rho_core_g,vgcmp_phase4}_reference.csv
-                                                 -> tests/golden/csv/
+  * pseudopotentials/nc/lda/{Al,As,Cl,Cu,Fe,Ga,Mg,Na,O}.upf (heavy-atom pins)
+                                                 -> tests/golden/upf/
+  * data/csv/{vloc_g_si,beta_q_si,dij_si,rho_core_g,vgcmp_phase4}_reference.csv,
+    data/csv/vgch_{beta_l,vloc}_heavy.csv        -> tests/golden/csv/
 The SCF goldens (E_total, E_F) are constants in tests/test_oracle_pins.py
 with their reference file:line.
 """
@@ -16,9 +18,9 @@ import os
 import shutil
 import sys
 
-UPFS = ["Si.upf", "Si_hgh.upf", "C.upf"]
+UPFS = ["Si.upf", "Si_hgh.upf", "C.upf"] + [f"{e}.upf" for e in ("Al", "As", "Cl", "Cu", "Fe", "Ga", "Mg", "Na", "O")]
 CSVS = ["vloc_g_si_reference.csv", "beta_q_si_reference.csv", "dij_si_reference.csv",
-        "rho_core_g_reference.csv", "vgcmp_phase4_reference.csv"]
+        "rho_core_g_reference.csv", "vgcmp_phase4_reference.csv", "vgch_beta_l_heavy.csv", "vgch_vloc_heavy.csv"]
 
 
 def main(ref_root: str):

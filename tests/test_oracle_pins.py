@@ -202,3 +202,38 @@ def test_ewald_fe_bcc_vs_qe():
     cr = Crystal(Lattice(a / 2 * np.array([-1.0, 1.0, 1.0]), a / 2 * np.array([1.0, -1.0, 1.0]),
                          a / 2 * np.array([1.0, 1.0, -1.0])), [Atom("Fe", (0.0, 0.0, 0.0))])
     assert abs(ewald_energy(cr, [16.0]) - (-171.77906580 * RY_TO_EV)) < 0.01
+
+
+def test_heavy_atom_beta_form_factors_match_reference_csv():
+    """F_l(q) of every projector of 11 LDA UPFs (Si, C, Al, Fe, Cu, Ga, As,
+    Na, Cl, Mg, O; l up to 2) against data/csv/vgch_beta_l_heavy.csv to
+    1e-8 Bohr^(3/2) (tests/vgch_beta_l_heavy.rs:39-46, 130-256)."""
+    from conftest import upf_path
+    from pwgpu.upf import load_upf
+    _, rows = _csv("vgch_beta_l_heavy.csv")
+    pps = {}
+    worst = 0.0
+    for r in rows:
+        el, ip, l = r[0], int(r[1]), int(r[2])
+        if el not in pps:
+            pps[el] = load_upf(upf_path(f"{el}.upf"))
+        assert pps[el].beta_l[ip] == l
+        f = beta_form_factor(pps[el], ip, np.array([float(r[4])]))[0] / BOHR_TO_ANG ** 1.5
+        worst = max(worst, abs(f - float(r[5])))
+    assert len(pps) == 11 and len(rows) == 590
+    assert worst < 1e-8
+
+
+def test_heavy_atom_vloc_g0_matches_reference_csv():
+    """V_loc(G=0) = (4 pi / Omega) int r^2 [V_loc(r) + Z e^2 / r] dr of the
+    same 11 UPFs in their cells against data/csv/vgch_vloc_heavy.csv, to the
+    reference's V_loc tolerance of 1e-4 Ry (tests/vgcmp_vloc_cross_check.rs)."""
+    from conftest import upf_path
+    from pwgpu.upf import load_upf
+    _, rows = _csv("vgch_vloc_heavy.csv")
+    assert len(rows) == 11
+    for r in rows:
+        pp = load_upf(upf_path(f"{r[0]}.upf"))
+        assert pp.z_valence == float(r[1])
+        v = v_local_of_g(pp, np.array([0.0]), float(r[2]) * BOHR_TO_ANG ** 3)[0]
+        assert abs(v - float(r[4])) < 1e-4 * RY_TO_EV, (r[0], v, float(r[4]))
