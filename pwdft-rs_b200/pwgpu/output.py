@@ -13,6 +13,12 @@ Density checkpoint (.npz, numpy's zip of arrays):
   through one transplanted iteration), rho_g_basis (n_pw complex, the total
   rho(G) in basis order as ScfResult::rho_g, scf/mod.rs:269-322).
 
+QE density bundle (read only): the VGCH2BIN files the reference's transplant
+tests seed from (tests/vgch_transplant_c.rs:45-158): magic "VGCH2BIN",
+u32 version 1, u8 gamma_only, i32 nspin, i32 ngm, the reciprocal vectors
+(9 f64), ngm Miller triples (i32), nspin x ngm complex rho(G) in Bohr^-3,
+all little-endian.
+
 Band table (text): '#' header lines with the Fermi level and counts, then one
 row per (spin, k-point): spin, k index, k (Å^-1, 3 numbers), weight, and
 the n_bands eigenvalues in eV, ascending.
@@ -68,6 +74,46 @@ def restart_rho_g(sys_, checkpoint: dict) -> np.ndarray:
     if abs(checkpoint["omega"] - sys_.omega) > 1e-9 * sys_.omega:
         raise ValueError("checkpoint cell volume differs from the system's")
     return checkpoint["rho_g_fft"]
+
+
+def read_qe_density_bundle(path: str) -> dict:
+    """Parse a VGCH2BIN density bundle: {"nspin", "miller" (ngm, 3) int,
+    "rho_g" (nspin, ngm) complex in Bohr^-3}.  Raises ValueError on a bad
+    magic, version, a Gamma-only bundle or a truncated file."""
+    import struct
+    with open(path, "rb") as f:
+        b = f.read()
+    if len(b) < 8 + 4 + 1 + 4 + 4 + 72 or b[:8] != b"VGCH2BIN":
+        raise ValueError(f"{path}: not a VGCH2BIN bundle")
+    off = 8
+    (version,) = struct.unpack_from("<I", b, off)
+    off += 4
+    if version != 1:
+        raise ValueError(f"{path}: unsupported VGCH2BIN version {version}")
+    if b[off] != 0:
+        raise ValueError(f"{path}: Gamma-only bundles are not supported")
+    off += 1
+    nspin, ngm = struct.unpack_from("<ii", b, off)
+    off += 8 + 72
+    if nspin < 1 or ngm < 1 or off + 12 * ngm + 16 * nspin * ngm > len(b):
+        raise ValueError(f"{path}: truncated or inconsistent bundle")
+    mill = np.frombuffer(b, dtype="<i4", count=3 * ngm, offset=off).reshape(ngm, 3).astype(np.int64)
+    off += 12 * ngm
+    rho = np.frombuffer(b, dtype="<c16", count=nspin * ngm, offset=off).reshape(nspin, ngm).astype(np.complex128)
+    return {"nspin": nspin, "miller": mill, "rho_g": rho}
+
+
+def qe_rho_g_on_grid(bundle: dict, dims, spin: int = 0) -> np.ndarray:
+    """The bundle's rho(G) of one spin channel on the FFT grid in Å^-3,
+    negative Miller indices wrapped (the scatter of tests/vgch_transplant_c.rs:
+    125-153): the rho_g input of pwgpu_scf_iter1_from_rho_g."""
+    from .consts import BOHR_TO_ANG
+    d = np.asarray(dims, dtype=np.int64)
+    m = bundle["miller"] % d
+    idx = (m[:, 0] * d[1] + m[:, 1]) * d[2] + m[:, 2]
+    out = np.zeros(int(np.prod(d)), dtype=np.complex128)
+    out[idx] = bundle["rho_g"][spin] / BOHR_TO_ANG ** 3
+    return out
 
 
 def write_bands(path: str, sys_, eigenvalues: np.ndarray, fermi_energy: float) -> None:

@@ -10,6 +10,8 @@ Copied verbatim (data files, not source):
                                                  -> tests/golden/upf/
   * data/csv/{vloc_g_si,beta_q_si,dij_si,rho_core_g,vgcmp_phase4}_reference.csv,
     data/csv/vgch_{beta_l,vloc}_heavy.csv        -> tests/golden/csv/
+  * data/qe/c_rho_qe.bin (QE's converged C-diamond density, VGCH2BIN bundle)
+                                                 -> tests/golden/qe/
 The SCF goldens (E_total, E_F) are constants in tests/test_oracle_pins.py
 with their reference file:line.
 """
@@ -31,6 +33,8 @@ def main(ref_root: str):
         shutil.copyfile(os.path.join(ref_root, "pseudopotentials", "nc", "lda", f), os.path.join(here, "upf", f))
     for f in CSVS:
         shutil.copyfile(os.path.join(ref_root, "data", "csv", f), os.path.join(here, "csv", f))
+    os.makedirs(os.path.join(here, "qe"), exist_ok=True)
+    shutil.copyfile(os.path.join(ref_root, "data", "qe", "c_rho_qe.bin"), os.path.join(here, "qe", "c_rho_qe.bin"))
 
 
 if __name__ == "__main__":

@@ -74,3 +74,25 @@ def test_oracle_transplant_is_the_first_scf_iteration(si_pp):
     assert abs(again.total_energy - full.total_energy) < 1e-4
     with pytest.raises(ValueError):
         O.run_scf_iter1_from_rho_g(s, 4, np.zeros(10, dtype=complex), **kw)
+
+
+def test_qe_density_bundle_reads_and_integrates():
+    """The reference's QE C-diamond density (data/qe/c_rho_qe.bin) parses
+    and rho(G = 0) Omega = 8 electrons to 0.01 on its 20^3 grid
+    (tests/vgch_transplant_c.rs:188-237)."""
+    import os
+    from conftest import GOLDEN
+    from pwgpu.crystal import fcc_primitive
+    from pwgpu.output import qe_rho_g_on_grid, read_qe_density_bundle
+    b = read_qe_density_bundle(os.path.join(GOLDEN, "qe", "c_rho_qe.bin"))
+    assert b["nspin"] == 1 and b["miller"].shape == (1687, 3)
+    g = qe_rho_g_on_grid(b, (20, 20, 20))
+    assert abs(g[0].real * fcc_primitive(3.567).volume() - 8.0) < 0.01
+
+
+def test_qe_density_bundle_rejects_bad_files(tmp_path):
+    from pwgpu.output import read_qe_density_bundle
+    p = tmp_path / "bad.bin"
+    p.write_bytes(b"NOTABUNDLE" + bytes(100))
+    with pytest.raises(ValueError):
+        read_qe_density_bundle(str(p))
