@@ -237,3 +237,44 @@ def test_heavy_atom_vloc_g0_matches_reference_csv():
         assert pp.z_valence == float(r[1])
         v = v_local_of_g(pp, np.array([0.0]), float(r[2]) * BOHR_TO_ANG ** 3)[0]
         assert abs(v - float(r[4])) < 1e-4 * RY_TO_EV, (r[0], v, float(r[4]))
+
+
+def test_qe_validation_c_diamond_fermi():
+    """C diamond (a = 3.567 A), 30 Ry, full 4x4x4 Gamma-centred mesh, 8
+    bands, Fermi-Dirac 0.01 Ry, Broyden + Kerker: E_F against QE's 15.8873
+    eV to 0.1 eV (tests/qe_validation.rs:522-543).  The total energy sits
+    1.45 eV from QE's, the gap the reference records for this cell."""
+    from conftest import upf_path
+    from pwgpu.crystal import Atom, Crystal, fcc_primitive, monkhorst_pack
+    from pwgpu.upf import load_upf
+    cr = Crystal(fcc_primitive(3.567), [Atom("C", (0.0, 0.0, 0.0)), Atom("C", (0.25, 0.25, 0.25))])
+    s = build_system(cr, {"C": load_upf(upf_path("C.upf"))}, 30.0 * RY_TO_EV,
+                     monkhorst_pack((4, 4, 4), "gamma", cr.lattice), SymmetryInfo.from_crystal(cr, 1e-5))
+    r = O.run_scf_unpolarized(s, 8, max_iter=80, conv_threshold=1e-8, energy_threshold=1e-6, mixing_beta=0.3,
+                              mixing_ndim=8, smearing="fermi_dirac", sigma=0.01 * RY_TO_EV, mixer="broyden",
+                              kerker=True)
+    assert r.n_iterations < 80
+    assert abs(r.fermi_energy - 15.8873) < 0.100
+    assert abs(r.total_energy - (-23.84343910 * RY_TO_EV) - 1.45) < 0.05
+
+
+def test_qe_validation_al_fcc():
+    """Al FCC (a = 4.05 A), 24 Ry, 8x8x8 Gamma-centred mesh (its 29-point
+    IBZ; QE samples the IBZ too), 6 bands, Fermi-Dirac 0.02 Ry, Kerker:
+    QE's -4.72724484 Ry to 90 meV, E_F 7.5876 eV to 0.15 eV, one-electron
+    sum 2.88539588 Ry to 120 meV (tests/qe_validation.rs:683-708)."""
+    from conftest import upf_path
+    from pwgpu.crystal import Atom, Crystal, fcc_primitive
+    from pwgpu.symmetry import reduce_kpoints
+    from pwgpu.upf import load_upf
+    cr = Crystal(fcc_primitive(4.05), [Atom("Al", (0.0, 0.0, 0.0))])
+    sym = SymmetryInfo.from_crystal(cr, 1e-5)
+    s = build_system(cr, {"Al": load_upf(upf_path("Al.upf"))}, 24.0 * RY_TO_EV,
+                     reduce_kpoints((8, 8, 8), "gamma", sym, cr.lattice), sym)
+    r = O.run_scf_unpolarized(s, 6, max_iter=80, conv_threshold=1e-8, energy_threshold=1e-6, mixing_beta=0.3,
+                              mixing_ndim=8, smearing="fermi_dirac", sigma=0.02 * RY_TO_EV, kerker=True)
+    c = r.components
+    assert r.n_iterations < 80
+    assert abs(r.total_energy - (-4.72724484 * RY_TO_EV)) < 0.090
+    assert abs(r.fermi_energy - 7.5876) < 0.15
+    assert abs(c["e_kinetic"] + c["e_local"] + c["e_nonlocal"] - 2.88539588 * RY_TO_EV) < 0.120
