@@ -38,7 +38,7 @@ def _rank_main(rank, world, port, out):
 def test_two_rank_max_over_ranks():
     world = 2
     port = _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:  # no fork of this multi-threaded process
         out = m.dict()
         mp.spawn(_rank_main, args=(world, port, out), nprocs=world, join=True)
         res = dict(out)
