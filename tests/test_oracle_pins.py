@@ -278,3 +278,58 @@ def test_qe_validation_al_fcc():
     assert abs(r.total_energy - (-4.72724484 * RY_TO_EV)) < 0.090
     assert abs(r.fermi_energy - 7.5876) < 0.15
     assert abs(c["e_kinetic"] + c["e_local"] + c["e_nonlocal"] - 2.88539588 * RY_TO_EV) < 0.120
+
+
+def test_ccmx_fe_bcc_free_magnetization_converges():
+    """Fe BCC, nspin 2, starting moment 0.5, 15 Ry, the full shifted 4x4x4
+    mesh, 8 bands, Fermi-Dirac 0.02 Ry, Anderson + Kerker on the (total,
+    magnetisation) pair (tests/spin_polarization.rs:240-330): converges, the
+    Harris-Foulkes and Kohn-Sham energies agree to 1e-3 eV and the moment
+    collapses (< 0.05 muB) for this non-magnetic pseudopotential."""
+    from conftest import upf_path
+    from pwgpu.crystal import Atom, Crystal, Lattice, monkhorst_pack
+    from pwgpu.upf import load_upf
+    a = 2.87
+    cr = Crystal(Lattice(a / 2 * np.array([-1.0, 1.0, 1.0]), a / 2 * np.array([1.0, -1.0, 1.0]),
+                         a / 2 * np.array([1.0, 1.0, -1.0])), [Atom("Fe", (0.0, 0.0, 0.0))])
+    s = build_system(cr, {"Fe": load_upf(upf_path("Fe.upf"))}, 15.0 * RY_TO_EV,
+                     monkhorst_pack((4, 4, 4), "mp1976", cr.lattice), SymmetryInfo.from_crystal(cr, 1e-5), nspin=2)
+    r = O.run_scf_spin(s, 8, max_iter=80, conv_threshold=1e-3, energy_threshold=1e-3, mixing_beta=0.3,
+                       mixing_ndim=8, smearing="fermi_dirac", sigma=0.02 * RY_TO_EV, kerker=True,
+                       starting_magnetization=0.5)
+    assert r.n_iterations < 80
+    assert abs(r.harris_foulkes_energy - r.total_energy) < 1e-3
+    assert abs(r.magnetization) < 0.05
+
+
+def test_nonlocal_symmetry_at_gamma(si_pp):
+    """Si diamond at Gamma, 204.09 eV (tests/nonlocal_symmetry.rs:61-153):
+    the diagonal of B D B^H is the same for every G of a |G| shell (1e-8),
+    and the lowest eigenvalues of T + V_NL carry the triply degenerate
+    p-like bands 2-4 (spread < 0.1 eV)."""
+    import scipy.linalg as sl
+    s = build_system(diamond_primitive("Si", 5.431), {"Si": si_pp}, 204.09, gamma_only(),
+                     SymmetryInfo.identity_only())
+    p = s.projectors[0]
+    h_nl = p.b @ p.d_dense() @ p.b.conj().T
+    g2 = np.rint(s.kinetic[0] * 1e6).astype(np.int64)  # |G|^2 shells (kinetic = hbar^2/2m |G|^2 at Gamma)
+    diag = h_nl.diagonal().real
+    for key in np.unique(g2):
+        vals = diag[g2 == key]
+        assert np.max(vals) - np.min(vals) < 1e-8
+    w = sl.eigh(h_nl + np.diag(s.kinetic[0]), eigvals_only=True, subset_by_index=[0, 7])
+    assert w[3] - w[1] < 0.1
+
+
+def test_beta_form_factor_at_q_zero(si_pp):
+    """F_i(0) = 4 pi int [r beta_i] r dr for l = 0 (j_0(0) = 1) to 1e-14
+    relative and exactly 0 for l > 0 (tests/kb_projector_validation.rs:
+    266-304)."""
+    from pwgpu.upf import simpson_rows
+    f0 = [beta_form_factor(si_pp, i, np.array([0.0]))[0] for i in range(si_pp.n_proj)]
+    for i, l in enumerate(si_pp.beta_l):
+        if l == 0:
+            want = 4.0 * math.pi * simpson_rows((si_pp.beta[i] * si_pp.r)[None, :], si_pp.rab)[0]
+            assert abs(f0[i] - want) < 1e-14 * max(abs(f0[i]), 1.0)
+        else:
+            assert abs(f0[i]) < 1e-20
