@@ -333,3 +333,22 @@ def test_beta_form_factor_at_q_zero(si_pp):
             assert abs(f0[i] - want) < 1e-14 * max(abs(f0[i]), 1.0)
         else:
             assert abs(f0[i]) < 1e-20
+
+
+def test_local_potential_symmetry_at_gamma(si_pp):
+    """Si diamond, 204.09 eV (tests/nonlocal_symmetry.rs:157-372): |V_loc(G)|
+    with its structure factor is constant over each |G| shell of the basis
+    (1e-4), and T + V_loc(G - G') from the FFT-grid lookup carries the
+    triply degenerate bands 3-5 at Gamma (spread < 1e-3 eV)."""
+    import scipy.linalg as sl
+    s = build_system(diamond_primitive("Si", 5.431), {"Si": si_pp}, 204.09, gamma_only(),
+                     SymmetryInfo.identity_only())
+    v = np.abs(s.v_local_g[s.g_to_fft])
+    g2 = np.rint(s.kinetic[0] * 1e6).astype(np.int64)
+    for key in np.unique(g2):
+        vals = v[g2 == key]
+        assert np.max(vals) - np.min(vals) < 1e-4
+    p = s.projectors[0]
+    h = O.dense_hamiltonian(s.basis.miller, s.kinetic[0], s.v_local_g, s.dims, p.b, 0.0 * p.d_dense())
+    w = sl.eigh(h, eigvals_only=True, subset_by_index=[0, 7])
+    assert w[4] - w[2] < 1e-3
