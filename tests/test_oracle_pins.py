@@ -352,3 +352,30 @@ def test_local_potential_symmetry_at_gamma(si_pp):
     h = O.dense_hamiltonian(s.basis.miller, s.kinetic[0], s.v_local_g, s.dims, p.b, 0.0 * p.d_dense())
     w = sl.eigh(h, eigvals_only=True, subset_by_index=[0, 7])
     assert w[4] - w[2] < 1e-3
+
+
+def test_lda_lsda_unit_properties():
+    """The reference's PZ-LDA / LSDA unit tests (potential/xc.rs:1820-1950)
+    on the oracle's restatement: zero at rho = 0, negative energy and
+    potential, |v_xc| rising with rho, eps_xc in the quoted ranges at 0.044
+    and 0.20 e/A^3, both PZ regimes, the zeta = 0 limit of LSDA to 1e-10,
+    the fully polarised eps_xc below the unpolarised one, and spin-swap
+    symmetry to 1e-12."""
+    e0, v0 = O.lda_xc(np.array([0.0]))
+    assert e0[0] == 0.0 and v0[0] == 0.0
+    e, v = O.lda_xc(np.array([0.05]))
+    assert e[0] < 0.0 and v[0] < 0.0
+    assert abs(O.lda_xc(np.array([0.1]))[1][0]) > abs(O.lda_xc(np.array([0.01]))[1][0])
+    assert -6.0 < O.lda_xc(np.array([0.044]))[0][0] < -3.0
+    assert -10.0 < O.lda_xc(np.array([0.20]))[0][0] < -5.0
+    assert O.lda_xc(np.array([0.001]))[0][0] < 0.0 and O.lda_xc(np.array([2.0]))[0][0] < 0.0
+    rho = np.array([0.01, 0.05, 0.1, 0.2, 0.5, 1.0, 2.0])
+    eu, vu = O.lda_xc(rho)
+    es, vup, vdn = O.lsda_xc(rho / 2, rho / 2)
+    assert np.max(np.abs(eu - es)) < 1e-10
+    assert np.max(np.abs(vu - vup)) < 1e-10 and np.max(np.abs(vup - vdn)) < 1e-10
+    ep, _, _ = O.lsda_xc(np.array([0.1]), np.array([0.0]))
+    assert ep[0] < 0.0 and ep[0] < O.lda_xc(np.array([0.1]))[0][0]
+    e1, u1, d1 = O.lsda_xc(np.array([0.15]), np.array([0.05]))
+    e2, u2, d2 = O.lsda_xc(np.array([0.05]), np.array([0.15]))
+    assert abs(e1[0] - e2[0]) < 1e-12 and abs(u1[0] - d2[0]) < 1e-12 and abs(d1[0] - u2[0]) < 1e-12
