@@ -379,3 +379,28 @@ def test_lda_lsda_unit_properties():
     e1, u1, d1 = O.lsda_xc(np.array([0.15]), np.array([0.05]))
     e2, u2, d2 = O.lsda_xc(np.array([0.05]), np.array([0.15]))
     assert abs(e1[0] - e2[0]) < 1e-12 and abs(u1[0] - d2[0]) < 1e-12 and abs(d1[0] - u2[0]) < 1e-12
+
+
+def test_fft_grid_size_rule():
+    """fft.rs:324-341: smallest 2,3,5-smooth n >= 2 n_max + 1."""
+    from pwgpu.crystal import fft_grid_size, is_fft_friendly
+    assert (fft_grid_size(3), fft_grid_size(4), fft_grid_size(5)) == (8, 9, 12)
+    assert all(is_fft_friendly(n) for n in (1, 2, 4, 8, 30))
+    assert not any(is_fft_friendly(n) for n in (7, 11))
+
+
+def test_ewald_nacl_madelung():
+    """Point charges +1/-1 on the conventional rock-salt cell, a = 5.64 A:
+    -M e^2 / (a/2) per ion pair, M = 1.747565, four pairs, to 1 %
+    (ewald.rs:171-205)."""
+    from pwgpu.consts import E2_COULOMB
+    from pwgpu.context import ewald_energy
+    from pwgpu.crystal import Atom, Crystal, Lattice
+    a = 5.64
+    na = [(0.0, 0.0, 0.0), (0.5, 0.5, 0.0), (0.5, 0.0, 0.5), (0.0, 0.5, 0.5)]
+    cl = [(0.5, 0.0, 0.0), (0.0, 0.5, 0.0), (0.0, 0.0, 0.5), (0.5, 0.5, 0.5)]
+    cr = Crystal(Lattice(np.array([a, 0.0, 0.0]), np.array([0.0, a, 0.0]), np.array([0.0, 0.0, a])),
+                 [Atom("Na", f) for f in na] + [Atom("Cl", f) for f in cl])
+    e = ewald_energy(cr, [1.0] * 4 + [-1.0] * 4)
+    want = -1.747565 * E2_COULOMB / (a / 2.0) * 4.0
+    assert abs((e - want) / want) < 0.01
