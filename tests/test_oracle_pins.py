@@ -404,3 +404,19 @@ def test_ewald_nacl_madelung():
     e = ewald_energy(cr, [1.0] * 4 + [-1.0] * 4)
     want = -1.747565 * E2_COULOMB / (a / 2.0) * 4.0
     assert abs((e - want) / want) < 0.01
+
+
+def test_sad_start_density_properties(si_pp):
+    """The SAD start density of Si (100 eV) integrates to 8 electrons
+    (1e-7), is non-negative, and on a 16^3 grid takes the same value at the
+    fractional grid points (1,0,0), (0,1,0) and (0,0,1) (1e-10)
+    (scf/initial_density.rs:226-280)."""
+    cr = diamond_primitive("Si", 5.431)
+    s = build_system(cr, {"Si": si_pp}, 100.0, gamma_only(), SymmetryInfo.identity_only())
+    rho = s.rho_init_r
+    assert abs(rho.sum() * s.omega / rho.size - 8.0) < 8.0 * 1e-7
+    assert np.all(rho >= 0.0)
+    s16 = build_system(cr, {"Si": si_pp}, 100.0, gamma_only(), SymmetryInfo.identity_only(), fft_grid=(16, 16, 16))
+    r = s16.rho_init_r.reshape(16, 16, 16)
+    assert abs(r[1, 0, 0] - r[0, 1, 0]) <= 1e-10 * abs(r[1, 0, 0])
+    assert abs(r[1, 0, 0] - r[0, 0, 1]) <= 1e-10 * abs(r[1, 0, 0])
