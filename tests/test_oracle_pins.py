@@ -420,3 +420,13 @@ def test_sad_start_density_properties(si_pp):
     r = s16.rho_init_r.reshape(16, 16, 16)
     assert abs(r[1, 0, 0] - r[0, 1, 0]) <= 1e-10 * abs(r[1, 0, 0])
     assert abs(r[1, 0, 0] - r[0, 0, 1]) <= 1e-10 * abs(r[1, 0, 0])
+
+
+def test_hartree_and_density_diff_units():
+    """energy.rs:745-785: V_H(G = 0) = 0 and V_H > 0 for a positive rho(G);
+    the rms density change is 0 for equal densities and 1 between the
+    uniform densities 1 and 2."""
+    vh = O.hartree(np.ones(10, dtype=np.complex128), np.arange(10.0))
+    assert abs(vh[0]) < 1e-15 and np.all(vh[1:].real > 0.0)
+    assert O.density_diff(np.ones(100), np.ones(100), 40.0) < 1e-15
+    assert abs(O.density_diff(np.ones(100), 2.0 * np.ones(100), 40.0) - 1.0) < 1e-10
