@@ -79,3 +79,33 @@ def test_si_ibz_sizes():
         assert abs(sum(k.weight for k in kp) - 1.0) < 1e-12
     kp = reduce_kpoints((4, 4, 4), "gamma", SymmetryInfo.identity_only(), cr.lattice)
     assert len(kp) == 64 == len(monkhorst_pack((4, 4, 4), "gamma", cr.lattice))
+
+
+def test_monkhorst_pack_meshes():
+    """kpoints.rs:398-470: 64 points, weights sum to 1, Gamma in the
+    Gamma-centred 4x4x4 and 3x3x3 meshes and not in the shifted 4x4x4, and
+    per-axis flags (0,0,0) / (1,1,1) equal to the named shifts."""
+    lat = si_fcc().lattice
+    g4 = monkhorst_pack((4, 4, 4), "gamma", lat)
+    assert len(g4) == 64 and abs(sum(k.weight for k in g4) - 1.0) < 1e-12
+    has_gamma = lambda kp: any(np.linalg.norm(k.k) < 1e-12 for k in kp)
+    assert has_gamma(g4) and has_gamma(monkhorst_pack((3, 3, 3), "gamma", lat))
+    s4 = monkhorst_pack((4, 4, 4), "mp1976", lat)
+    assert not has_gamma(s4)
+    for named, flags in ((g4, (0, 0, 0)), (s4, (1, 1, 1))):
+        custom = monkhorst_pack((4, 4, 4), flags, lat)
+        assert len(custom) == len(named)
+        assert all(np.linalg.norm(a.k - b.k) < 1e-14 for a, b in zip(named, custom))
+
+
+def test_basis_properties():
+    """basis.rs:122-185 at 200 eV: 259 plane waves, G = 0 present, every
+    kinetic energy within the cutoff, Miller indices unique."""
+    from pwgpu.consts import HBAR2_OVER_2M
+    from pwgpu.crystal import BasisSet
+    b = BasisSet(si_fcc().lattice, 200.0)
+    assert len(b) == 259
+    ke = HBAR2_OVER_2M * np.einsum("ij,ij->i", b.g, b.g)
+    assert np.min(ke) < 1e-12 and np.max(ke) <= 200.0 + 1e-10
+    assert (b.miller == 0).all(axis=1).sum() == 1
+    assert len({tuple(m) for m in b.miller.tolist()}) == len(b)
