@@ -44,3 +44,20 @@ def test_create_rejects_null_system_without_touching_device():
     rc = lib.pwgpu_create(None, None, ctypes.byref(h))
     assert rc == -1
     assert b"NULL" in lib.pwgpu_last_error()
+
+
+def test_header_compiles_as_c99_and_cxx(tmp_path):
+    """A C caller's view: include/pwgpu.h alone compiles as strict C99 and
+    as C++17 (no C++ or torch types cross the boundary)."""
+    import shutil
+    import subprocess
+    import pytest
+    if shutil.which("gcc") is None or shutil.which("g++") is None:
+        pytest.skip("no host C compiler")
+    src = tmp_path / "use_header.c"
+    src.write_text('#include "pwgpu.h"\nint main(void) { return pwgpu_version() == 0; }\n')
+    inc = os.path.join(ROOT, "include")
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-fsyntax-only", "-I", inc,
+                    str(src)], check=True)
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", "-I", inc, "-x", "c++", str(src)],
+                   check=True)
