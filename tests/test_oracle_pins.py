@@ -430,3 +430,18 @@ def test_hartree_and_density_diff_units():
     assert abs(vh[0]) < 1e-15 and np.all(vh[1:].real > 0.0)
     assert O.density_diff(np.ones(100), np.ones(100), 40.0) < 1e-15
     assert abs(O.density_diff(np.ones(100), 2.0 * np.ones(100), 40.0) - 1.0) < 1e-10
+
+
+def test_simpson_rule_units():
+    """numerics.rs:62-170 on the host Simpson rule: exact for x^3 on 101
+    points and x^2 on 51 points (1e-12), within 1e-4 on an even 50-point
+    mesh, and sqrt(pi)/2 for exp(-r^2) on [0, 5]."""
+    from pwgpu.upf import simpson
+    x = np.linspace(0.0, 1.0, 101)
+    assert abs(simpson(x ** 3, np.full(101, x[1])) - 0.25) < 1e-12 * 0.25
+    x = np.linspace(0.0, 2.0, 51)
+    assert abs(simpson(x ** 2, np.full(51, x[1])) - 8.0 / 3.0) < 1e-12 * 8.0 / 3.0
+    x = np.linspace(0.0, 2.0, 50)
+    assert abs(simpson(x ** 2, np.full(50, x[1])) - 8.0 / 3.0) < 1e-4
+    x = np.linspace(0.0, 5.0, 101)
+    assert abs(simpson(np.exp(-x * x), np.full(101, x[1])) - math.sqrt(math.pi) / 2.0) < 1e-6
