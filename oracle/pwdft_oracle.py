@@ -10,7 +10,12 @@ Rust crate cannot be built here (no Rust toolchain, and the snapshot does
 not compile), so parity is pinned through the reference's golden numbers:
   * SCF golden  -- tests/cpu_scf_baseline.rs:43-44 (E=-213.028339 eV,
                    E_F=8.052064 eV, Si prim, 100 eV, 16^3, Γ, 4 bands)
-  * component CSVs -- data/csv/{vloc_g,beta_q,dij,rho_core_g}_si_reference.csv
+  * QE pins        -- tests/qe_validation.rs (Si 4x4x4 15 Ry: -231.6544 eV,
+                      E_F, QE energy and one-electron sum; C diamond E_F;
+                      Al FCC energy, E_F and one-electron sum; Fe Ewald)
+  * component CSVs -- data/csv/{vloc_g,beta_q,dij,rho_core_g}_si_reference.csv,
+                      the heavy-atom data/csv/vgch_{beta_l,vloc}_heavy.csv
+  * per-component energies -- tests/vgc5_per_component_si.rs
   * basis counts   -- basis.rs:139-148 (259 G at 200 eV)
 Third-party numerics: rustfft 6.4.1 (restated by numpy.fft, same sign and
 normalisation conventions), faer 0.24 self_adjoint_eigen (restated by
