@@ -445,3 +445,15 @@ def test_simpson_rule_units():
     assert abs(simpson(x ** 2, np.full(50, x[1])) - 8.0 / 3.0) < 1e-4
     x = np.linspace(0.0, 5.0, 101)
     assert abs(simpson(np.exp(-x * x), np.full(101, x[1])) - math.sqrt(math.pi) / 2.0) < 1e-6
+
+
+def test_real_to_g_units():
+    """energy.rs:680-725: a constant c maps to rho(G = 0) = c and zero
+    elsewhere; rho(G) = FFT / N followed by the unnormalised inverse returns
+    rho(r) (1e-10)."""
+    dims = (8, 8, 8)
+    g = O.density_r_to_g(np.full(512, 3.5), dims)
+    assert abs(g[0] - 3.5) < 1e-10 and np.max(np.abs(g[1:])) < 1e-10
+    r = np.sin(np.arange(512) * 0.1)
+    back = O.ifft3(O.density_r_to_g(r, dims), dims)
+    assert np.max(np.abs(back.real - r)) < 1e-10 and np.max(np.abs(back.imag)) < 1e-10
