@@ -457,3 +457,17 @@ def test_real_to_g_units():
     r = np.sin(np.arange(512) * 0.1)
     back = O.ifft3(O.density_r_to_g(r, dims), dims)
     assert np.max(np.abs(back.real - r)) < 1e-10 and np.max(np.abs(back.imag)) < 1e-10
+
+
+def test_spin_xc_consistency_si(si_pp):
+    """Si nspin 2 from a 0.2 starting moment (100 eV, Gamma, 16^3, 4 bands,
+    plain Anderson, ndim 4, Fermi-Dirac 0.05 eV): Harris-Foulkes and
+    Kohn-Sham energies within 1e-5 eV and the moment relaxes below 0.05
+    (tests/spin_polarization.rs:143-238)."""
+    s = build_system(diamond_primitive("Si", 5.431), {"Si": si_pp}, 100.0, gamma_only(),
+                     SymmetryInfo.identity_only(), fft_grid=(16, 16, 16), nspin=2)
+    r = O.run_scf_spin(s, 4, max_iter=60, conv_threshold=1e-6, energy_threshold=1e-6, mixing_beta=0.3,
+                       mixing_ndim=4, smearing="fermi_dirac", sigma=0.05, starting_magnetization=0.2)
+    assert r.n_iterations < 60
+    assert abs(r.harris_foulkes_energy - r.total_energy) < 1e-5
+    assert abs(r.magnetization) < 0.05
