@@ -268,6 +268,14 @@ pwgpu_status pwgpu_eigensolve(pwgpu_handle* h, int32_t spin, int32_t ik, int32_t
                               int32_t max_iter, const double* psi_in, double* evals, double* psi_out,
                               int32_t* iters, double* max_residual);
 
+/* The bands of (spin, ik) left on the device by the last pwgpu_scf_run (its
+ * final eigensolve) or pwgpu_eigensolve: the first n_bands eigenvectors as
+ * complex columns (n_pw x n_bands, column-major, basis order), ascending in
+ * energy.  The eigenvector half of diagonalize_dispatch's EigenResult
+ * (scf/driver.rs:125-184), which ScfResult does not carry; PWGPU_E_STATE
+ * before any solve. */
+pwgpu_status pwgpu_get_bands(pwgpu_handle* h, int32_t spin, int32_t ik, int32_t n_bands, double* psi_out);
+
 /* rho(r) = sum_k w_k sum_b occ f |IFFT psi|^2, renormalised to N_el and
  * symmetrised (compute_density, scf/density.rs:41-111, then
  * symmetrize_density_g).  occ: n_k x n_bands; psi: n_k blocks n_pw x n_bands. */
@@ -327,6 +335,20 @@ pwgpu_status pwgpu_apply_h_local_noalloc(pwgpu_handle* h, int32_t spin, int32_t 
  * kernel, exposed for testing.  evals batch x nev ascending; C batch x m x nev. */
 pwgpu_status pwgpu_small_geneig(int32_t batch, int32_t m, int32_t nev, const double* H, const double* S,
                                 double* evals, double* C);
+
+/* Lowest nev eigenpairs of a dense m x m Hermitian (complex_matrix != 0,
+ * interleaved complex) or real symmetric matrix, column-major, both triangles
+ * given: the subspace eigensolver of the Rayleigh-Ritz step (one thread-block
+ * cluster; Householder tridiagonalisation in distributed shared memory,
+ * multisection, inverse iteration, back-transform), exposed for testing.
+ * Stands in for the dense self_adjoint_eigen of eigensolver/dense.rs:50-98
+ * inside the subspace.  w: nev ascending; Z: m x nev eigenvectors.
+ * *cluster_ctas (may be NULL) receives the cluster size used, *kernel_ms
+ * (may be NULL) the device time of the solve (CUDA events around its one
+ * launch).  PWGPU_E_INVALID beyond the supported size (m <= 544 real;
+ * complex as shared memory allows). */
+pwgpu_status pwgpu_dense_eigh(int32_t m, int32_t nev, int32_t complex_matrix, const double* A, double* w,
+                              double* Z, int32_t* cluster_ctas, double* kernel_ms);
 
 /*
  * Serving: a job queue in front of pwgpu_scf_run.  No counterpart in the

@@ -391,6 +391,12 @@ pwgpu_status pwgpu_eigensolve(pwgpu_handle* ph, int32_t spin, int32_t ik, int32_
                       ph->precision);
 }
 
+pwgpu_status pwgpu_get_bands(pwgpu_handle* ph, int32_t spin, int32_t ik, int32_t n_bands, double* psi_out) {
+  if (!ph || !psi_out) return fail(kInvalid, "pwgpu_get_bands: NULL argument");
+  PW_CUDA_TRY(cudaSetDevice(ph->h.device));
+  return bands_to_host(ph->h, spin, ik, n_bands, psi_out);
+}
+
 pwgpu_status pwgpu_mix(pwgpu_handle* ph, int32_t channel, int32_t mode, const double* rho_in, const double* rho_out,
                        double* rho_next, double beta, int32_t ndim, int32_t period, double q_tf) {
   if (!ph || !rho_in || !rho_out || !rho_next) return fail(kInvalid, "pwgpu_mix: NULL argument");
@@ -483,21 +489,79 @@ pwgpu_status pwgpu_small_geneig(int32_t batch, int32_t m, int32_t nev, const dou
     cleanup();
     return fail(kOom, "pwgpu_small_geneig: allocation failed");
   }
-  cudaMemcpy(dh, H, mm * sizeof(double2), cudaMemcpyHostToDevice);
-  cudaMemcpy(ds, S, mm * sizeof(double2), cudaMemcpyHostToDevice);
+  // the first failing copy, launch or synchronisation ends the call
+  cudaError_t e = cudaMemcpy(dh, H, mm * sizeof(double2), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(ds, S, mm * sizeof(double2), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cleanup();
+    return fail(kCuda, std::string("pwgpu_small_geneig: copy to the device: ") + cudaGetErrorString(e));
+  }
   st = small_geneig_batched(dh, ds, m, (long)m * m, m, nev, batch, de, dc, m, (long)m * nev, dst, 0);
   std::vector<int> stat(batch, 0);
   if (st == kOk) {
-    cudaError_t e = cudaDeviceSynchronize();
-    if (e != cudaSuccess) st = fail(kCuda, cudaGetErrorString(e));
+    e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(evals, de, (size_t)nev * batch * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(C, dc, (size_t)m * nev * batch * sizeof(double2), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(stat.data(), dst, batch * sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) st = fail(kCuda, std::string("pwgpu_small_geneig: ") + cudaGetErrorString(e));
   }
-  if (st == kOk) {
-    cudaMemcpy(evals, de, (size_t)nev * batch * sizeof(double), cudaMemcpyDeviceToHost);
-    cudaMemcpy(C, dc, (size_t)m * nev * batch * sizeof(double2), cudaMemcpyDeviceToHost);
-    cudaMemcpy(stat.data(), dst, batch * sizeof(int), cudaMemcpyDeviceToHost);
+  if (st == kOk)
     for (int b = 0; b < batch; ++b)
       if (stat[b] == 1) { st = fail(kInvalid, "pwgpu_small_geneig: S is not positive definite"); break; }
+  cleanup();
+  return st;
+}
+
+pwgpu_status pwgpu_dense_eigh(int32_t m, int32_t nev, int32_t complex_matrix, const double* A, double* w,
+                              double* Z, int32_t* cluster_ctas, double* kernel_ms) {
+  if (!A || !w || !Z) return fail(kInvalid, "pwgpu_dense_eigh: NULL argument");
+  if (m < 1 || nev < 1 || nev > m) return fail(kInvalid, "pwgpu_dense_eigh: need 1 <= nev <= m");
+  const bool cpx = complex_matrix != 0;
+  if (!eigh_cluster_supported(m, cpx)) return fail(kInvalid, "pwgpu_dense_eigh: m too large for the cluster solver");
+  if (cluster_ctas) *cluster_ctas = eigh_cluster_size(m, cpx);
+  const size_t es = cpx ? sizeof(double2) : sizeof(double);
+  void *da = nullptr, *dz = nullptr;
+  double *dw = nullptr, *dwork = nullptr;
+  int* dst = nullptr;
+  auto cleanup = [&]() { cudaFree(da); cudaFree(dz); cudaFree(dw); cudaFree(dwork); cudaFree(dst); };
+  if (cudaMalloc(&da, (size_t)m * m * es) != cudaSuccess || cudaMalloc(&dz, (size_t)m * nev * es) != cudaSuccess ||
+      cudaMalloc((void**)&dw, (size_t)nev * sizeof(double)) != cudaSuccess ||
+      cudaMalloc((void**)&dwork, eigh_cluster_work_doubles(m, nev) * sizeof(double)) != cudaSuccess ||
+      cudaMalloc((void**)&dst, sizeof(int)) != cudaSuccess) {
+    cleanup();
+    return fail(kOom, "pwgpu_dense_eigh: allocation failed");
   }
+  cudaError_t e = cudaMemcpy(da, A, (size_t)m * m * es, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cleanup();
+    return fail(kCuda, std::string("pwgpu_dense_eigh: ") + cudaGetErrorString(e));
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (kernel_ms) {
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, 0);
+  }
+  Status st = cpx ? eigh_cluster(static_cast<const double2*>(da), m, m, nev, dw, static_cast<double2*>(dz), m, dwork,
+                                 dst, 0)
+                  : eigh_cluster(static_cast<const double*>(da), m, m, nev, dw, static_cast<double*>(dz), m, dwork,
+                                 dst, 0);
+  if (kernel_ms) {
+    cudaEventRecord(e1, 0);
+    float ms = 0.f;
+    if (cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) *kernel_ms = ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  int flag = 0;
+  if (st == kOk) {
+    e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(w, dw, (size_t)nev * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(Z, dz, (size_t)m * nev * es, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&flag, dst, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) st = fail(kCuda, std::string("pwgpu_dense_eigh: ") + cudaGetErrorString(e));
+  }
+  if (st == kOk && flag != 0) st = fail(kNotConverged, "pwgpu_dense_eigh: non-finite eigenpair");
   cleanup();
   return st;
 }

@@ -1408,6 +1408,25 @@ Status eigensolve_k(Handle& h, int spin, int ik, int n_bands, double tol, int ma
   return kOk;
 }
 
+Status bands_to_host(Handle& h, int spin, int ik, int n_bands, double* psi_out) {
+  if (ik < 0 || ik >= h.n_k || spin < 0 || spin >= h.nspin) return fail(kInvalid, "get_bands: index out of range");
+  ScfState* st = h.scf;
+  if (!st || st->ks.empty() || !st->ks[(size_t)spin * h.n_k + ik].init)
+    return fail(kState, "get_bands: no bands on the device (run the SCF or an eigensolve first)");
+  if (n_bands < 1 || n_bands > st->nd) return fail(kInvalid, "get_bands: n_bands out of range");
+  EigVecs& k = st->ks[(size_t)spin * h.n_k + ik];
+  const long n = h.n_pw;
+  const double2* src = k.V;
+  if (h.gam.on) {
+    Status r = gamma_unpack(h, reinterpret_cast<const double*>(k.V), n, n_bands, st->ew.T, n, h.stream);
+    if (r != kOk) return r;
+    src = st->ew.T;
+  }
+  PW_CUDA_TRY(cudaMemcpyAsync(psi_out, src, n * n_bands * sizeof(double2), cudaMemcpyDeviceToHost, h.stream));
+  PW_CUDA_TRY(cudaStreamSynchronize(h.stream));
+  return kOk;
+}
+
 Status density_from_host(Handle& h, int n_bands, const double* occ, const double* psi_all, double* rho_out) {
   if (n_bands < 1 || n_bands > h.n_pw) return fail(kInvalid, "density: n_bands out of range");
   Status r = ensure_state(h, n_bands, n_bands, 1);

@@ -64,6 +64,9 @@ Status scf_iter1_from_rho_g(Handle& h, const ScfParams& p, const double* rho_g_f
 // Pieces exposed through the C-ABI for parity tests.
 Status eigensolve_k(Handle& h, int spin, int ik, int n_bands, double tol, int max_iter, const double* psi_in,
                     double* evals, double* psi_out, int* iters, double* max_res, int precision);
+// The first n_bands bands of (spin, ik) left on the device by the last SCF
+// run or eigensolve, as complex columns (n_pw x n_bands, basis order).
+Status bands_to_host(Handle& h, int spin, int ik, int n_bands, double* psi_out);
 Status density_from_host(Handle& h, int n_bands, const double* occ, const double* psi_all, double* rho_out);
 Status symmetrize_host(Handle& h, double* rho);
 Status potentials_host(Handle& h, const double* rho, double* veff_g, double* energies);

@@ -11,11 +11,13 @@ The displaced cell keeps only the identity operation, so the density is not
 symmetrised (SymmetryInfo::identity_only, as the reference does for n_ops <= 1).
 """
 
-from .consts import RY_TO_EV
+import numpy as np
+
+from .consts import BOHR_TO_ANG, RY_TO_EV
 from .context import build_system
-from .crystal import gamma_only
+from .crystal import diamond_supercell, gamma_only
 from .symmetry import SymmetryInfo
-from .workloads import si64_crystal
+from .workloads import SEED, si64_crystal
 
 SCF_KW = dict(n_bands=160, max_iter=80, conv_threshold=1e-6, energy_threshold=1e-6, mixing_beta=0.4,
               mixing_ndim=8, kerker=True, smearing="gaussian", sigma=0.01 * RY_TO_EV)
@@ -25,4 +27,16 @@ FP64_SWITCH = 1e-6
 
 def config3_system(pp, ecut_ry: float = 30.0, seed=None):
     cr = si64_crystal() if seed is None else si64_crystal(seed)
+    return build_system(cr, {"Si": pp}, ecut_ry * RY_TO_EV, gamma_only(), SymmetryInfo.identity_only())
+
+
+# The same physics on one conventional cell (8 atoms, a = 10.26 bohr, seeded
+# ±0.05 bohr displacements; n_pw 2,945 on 36^3): small enough for the dense
+# oracle, with 20 bands (the 64-atom case's 160 scaled by the cell).  Tight
+# thresholds so that both loops stop at the same fixed point.
+SI8_SCF_KW = dict(SCF_KW, n_bands=20, max_iter=120, conv_threshold=1e-9, energy_threshold=1e-9)
+
+
+def config3_si8_system(pp, ecut_ry: float = 30.0, seed: int = SEED):
+    cr = diamond_supercell("Si", 10.26 * BOHR_TO_ANG, (1, 1, 1), 0.05 * BOHR_TO_ANG, np.random.default_rng(seed))
     return build_system(cr, {"Si": pp}, ecut_ry * RY_TO_EV, gamma_only(), SymmetryInfo.identity_only())

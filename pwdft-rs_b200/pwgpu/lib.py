@@ -180,6 +180,8 @@ def load_library(path: str = LIB_PATH):
                                   _f64p]
     lib.pwgpu_eigensolve.argtypes = [vp, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_double, ct.c_int32, _f64p, _f64p,
                                      _f64p, _i32p, _f64p]
+    lib.pwgpu_get_bands.argtypes = [vp, ct.c_int32, ct.c_int32, ct.c_int32, _f64p]
+    lib.pwgpu_dense_eigh.argtypes = [ct.c_int32, ct.c_int32, ct.c_int32, _f64p, _f64p, _f64p, _i32p, _f64p]
     lib.pwgpu_density.argtypes = [vp, ct.c_int32, _f64p, _f64p, _f64p]
     lib.pwgpu_symmetrize.argtypes = [vp, _f64p]
     lib.pwgpu_potentials.argtypes = [vp, _f64p, _f64p, _f64p]
@@ -430,6 +432,12 @@ class PwGpu:
             raise PwGpuError(rc, self.lib.pwgpu_last_error().decode(errors="replace"))
         return res.as_dict(), ev, rho, rg
 
+    def get_bands(self, n_bands: int, ik: int = 0, spin: int = 0) -> np.ndarray:
+        """Eigenvectors of (spin, ik) left by the last SCF run or eigensolve: (n_pw, n_bands) complex."""
+        out = np.zeros((n_bands, self.n_pw), dtype=np.complex128)  # row b = band b (column-major n_pw x nb)
+        _check(self.lib, self.lib.pwgpu_get_bands(self.h, spin, ik, n_bands, out.view(np.float64).ctypes.data_as(_f64p)))
+        return out.T
+
     def scf_iter1_from_rho_g(self, rho_g_fft: np.ndarray, n_bands: int, smearing: str = "fermi_dirac",
                              sigma: float = 0.01, diag_tol: float = 1e-10, diag_max_iter: int = 60,
                              diag_extra_bands: int = -1, precision: int = PRECISION_FP64):
@@ -568,3 +576,22 @@ def small_geneig(H: np.ndarray, S: np.ndarray, nev: int):
                                        sf.view(np.float64).ctypes.data_as(_f64p), _f64(ev),
                                        c.view(np.float64).ctypes.data_as(_f64p)))
     return ev, np.transpose(c, (0, 2, 1))
+
+
+def dense_eigh(A: np.ndarray, nev: int, timed: bool = False):
+    """Lowest nev eigenpairs of a dense Hermitian or real symmetric matrix
+    through the device's cluster eigensolver.  Returns (w [nev], Z [m, nev],
+    cluster CTAs used), plus the kernel's device ms when timed."""
+    lib = load_library()
+    m = A.shape[0]
+    cpx = np.iscomplexobj(A)
+    dt = np.complex128 if cpx else np.float64
+    af = np.asfortranarray(A, dtype=dt)
+    w = np.zeros(nev)
+    z = np.zeros((nev, m), dtype=dt)  # row j = eigenvector j (column-major m x nev)
+    nc = ct.c_int32(0)
+    ms = ct.c_double(0.0)
+    _check(lib, lib.pwgpu_dense_eigh(m, nev, 1 if cpx else 0, af.ravel(order="F").view(np.float64).ctypes.data_as(_f64p),
+                                     _f64(w), z.view(np.float64).ctypes.data_as(_f64p), ct.byref(nc),
+                                     ct.byref(ms) if timed else None))
+    return (w, z.T, nc.value, ms.value) if timed else (w, z.T, nc.value)
