@@ -339,8 +339,8 @@ def kernel_bench(local, steps, warmup, flush, hbm_peak, peak_kind):
         traffic = (cap - v_bytes) / cap_bands * (nb / nl) + v_bytes
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved / hbm_peak,
-                # DRAM bytes of the mixed x-pass kernel from one ncu capture of a 22-band launch
-                # (profiles/hpsi_fft_kernels_si64.md), scaled to this launch's average band count
+                # DRAM bytes of the mixed x-pass kernel from one ncu capture of a 22-band launch,
+                # scaled to this launch's average band count
                 "traffic": traffic, "traffic_unit": "bytes per launch (ncu capture of 22 bands, scaled by bands)",
                 "peak_kind": peak_kind,
                 "alg_bytes_per_launch": alg, "ms_per_launch": ms_launch,

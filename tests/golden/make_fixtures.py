@@ -1,8 +1,9 @@
 """Copy the reference's test fixtures used by the parity tests into tests/golden/.
 
-Run once in a checkout that has the reference tree available:
+Run once in a checkout that has the reference tree available, giving the
+root of that tree (the directory holding pseudopotentials/ and data/):
 
-    python tests/golden/make_fixtures.py /root/reference
+    python tests/golden/make_fixtures.py <reference-root>
 
 Copied verbatim (data files, not source):
   * pseudopotentials/nc/lda/{Si,Si_hgh,C}.upf   -> tests/golden/upf/
@@ -38,4 +39,6 @@ def main(ref_root: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_fixtures.py <reference-root>")
+    main(sys.argv[1])
