@@ -18,4 +18,17 @@ size_t small_geneig_smem(int m);
 // eigenvectors in H).
 Status large_geneig(Handle& h, double2* Hm, double2* Sm, int m, double* w, cudaStream_t s);
 
+// Lowest nev eigenpairs of the Hermitian (complex) or symmetric (real) m x m
+// matrix A (both triangles stored, leading dim lda), one thread-block
+// cluster (eigh.cu): w ascending (nev), eigenvectors in Z (m x nev, ld ldz).
+// work: eigh_cluster_work_doubles(m, nev) doubles; status_dev (zeroed here)
+// becomes 1 if a non-finite value appeared.  A is read only.
+size_t eigh_cluster_work_doubles(int m, int nev);
+bool eigh_cluster_supported(int m, bool complex_matrix);
+int eigh_cluster_size(int m, bool complex_matrix);
+Status eigh_cluster(const double* A, long lda, int m, int nev, double* w, double* Z, long ldz, double* work,
+                    int* status_dev, cudaStream_t s);
+Status eigh_cluster(const double2* A, long lda, int m, int nev, double* w, double2* Z, long ldz, double* work,
+                    int* status_dev, cudaStream_t s);
+
 }  // namespace pwgpu

@@ -495,6 +495,26 @@ template <typename T> Status subspace_eig(Ctx& c, int m, int nev, T** C, bool al
     }
     return kOk;
   }
+  if (eigh_cluster_supported(m, !std::is_same<T, double>::value)) {
+    // this project's cluster eigensolver: lowest nev pairs, vectors into Cs
+    const size_t need = eigh_cluster_work_doubles(m, nev);
+    if (need > c.w.eigh_work_len) {
+      if (c.w.eigh_work) cudaFree(c.w.eigh_work);
+      c.w.eigh_work = nullptr;
+      c.w.eigh_work_len = 0;
+      if ((r = walloc(&c.w.eigh_work, need)) != kOk) return r;
+      c.w.eigh_work_len = need;
+    }
+    T* Cv = as<T>(c.w.Cs);
+    if ((r = eigh_cluster(Hs, m, m, nev, c.w.lam, Cv, m, c.w.eigh_work, c.w.status, c.s)) != kOk) return r;
+    int st = 0;
+    PW_CUDA_TRY(cudaMemcpyAsync(&st, c.w.status, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+    PW_CUDA_TRY(cudaStreamSynchronize(c.s));
+    if (st != 0) return fail(kNotConverged, "eigensolver: subspace eigensolve produced non-finite values");
+    *C = Cv;
+    return kOk;
+  }
+  // beyond the cluster solver's size (m > 544, or complex m beyond its shared memory)
   if ((r = ensure_solver(c)) != kOk) return r;
   if ((r = heevd(c, Hs, m, c.w.lam)) != kOk) return r;
   int info = 0;
@@ -839,6 +859,7 @@ void eig_work_release(EigWork& w) {
   auto f = [](void* p) { if (p) cudaFree(p); };
   f(w.T); f(w.HXn); f(w.Pn); f(w.HPn); f(w.Hs); f(w.Cs); f(w.G); f(w.Z); f(w.Id);
   f(w.lam); f(w.lam0); f(w.colsq); f(w.partials); f(w.idx); f(w.status); f(w.solver_work); f(w.info);
+  f(w.eigh_work);
   w = EigWork();
 }
 

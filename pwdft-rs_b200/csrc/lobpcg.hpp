@@ -40,6 +40,8 @@ struct EigWork {
   double2* solver_work = nullptr;
   size_t solver_lwork = 0;
   int* info = nullptr;
+  double* eigh_work = nullptr;  // scratch of the cluster eigensolver (eigh.cu)
+  size_t eigh_work_len = 0;
 };
 
 struct EigStats {
