@@ -15,9 +15,20 @@ end-to-end time the same C-ABI calls by wall clock (they include the
 host->device copies of the start densities and the device->host copies of
 eigenvalues and densities).
 
-Beside it, the synthetic H|psi> kernel bench of the same cell (160 seeded
-bands, 256 Gaussian KB channels, V_eff seeded in [-1, 0] Ha) gives the
+Beside it: the plain FP64 form batched the same way (separating the gain of
+the precision form from that of concurrency); the accuracy gate against the
+FP64 oracle (one transplanted FP64 iteration from cell 0's converged
+density handed to the oracle's H, occupations, density and energy, checker
+only); end to end with pwgpu_create inside the clock; the plain-method case
+(Si2, 10 k-points) as complete solves on the GPU and on the oracle over all
+host cores; and the synthetic H|psi> kernel bench of the same cell (160
+seeded bands, 256 Gaussian KB channels, V_eff seeded in [-1, 0] Ha) for the
 per-stage device times and the roofline of the dominant own kernel.
+
+The reference arm (--impl reference) times bounded samples of the headline
+FP64 solve on the host cores (the oracle's H|psi> of 8 bands and their share
+of the subspace products); its value is the solve fraction a step completes
+over the step's measured time.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pwgpu|reference]
 
@@ -139,6 +150,14 @@ def scf_kwargs():
     return nb, kw, FP64_SWITCH
 
 
+# Band applications of H in the FP64 device solve of the headline cell (the GPU
+# arm measures it on every run and reports it under accuracy); the CPU arm's
+# samples are fractions of a solve of this size.
+HEADLINE_H_APPS = 12574
+SAMPLE_BANDS = 8
+SUBSPACE_ND = 180  # columns of the eigensolver block (160 bands + 20 buffer bands)
+
+
 def sad_veff(sys_):
     """V_eff(G) of the start density, as the solve's first iteration builds it (for CPU sampling)."""
     from oracle import pwdft_oracle as O
@@ -147,56 +166,156 @@ def sad_veff(sys_):
     return sys_.v_local_g + O.hartree(rho_g, sys_.g_squared) + O.density_r_to_g(vxc, sys_.dims)
 
 
-def cpu_solve_sample(sys_, h_applications: int, nb_sample: int = 8):
-    """Oracle FP64 H|psi> (FFT form + projector GEMMs, all host threads) on a
-    band sample, scaled by the band applications of the FP64 GPU solve."""
-    from oracle import pwdft_oracle as O
-    O.set_workers(-1)
-    p = sys_.projectors[0]
-    d = p.d_dense()
-    veff = sad_veff(sys_)
-    rng = np.random.default_rng(1)
-    psi = rng.standard_normal((sys_.n_pw, nb_sample)) + 1j * rng.standard_normal((sys_.n_pw, nb_sample))
-    O.apply_h_fft(sys_.g_to_fft, sys_.kinetic[0], veff, sys_.dims, p.b, d, psi[:, :1])  # warm
-    t0 = time.perf_counter()
-    reps = 0
-    while True:
-        O.apply_h_fft(sys_.g_to_fft, sys_.kinetic[0], veff, sys_.dims, p.b, d, psi)
-        reps += 1
-        if time.perf_counter() - t0 > 10.0 or reps >= 3:
-            break
-    per_band = (time.perf_counter() - t0) / reps / nb_sample
-    solve_s = per_band * h_applications
-    return {"value": 1.0 / solve_s, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-            "sample": (f"oracle FP64 H|psi> on {nb_sample} bands x {reps} rep(s) ({per_band * 1e3:.2f} ms/band), "
-                       f"scaled by the {h_applications} band applications of the FP64 GPU solve; "
-                       "subspace algebra, density and potentials not counted (lower bound on CPU time)")}
+class CpuSample:
+    """One bounded sample step of the headline FP64 solve on the host cores:
+    the oracle's H|psi> (FFT form + projector GEMMs) of SAMPLE_BANDS bands and
+    those bands' share of the block eigensolver's subspace products (two
+    projections against the 180-column block and the Rayleigh-Ritz update of
+    a 540-column basis), all host threads through numpy/scipy.  A step is
+    SAMPLE_BANDS band applications of a solve that needs h_apps of them."""
+
+    def __init__(self, sys_):
+        from oracle import pwdft_oracle as O
+        O.set_workers(-1)
+        self.O = O
+        self.sys = sys_
+        p = sys_.projectors[0]
+        self.b, self.d = p.b, p.d_dense()
+        self.veff = sad_veff(sys_)
+        rng = np.random.default_rng(1)
+        n = sys_.n_pw
+        self.psi = rng.standard_normal((n, SAMPLE_BANDS)) + 1j * rng.standard_normal((n, SAMPLE_BANDS))
+        self.x = np.linalg.qr(rng.standard_normal((n, SUBSPACE_ND)) + 0j)[0]
+        self.v3 = rng.standard_normal((n, 3 * SUBSPACE_ND)) + 0j
+        self.c3 = rng.standard_normal((3 * SUBSPACE_ND, SAMPLE_BANDS)) + 0j
+
+    def step(self) -> float:
+        s, O = self.sys, self.O
+        t0 = time.perf_counter()
+        h = O.apply_h_fft(s.g_to_fft, s.kinetic[0], self.veff, s.dims, self.b, self.d, self.psi)
+        for _ in range(2):
+            h = h - self.x @ (self.x.conj().T @ h)
+        u = self.v3 @ self.c3
+        t = time.perf_counter() - t0
+        if not np.isfinite(u[0, 0]):
+            raise RuntimeError("CPU sample produced non-finite values")
+        return t
+
+    def describe(self, h_apps, reps, step_s):
+        return (f"one step = the oracle's FP64 H|psi> of {SAMPLE_BANDS} bands of the Si64 cell plus their share of "
+                f"the eigensolver's subspace products ({reps} timed step(s), {step_s * 1e3:.1f} ms each); a solve "
+                f"is {h_apps} band applications, so value = ({SAMPLE_BANDS}/{h_apps} solve) / step time; density, "
+                "potentials, mixing and the dense subspace eigensolves are not counted (favours the CPU)")
+
+
+def cpu_sample_baseline(sys_, h_apps, steps=3):
+    smp = CpuSample(sys_)
+    smp.step()  # warm
+    ts = [smp.step() for _ in range(steps)]
+    step_s = statistics.mean(ts)
+    v = (SAMPLE_BANDS / h_apps) / step_s
+    return {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": smp.describe(h_apps, steps, step_s), "projected_solve_s": step_s * h_apps / SAMPLE_BANDS}
+
+
+def headline_config(sys_, nb, world):
+    return {"workload": "si64_scf_gamma_30ry", "n_pw": sys_.n_pw, "grid": list(sys_.dims),
+            "n_bands": nb, "n_ch": sys_.projectors[0].n_ch, "n_atoms": len(sys_.crystal.atoms),
+            "smearing": "gaussian 0.01 Ry", "mixing": "anderson beta 0.4 + kerker",
+            "batch": f"{BATCH} cells (displacement seeds {SEED}..{SEED + BATCH - 1}) solved "
+                     "concurrently, one handle and stream each; a step = the batch",
+            "l2": "flushed before every step (256 MB write); working set > L2",
+            "parallelism": f"replicas x{world}"}
 
 
 def run_reference(args, world, rank):
-    """CPU arm: the oracle restatement of the reference's per-iteration operator
-    on all host cores, bounded samples scaled to one solve."""
+    """CPU arm: K bounded sample steps of the headline FP64 solve on the host
+    cores (the oracle restatement of the reference's operator); value = the
+    fraction of a solve each step completes / its measured time."""
     if rank != 0:
         return
     from pwgpu.config3 import config3_system
     from pwgpu.upf import load_upf
     sys_ = config3_system(load_upf(SI_UPF))
-    h_apps = 12574  # band applications of the FP64 GPU solve of this cell (measured, bench "accuracy" block)
-    vals = []
-    base = None
-    for i in range(args.warmup + args.steps):
-        base = cpu_solve_sample(sys_, h_apps, nb_sample=4)
-        if i >= args.warmup:
-            vals.append(1.0 / base["value"])
-    v = 1.0 / statistics.mean(vals)
+    nb = scf_kwargs()[0]
+    smp = CpuSample(sys_)
+    for _ in range(args.warmup):
+        smp.step()
+    ts = [smp.step() for _ in range(args.steps)]
+    step_s = statistics.mean(ts)
+    frac = SAMPLE_BANDS / HEADLINE_H_APPS
+    v = frac / step_s
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded Si64 cell)",
-            "config": {"workload": "si64_scf_gamma_30ry", "n_pw": sys_.n_pw, "grid": list(sys_.dims),
-                       "n_bands": 160, "n_ch": sys_.projectors[0].n_ch},
-            "cpu_baseline": {**base, "value": v},
+            "config": headline_config(sys_, nb, world),
+            "solve_fraction_per_step": frac,
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                             "sample": smp.describe(HEADLINE_H_APPS, args.steps, step_s),
+                             "projected_solve_s": step_s / frac},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def config1_comparison(local):
+    """The plain-method case as complete solves on both sides: the Si2 fcc cell
+    (a = 10.26 bohr, 20 Ry, shifted 4x4x4 MP -> 10 IBZ k-points, 8 bands,
+    Si_hgh.upf, fixed occupations, Anderson 0.7) from the SAD start density to
+    convergence, FP64, through pwgpu_create + pwgpu_scf_run on the GPU and
+    through the oracle's dense loop (the reference's algorithm) on every host
+    core, its k-points spread over a process pool as the reference's rayon loop
+    spreads them.  Both clocks are wall clocks around complete solves."""
+    import concurrent.futures
+    import multiprocessing
+
+    from oracle import pwdft_oracle as O
+    from pwgpu.config1 import SCF_KW, config1_system
+    from pwgpu.lib import PRECISION_FP64, PwGpu
+    from pwgpu.upf import load_upf
+    s = config1_system(load_upf(os.path.join(ROOT, "tests", "golden", "upf", "Si_hgh.upf")))
+    kw = dict(SCF_KW)
+    nb = kw.pop("n_bands")
+    gpu = []
+    res = None
+    for _ in range(3):
+        t0 = time.perf_counter()
+        with PwGpu(s, device=local) as dev:
+            t1 = time.perf_counter()
+            res, _, _, _ = dev.scf_run(s.rho_init_r, nb, precision=PRECISION_FP64, **kw)
+        t2 = time.perf_counter()
+        gpu.append((t2 - t0, t2 - t1))
+    g_create, g_solve = min(x[0] for x in gpu[1:]), min(x[1] for x in gpu[1:])
+    workers = min(len(s.kpoints), os.cpu_count() or 1)
+    ctx = multiprocessing.get_context("spawn")
+    with concurrent.futures.ProcessPoolExecutor(max_workers=workers, mp_context=ctx,
+                                                initializer=_blas_one_thread) as pool:
+        list(pool.map(_noop, range(workers)))  # workers started before the clock
+        kw2 = dict(SCF_KW)
+        kw2.pop("n_bands")
+        t0 = time.perf_counter()
+        r = O.run_scf_unpolarized(s, nb, smearing=kw2.pop("smearing"), sigma=kw2.pop("sigma"), kmap=pool.map, **kw2)
+        cpu_s = time.perf_counter() - t0
+    return {"workload": "si2_fcc_20ry_mp444_10k_8bands_si_hgh", "n_pw": s.n_pw, "grid": list(s.dims),
+            "n_k": len(s.kpoints), "gpu_solve_s": g_solve, "gpu_create_and_solve_s": g_create,
+            "gpu_solves_per_s": 1.0 / g_solve, "gpu_solves_per_s_with_create": 1.0 / g_create,
+            "cpu_oracle_solve_s": cpu_s, "cpu_solves_per_s": 1.0 / cpu_s, "cpu_processes": workers,
+            "ratio_gpu_over_cpu": cpu_s / g_solve, "ratio_with_create": cpu_s / g_create,
+            "dE_gpu_vs_oracle_ev": abs(res["total_energy"] - r.total_energy),
+            "iterations_gpu": res["n_iterations"], "iterations_oracle": r.n_iterations,
+            "note": "complete solves on both sides, measured (no projection); the CPU side is the oracle's "
+                    "dense-H loop with one process per k-point"}
+
+
+def _blas_one_thread():
+    try:
+        from threadpoolctl import threadpool_limits
+        threadpool_limits(1)
+    except ImportError:
+        pass
+
+
+def _noop(_):
+    return 0
 
 
 def run_once():
@@ -416,9 +535,9 @@ def main():
 
     def solve_one(i, prec, out):
         t0 = time.perf_counter()
-        res, ev, _, _ = devs[i].scf_run(systems[i].rho_init_r, nb, precision=prec, fp64_switch=sw,
-                                        raise_on_unconverged=False, **kw)
-        out[i] = (time.perf_counter() - t0, res, ev)
+        res, ev, rho, _ = devs[i].scf_run(systems[i].rho_init_r, nb, precision=prec, fp64_switch=sw,
+                                          raise_on_unconverged=False, **kw)
+        out[i] = (time.perf_counter() - t0, res, ev, rho)
 
     def solve_batch(prec, idx):
         """The solves of systems idx, concurrently (one host thread each);
@@ -450,13 +569,16 @@ def main():
     with ClockSampler(local) as clk:
         runs = [solve_batch(PRECISION_MIXED, every) for _ in range(args.steps)]
     n_launch = kernel_launches() - n0
-    # the plain FP64 form: one solve at a time, every cell once
+    # the plain FP64 form: one solve at a time, every cell once; then the FP64 form batched like the
+    # headline, which separates the gain of the precision form from the gain of concurrency
     fp64_runs = [solve_batch(PRECISION_FP64, [i]) for i in every]
+    fp64_batched = solve_batch(PRECISION_FP64, every)
     ms = statistics.mean(r[0] for r in runs)
     wall = statistics.mean(r[1] for r in runs)
     ms64 = statistics.mean(r[0] for r in fp64_runs)
+    ms64b = fp64_batched[0]
     lat = sorted(o[0] for r in runs for o in r[2].values())
-    ms, wall, ms64 = max_over_ranks([ms, wall, ms64], dist, f"cuda:{local}")
+    ms, wall, ms64, ms64b = max_over_ranks([ms, wall, ms64, ms64b], dist, f"cuda:{local}")
     n_at = len(sys_.crystal.atoms)
     last = runs[-1][2]
     de = [abs(last[i][1]["total_energy"] - fp64_runs[i][2][i][1]["total_energy"]) / n_at / HA_TO_EV for i in every]
@@ -473,35 +595,58 @@ def main():
     accuracy["gate_pass"] = bool(accuracy["converged_mixed"] and accuracy["converged_fp64"]
                                  and accuracy["dE_total_per_atom_ha"] <= 1e-6
                                  and accuracy["max_eigenvalue_dev_ha"] <= 1e-5)
+    checker = rank == 0 and world == 1 and not args.no_cpu_baseline
+    if checker:
+        accuracy["vs_oracle"] = oracle_check(devs[0], sys_, fp64_runs[0][2][0], last[0], nb, kw)
 
+    # end to end with the handle's creation inside the clock (the reference's run_scf builds its
+    # ScfContext on every call): one more batch, each thread creating, solving and destroying
     for d in devs:
         d.close()
+    out_c = {}
+
+    def create_and_solve(i):
+        t0 = time.perf_counter()
+        with PwGpu(systems[i], device=local, lanes=1) as dv:
+            res, _, _, _ = dv.scf_run(systems[i].rho_init_r, nb, precision=PRECISION_MIXED, fp64_switch=sw,
+                                      raise_on_unconverged=False, **kw)
+        out_c[i] = (time.perf_counter() - t0, res)
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    th = [threading.Thread(target=create_and_solve, args=(i,)) for i in every]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    torch.cuda.synchronize()
+    wall_create = time.perf_counter() - t0
     kb, roofline, kb_cfg = kernel_bench(local, 5, 3, flush, hbm_peak, peak_kind)
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_solve_sample(sys_, int(r64["h_applications"]))
+    c1 = None
+    if checker:
+        cpu = cpu_sample_baseline(sys_, int(r64["h_applications"]))
+        c1 = config1_comparison(local)
     if rank == 0:
         value = world * BATCH * 1e3 / ms
         fp64_value = world * 1e3 / ms64
+        fp64_b_value = world * BATCH * 1e3 / ms64b
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "mixed: c64 FFT/V_eff product, c128 projector GEMMs, f64 subspace/energies/mixing",
+            "dtype": "mixed: c64 FFT/V_eff product, f64 subspace/energies/mixing (Gamma-real bands)",
             "data": "synthetic (seeded Si64 cells; reference Si.upf)",
-            "config": {"workload": "si64_scf_gamma_30ry", "n_pw": sys_.n_pw, "grid": list(sys_.dims),
-                       "n_bands": nb, "n_ch": sys_.projectors[0].n_ch, "n_atoms": n_at,
-                       "smearing": "gaussian 0.01 Ry", "mixing": "anderson beta 0.4 + kerker",
-                       "batch": f"{BATCH} cells (displacement seeds {SEED}..{SEED + BATCH - 1}) solved "
-                                "concurrently, one handle and stream each; a step = the batch",
-                       "l2": "flushed before every step (256 MB write); working set > L2",
-                       "parallelism": f"replicas x{world}"},
+            "config": headline_config(sys_, nb, world),
             "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                           "per": "solve, inside the concurrent batch"},
             "fp64": {"value": fp64_value, "unit": UNIT, "ms_per_step": ms64,
                      "form": "plain FP64, one solve at a time"},
+            "fp64_batched": {"value": fp64_b_value, "unit": UNIT, "ms_per_step": ms64b,
+                             "form": f"plain FP64, {BATCH} cells concurrently (as the headline)"},
             "mixed_batched_over_fp64_plain": value / fp64_value,
+            "mixed_batched_over_fp64_batched": value / fp64_b_value,
             "accuracy": accuracy,
             "roofline": roofline,
             "kernel_bench": {"workload": "si64_hpsi_gamma_30ry", **kb_cfg, **kb},
@@ -509,15 +654,53 @@ def main():
             "e2e": {"value": world * BATCH / wall, "unit": UNIT,
                     "h2d_bytes_per_step": int(BATCH * 8 * sys_.n_grid),
                     "d2h_bytes_per_step": int(BATCH * (8 * sys_.n_grid + 8 * nb + 16 * sys_.n_pw)),
-                    "path": "pwgpu_scf_run per cell (C-ABI, host start density in, host eigenvalues/density out)"},
+                    "path": "pwgpu_scf_run per cell (C-ABI, host start density in, host eigenvalues/density out)",
+                    "with_create": {"value": world * BATCH / wall_create, "unit": UNIT,
+                                    "path": "pwgpu_create (device setup of projectors, V_loc, core and start "
+                                            "densities) + pwgpu_scf_run + pwgpu_destroy per cell, one batch"}},
             "clocks": clk.summary(),
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if c1:
+            line["config1_complete_solves"] = c1
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def oracle_check(dev, sys_, fp64_out, mixed_out, nb, kw):
+    """The headline cell against the FP64 oracle (checker, outside the timed
+    region): one transplanted FP64 iteration from cell 0's converged FP64
+    density on the device, handed to the oracle (its V_eff from that density,
+    its FFT-form H on the device's bands, its occupations, density and total
+    energy); the mixed solve of the same cell is compared with that energy and
+    with the oracle's Rayleigh quotients."""
+    from oracle import pwdft_oracle as O
+    _, _, ev64, rho64 = fp64_out
+    _, rmix, evmix, _ = mixed_out
+    r1, ev1, _, _, rho_in1 = dev.scf_iter1_from_rho_g(O.density_r_to_g(rho64, sys_.dims), nb,
+                                                       smearing=kw["smearing"], sigma=kw["sigma"], diag_tol=1e-9,
+                                                       diag_max_iter=300)
+    psi = dev.get_bands(nb)
+    chk = O.fixed_point_check(sys_, rho_in1, psi, kw["smearing"], kw["sigma"])
+    n_at = len(sys_.crystal.atoms)
+    out = {"cell": 0,
+           "dE_fp64_iteration_vs_oracle_ha": abs(chk["total_energy"] - r1["total_energy"]) / HA_TO_EV,
+           "max_eigenvalue_dev_fp64_vs_oracle_ha": float(np.max(np.abs(chk["rayleigh"] - ev1[0]))) / HA_TO_EV,
+           "max_residual_vs_oracle_h_ev": float(np.max(chk["residual"])),
+           "drho_oracle_map_at_fixed_point": float(chk["drho_in_out"]),
+           "dE_mixed_per_atom_vs_oracle_ha": abs(rmix["total_energy"] - chk["total_energy"]) / n_at / HA_TO_EV,
+           "max_eigenvalue_dev_mixed_vs_oracle_ha": float(np.max(np.abs(evmix[0] - chk["rayleigh"]))) / HA_TO_EV,
+           "bar": "plain FP64: 1e-8 Ha total, 1e-7 Ha eigenvalues; mixed: 1e-6 Ha/atom, 1e-5 Ha",
+           "how": "one transplanted FP64 iteration from the converged FP64 density; the oracle rebuilds V_eff, "
+                  "applies its FFT-form H to the device's bands, and builds occupations, density and energy"}
+    out["gate_pass"] = bool(out["dE_fp64_iteration_vs_oracle_ha"] <= 1e-8
+                            and out["max_eigenvalue_dev_fp64_vs_oracle_ha"] <= 1e-7
+                            and out["dE_mixed_per_atom_vs_oracle_ha"] <= 1e-6
+                            and out["max_eigenvalue_dev_mixed_vs_oracle_ha"] <= 1e-5)
+    return out
 
 
 if __name__ == "__main__":

@@ -527,10 +527,19 @@ class OracleResult:
     components: dict = None    # EnergyComponents (energy.rs:597-670) of the final iteration
 
 
+def diag_k_task(args):
+    """Dense H of one k-point and its lowest eigenpairs (the per-k body of
+    driver.rs:459-472); a top-level function so that a process pool can run
+    the k-points in parallel, as the reference's rayon loop does."""
+    miller, kinetic, veff, dims, b, d_dense, n_bands = args
+    return lowest_eigenpairs(dense_hamiltonian(miller, kinetic, veff, dims, b, d_dense), n_bands)
+
+
 def run_scf_unpolarized(sys, n_bands, max_iter=100, conv_threshold=1e-6, energy_threshold=1e-5,
                         mixing_beta=0.3, mixing_ndim=8, smearing="fermi_dirac", sigma=0.01,
-                        kerker=False, q_tf=None, verbose=False, mixer="anderson", mixing_period=3):
-    """Dense-H SCF loop of driver.rs:353-735 on an ScfSystem (pwgpu.context)."""
+                        kerker=False, q_tf=None, verbose=False, mixer="anderson", mixing_period=3, kmap=map):
+    """Dense-H SCF loop of driver.rs:353-735 on an ScfSystem (pwgpu.context).
+    kmap: map over the per-k diagonalisations (e.g. a process pool's map)."""
     dims = sys.dims
     n = sys.n_grid
     omega = sys.omega
@@ -558,9 +567,9 @@ def run_scf_unpolarized(sys, n_bands, max_iter=100, conv_threshold=1e-6, energy_
         exc_in, vxc_in = lda_xc(rxc)
         veff = sys.v_local_g + vh + density_r_to_g(vxc_in, dims)
         evals, psis = [], []
-        for ik in range(len(sys.kpoints)):
-            h = dense_hamiltonian(sys.basis.miller, sys.kinetic[ik], veff, dims, sys.projectors[ik].b, d_dense[ik])
-            w, v = lowest_eigenpairs(h, n_bands)
+        tasks = [(sys.basis.miller, sys.kinetic[ik], veff, dims, sys.projectors[ik].b, d_dense[ik], n_bands)
+                 for ik in range(len(sys.kpoints))]
+        for w, v in kmap(diag_k_task, tasks):
             evals.append(w)
             psis.append(v)
         ef = find_fermi_energy(evals, weights, sys.n_electrons, sigma, smearing, spin_factor)
