@@ -265,10 +265,6 @@ def config1_comparison(local):
     through the oracle's dense loop (the reference's algorithm) on every host
     core, its k-points spread over a process pool as the reference's rayon loop
     spreads them.  Both clocks are wall clocks around complete solves."""
-    import concurrent.futures
-    import multiprocessing
-
-    from oracle import pwdft_oracle as O
     from pwgpu.config1 import SCF_KW, config1_system
     from pwgpu.lib import PRECISION_FP64, PwGpu
     from pwgpu.upf import load_upf
@@ -285,16 +281,11 @@ def config1_comparison(local):
         t2 = time.perf_counter()
         gpu.append((t2 - t0, t2 - t1))
     g_create, g_solve = min(x[0] for x in gpu[1:]), min(x[1] for x in gpu[1:])
-    workers = min(len(s.kpoints), os.cpu_count() or 1)
-    ctx = multiprocessing.get_context("spawn")
-    with concurrent.futures.ProcessPoolExecutor(max_workers=workers, mp_context=ctx,
-                                                initializer=_blas_one_thread) as pool:
-        list(pool.map(_noop, range(workers)))  # workers started before the clock
-        kw2 = dict(SCF_KW)
-        kw2.pop("n_bands")
-        t0 = time.perf_counter()
-        r = O.run_scf_unpolarized(s, nb, smearing=kw2.pop("smearing"), sigma=kw2.pop("sigma"), kmap=pool.map, **kw2)
-        cpu_s = time.perf_counter() - t0
+    cpu = oracle_config1_solve(s, nb)
+    if "unfinished" in cpu:
+        return {"workload": "si2_fcc_20ry_mp444_10k_8bands_si_hgh", "gpu_solve_s": g_solve,
+                "gpu_create_and_solve_s": g_create, "cpu_oracle_solve_s": None, "cpu_unfinished": cpu["unfinished"]}
+    r, cpu_s, workers = cpu["result"], cpu["seconds"], cpu["workers"]
     return {"workload": "si2_fcc_20ry_mp444_10k_8bands_si_hgh", "n_pw": s.n_pw, "grid": list(s.dims),
             "n_k": len(s.kpoints), "gpu_solve_s": g_solve, "gpu_create_and_solve_s": g_create,
             "gpu_solves_per_s": 1.0 / g_solve, "gpu_solves_per_s_with_create": 1.0 / g_create,
@@ -303,15 +294,61 @@ def config1_comparison(local):
             "dE_gpu_vs_oracle_ev": abs(res["total_energy"] - r.total_energy),
             "iterations_gpu": res["n_iterations"], "iterations_oracle": r.n_iterations,
             "note": "complete solves on both sides, measured (no projection); the CPU side is the oracle's "
-                    "dense-H loop with one process per k-point"}
+                    "dense-H loop with one single-threaded process per k-point"}
 
 
-def _blas_one_thread():
+_BLAS_ENV = ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS", "MKL_NUM_THREADS")
+CPU_SOLVE_LIMIT_S = 240.0
+
+
+def stage(msg):
+    """Progress of the bench's legs on stderr (the JSON line alone goes to stdout)."""
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
+
+
+def oracle_config1_solve(s, nb):
+    """The oracle's dense loop on the plain-method case over all host cores:
+    one single-threaded process per k-point (spawned), bounded by
+    CPU_SOLVE_LIMIT_S.  Returns {"result", "seconds", "workers"} or
+    {"unfinished": why}."""
+    import concurrent.futures
+    import multiprocessing
+
+    from oracle import pwdft_oracle as O
+    from pwgpu.config1 import SCF_KW
+    workers = min(len(s.kpoints), os.cpu_count() or 1)
+    ctx = multiprocessing.get_context("spawn")
+    # one BLAS thread per worker process: set in the environment the workers start with, before any
+    # of them loads a BLAS library
+    saved = {k: os.environ.get(k) for k in _BLAS_ENV}
+    os.environ.update({k: "1" for k in _BLAS_ENV})
     try:
-        from threadpoolctl import threadpool_limits
-        threadpool_limits(1)
-    except ImportError:
-        pass
+        pool = concurrent.futures.ProcessPoolExecutor(max_workers=workers, mp_context=ctx)
+        list(pool.map(_noop, range(workers)))  # workers started before the clock
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    deadline = time.perf_counter() + CPU_SOLVE_LIMIT_S
+
+    def kmap(fn, tasks):
+        if time.perf_counter() > deadline:
+            raise TimeoutError(f"the oracle's solve ran past {CPU_SOLVE_LIMIT_S} s")
+        return pool.map(fn, tasks)
+
+    kw2 = dict(SCF_KW)
+    kw2.pop("n_bands")
+    t0 = time.perf_counter()
+    try:
+        r = O.run_scf_unpolarized(s, nb, smearing=kw2.pop("smearing"), sigma=kw2.pop("sigma"), kmap=kmap, **kw2)
+    except TimeoutError as e:
+        pool.shutdown(cancel_futures=True)
+        return {"unfinished": str(e)}
+    cpu_s = time.perf_counter() - t0
+    pool.shutdown()
+    return {"result": r, "seconds": cpu_s, "workers": workers}
 
 
 def _noop(_):
@@ -560,17 +597,20 @@ def main():
         return e0.elapsed_time(e1), wall, out
 
     every = list(range(BATCH))
+    stage("warm-up batches")
     for _ in range(args.warmup):
         solve_batch(PRECISION_MIXED, every)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     n0 = kernel_launches()
+    stage("timed batches")
     with ClockSampler(local) as clk:
         runs = [solve_batch(PRECISION_MIXED, every) for _ in range(args.steps)]
     n_launch = kernel_launches() - n0
     # the plain FP64 form: one solve at a time, every cell once; then the FP64 form batched like the
     # headline, which separates the gain of the precision form from the gain of concurrency
+    stage("FP64 solves")
     fp64_runs = [solve_batch(PRECISION_FP64, [i]) for i in every]
     fp64_batched = solve_batch(PRECISION_FP64, every)
     ms = statistics.mean(r[0] for r in runs)
@@ -597,6 +637,7 @@ def main():
                                  and accuracy["max_eigenvalue_dev_ha"] <= 1e-5)
     checker = rank == 0 and world == 1 and not args.no_cpu_baseline
     if checker:
+        stage("oracle check of the headline cell")
         accuracy["vs_oracle"] = oracle_check(devs[0], sys_, fp64_runs[0][2][0], last[0], nb, kw)
 
     # end to end with the handle's creation inside the clock (the reference's run_scf builds its
@@ -612,6 +653,7 @@ def main():
                                       raise_on_unconverged=False, **kw)
         out_c[i] = (time.perf_counter() - t0, res)
 
+    stage("end to end with handle creation")
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     th = [threading.Thread(target=create_and_solve, args=(i,)) for i in every]
@@ -621,13 +663,17 @@ def main():
         t.join()
     torch.cuda.synchronize()
     wall_create = time.perf_counter() - t0
+    stage("kernel bench")
     kb, roofline, kb_cfg = kernel_bench(local, 5, 3, flush, hbm_peak, peak_kind)
 
     cpu = None
     c1 = None
     if checker:
+        stage("CPU sample of the headline solve")
         cpu = cpu_sample_baseline(sys_, int(r64["h_applications"]))
+        stage("plain-method case: complete solves on GPU and CPU")
         c1 = config1_comparison(local)
+        stage("done")
     if rank == 0:
         value = world * BATCH * 1e3 / ms
         fp64_value = world * 1e3 / ms64
