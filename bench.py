@@ -64,6 +64,9 @@ BATCH = 4  # Si64 cells solved concurrently in one step
 # each band plus one FP32 V(r) read (the output stays in L2), so it is scaled
 # to a launch's band count as (capture - V) / 22 per band + V.
 XV_TRAFFIC_CAPTURE = (33503744 + 3072, 22)
+# the fused middle kernel (k_yxy<float>) on the same grid: DRAM bytes of one
+# launch and its band count, from one ncu capture (None until captured)
+YXY_TRAFFIC_CAPTURE = (None, 20)
 
 
 def load_peaks():
@@ -456,7 +459,7 @@ def kernel_bench(local, steps, warmup, flush, hbm_peak, peak_kind):
                         ms.append((e0, e1))
             torch.cuda.synchronize()
             out[tag] = {"ms_per_block": statistics.mean(a.elapsed_time(b) for a, b in ms)}
-        names = ["fft_z_inv_scatter", "fft_y_inv", "fft_x_inv_v_fwd", "fft_y_fwd", "fft_z_fwd_gather",
+        names = ["fft_z_inv_scatter", "fft_y_inv", "fft_x_mid", "fft_y_fwd", "fft_z_fwd_gather",
                  "nl_bh_psi_zgemm", "nl_d_apply", "nl_b_q_zgemm"]
         for prec, tag in ((PRECISION_MIXED, "mixed"), (PRECISION_FP64, "fp64")):
             dev.set_precision(prec)
@@ -470,42 +473,59 @@ def kernel_bench(local, steps, warmup, flush, hbm_peak, peak_kind):
             out[tag]["stage_ms"] = dict(zip(names, [round(float(x), 5) for x in acc]))
             out[tag]["launches"] = dict(zip(names, [int(x) for x in st_n]))
     p = out["mixed"]
-    own = {k: v for k, v in p["stage_ms"].items() if not k.endswith("zgemm")}
+    own = {k: v for k, v in p["stage_ms"].items() if not k.endswith("zgemm") and p["launches"][k] > 0}
     dom = max(own, key=own.get)
     nl = max(1, p["launches"][dom])
     m = np.abs(sys_.basis.miller).max(axis=0)
     Xp, Yp = 2 * int(m[0]) + 1, 2 * int(m[1]) + 1
     d0, d1, d2 = sys_.dims
     cb = 8  # complex FP32 in the mixed form
-    per_band = {
-        "fft_z_inv_scatter": 16 * n_pw + cb * Xp * Yp * d2,
-        "fft_y_inv": cb * Xp * Yp * d2 + cb * Xp * d1 * d2,
-        "fft_x_inv_v_fwd": 2 * cb * Xp * d1 * d2 + 4.0 * N / (nb / nl),
-        "fft_y_fwd": cb * Xp * d1 * d2 + cb * Xp * Yp * d2,
-        "fft_z_fwd_gather": cb * Xp * Yp * d2 + 3 * 16 * n_pw,
-        "nl_d_apply": 2 * 16 * 256,
+    # fused middle kernel (one per z-plane and group of bands, the plane in shared memory) unless the
+    # grid needed the three-kernel fallback
+    fused = p["launches"]["fft_y_inv"] == 0
+    bands = nb / nl
+    per_launch = {
+        "fft_z_inv_scatter": (16 * n_pw + cb * Xp * Yp * d2) * bands,
+        "fft_y_inv": (cb * Xp * Yp * d2 + cb * Xp * d1 * d2) * bands,
+        # fused: the middle kernel performs the x and y axes of both transforms and the V(r)
+        # product, so it carries that share of the per-band algorithmic bytes of the local
+        # H|psi> (2c n_pw + 4c N + (c/2) N): two thirds of the transforms' 4c N and the (c/2) N of
+        # V(r); three-kernel form: the x pass's compact rows in and out and V(r) once per band
+        "fft_x_mid": ((2.0 / 3.0) * 4 * cb * N + 0.5 * cb * N) * bands if fused
+        else (2 * cb * Xp * d1 * d2 + 4.0 * N) * bands,
+        "fft_y_fwd": (cb * Xp * d1 * d2 + cb * Xp * Yp * d2) * bands,
+        "fft_z_fwd_gather": (cb * Xp * Yp * d2 + 3 * 16 * n_pw) * bands,
+        "nl_d_apply": 2 * 16 * 256 * bands,
     }[dom]
-    alg = per_band * nb / nl
+    alg = per_launch
     ms_launch = own[dom] / nl
     achieved = alg / (ms_launch * 1e-3) / 1e9
     traffic = None
-    if dom == "fft_x_inv_v_fwd" and (d0, d1, d2) == (72, 72, 72):
+    if dom == "fft_x_mid" and not fused and (d0, d1, d2) == (72, 72, 72):
         cap, cap_bands = XV_TRAFFIC_CAPTURE
         v_bytes = 4.0 * N
-        traffic = (cap - v_bytes) / cap_bands * (nb / nl) + v_bytes
+        traffic = (cap - v_bytes) / cap_bands * bands + v_bytes
+    elif dom == "fft_x_mid" and fused and (d0, d1, d2) == (72, 72, 72):
+        cap, cap_bands = YXY_TRAFFIC_CAPTURE
+        traffic = None if cap is None else cap / cap_bands * bands
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved / hbm_peak,
-                # DRAM bytes of the mixed x-pass kernel from one ncu capture of a 22-band launch,
-                # scaled to this launch's average band count
-                "traffic": traffic, "traffic_unit": "bytes per launch (ncu capture of 22 bands, scaled by bands)",
+                "traffic": traffic, "traffic_unit": "DRAM bytes per launch from one ncu capture, scaled by bands",
                 "peak_kind": peak_kind,
-                "alg_bytes_per_launch": alg, "ms_per_launch": ms_launch,
-                "note": "dominant own kernel of H|psi> (the inner operator of every SCF step); "
-                        "alg bytes = compact-grid read+write per band x bands per launch, V(r) FP32 read"}
+                "alg_bytes_per_launch": alg, "ms_per_launch": ms_launch, "fused_middle": fused,
+                "note": "dominant own kernel of H|psi> (the inner operator of every SCF step); fused middle "
+                        "(y/x passes of both transforms and the V(r) product, the plane in shared memory): alg "
+                        "bytes = its share of the local H|psi>'s per-band bytes, (2/3) 4c N + (c/2) N, c = 8 B"}
+    if fused:
+        comp = (2 * cb * Xp * Yp * d2) * bands + 4.0 * N
+        roofline["compulsory_bytes_per_launch"] = comp
+        roofline["compulsory_frac"] = comp / (ms_launch * 1e-3) / 1e9 / hbm_peak
+        roofline["compulsory_note"] = ("what the fused kernel must move: the compact planes read and written once "
+                                       "per band and V(r) once; it is bound by shared memory, not HBM")
     # the whole local H|psi> (the five FFT kernels) against its per-band algorithmic bytes
     # 2c n_pw + 4c N + (c/2) N, c = 8 B (FP32 complex)
     pipe_bytes = hpsi_algorithmic_bytes(n_pw, N, 8) * nb
-    fft_stages = ("fft_z_inv_scatter", "fft_y_inv", "fft_x_inv_v_fwd", "fft_y_fwd", "fft_z_fwd_gather")
+    fft_stages = ("fft_z_inv_scatter", "fft_y_inv", "fft_x_mid", "fft_y_fwd", "fft_z_fwd_gather")
     pipe_ms = sum(p["stage_ms"][k] for k in fft_stages)
     pipe_gbs = pipe_bytes / (pipe_ms * 1e-3) / 1e9
     roofline["local_hpsi"] = {"bound": "hbm", "achieved": pipe_gbs, "peak": hbm_peak, "unit": "GB/s",

@@ -49,7 +49,7 @@ static void release(Handle& h) {
   h.kp.clear();
   f(h.ch_atom); f(h.atom_ch_start); f(h.d_off); f(h.d_vals);
   f(h.v_local_g); f(h.g_squared); f(h.rho_core_r); f(h.rho_sad); f(h.sym_src); f(h.sym_arg);
-  for (int s = 0; s < 2; ++s) { f(h.veff_r[s]); f(h.veff_r32[s]); }
+  for (int s = 0; s < 2; ++s) { f(h.veff_r[s]); f(h.veff_r32[s]); f(h.veff_rz[s]); f(h.veff_rz32[s]); }
   f(h.work_a); f(h.work_b); f(h.nl_p); f(h.nl_q); f(h.tmp_grid);
   release_scf(h);
   release_nl_mixed(h);
@@ -171,8 +171,12 @@ static Status create(const pwgpu_system* s, const pwgpu_options* o, pwgpu_handle
   for (int sp = 0; sp < h.nspin; ++sp) {
     if ((st = upload<double>(&h.veff_r[sp], nullptr, (size_t)N)) != kOk) return st;
     if ((st = upload<float>(&h.veff_r32[sp], nullptr, (size_t)N)) != kOk) return st;
+    if ((st = upload<double>(&h.veff_rz[sp], nullptr, (size_t)N)) != kOk) return st;
+    if ((st = upload<float>(&h.veff_rz32[sp], nullptr, (size_t)N)) != kOk) return st;
     PW_CUDA_TRY(cudaMemset(h.veff_r[sp], 0, N * sizeof(double)));
     PW_CUDA_TRY(cudaMemset(h.veff_r32[sp], 0, N * sizeof(float)));
+    PW_CUDA_TRY(cudaMemset(h.veff_rz[sp], 0, N * sizeof(double)));
+    PW_CUDA_TRY(cudaMemset(h.veff_rz32[sp], 0, N * sizeof(float)));
   }
   // Gamma-only systems run with real wavefunctions unless the caller keeps them complex
   if (!(o && o->gamma_complex) &&

@@ -242,4 +242,152 @@ __device__ __forceinline__ C* fft_lines(C* a, C* b, const FftPlan& p, int W, con
   return src;
 }
 
+// ---------------------------------------------------------------------------
+// The same transforms for a tile of nl interleaved lines on a 1-D thread
+// block (element e of line l at e*nl + l), any nl: butterfly t of a stage is
+// line t mod nl, position t / nl, so consecutive threads touch consecutive
+// words.  nlm = div_magic(nl).
+// ---------------------------------------------------------------------------
+
+template <int R_, int Ns, int L, int S, typename C>
+__device__ __forceinline__ void stage_nl_ct(const C* __restrict__ src, C* __restrict__ dst, int nl, unsigned nlm,
+                                            const C* __restrict__ tw) {
+  constexpr int LR = L / R_;
+  constexpr int twstep = L / (Ns * R_);
+  for (int t = threadIdx.x; t < nl * LR; t += blockDim.x) {
+    const int j = fast_div(t, nl, nlm);
+    const int l = t - j * nl;
+    const int jq = j / Ns;
+    const int k = j - jq * Ns;
+    C v[R_];
+#pragma unroll
+    for (int r = 0; r < R_; ++r) {
+      C x = src[(j + r * LR) * nl + l];
+      if (r > 0 && Ns > 1) {
+        const C w = tw[k * r * twstep];
+        x = (S < 0) ? cmul(x, w) : cmulc(x, w);
+      }
+      v[r] = x;
+    }
+    dft<R_, S>(v);
+    const int ob = (jq * Ns * R_ + k) * nl + l;
+#pragma unroll
+    for (int q = 0; q < R_; ++q) dst[ob + q * Ns * nl] = v[q];
+  }
+  __syncthreads();
+}
+
+template <int R_, int S, typename C>
+__device__ __forceinline__ void stage_nl(const C* __restrict__ src, C* __restrict__ dst, int L, int Ns, unsigned nsm,
+                                         int nl, unsigned nlm, const C* __restrict__ tw) {
+  const int LR = L / R_;
+  const int twstep = L / (Ns * R_);
+  for (int t = threadIdx.x; t < nl * LR; t += blockDim.x) {
+    const int j = fast_div(t, nl, nlm);
+    const int l = t - j * nl;
+    const int jq = fast_div(j, Ns, nsm);
+    const int k = j - jq * Ns;
+    C v[R_];
+#pragma unroll
+    for (int r = 0; r < R_; ++r) {
+      C x = src[(j + r * LR) * nl + l];
+      if (r > 0 && Ns > 1) {
+        const C w = tw[k * r * twstep];
+        x = (S < 0) ? cmul(x, w) : cmulc(x, w);
+      }
+      v[r] = x;
+    }
+    dft<R_, S>(v);
+    const int ob = (jq * Ns * R_ + k) * nl + l;
+#pragma unroll
+    for (int q = 0; q < R_; ++q) dst[ob + q * Ns * nl] = v[q];
+  }
+  __syncthreads();
+}
+
+template <int S, int R0, int R1, typename C>
+__device__ __forceinline__ C* line_fft_2(C* a, C* b, int nl, unsigned nlm, const C* __restrict__ tw) {
+  stage_nl_ct<R0, 1, R0 * R1, S>(a, b, nl, nlm, tw);
+  stage_nl_ct<R1, R0, R0 * R1, S>(b, a, nl, nlm, tw);
+  return a;
+}
+
+// Full 1-D transform of the nl interleaved lines of a tile; the result is in
+// `a` for an even number of stages and in `b` for an odd number.
+template <int S, typename C>
+__device__ __forceinline__ C* line_fft(C* a, C* b, const FftPlan& p, int nl, unsigned nlm, const C* __restrict__ tw) {
+  if (p.nstages == 2) {
+    switch (p.radix[0] * 16 + p.radix[1]) {
+      case 8 * 16 + 9: return line_fft_2<S, 8, 9>(a, b, nl, nlm, tw);   // 72
+      case 8 * 16 + 5: return line_fft_2<S, 8, 5>(a, b, nl, nlm, tw);   // 40
+      case 8 * 16 + 8: return line_fft_2<S, 8, 8>(a, b, nl, nlm, tw);   // 64
+      case 8 * 16 + 4: return line_fft_2<S, 8, 4>(a, b, nl, nlm, tw);   // 32
+      case 8 * 16 + 3: return line_fft_2<S, 8, 3>(a, b, nl, nlm, tw);   // 24
+      case 9 * 16 + 5: return line_fft_2<S, 9, 5>(a, b, nl, nlm, tw);   // 45
+      case 9 * 16 + 4: return line_fft_2<S, 9, 4>(a, b, nl, nlm, tw);   // 36
+      case 5 * 16 + 5: return line_fft_2<S, 5, 5>(a, b, nl, nlm, tw);   // 25
+      default: break;
+    }
+  }
+  C* src = a;
+  C* dst = b;
+#pragma unroll
+  for (int s = 0; s < kMaxStages; ++s) {
+    if (s < p.nstages) {
+      const int Ns = p.ns[s];
+      const unsigned m = p.nsm[s];
+      const int R = p.radix[s];
+      if (R == 8) stage_nl<8, S>(src, dst, p.L, Ns, m, nl, nlm, tw);
+      else if (R == 9) stage_nl<9, S>(src, dst, p.L, Ns, m, nl, nlm, tw);
+      else if (R == 4) stage_nl<4, S>(src, dst, p.L, Ns, m, nl, nlm, tw);
+      else if (R == 5) stage_nl<5, S>(src, dst, p.L, Ns, m, nl, nlm, tw);
+      else if (R == 3) stage_nl<3, S>(src, dst, p.L, Ns, m, nl, nlm, tw);
+      else stage_nl<2, S>(src, dst, p.L, Ns, m, nl, nlm, tw);
+      C* t = src; src = dst; dst = t;
+    }
+  }
+  return src;
+}
+
+// Stage with caller-supplied element access: ld(e, l) returns element e of
+// line l of the input, st(e, l, v) stores element e of line l of the output,
+// so the first and last stages of a transform can gather, scale or scatter
+// on the way (no separate passes).
+template <int R_, int Ns, int L, int S, typename C, typename Ld, typename St>
+__device__ __forceinline__ void stage_f(int nl, unsigned nlm, const C* __restrict__ tw, Ld ld, St st) {
+  constexpr int LR = L / R_;
+  constexpr int twstep = L / (Ns * R_);
+  for (int t = threadIdx.x; t < nl * LR; t += blockDim.x) {
+    const int j = fast_div(t, nl, nlm);
+    const int l = t - j * nl;
+    const int jq = j / Ns;
+    const int k = j - jq * Ns;
+    C v[R_];
+#pragma unroll
+    for (int r = 0; r < R_; ++r) {
+      C x = ld(j + r * LR, l);
+      if (r > 0 && Ns > 1) {
+        const C w = tw[k * r * twstep];
+        x = (S < 0) ? cmul(x, w) : cmulc(x, w);
+      }
+      v[r] = x;
+    }
+    dft<R_, S>(v);
+    const int ob = jq * Ns * R_ + k;
+#pragma unroll
+    for (int q = 0; q < R_; ++q) st(ob + q * Ns, l, v[q]);
+  }
+  __syncthreads();
+}
+
+// Two-stage transform of length R0 * R1 over nl lines: stage one reads
+// through ld and writes tmp (interleaved), stage two reads tmp and writes
+// through st.
+template <int S, int R0, int R1, typename C, typename Ld, typename St>
+__device__ __forceinline__ void line_fft2_f(int nl, unsigned nlm, const C* __restrict__ tw, C* __restrict__ tmp, Ld ld,
+                                            St st) {
+  stage_f<R0, 1, R0 * R1, S>(nl, nlm, tw, ld, [&](int e, int l, C v) { tmp[e * nl + l] = v; });
+  stage_f<R1, R0, R0 * R1, S>(nl, nlm, tw, [&](int e, int l) { return tmp[e * nl + l]; }, st);
+}
+
 }  // namespace pwgpu

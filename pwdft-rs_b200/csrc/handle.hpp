@@ -80,6 +80,9 @@ struct Handle {
   // effective potential per spin in real space
   double* veff_r[2] = {nullptr, nullptr};
   float* veff_r32[2] = {nullptr, nullptr};
+  // the same potential z-major ([z][x][y]): the fused y/x pass reads one z-plane contiguously
+  double* veff_rz[2] = {nullptr, nullptr};
+  float* veff_rz32[2] = {nullptr, nullptr};
   // H|psi> scratch: band-chunked compact grids (L2-resident per chunk)
   int chunk = 1;
   void* work_a = nullptr;   // chunk * ncol * d2 complex (FP64 size)
@@ -142,6 +145,8 @@ Status build_grid_maps(Handle& h, const int* miller_host);
 Status apply_h_device(Handle& h, int spin, int ik, const double2* psi, long ldpsi, int nb, double2* hpsi,
                       long ldh, int precision, cudaStream_t stream, StageTimer* timer = nullptr);
 Status set_veff_from_g(Handle& h, int spin, const double2* veff_g_dev, cudaStream_t stream);
+// Refresh the z-major copies (veff_rz, veff_rz32) of veff_r[spin].
+Status veff_zmajor(Handle& h, int spin, cudaStream_t stream);
 Status ensure_nl_capacity(Handle& h, int nb);
 // P = B^H psi into h.nl_p and Q = D P into h.nl_q (FP64), nb columns.
 Status nonlocal_pq(Handle& h, int ik, const double2* psi, long ldpsi, int nb, cudaStream_t s,

@@ -11,11 +11,16 @@
 //
 // Pipeline per chunk of bands (intermediates sized to stay in L2):
 //   K1 z-inverse on the Xp*Yp sphere columns, scattering psi(G)   -> A
+//   K234, one kernel per z-plane of A (z-major) and group of bands, the plane
+//        in shared memory: y-inverse of the Xp compact x-planes, x-inverse,
+//        multiply by V(r), x-forward, y-forward keeping the Yp sphere rows
+//   K5 z-forward, gather the sphere, scale 1/N, add T psi          A -> Hpsi
+// then  P = B^H psi,  Q = D P (block diagonal),  Hpsi += B Q.
+// Grids whose plane does not fit shared memory run the middle as three
+// kernels over a second intermediate B (column-major A):
 //   K2 y-inverse per compact x-plane                               A -> B
 //   K3 x-inverse, multiply by V(r), x-forward (in place)           B
 //   K4 y-forward, keep the Yp sphere rows                          B -> A
-//   K5 z-forward, gather the sphere, scale 1/N, add T psi          A -> Hpsi
-// then  P = B^H psi,  Q = D P (block diagonal),  Hpsi += B Q.
 #include <cublas_v2.h>
 
 #include <algorithm>
@@ -48,12 +53,15 @@ template <typename C> __device__ __forceinline__ C to_c(double2 v) { return cmak
 // interleaved lines of the tile, threadIdx.y strides along the lines.
 
 // K1: scatter sphere coefficients of W columns and z-inverse-FFT them.
-template <typename R>
+// ZM: A is z-major ([band][z][column]) for the fused middle kernel, else
+// column-major ([band][column][z]).
+template <typename R, bool ZM = false>
 __global__ void __launch_bounds__(kThreads) k_zinv(const double2* __restrict__ psi, long ldpsi,
                                                   cplx<R>* __restrict__ A, const int* __restrict__ col_start,
                                                   const int* __restrict__ pt_ig, const int* __restrict__ pt_col,
                                                   const int* __restrict__ pt_z, int ncol, int d2, unsigned md2,
-                                                  FftPlan pz, const cplx<R>* __restrict__ twz) {
+                                                  FftPlan pz, const cplx<R>* __restrict__ twz,
+                                                  unsigned mw = 0) {
   using C = cplx<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int W = blockDim.x;
@@ -71,22 +79,30 @@ __global__ void __launch_bounds__(kThreads) k_zinv(const double2* __restrict__ p
   for (int i = i0 + tid; i < i1; i += T) buf[pt_z[i] * W + (pt_col[i] - c0)] = to_c<C>(ps[pt_ig[i]]);
   __syncthreads();
   const C* res = fft_lines<+1>(buf, scr, pz, W, twz);
-  C* out = A + ((long)b * ncol + c0) * d2;
-  for (int i = tid; i < nl * d2; i += T) {
-    const int c = fast_div(i, d2, md2), e = i - c * d2;
-    out[i] = res[e * W + c];
+  if constexpr (ZM) {
+    C* out = A + (long)b * d2 * ncol + c0;
+    for (int i = tid; i < W * d2; i += T) {
+      const int e = fast_div(i, W, mw), c = i - e * W;
+      if (c < nl) out[(long)e * ncol + c] = res[e * W + c];
+    }
+  } else {
+    C* out = A + ((long)b * ncol + c0) * d2;
+    for (int i = tid; i < nl * d2; i += T) {
+      const int c = fast_div(i, d2, md2), e = i - c * d2;
+      out[i] = res[e * W + c];
+    }
   }
 }
 
 // K5: z-forward-FFT W columns, gather the sphere, Hpsi = buf/N + T psi.
-template <typename R>
+template <typename R, bool ZM = false>
 __global__ void __launch_bounds__(kThreads) k_zfwd(const cplx<R>* __restrict__ A, const double2* __restrict__ psi,
                                                   long ldpsi, double2* __restrict__ hpsi, long ldh,
                                                   const double* __restrict__ kin, double scale,
                                                   const int* __restrict__ col_start, const int* __restrict__ pt_ig,
                                                   const int* __restrict__ pt_col, const int* __restrict__ pt_z,
                                                   int ncol, int d2, unsigned md2, FftPlan pz,
-                                                  const cplx<R>* __restrict__ twz) {
+                                                  const cplx<R>* __restrict__ twz, unsigned mw = 0) {
   using C = cplx<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int W = blockDim.x;
@@ -97,11 +113,20 @@ __global__ void __launch_bounds__(kThreads) k_zfwd(const cplx<R>* __restrict__ A
   const int nl = min(W, ncol - c0);
   const int tid = threadIdx.y * W + threadIdx.x;
   const int T = W * blockDim.y;
-  const C* in = A + ((long)b * ncol + c0) * d2;
   // asynchronous copies, columns past the last one zero-filled
-  for (int i = tid; i < W * d2; i += T) {
-    const int c = fast_div(i, d2, md2), e = i - c * d2;
-    cp_async_zfill<sizeof(C)>(&buf[e * W + c], c < nl ? (const void*)(in + i) : (const void*)A, c < nl);
+  if constexpr (ZM) {
+    const C* in = A + (long)b * d2 * ncol + c0;
+    for (int i = tid; i < W * d2; i += T) {
+      const int e = fast_div(i, W, mw), c = i - e * W;
+      cp_async_zfill<sizeof(C)>(&buf[e * W + c], c < nl ? (const void*)(in + (long)e * ncol + c) : (const void*)A,
+                                c < nl);
+    }
+  } else {
+    const C* in = A + ((long)b * ncol + c0) * d2;
+    for (int i = tid; i < W * d2; i += T) {
+      const int c = fast_div(i, d2, md2), e = i - c * d2;
+      cp_async_zfill<sizeof(C)>(&buf[e * W + c], c < nl ? (const void*)(in + i) : (const void*)A, c < nl);
+    }
   }
   cp_async_commit();
   cp_async_wait<0>();
@@ -211,6 +236,206 @@ __global__ void __launch_bounds__(kThreads) k_xv(cplx<R>* __restrict__ B, const 
   const C* r2 = fft_lines<-1>(r1, r1 == buf ? scr : buf, px, W, twx);
   if (!live) return;
   for (int q = threadIdx.y; q < Xp; q += blockDim.y) base[(long)q * plane] = r2[wrap_idx(q - m0, d0) * W + w];
+}
+
+// K234: one z-plane of the z-major A (ncol = Xp*Yp compact columns) for a
+// group of bands, the whole plane in shared memory: y-inverse of the Xp
+// compact x-planes (Xp lines of length d1), expansion to all d0 x rows,
+// x-inverse (d1 lines of length d0), multiplication by this plane of V(r),
+// x-forward, compaction to the Xp x-planes, y-forward, and the Yp sphere rows
+// written back in place.  Shared memory: the plane XB (d0 x d1, lines along
+// x interleaved by y), its Stockham scratch XS (which also holds the y-lines
+// YB/YS, Xp x d1 each, element y of line p at y*Xp + p) and the V(r) plane.
+// The x transforms run inverse then forward on the same plan, so their
+// result is back in XB whatever the stage count, and the y buffers in XS are
+// free again.  Global traffic per band: the compact plane read and written
+// once (contiguous), V(r) once per block.
+template <typename R>
+__global__ void __launch_bounds__(kThreads) k_yxy(cplx<R>* __restrict__ A, const R* __restrict__ vz, int nb, int bpc,
+                                                 int Xp, int Yp, int m0, int m1, int d0, int d1, int d2,
+                                                 unsigned mXp, unsigned mYp, unsigned md1, FftPlan px, FftPlan py,
+                                                 const cplx<R>* __restrict__ twx, const cplx<R>* __restrict__ twy) {
+  using C = cplx<R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int z = blockIdx.x;
+  const int plane = d0 * d1;
+  const int ncol = Xp * Yp;
+  const int ny = Xp * d1;
+  C* XB = reinterpret_cast<C*>(smem_raw);
+  C* XS = XB + plane;
+  R* VP = reinterpret_cast<R*>(XS + plane);
+  C* YB = XS;
+  C* YS = XS + ny;
+  const int tid = threadIdx.x, T = blockDim.x;
+  for (int i = tid; i < plane; i += T) VP[i] = vz[(long)z * plane + i];
+  const int b0 = blockIdx.y * bpc;
+  const int b1 = min(nb, b0 + bpc);
+  for (int b = b0; b < b1; ++b) {
+    C* Ab = A + ((long)b * d2 + z) * ncol;
+    // compact rows q < Yp into y = wrap(q - m1); the rows between stay zero
+    for (int i = tid; i < ncol; i += T) {
+      const int p = fast_div(i, Yp, mYp), q = i - p * Yp;
+      const int y = q - m1 < 0 ? q - m1 + d1 : q - m1;
+      YB[y * Xp + p] = Ab[i];
+    }
+    for (int i = tid; i < (d1 - Yp) * Xp; i += T) YB[(m1 + 1) * Xp + i] = cmake<C>(0.0, 0.0);
+    __syncthreads();
+    const C* yr = line_fft<+1>(YB, YS, py, Xp, mXp, twy);
+    // expand: x row wrap(p - m0) <- compact plane p, the other x rows zero
+    for (int i = tid; i < plane; i += T) {
+      const int x = fast_div(i, d1, md1), y = i - x * d1;
+      const int p = x <= m0 ? x + m0 : (x >= d0 - m0 ? x - d0 + m0 : -1);
+      XB[i] = p >= 0 ? yr[y * Xp + p] : cmake<C>(0.0, 0.0);
+    }
+    __syncthreads();
+    C* xr = line_fft<+1>(XB, XS, px, d1, md1, twx);
+    for (int i = tid; i < plane; i += T) xr[i] = xr[i] * VP[i];
+    __syncthreads();
+    C* xf = line_fft<-1>(xr, xr == XB ? XS : XB, px, d1, md1, twx);  // == XB
+    for (int i = tid; i < ny; i += T) {
+      const int y = fast_div(i, Xp, mXp), p = i - y * Xp;
+      const int x = p - m0 < 0 ? p - m0 + d0 : p - m0;
+      YB[i] = xf[x * d1 + y];
+    }
+    __syncthreads();
+    const C* yf = line_fft<-1>(YB, YS, py, Xp, mXp, twy);
+    for (int i = tid; i < ncol; i += T) {
+      const int p = fast_div(i, Yp, mYp), q = i - p * Yp;
+      const int y = q - m1 < 0 ? q - m1 + d1 : q - m1;
+      Ab[i] = yf[y * Xp + p];
+    }
+    __syncthreads();
+  }
+}
+
+// The same pass with both axes of two-stage lengths known at compile time
+// (x: X0 * X1, y: Y0 * Y1) and the data movement folded into the stages:
+// the y-inverse's second stage scatters into the x layout, the x-inverse's
+// first stage gathers the compact x-planes (other rows zero), the x-forward's
+// first stage multiplies by V(r), its second stage keeps only the compact
+// x-planes in the y layout.  Twiddles staged in shared memory.  Buffers:
+// P0 (d0 x d1), P1 (d0 x d1), YB/YS inside P1 while the y-lines are live.
+constexpr int kYxyThreads = 512;
+template <typename R, int X0, int X1, int Y0, int Y1>
+__global__ void __launch_bounds__(kYxyThreads) k_yxy_ct(cplx<R>* __restrict__ A, const R* __restrict__ vz, int nb,
+                                                       int bpc, int Xp, int Yp, int m0, int m1, int d2, unsigned mXp,
+                                                       unsigned mYp, unsigned md1, const cplx<R>* __restrict__ twx,
+                                                       const cplx<R>* __restrict__ twy) {
+  using C = cplx<R>;
+  constexpr int d0 = X0 * X1, d1 = Y0 * Y1, plane = d0 * d1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int z = blockIdx.x;
+  const int ncol = Xp * Yp;
+  const int ny = Xp * d1;
+  C* P0 = reinterpret_cast<C*>(smem_raw);
+  C* P1 = P0 + plane;
+  R* VP = reinterpret_cast<R*>(P1 + plane);
+  C* TX = reinterpret_cast<C*>(VP + plane);  // d0 twiddles of x
+  C* TY = TX + d0;                            // d1 twiddles of y
+  C* YB = P1;
+  C* YS = P1 + ny;
+  const int tid = threadIdx.x, T = blockDim.x;
+  for (int i = tid; i < plane; i += T) VP[i] = vz[(long)z * plane + i];
+  for (int i = tid; i < d0; i += T) TX[i] = twx[i];
+  for (int i = tid; i < d1; i += T) TY[i] = twy[i];
+  const int b0 = blockIdx.y * bpc;
+  const int b1 = min(nb, b0 + bpc);
+  for (int b = b0; b < b1; ++b) {
+    C* Ab = A + ((long)b * d2 + z) * ncol;
+    __syncthreads();  // the previous band's readers of YB are done (and the staging above is visible)
+    for (int i = tid; i < ncol; i += T) {
+      const int p = fast_div(i, Yp, mYp), q = i - p * Yp;
+      const int y = q - m1 < 0 ? q - m1 + d1 : q - m1;
+      YB[y * Xp + p] = Ab[i];
+    }
+    for (int i = tid; i < (d1 - Yp) * Xp; i += T) YB[(m1 + 1) * Xp + i] = cmake<C>(0.0, 0.0);
+    __syncthreads();
+    // y-inverse: Xp lines (element y of line p at y*Xp + p); the result goes straight to the x
+    // layout of P0 (element x of line y at x*d1 + y) at x = wrap(p - m0)
+    line_fft2_f<+1, Y0, Y1>(Xp, mXp, TY, YS, [&](int e, int l) { return YB[e * Xp + l]; },
+                            [&](int e, int l, C v) {
+                              const int x = l - m0 < 0 ? l - m0 + d0 : l - m0;
+                              P0[x * d1 + e] = v;
+                            });
+    // x-inverse: d1 lines; rows outside the compact x range are zero (never stored above)
+    line_fft2_f<+1, X0, X1>(d1, md1, TX, P1,
+                            [&](int e, int l) {
+                              return (e <= m0 || e >= d0 - m0) ? P0[e * d1 + l] : cmake<C>(0.0, 0.0);
+                            },
+                            [&](int e, int l, C v) { P0[e * d1 + l] = v * VP[e * d1 + l]; });
+    // x-forward; the second stage keeps the compact x-planes, in the y layout of YB
+    line_fft2_f<-1, X0, X1>(d1, md1, TX, P1, [&](int e, int l) { return P0[e * d1 + l]; },
+                            [&](int e, int l, C v) {
+                              if (e <= m0 || e >= d0 - m0) {
+                                const int p = e <= m0 ? e + m0 : e - d0 + m0;
+                                P0[l * Xp + p] = v;
+                              }
+                            });
+    // y-forward on the compact planes (now in P0 as y-lines), the sphere rows back to A
+    line_fft2_f<-1, Y0, Y1>(Xp, mXp, TY, P1, [&](int e, int l) { return P0[e * Xp + l]; },
+                            [&](int e, int l, C v) {
+                              if (e <= m1 || e >= d1 - m1) {
+                                const int q = e <= m1 ? e + m1 : e - d1 + m1;
+                                Ab[l * Yp + q] = v;
+                              }
+                            });
+  }
+}
+
+template <typename R> inline size_t yxy_ct_smem(int d0, int d1) {
+  return 2 * (size_t)d0 * d1 * sizeof(cplx<R>) + (size_t)d0 * d1 * sizeof(R) + (size_t)(d0 + d1) * sizeof(cplx<R>);
+}
+
+// Shared memory of a k_yxy block: two d0 x d1 planes and the V(r) plane.
+template <typename R> inline size_t yxy_smem(int d0, int d1) {
+  return 2 * (size_t)d0 * d1 * sizeof(cplx<R>) + (size_t)d0 * d1 * sizeof(R);
+}
+constexpr size_t kFusedSmemMax = 227 * 1024;
+
+// The fused middle kernel serves grids whose plane (two copies plus V(r))
+// fits shared memory and whose y-lines (2 Xp d1) fit in one plane.
+template <typename R> inline bool fused_ok(const GridMaps& g) {
+  return yxy_smem<R>(g.d[0], g.d[1]) <= kFusedSmemMax && 2 * g.Xp <= g.d[0];
+}
+
+// Launch the compile-time form of the fused pass when the x and y lengths
+// are one of the instantiated two-stage lengths (72, 40, 25, 24 on both
+// axes); false otherwise (the caller runs the generic k_yxy).
+template <typename R, int X0, int X1>
+void launch_yxy_ct_n(const GridMaps& g, cplx<R>* A, const R* vz, int nb, int bpc, const cplx<R>* twx,
+                     const cplx<R>* twy, cudaStream_t s) {
+  k_yxy_ct<R, X0, X1, X0, X1><<<dim3(g.d[2], (nb + bpc - 1) / bpc), kYxyThreads, yxy_ct_smem<R>(g.d[0], g.d[1]), s>>>(
+      A, vz, nb, bpc, g.Xp, g.Yp, g.m[0], g.m[1], g.d[2], div_magic(g.Xp), div_magic(g.Yp), div_magic(g.d[1]), twx,
+      twy);
+  count_launch();
+}
+inline int two_stage_key(const FftPlan& p) { return p.nstages == 2 ? p.radix[0] * 16 + p.radix[1] : -1; }
+template <typename R>
+bool launch_yxy_ct(const GridMaps& g, cplx<R>* A, const R* vz, int nb, int bpc, const cplx<R>* twx,
+                   const cplx<R>* twy, cudaStream_t s) {
+  const int kx = two_stage_key(g.plan[0]);
+  if (kx != two_stage_key(g.plan[1]) || yxy_ct_smem<R>(g.d[0], g.d[1]) > kFusedSmemMax) return false;
+  switch (kx) {
+    case 8 * 16 + 9: launch_yxy_ct_n<R, 8, 9>(g, A, vz, nb, bpc, twx, twy, s); return true;
+    case 8 * 16 + 5: launch_yxy_ct_n<R, 8, 5>(g, A, vz, nb, bpc, twx, twy, s); return true;
+    case 5 * 16 + 5: launch_yxy_ct_n<R, 5, 5>(g, A, vz, nb, bpc, twx, twy, s); return true;
+    case 8 * 16 + 3: launch_yxy_ct_n<R, 8, 3>(g, A, vz, nb, bpc, twx, twy, s); return true;
+    default: return false;
+  }
+}
+
+// V(r) [x][y][z] -> [z][x][y], FP64 and FP32
+__global__ void k_zmajor(const double* __restrict__ vr, double* __restrict__ vz64, float* __restrict__ vz32, int d0,
+                         int d1, int d2) {
+  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long n = (long)d0 * d1 * d2;
+  if (i >= n) return;
+  const int z = (int)(i % d2);
+  const long xy = i / d2;
+  const long o = (long)z * d0 * d1 + xy;
+  const double v = vr[i];
+  vz64[o] = v;
+  vz32[o] = (float)v;
 }
 
 // Shared memory of a k_xv tile: two W x d0 line buffers, plus the V(r) rows
@@ -418,6 +643,19 @@ Status configure_kernels() {
   set((const void*)k_xv<double>); set((const void*)k_xv<float>);
   set((const void*)k_fft_axis<1>); set((const void*)k_fft_axis<-1>);
   set((const void*)k_x_density);
+  set((const void*)k_zinv<double, true>); set((const void*)k_zinv<float, true>);
+  set((const void*)k_zfwd<double, true>); set((const void*)k_zfwd<float, true>);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)k_yxy<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFusedSmemMax);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute((const void*)k_yxy<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFusedSmemMax);
+  auto set_big = [&](const void* f) {
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFusedSmemMax);
+  };
+  set_big((const void*)k_yxy_ct<double, 8, 9, 8, 9>); set_big((const void*)k_yxy_ct<float, 8, 9, 8, 9>);
+  set_big((const void*)k_yxy_ct<double, 8, 5, 8, 5>); set_big((const void*)k_yxy_ct<float, 8, 5, 8, 5>);
+  set_big((const void*)k_yxy_ct<double, 5, 5, 5, 5>); set_big((const void*)k_yxy_ct<float, 5, 5, 5, 5>);
+  set_big((const void*)k_yxy_ct<double, 8, 3, 8, 3>); set_big((const void*)k_yxy_ct<float, 8, 3, 8, 3>);
   if (e != cudaSuccess) return fail(kCuda, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
   done_devices.insert(dev);
   return kOk;
@@ -654,6 +892,15 @@ Status set_veff_from_g(Handle& h, int spin, const double2* veff_g_dev, cudaStrea
   if (st != kOk) return st;
   k_real_to_r32<<<(unsigned)((N + 255) / 256), 256, 0, stream>>>(h.tmp_grid, h.veff_r[spin], h.veff_r32[spin], N); count_launch();
   PW_CUDA_TRY(cudaGetLastError());
+  return veff_zmajor(h, spin, stream);
+}
+
+Status veff_zmajor(Handle& h, int spin, cudaStream_t stream) {
+  const long N = h.g.N;
+  k_zmajor<<<(unsigned)((N + 255) / 256), 256, 0, stream>>>(h.veff_r[spin], h.veff_rz[spin], h.veff_rz32[spin], h.g.d[0],
+                                                            h.g.d[1], h.g.d[2]);
+  count_launch();
+  PW_CUDA_TRY(cudaGetLastError());
   return kOk;
 }
 
@@ -692,6 +939,28 @@ static Status local_chunk(Handle& h, int spin, int ik, const double2* psi, long 
   const C* tw2 = std::is_same<R, double>::value ? (const C*)g.tw64[2] : (const C*)g.tw32[2];
   const R* vr = std::is_same<R, double>::value ? (const R*)h.veff_r[spin] : (const R*)h.veff_r32[spin];
   const double scale = 1.0 / (double)g.N;
+  if (fused_ok<R>(g)) {
+    // K1 (z-major A), K234 fused per z-plane, K5
+    const R* vz = std::is_same<R, double>::value ? (const R*)h.veff_rz[spin] : (const R*)h.veff_rz32[spin];
+    k_zinv<R, true><<<dim3((g.ncol + wz - 1) / wz, nb), block_for(wz), 2 * (size_t)wz * d2 * sizeof(C), s>>>(
+        psi, ldpsi, A, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2, div_magic(d2), g.plan[2], tw2,
+        div_magic(wz)); count_launch();
+    mark(tm, 0, s);
+    const int groups = std::max(1, std::min(nb, (2 * 148 + d2 - 1) / d2));
+    const int bpc = (nb + groups - 1) / groups;
+    if (!launch_yxy_ct<R>(g, A, vz, nb, bpc, tw0, tw1, s)) {
+      k_yxy<R><<<dim3(d2, (nb + bpc - 1) / bpc), kThreads, yxy_smem<R>(d0, d1), s>>>(
+          A, vz, nb, bpc, g.Xp, g.Yp, g.m[0], g.m[1], d0, d1, d2, div_magic(g.Xp), div_magic(g.Yp), div_magic(d1),
+          g.plan[0], g.plan[1], tw0, tw1); count_launch();
+    }
+    mark(tm, 2, s);
+    k_zfwd<R, true><<<dim3((g.ncol + wz - 1) / wz, nb), block_for(wz), 2 * (size_t)wz * d2 * sizeof(C), s>>>(
+        A, psi, ldpsi, hpsi, ldh, h.kp[ik].kinetic, scale, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2,
+        div_magic(d2), g.plan[2], tw2, div_magic(wz)); count_launch();
+    mark(tm, 4, s);
+    PW_CUDA_TRY(cudaGetLastError());
+    return kOk;
+  }
   {
     dim3 grid((g.ncol + wz - 1) / wz, nb);
     k_zinv<R><<<grid, block_for(wz), 2 * (size_t)wz * d2 * sizeof(C), s>>>(

@@ -641,6 +641,7 @@ static Status potentials(Handle& h, const double* rho, bool set_hpsi, PotEnergie
     PW_CUDA_TRY(cudaMemcpyAsync(h.tmp_grid, st->cg2, N * sizeof(double2), cudaMemcpyDeviceToDevice, s));
     if ((r = fft3d_full(h, h.tmp_grid, +1, s)) != kOk) return r;
     k_real_part_both<<<blocks_for(N), 256, 0, s>>>(h.tmp_grid, h.veff_r[0], h.veff_r32[0], N); count_launch();
+    if ((r = veff_zmajor(h, 0, s)) != kOk) return r;
   }
   PW_CUDA_TRY(cudaGetLastError());
   return kOk;
@@ -1115,6 +1116,7 @@ static Status potentials_spin(Handle& h, const double* up, const double* dn, boo
     PW_CUDA_TRY(cudaMemcpyAsync(h.tmp_grid, st->cg2, N * sizeof(double2), cudaMemcpyDeviceToDevice, s));
     if ((r = fft3d_full(h, h.tmp_grid, +1, s)) != kOk) return r;
     k_real_part_both<<<blocks_for(N), 256, 0, s>>>(h.tmp_grid, h.veff_r[sp], h.veff_r32[sp], N); count_launch();
+    if ((r = veff_zmajor(h, sp, s)) != kOk) return r;
   }
   PW_CUDA_TRY(cudaGetLastError());
   return kOk;
