@@ -268,6 +268,17 @@ pwgpu_status pwgpu_eigensolve(pwgpu_handle* h, int32_t spin, int32_t ik, int32_t
                               int32_t max_iter, const double* psi_in, double* evals, double* psi_out,
                               int32_t* iters, double* max_residual);
 
+/* H applied to nb bands of a Gamma-real handle in its packed real form
+ * (u = [Re psi(0), sqrt2 Re psi(G_p), sqrt2 Im psi(G_p)] over the half
+ * sphere, n_pw reals per band, column-major), at the handle's precision: the
+ * operator the Gamma-only eigensolver applies (two bands per complex FFT; in
+ * the mixed form the projector products as 3xBF16 tensor-core GEMMs).
+ * Diagnostic; the packing itself has no reference counterpart (the
+ * reference keeps complex bands), the operator is H of
+ * scf/potentials.rs:163-190 + potential/nonlocal.rs:432-450.
+ * PWGPU_E_STATE on a handle with complex bands. */
+pwgpu_status pwgpu_apply_h_packed(pwgpu_handle* h, int32_t spin, const double* u, int32_t nb, double* hu);
+
 /* The bands of (spin, ik) left on the device by the last pwgpu_scf_run (its
  * final eigensolve) or pwgpu_eigensolve: the first n_bands eigenvectors as
  * complex columns (n_pw x n_bands, column-major, basis order), ascending in

@@ -395,6 +395,32 @@ pwgpu_status pwgpu_eigensolve(pwgpu_handle* ph, int32_t spin, int32_t ik, int32_
                       ph->precision);
 }
 
+pwgpu_status pwgpu_apply_h_packed(pwgpu_handle* ph, int32_t spin, const double* u, int32_t nb, double* hu) {
+  if (!ph || !u || !hu) return fail(kInvalid, "pwgpu_apply_h_packed: NULL argument");
+  Handle& h = ph->h;
+  if (!h.gam.on) return fail(kState, "pwgpu_apply_h_packed: not a Gamma-real handle");
+  if (spin < 0 || spin >= h.nspin) return fail(kInvalid, "pwgpu_apply_h_packed: spin index out of range");
+  if (nb <= 0) return kOk;
+  PW_CUDA_TRY(cudaSetDevice(h.device));
+  const size_t bytes = (size_t)h.n_pw * nb * sizeof(double);
+  double *du = nullptr, *dh = nullptr;
+  if (cudaMalloc((void**)&du, bytes) != cudaSuccess || cudaMalloc((void**)&dh, bytes) != cudaSuccess) {
+    cudaFree(du);
+    cudaFree(dh);
+    return fail(kOom, "pwgpu_apply_h_packed: allocation failed");
+  }
+  Status st = kOk;
+  cudaError_t e = cudaMemcpyAsync(du, u, bytes, cudaMemcpyHostToDevice, h.stream);
+  if (e == cudaSuccess) st = apply_h_real(h, spin, du, h.n_pw, nb, dh, h.n_pw, ph->precision, h.stream);
+  if (e == cudaSuccess && st == kOk) e = cudaMemcpyAsync(hu, dh, bytes, cudaMemcpyDeviceToHost, h.stream);
+  if (e == cudaSuccess && st == kOk) e = cudaStreamSynchronize(h.stream);
+  cudaFree(du);
+  cudaFree(dh);
+  if (st != kOk) return st;
+  if (e != cudaSuccess) return fail(kCuda, std::string("pwgpu_apply_h_packed: ") + cudaGetErrorString(e));
+  return kOk;
+}
+
 pwgpu_status pwgpu_get_bands(pwgpu_handle* ph, int32_t spin, int32_t ik, int32_t n_bands, double* psi_out) {
   if (!ph || !psi_out) return fail(kInvalid, "pwgpu_get_bands: NULL argument");
   PW_CUDA_TRY(cudaSetDevice(ph->h.device));

@@ -341,25 +341,20 @@ Status gamma_unpack(Handle& h, const double* u, long ldu, int ncols, double2* x,
   return kOk;
 }
 
-Status nonlocal_pq_real(Handle& h, const double* u, long ldu, int nb, cudaStream_t s) {
-  if (!h.gam.on) return fail(kState, "nonlocal_pq_real: not a Gamma-real handle");
-  if (h.n_ch <= 0 || nb <= 0) return kOk;
+Status ensure_gamma_pq(Handle& h, int nb) {
+  if (nb <= h.gam_pcap) return kOk;
+  if (h.gam_p) cudaFree(h.gam_p);
+  if (h.gam_q) cudaFree(h.gam_q);
+  h.gam_p = h.gam_q = nullptr;
+  h.gam_pcap = 0;
   Status r;
-  if (nb > h.gam_pcap) {
-    if (h.gam_p) cudaFree(h.gam_p);
-    if (h.gam_q) cudaFree(h.gam_q);
-    h.gam_p = h.gam_q = nullptr;
-    h.gam_pcap = 0;
-    if ((r = galloc(&h.gam_p, (size_t)h.n_ch * nb)) != kOk) return r;
-    if ((r = galloc(&h.gam_q, (size_t)h.n_ch * nb)) != kOk) return r;
-    h.gam_pcap = nb;
-  }
-  const int n = h.n_pw;
-  cublasSetStream(h.blas, s);
-  const double one = 1.0, zero = 0.0;
-  if (cublasDgemm(h.blas, CUBLAS_OP_T, CUBLAS_OP_N, h.n_ch, nb, n, &one, h.gam.b_real, n, u, (int)ldu, &zero, h.gam_p,
-                  h.n_ch) != CUBLAS_STATUS_SUCCESS)
-    return fail(kCuda, "cublasDgemm (B^T u) failed");
+  if ((r = galloc(&h.gam_p, (size_t)h.n_ch * nb)) != kOk) return r;
+  if ((r = galloc(&h.gam_q, (size_t)h.n_ch * nb)) != kOk) return r;
+  h.gam_pcap = nb;
+  return kOk;
+}
+
+Status apply_d_real(Handle& h, int nb, cudaStream_t s) {
   const long tot = (long)h.n_ch * nb;
   k_apply_d_real<<<blocks_for(tot), 256, 0, s>>>(h.gam_p, h.gam_q, h.n_ch, nb, h.ch_atom, h.atom_ch_start, h.d_off,
                                                  h.d_vals);
@@ -367,6 +362,27 @@ Status nonlocal_pq_real(Handle& h, const double* u, long ldu, int nb, cudaStream
   PW_CUDA_TRY(cudaGetLastError());
   return kOk;
 }
+
+Status nonlocal_pq_real(Handle& h, const double* u, long ldu, int nb, cudaStream_t s) {
+  if (!h.gam.on) return fail(kState, "nonlocal_pq_real: not a Gamma-real handle");
+  if (h.n_ch <= 0 || nb <= 0) return kOk;
+  Status r;
+  if ((r = ensure_gamma_pq(h, nb)) != kOk) return r;
+  const int n = h.n_pw;
+  cublasSetStream(h.blas, s);
+  const double one = 1.0, zero = 0.0;
+  if (cublasDgemm(h.blas, CUBLAS_OP_T, CUBLAS_OP_N, h.n_ch, nb, n, &one, h.gam.b_real, n, u, (int)ldu, &zero, h.gam_p,
+                  h.n_ch) != CUBLAS_STATUS_SUCCESS)
+    return fail(kCuda, "cublasDgemm (B^T u) failed");
+  return apply_d_real(h, nb, s);
+}
+
+// Blocks narrower than this keep the FP64 projector GEMMs in the mixed form:
+// both forms then stream the projector matrix once per product (the split
+// operands hold 12 bytes per element against 16 in FP64), so the tensor
+// cores gain little while their 128x128 tiles crowd the batch's other
+// solves (measured on the four-cell Si64 batch).
+constexpr int kMixedRealMinBands = 96;
 
 Status apply_h_real(Handle& h, int spin, const double* u, long ldu, int nb, double* hu, long ldh, int precision,
                     cudaStream_t s) {
@@ -383,7 +399,10 @@ Status apply_h_real(Handle& h, int spin, const double* u, long ldu, int nb, doub
   if ((r = apply_local_device(h, spin, 0, h.gam_c1, n, npairs, h.gam_c2, n, precision, s)) != kOk) return r;
   k_pack_pairs<<<grid, 256, 0, s>>>(h.gam_c2, n, nb, hu, ldh, g.half_idx, g.half_neg, g.zero, g.nh);
   count_launch();
-  if (h.n_ch > 0) {
+  if (h.n_ch > 0 && precision == 1 && nl_mixed_eligible(h) && nb >= kMixedRealMinBands) {
+    // mixed form, wide blocks: both projector products as 3xBF16 tensor-core GEMMs
+    if ((r = nonlocal_mixed_real(h, u, ldu, nb, hu, ldh, s)) != kOk) return r;
+  } else if (h.n_ch > 0) {
     if ((r = nonlocal_pq_real(h, u, ldu, nb, s)) != kOk) return r;
     const double one = 1.0;
     if (cublasDgemm(h.blas, CUBLAS_OP_N, CUBLAS_OP_N, n, nb, h.n_ch, &one, g.b_real, n, h.gam_q, h.n_ch, &one, hu,

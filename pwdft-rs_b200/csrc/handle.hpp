@@ -99,6 +99,7 @@ struct Handle {
   int* solver_info = nullptr;
   struct ScfState* scf = nullptr;  // device state of the SCF loop (scf.cu)
   struct NlMixed* nlm = nullptr;   // split projector operands of the mixed form (nl_mixed.cu)
+  struct NlMixed* nlm_real = nullptr;  // the same for the packed real projectors of Gamma-real handles
   GammaData gam;
   // per-call scratch of the Gamma path (lane-owned like nl_p / nl_q)
   double2* gam_c1 = nullptr;
@@ -132,6 +133,8 @@ Status apply_d_blocks(Handle& h, int nb, cudaStream_t s);
 bool nl_mixed_eligible(const Handle& h);
 Status nonlocal_mixed(Handle& h, int ik, const double2* psi, long ldpsi, int nb, double2* hpsi, long ldh,
                       cudaStream_t s, StageTimer* tm = nullptr);
+// The same for packed real bands of a Gamma-real handle: hu += B_r D B_r^T u.
+Status nonlocal_mixed_real(Handle& h, const double* u, long ldu, int nb, double* hu, long ldh, cudaStream_t s);
 void release_nl_mixed(Handle& h);
 
 // Per-band kinetic and nonlocal expectations of nb columns of V at k-point ik
@@ -208,6 +211,9 @@ void release_gamma_scratch(Handle& h);
 // one complex vector, then real projector GEMMs).
 Status apply_h_real(Handle& h, int spin, const double* u, long ldu, int nb, double* hu, long ldh, int precision,
                     cudaStream_t s);
+// Capacity of the Gamma path's P / Q buffers (n_ch x nb), and Q = D P on them.
+Status ensure_gamma_pq(Handle& h, int nb);
+Status apply_d_real(Handle& h, int nb, cudaStream_t s);
 // P = B_r^T u into h.gam_p and Q = D P into h.gam_q for nb packed real bands.
 Status nonlocal_pq_real(Handle& h, const double* u, long ldu, int nb, cudaStream_t s);
 // rho += sum_b fw[b] |psi_b(r)|^2 for nb packed real bands (fw on the host).

@@ -12,6 +12,12 @@
 // into split-K slices through the GEMM's batch index; the slice partials
 // are summed in FP64 by the epilogue kernel that also forms complex P.  The
 // projector operands are constant per k-point and are split once.
+//
+// Gamma-real handles hold their bands and projectors as packed real vectors
+// (B_r, n_pw x n_ch); their two products are real from the start:
+//   P = B_r^T u = hi(B_r^T) [u_hi | u_lo] + lo(B_r^T) u_hi
+//   Y = B_r Q   = hi(B_r) [Q_hi | Q_lo] + lo(B_r) Q_hi
+// each operand stored once as hi and once as lo (two GEMM calls a product).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -152,6 +158,71 @@ __global__ void k_add_nl(const float* __restrict__ d2, long m2pad, int n_pw, int
   hpsi[g + b * ldh] = h;
 }
 
+// Real forms for Gamma-real handles (b: packed B_r, n x n_ch column-major).
+// Each operand is stored once as hi and once as lo (no duplicated hi), and a
+// product is two GEMM calls: hi x [x_hi | x_lo] and lo x x_hi, the three
+// partial results summed in FP64 by the epilogue.
+// A[r][k] (r < rows_pad, k < kpad) = hi or lo of B_r(k, r) (transposed: T) or
+// B_r(r, k) (not transposed), zero outside; one flat index per element.
+template <bool Trans>
+__global__ void k_build_hilo_real(const double* __restrict__ b, int n, int n_ch, long rows_pad, long kpad,
+                                  __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
+  // one grid row per output row r, threads along k (coalesced for the transposed form, whose source
+  // column r is contiguous; the other form reads row r of B_r with stride n)
+  const long rows = Trans ? n_ch : n, kk = Trans ? n : n_ch;
+  for (long r = blockIdx.y; r < rows_pad; r += gridDim.y) {
+    for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < kpad; k += (long)gridDim.x * blockDim.x) {
+      __nv_bfloat16 h = __float2bfloat16_rn(0.0f), l = h;
+      if (r < rows && k < kk) split_bf16(Trans ? b[k + r * (long)n] : b[r + k * (long)n], h, l);
+      hi[r * kpad + k] = h;
+      lo[r * kpad + k] = l;
+    }
+  }
+}
+
+// Columns of X (rows x nc, ld ldx) split into out[j] = hi(X(:, j)) and
+// out[nc + j] = lo(X(:, j)), each column kpad long (zero-padded); one grid
+// row per column j.
+__global__ void k_split_hilo_cols(const double* __restrict__ x, long ldx, int rows, int nc, long kpad,
+                                  __nv_bfloat16* __restrict__ out) {
+  const int j = blockIdx.y;
+  const double* col = x + (long)j * ldx;
+  __nv_bfloat16* oh = out + (long)j * kpad;
+  __nv_bfloat16* ol = out + (long)(nc + j) * kpad;
+  for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < kpad; k += (long)gridDim.x * blockDim.x) {
+    __nv_bfloat16 h = __float2bfloat16_rn(0.0f), l = h;
+    if (k < rows) split_bf16(col[k], h, l);
+    oh[k] = h;
+    ol[k] = l;
+  }
+}
+
+// P[c + b n_ch] = sum over slices of (hi x [u_hi | u_lo]) + (lo x u_hi):
+// D1 holds per slice an m1pad x 2nb block, D3 per slice an m1pad x nb block
+__global__ void k_sum_p_real(const float* __restrict__ d1, const float* __restrict__ d3, int m1pad, int nb, int slices,
+                             long stride1, long stride3, int n_ch, double* __restrict__ p) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)n_ch * nb) return;
+  const int c = (int)(t % n_ch);
+  const int b = (int)(t / n_ch);
+  double acc = 0.0;
+  for (int s = 0; s < slices; ++s) {
+    acc += (double)d1[s * stride1 + c + (long)b * m1pad] + (double)d1[s * stride1 + c + (long)(nb + b) * m1pad];
+    acc += d3[s * stride3 + c + (long)b * m1pad];
+  }
+  p[t] = acc;
+}
+
+// hu[G, b] += D2[G, b] + D2[G, nb + b] + D4[G, b]
+__global__ void k_add_nl_real(const float* __restrict__ d2, const float* __restrict__ d4, long m2pad, int n, int nb,
+                              double* __restrict__ hu, long ldh) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)n * nb) return;
+  const long g = t % n;
+  const long b = t / n;
+  hu[g + b * ldh] += ((double)d2[g + b * m2pad] + (double)d2[g + (nb + b) * m2pad]) + (double)d4[g + b * m2pad];
+}
+
 inline unsigned grid_for(long n) { return (unsigned)std::min<long>(148L * 16, std::max<long>(1, (n + 255) / 256)); }
 
 }  // namespace
@@ -168,8 +239,7 @@ struct NlMixed {
   int nb_cap = 0, slices_cap = 0;
 };
 
-void release_nl_mixed(Handle& h) {
-  NlMixed* m = h.nlm;
+static void release_one(NlMixed*& m) {
   if (!m) return;
   for (auto p : m->a1) if (p) cudaFree(p);
   for (auto p : m->a2) if (p) cudaFree(p);
@@ -179,7 +249,12 @@ void release_nl_mixed(Handle& h) {
   if (m->d2) cudaFree(m->d2);
   if (m->ws) cudaFree(m->ws);
   delete m;
-  h.nlm = nullptr;
+  m = nullptr;
+}
+
+void release_nl_mixed(Handle& h) {
+  release_one(h.nlm);
+  release_one(h.nlm_real);
 }
 
 // Below a few hundred channels and a few thousand plane waves the projector
@@ -191,6 +266,113 @@ bool nl_mixed_eligible(const Handle& h) { return h.n_ch >= 256 && h.n_pw >= 4096
 static Status nl_alloc(void** p, size_t bytes) {
   cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 16));
   if (e != cudaSuccess) return fail(kOom, std::string("cudaMalloc (mixed projectors): ") + cudaGetErrorString(e));
+  return kOk;
+}
+
+// Split-K slices of the first product: up to `target` 128x128 tiles in
+// flight, and the per-call operand buffers for n2 right-hand columns.
+static int pick_slices(const NlMixed& m, int n2, long target) {
+  const long tiles = ((m.m1pad + 127) / 128) * ((n2 + 127) / 128);
+  int slices = 1;
+  while (slices < 32 && tiles * slices * 2 <= target && m.k1pad / (slices * 2) >= 2048) slices *= 2;
+  return slices;
+}
+
+// Tiles in flight for the Gamma-real products: a third of the SMs, so that
+// the concurrent solves of a batch (each with its own handle and stream)
+// keep running beside them; each tile holds an SM's shared memory.
+constexpr long kRealTileTarget = 48;
+
+static Status ensure_call_buffers(NlMixed& m, int n2, int slices) {
+  if (n2 <= m.nb_cap && slices <= m.slices_cap) return kOk;
+  const int cap = std::max(n2, m.nb_cap);
+  const int scap = std::max(slices, m.slices_cap);
+  if (m.b1) cudaFree(m.b1);
+  if (m.b2) cudaFree(m.b2);
+  if (m.d1) cudaFree(m.d1);
+  if (m.d2) cudaFree(m.d2);
+  if (m.ws) cudaFree(m.ws);
+  m.b1 = m.b2 = nullptr;
+  m.d1 = m.d2 = nullptr;
+  m.ws = nullptr;
+  m.nb_cap = m.slices_cap = 0;
+  Status st;
+  if ((st = nl_alloc((void**)&m.b1, (size_t)cap * m.k1pad * 2)) != kOk) return st;
+  if ((st = nl_alloc((void**)&m.b2, (size_t)cap * m.k2pad * 2)) != kOk) return st;
+  if ((st = nl_alloc((void**)&m.d1, (size_t)m.m1pad * cap * scap * 4)) != kOk) return st;
+  if ((st = nl_alloc((void**)&m.d2, (size_t)m.m2pad * cap * 4)) != kOk) return st;
+  size_t ws = gemm_bf16_workspace((int)m.m2pad, cap, (int)m.k2pad, 1);
+  for (int sl = 1; sl <= scap; sl *= 2) ws = std::max(ws, gemm_bf16_workspace(m.m1pad, cap, (int)(m.k1pad / sl), sl));
+  if ((st = nl_alloc(&m.ws, ws)) != kOk) return st;
+  m.ws_bytes = ws;
+  m.nb_cap = cap;
+  m.slices_cap = scap;
+  return kOk;
+}
+
+Status nonlocal_mixed_real(Handle& h, const double* u, long ldu, int nb, double* hu, long ldh, cudaStream_t s) {
+  if (!h.gam.on) return fail(kState, "nonlocal_mixed_real: not a Gamma-real handle");
+  if (h.n_ch <= 0 || nb <= 0) return kOk;
+  const int n = h.n_pw;
+  if (!h.nlm_real) {
+    // a1 = {hi, lo} of B_r^T (n_ch x n), a2 = {hi, lo} of B_r (n x n_ch)
+    h.nlm_real = new NlMixed();
+    h.nlm_real->a1.assign(2, nullptr);
+    h.nlm_real->a2.assign(2, nullptr);
+    h.nlm_real->k1pad = round_up(n, 64L * 32);
+    h.nlm_real->k2pad = round_up(h.n_ch, 64);
+    h.nlm_real->m1pad = (int)round_up(h.n_ch, 8);
+    h.nlm_real->m2pad = round_up(n, 8);
+  }
+  NlMixed& m = *h.nlm_real;
+  Status st;
+  if (!m.a1[0]) {
+    for (int q = 0; q < 2; ++q) {
+      if ((st = nl_alloc((void**)&m.a1[q], (size_t)m.m1pad * m.k1pad * 2)) != kOk) return st;
+      if ((st = nl_alloc((void**)&m.a2[q], (size_t)m.m2pad * m.k2pad * 2)) != kOk) return st;
+    }
+    k_build_hilo_real<true><<<dim3((unsigned)std::min<long>(32, (m.k1pad + 255) / 256),
+                                   (unsigned)std::min<long>(m.m1pad, 65535)), 256, 0, s>>>(
+        h.gam.b_real, n, h.n_ch, m.m1pad, m.k1pad, m.a1[0], m.a1[1]);
+    count_launch();
+    k_build_hilo_real<false><<<dim3((unsigned)std::min<long>(32, (m.k2pad + 255) / 256),
+                                    (unsigned)std::min<long>(m.m2pad, 65535)), 256, 0, s>>>(
+        h.gam.b_real, n, h.n_ch, m.m2pad, m.k2pad, m.a2[0], m.a2[1]);
+    count_launch();
+  }
+  // operand columns: [x_hi | x_lo] (2 nb); D1 / D2: hi x [x_hi | x_lo], D3 / D4: lo x x_hi (after D1 / D2)
+  const int slices = pick_slices(m, 2 * nb, kRealTileTarget);
+  const long ks = m.k1pad / slices;
+  if ((st = ensure_call_buffers(m, 3 * nb, slices)) != kOk) return st;
+  if ((st = ensure_gamma_pq(h, nb)) != kOk) return st;
+  k_split_hilo_cols<<<dim3((unsigned)std::min<long>(64, (m.k1pad + 255) / 256), nb), 256, 0, s>>>(u, ldu, n, nb,
+                                                                                                  m.k1pad, m.b1);
+  count_launch();
+  const long stride1 = (long)m.m1pad * 2 * nb, stride3 = (long)m.m1pad * nb;
+  float* d3 = m.d1 + stride1 * slices;
+  if ((st = gemm_bf16_tn_f32(m.a1[0], m.k1pad, ks, m.b1, m.k1pad, ks, m.d1, m.m1pad, stride1, m.m1pad, 2 * nb,
+                             (int)ks, slices, m.ws, m.ws_bytes, s)) != kOk)
+    return st;
+  if ((st = gemm_bf16_tn_f32(m.a1[1], m.k1pad, ks, m.b1, m.k1pad, ks, d3, m.m1pad, stride3, m.m1pad, nb, (int)ks,
+                             slices, m.ws, m.ws_bytes, s)) != kOk)
+    return st;
+  k_sum_p_real<<<(unsigned)(((long)h.n_ch * nb + 255) / 256), 256, 0, s>>>(m.d1, d3, m.m1pad, nb, slices, stride1,
+                                                                           stride3, h.n_ch, h.gam_p);
+  count_launch();
+  if ((st = apply_d_real(h, nb, s)) != kOk) return st;
+  k_split_hilo_cols<<<dim3((unsigned)std::min<long>(64, (m.k2pad + 255) / 256), nb), 256, 0, s>>>(
+      h.gam_q, h.n_ch, h.n_ch, nb, m.k2pad, m.b2);
+  count_launch();
+  float* d4 = m.d2 + m.m2pad * 2 * nb;
+  if ((st = gemm_bf16_tn_f32(m.a2[0], m.k2pad, 0, m.b2, m.k2pad, 0, m.d2, m.m2pad, 0, (int)m.m2pad, 2 * nb,
+                             (int)m.k2pad, 1, m.ws, m.ws_bytes, s)) != kOk)
+    return st;
+  if ((st = gemm_bf16_tn_f32(m.a2[1], m.k2pad, 0, m.b2, m.k2pad, 0, d4, m.m2pad, 0, (int)m.m2pad, nb, (int)m.k2pad,
+                             1, m.ws, m.ws_bytes, s)) != kOk)
+    return st;
+  k_add_nl_real<<<(unsigned)(((long)n * nb + 255) / 256), 256, 0, s>>>(m.d2, d4, m.m2pad, n, nb, hu, ldh);
+  count_launch();
+  PW_CUDA_TRY(cudaGetLastError());
   return kOk;
 }
 

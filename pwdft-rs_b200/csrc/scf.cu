@@ -418,6 +418,7 @@ static Status create_lane(Handle& h, Lane& L, int nd, int nlanes) {
   v.nl_p = v.nl_q = nullptr;
   v.nl_cap = 0;
   v.nlm = nullptr;
+  v.nlm_real = nullptr;
   v.scf = nullptr;
   v.tmp_grid = nullptr;
   v.gam_c1 = v.gam_c2 = nullptr;

@@ -181,6 +181,7 @@ def load_library(path: str = LIB_PATH):
     lib.pwgpu_eigensolve.argtypes = [vp, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_double, ct.c_int32, _f64p, _f64p,
                                      _f64p, _i32p, _f64p]
     lib.pwgpu_get_bands.argtypes = [vp, ct.c_int32, ct.c_int32, ct.c_int32, _f64p]
+    lib.pwgpu_apply_h_packed.argtypes = [vp, ct.c_int32, _f64p, ct.c_int32, _f64p]
     lib.pwgpu_dense_eigh.argtypes = [ct.c_int32, ct.c_int32, ct.c_int32, _f64p, _f64p, _f64p, _i32p, _f64p]
     lib.pwgpu_density.argtypes = [vp, ct.c_int32, _f64p, _f64p, _f64p]
     lib.pwgpu_symmetrize.argtypes = [vp, _f64p]
@@ -431,6 +432,16 @@ class PwGpu:
         if rc != PWGPU_OK and (raise_on_unconverged or rc != -4):
             raise PwGpuError(rc, self.lib.pwgpu_last_error().decode(errors="replace"))
         return res.as_dict(), ev, rho, rg
+
+    def apply_h_packed(self, u: np.ndarray, spin: int = 0) -> np.ndarray:
+        """H on Gamma-packed real bands (n_pw, nb) at the handle's precision."""
+        uf = np.asfortranarray(u, dtype=np.float64)
+        if uf.ndim == 1:
+            uf = uf[:, None]
+        out = np.empty_like(uf, order="F")
+        _check(self.lib, self.lib.pwgpu_apply_h_packed(self.h, spin, uf.ravel(order="F").ctypes.data_as(_f64p),
+                                                       uf.shape[1], out.ravel(order="F").ctypes.data_as(_f64p)))
+        return out
 
     def get_bands(self, n_bands: int, ik: int = 0, spin: int = 0) -> np.ndarray:
         """Eigenvectors of (spin, ik) left by the last SCF run or eigensolve: (n_pw, n_bands) complex."""

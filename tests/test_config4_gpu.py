@@ -3,10 +3,11 @@ k-points, 24 bands, Fermi-Dirac 0.02 Ry) on the GPU against the committed
 oracle fixtures (tests/golden/make_config4_fixtures.py), and concurrent
 (spin, k) lanes against one-at-a-time execution.
 
-Both loops stop at the case's own thresholds (drho < 1e-6 e/Å^3, |dE| <
-1e-5 eV).  Tolerances: total and Harris-Foulkes energies 1e-4 eV (first
-order in drho over 8 atoms), Fermi level and eigenvalues 1e-4 eV,
-magnetisation 1e-4."""
+The fixtures are converged to a density rms of 1e-9 e/Å^3 and an energy
+change of 1e-9 eV, and the device loop is run to the same thresholds, so
+the plain FP64 form is held to the north-star bars: total and
+Harris-Foulkes energies within 1e-8 Ha, eigenvalues and Fermi level within
+1e-7 Ha, magnetisation within 1e-6."""
 
 import json
 import os
@@ -21,8 +22,11 @@ from pwgpu.upf import load_upf
 
 pytestmark = pytest.mark.gpu
 
-CASES = {"C": ("C", "C.upf", True), "C_nonlcc": ("C", "C.upf", False)}
-TIGHT = dict(max_iter=200)
+CASES = {"C": ("C", "C.upf", True), "C_nonlcc": ("C", "C.upf", False), "Si": ("Si", "Si.upf", True)}
+TIGHT = dict(max_iter=400, conv_threshold=1e-9, energy_threshold=1e-9)
+HA = 27.211386245988
+E_TOL = 1e-8 * HA
+EV_TOL = 1e-7 * HA
 
 
 def fixture(name):
@@ -33,12 +37,13 @@ def fixture(name):
         return json.load(f)
 
 
-def run(s, m, lanes=0):
+def run(s, m, lanes=0, tight=True):
     kw = dict(SCF_KW)
-    kw.update(TIGHT)
+    if tight:
+        kw.update(TIGHT)
     nb = kw.pop("n_bands")
     with PwGpu(s, lanes=lanes) as dev:
-        return dev.scf_run(s.rho_init_r, nb, starting_magnetization=m, **kw)
+        return dev.scf_run(s.rho_init_r, nb, starting_magnetization=m, diag_tol=1e-10 if tight else 1e-8, **kw)
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
@@ -47,19 +52,20 @@ def test_config4_cell_matches_oracle(name):
     species, upf, nlcc = CASES[name]
     s, m = config4_system(species, load_upf(os.path.join(GOLDEN, "upf", upf)), nlcc=nlcc)
     assert (s.n_pw, list(s.dims), len(s.kpoints)) == (ref["n_pw"], ref["dims"], ref["n_k"])
+    assert ref["thresholds"]["conv_threshold"] <= 1e-9
     res, ev, rho, rg = run(s, m)
     assert res["converged"] == 1
-    assert abs(res["total_energy"] - ref["total_energy"]) < 1e-4
-    assert abs(res["harris_foulkes_energy"] - ref["harris_foulkes_energy"]) < 1e-4
-    assert abs(res["fermi_energy"] - ref["fermi_energy"]) < 1e-4
-    assert abs(res["magnetization"] - ref["magnetization"]) < 1e-4
-    assert np.max(np.abs(ev - np.array(ref["eigenvalues"]))) < 1e-4
+    assert abs(res["total_energy"] - ref["total_energy"]) < E_TOL
+    assert abs(res["harris_foulkes_energy"] - ref["harris_foulkes_energy"]) < E_TOL
+    assert abs(res["fermi_energy"] - ref["fermi_energy"]) < EV_TOL
+    assert abs(res["magnetization"] - ref["magnetization"]) < 1e-6
+    assert np.max(np.abs(ev - np.array(ref["eigenvalues"]))) < EV_TOL
 
 
 def test_lanes_match_sequential(c_pp):
     s, m = config4_system("C", c_pp)
-    r1, ev1, _, _ = run(s, m, lanes=1)
-    r8, ev8, _, _ = run(s, m, lanes=0)
+    r1, ev1, _, _ = run(s, m, lanes=1, tight=False)
+    r8, ev8, _, _ = run(s, m, lanes=0, tight=False)
     assert abs(r1["total_energy"] - r8["total_energy"]) < 1e-4
     assert abs(r1["harris_foulkes_energy"] - r8["harris_foulkes_energy"]) < 1e-4
     assert np.max(np.abs(ev1 - ev8)) < 1e-4

@@ -78,3 +78,25 @@ def test_gamma_real_density_matches_oracle(si_pp):
         rho = dev.density(occ, [psi])
     ref = O.compute_density(s.g_to_fft, s.dims, [psi], [occ[0]], s.kpt_weights, s.n_electrons, s.omega)
     assert np.max(np.abs(rho - ref)) < 1e-10 * np.max(ref)
+
+
+def test_packed_operator_mixed_form_on_benchmark_block():
+    """The Gamma-real operator of the benchmark's H|psi> block (Si64 cell,
+    n_pw 23,847, 256 Gaussian KB channels) on packed real bands: in FP64 it
+    is symmetric to 1e-12 (u^T H v = v^T H u); the mixed form (FP32 FFT /
+    V(r) product, projector products as 3xBF16 tensor-core GEMMs) equals the
+    FP64 form to 3e-5 of max |H u|, the bar of the complex mixed path."""
+    from pwgpu.workloads import hpsi_system, si64_crystal
+    sys_, veff_g, _ = hpsi_system(si64_crystal())
+    g = np.random.default_rng(5)
+    u = g.standard_normal((sys_.n_pw, 24))
+    with PwGpu(sys_) as dev:
+        dev.set_veff_g(veff_g)
+        dev.set_precision(PRECISION_FP64)
+        h64 = dev.apply_h_packed(u)
+        dev.set_precision(PRECISION_MIXED)
+        hm = dev.apply_h_packed(u)
+    sym = np.abs(u.T @ h64 - (u.T @ h64).T).max() / np.abs(u.T @ h64).max()
+    assert sym < 1e-12
+    err = np.abs(hm - h64).max() / np.abs(h64).max()
+    assert err < 3e-5, f"mixed packed H vs FP64: {err:.2e}"
