@@ -1,16 +1,16 @@
 """Generate the oracle reference values of the batched-k LSDA case (the
 8-atom cubic Si and C diamond cells at 35 Ry, Gamma-centred 6x6x6 mesh
 reduced to 20 IBZ k-points, 24 bands, Fermi-Dirac 0.02 Ry, starting
-magnetisation 0 on Si and 0.125 on C), at the case's own thresholds
-(density rms 1e-6 e/Å^3, energy change 1e-5 eV): near convergence the
-plain-Anderson magnetisation channel contracts by ~7 % per iteration, so
-a 1e-8 target costs hours of dense diagonalisation on the CPU, while the
-total energy already moves by < 1e-7 eV per iteration at drho ~ 1e-6.
+magnetisation 0 on Si and 0.125 on C), converged far below the case's
+own thresholds: density rms 1e-9 e/Å^3 and energy change 1e-9 eV, so that
+the plain FP64 form can be held to 1e-8 Ha.  Near convergence the
+plain-Anderson magnetisation channel of the C cells contracts by ~7 % per
+iteration, hence the long tail of iterations.
 
     python tests/golden/make_config4_fixtures.py [C C_nonlcc Si]
 
-(CPU; the C cell takes minutes, the Si cell tens of minutes).  Writes
-tests/golden/config4_<cell>_oracle.json per cell.
+(CPU; each C cell takes about twenty minutes, the Si cell about an hour).
+Writes tests/golden/config4_<cell>_oracle.json per cell.
 """
 
 import json
@@ -27,7 +27,7 @@ from oracle import pwdft_oracle as O  # noqa: E402
 from pwgpu.config4 import SCF_KW, config4_system  # noqa: E402
 from pwgpu.upf import load_upf  # noqa: E402
 
-TIGHT = dict(max_iter=200)  # the case's own thresholds (ScfParams defaults)
+TIGHT = dict(max_iter=400, conv_threshold=1e-9, energy_threshold=1e-9)
 CASES = {"C": ("C", "C.upf", True), "C_nonlcc": ("C", "C.upf", False), "Si": ("Si", "Si.upf", True)}
 
 
