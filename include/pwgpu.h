@@ -362,6 +362,23 @@ pwgpu_status pwgpu_dense_eigh(int32_t m, int32_t nev, int32_t complex_matrix, co
                               double* Z, int32_t* cluster_ctas, double* kernel_ms);
 
 /*
+ * The eigensolver's orthonormalisation kernel on a host matrix: the
+ * Cholesky factor G = R^H R of the Hermitian (complex_matrix != 0,
+ * interleaved re/im) or symmetric positive definite q x q matrix G
+ * (column-major; upper triangle read) and its inverse.  Writes Ri = R^-1
+ * (q x q, zero below the diagonal), rdiag (q entries, may be NULL) = R's
+ * diagonal, and *info = 0, or 1 + the first row whose pivot is not positive
+ * (LAPACK potrf's count; Ri is then undefined).  cluster_ctas and kernel_ms
+ * (may be NULL) as for pwgpu_dense_eigh.  The reference keeps its bases
+ * orthonormal inside faer (the Gram-Schmidt of the Krylov-Schur solver,
+ * eigensolver/iterative.rs:1-20, and the dense solver's unitary
+ * eigenvectors, eigensolver/dense.rs:50-98); this is the Cholesky-QR step of
+ * the block eigensolver that replaces them, exposed for testing.
+ */
+pwgpu_status pwgpu_dense_cholesky_inverse(int32_t q, int32_t complex_matrix, const double* G, double* Ri,
+                                          double* rdiag, int32_t* info, int32_t* cluster_ctas, double* kernel_ms);
+
+/*
  * Serving: a job queue in front of pwgpu_scf_run.  No counterpart in the
  * reference (its front door, scf::run_scf at scf/mod.rs:344-402, runs one
  * solve per call); this is the submit/poll seam a service wraps around it.

@@ -596,6 +596,57 @@ pwgpu_status pwgpu_dense_eigh(int32_t m, int32_t nev, int32_t complex_matrix, co
   return st;
 }
 
+pwgpu_status pwgpu_dense_cholesky_inverse(int32_t q, int32_t complex_matrix, const double* G, double* Ri,
+                                          double* rdiag, int32_t* info, int32_t* cluster_ctas, double* kernel_ms) {
+  if (!G || !Ri || !info) return fail(kInvalid, "pwgpu_dense_cholesky_inverse: NULL argument");
+  if (q < 1) return fail(kInvalid, "pwgpu_dense_cholesky_inverse: need q >= 1");
+  const bool cpx = complex_matrix != 0;
+  if (cluster_ctas) *cluster_ctas = chol_inv_cluster_size(q, cpx);
+  const size_t es = cpx ? sizeof(double2) : sizeof(double);
+  const size_t bytes = (size_t)q * q * es;
+  void *dg = nullptr, *dr = nullptr;
+  double* dd = nullptr;
+  int* di = nullptr;
+  auto cleanup = [&]() { cudaFree(dg); cudaFree(dr); cudaFree(dd); cudaFree(di); };
+  if (cudaMalloc(&dg, bytes) != cudaSuccess || cudaMalloc(&dr, bytes) != cudaSuccess ||
+      cudaMalloc((void**)&dd, (size_t)q * sizeof(double)) != cudaSuccess ||
+      cudaMalloc((void**)&di, sizeof(int)) != cudaSuccess) {
+    cleanup();
+    return fail(kOom, "pwgpu_dense_cholesky_inverse: allocation failed");
+  }
+  cudaError_t e = cudaMemcpy(dg, G, bytes, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cleanup();
+    return fail(kCuda, std::string("pwgpu_dense_cholesky_inverse: ") + cudaGetErrorString(e));
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (kernel_ms) {
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, 0);
+  }
+  Status st = cpx ? chol_inv(static_cast<double2*>(dg), q, static_cast<double2*>(dr), dd, di, 0)
+                  : chol_inv(static_cast<double*>(dg), q, static_cast<double*>(dr), dd, di, 0);
+  if (kernel_ms) {
+    cudaEventRecord(e1, 0);
+    float ms = 0.f;
+    if (cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) *kernel_ms = ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  if (st == kOk) {
+    int inf = 0;
+    e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(&inf, di, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(Ri, dr, bytes, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && rdiag) e = cudaMemcpy(rdiag, dd, (size_t)q * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) st = fail(kCuda, std::string("pwgpu_dense_cholesky_inverse: ") + cudaGetErrorString(e));
+    *info = inf;
+  }
+  cleanup();
+  return st;
+}
+
 pwgpu_status pwgpu_kernel_launches(int64_t* count) {
   if (!count) return fail(kInvalid, "pwgpu_kernel_launches: NULL argument");
   *count = launch_counter().load();

@@ -44,6 +44,7 @@
 #include <string>
 
 #include "handle.hpp"
+#include "dense_ops.cuh"
 #include "linalg.hpp"
 
 namespace cg = cooperative_groups;
@@ -101,43 +102,7 @@ constexpr int kBisectRounds = 48;
 constexpr double kEps = 1.1102230246251565e-16;  // 2^-53
 constexpr size_t kSmemLimit = 227 * 1024;
 
-// ---- scalar helpers (double: real symmetric, double2: complex Hermitian) ----
-__device__ __forceinline__ double cj(double x) { return x; }
-__device__ __forceinline__ double2 cj(double2 x) { return make_double2(x.x, -x.y); }
-__device__ __forceinline__ double mul(double a, double b) { return a * b; }
-__device__ __forceinline__ double2 mul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ double2 mul(double2 a, double b) { return make_double2(a.x * b, a.y * b); }
-__device__ __forceinline__ double add(double a, double b) { return a + b; }
-__device__ __forceinline__ double2 add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ double sub(double a, double b) { return a - b; }
-__device__ __forceinline__ double2 sub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ double re(double x) { return x; }
-__device__ __forceinline__ double re(double2 x) { return x.x; }
-__device__ __forceinline__ double im(double) { return 0.0; }
-__device__ __forceinline__ double im(double2 x) { return x.y; }
-__device__ __forceinline__ double abs2(double x) { return x * x; }
-__device__ __forceinline__ double abs2(double2 x) { return x.x * x.x + x.y * x.y; }
-template <typename T> __device__ __forceinline__ T mk(double r, double i);
-template <> __device__ __forceinline__ double mk<double>(double r, double) { return r; }
-template <> __device__ __forceinline__ double2 mk<double2>(double r, double i) { return make_double2(r, i); }
-__device__ __forceinline__ bool finite(double x) { return isfinite(x); }
-__device__ __forceinline__ bool finite(double2 x) { return isfinite(x.x) && isfinite(x.y); }
-
-__device__ __forceinline__ double shfl_down(double v, int o) { return __shfl_down_sync(0xffffffffu, v, o); }
-__device__ __forceinline__ double2 shfl_down(double2 v, int o) {
-  return make_double2(__shfl_down_sync(0xffffffffu, v.x, o), __shfl_down_sync(0xffffffffu, v.y, o));
-}
-__device__ __forceinline__ double shfl(double v, int l) { return __shfl_sync(0xffffffffu, v, l); }
-__device__ __forceinline__ double2 shfl(double2 v, int l) {
-  return make_double2(__shfl_sync(0xffffffffu, v.x, l), __shfl_sync(0xffffffffu, v.y, l));
-}
-// sum over the warp, result in every lane
-template <typename T> __device__ __forceinline__ T warp_sum(T v) {
-  for (int o = 16; o > 0; o >>= 1) v = add(v, shfl_down(v, o));
-  return shfl(v, 0);
-}
+using namespace dense;
 
 // Shared-memory layout of one CTA (identical on host and device).
 struct Layout {
@@ -810,10 +775,25 @@ __global__ void __launch_bounds__(kThreads, 1)
   cluster.sync();  // no CTA leaves while another may still read its shared memory
 }
 
-int pick_cluster(int m, int tsz) {
+// The smallest cluster whose CTAs hold the matrix in shared memory (0: none).
+int min_cluster(int m, int tsz) {
   for (int C = 1; C <= kMaxCluster; C *= 2)
     if (layout(m, C, tsz).total + 2 * kMaxM * sizeof(double) <= kSmemLimit) return C;
   return 0;
+}
+
+// The cluster size to use: measured on B200, a 16-CTA cluster is fastest
+// for every m > 64 (at m = 135 / 180 / 270 the solve takes 0.43 / 0.53 /
+// 0.74 of its time on the smallest cluster that fits, mostly through the
+// back-transform, bisection and inverse iteration that spread over the
+// CTAs) and within a few percent at m = 360; 8 CTAs below, and never more
+// CTAs than columns.
+int pick_cluster(int m, int tsz) {
+  const int c0 = min_cluster(m, tsz);
+  if (c0 == 0) return 0;
+  int want = m > 64 ? 16 : 8;
+  while (want > m) want /= 2;
+  return std::max(c0, want);
 }
 
 template <typename T> Status set_attributes() {
@@ -855,9 +835,9 @@ template <typename T> bool cluster_fits(int m, int C) {
   int& c = cache[slot][C];
   if (c == 0) {
     if (set_attributes<T>() != kOk) return false;
-    int mm = 1;
+    int mm = 1;  // the largest m a cluster of C CTAs can hold: the most shared memory
     for (int t = 1; t <= kMaxM; ++t)
-      if (pick_cluster(t, (int)sizeof(T)) == C) mm = t;
+      if (layout(t, C, (int)sizeof(T)).total + 2 * kMaxM * sizeof(double) <= kSmemLimit) mm = t;
     cudaLaunchAttribute attr[1];
     cudaLaunchConfig_t cfg = launch_config<T>(mm, C, attr, nullptr);
     int n = 0;
@@ -868,11 +848,22 @@ template <typename T> bool cluster_fits(int m, int C) {
   return c == 1;
 }
 
+// The preferred cluster size, halved while such a cluster cannot be
+// resident on this device (0 when none can).
+template <typename T> int choose_cluster(int m) {
+  if (m < 1 || m > kMaxM) return 0;
+  const int c0 = min_cluster(m, (int)sizeof(T));
+  if (c0 == 0) return 0;
+  int C = pick_cluster(m, (int)sizeof(T));
+  while (C > c0 && !cluster_fits<T>(m, C)) C /= 2;
+  return cluster_fits<T>(m, C) ? C : 0;
+}
+
 template <typename T>
 Status launch_eigh(const T* A, long lda, int m, int nev, double* w, T* Z, long ldz, double* work, int* status,
                    cudaStream_t s) {
-  const int C = pick_cluster(m, (int)sizeof(T));
-  if (C == 0 || m > kMaxM) return fail(kInvalid, "eigh_cluster: matrix too large for the cluster eigensolver");
+  const int C = choose_cluster<T>(m);
+  if (C == 0) return fail(kInvalid, "eigh_cluster: matrix too large for the cluster eigensolver");
   Status r = set_attributes<T>();
   if (r != kOk) return r;
   auto kern = k_eigh_cluster<T>;
@@ -894,14 +885,11 @@ size_t eigh_cluster_work_doubles(int m, int nev) {
 }
 
 bool eigh_cluster_supported(int m, bool complex_matrix) {
-  if (m < 1 || m > kMaxM) return false;
-  const int C = pick_cluster(m, complex_matrix ? (int)sizeof(double2) : (int)sizeof(double));
-  if (C == 0) return false;
-  return complex_matrix ? cluster_fits<double2>(m, C) : cluster_fits<double>(m, C);
+  return eigh_cluster_size(m, complex_matrix) > 0;
 }
 
 int eigh_cluster_size(int m, bool complex_matrix) {
-  return pick_cluster(m, complex_matrix ? (int)sizeof(double2) : (int)sizeof(double));
+  return complex_matrix ? choose_cluster<double2>(m) : choose_cluster<double>(m);
 }
 
 Status eigh_cluster(const double* A, long lda, int m, int nev, double* w, double* Z, long ldz, double* work,

@@ -31,4 +31,14 @@ Status eigh_cluster(const double* A, long lda, int m, int nev, double* w, double
 Status eigh_cluster(const double2* A, long lda, int m, int nev, double* w, double2* Z, long ldz, double* work,
                     int* status_dev, cudaStream_t s);
 
+// Cholesky factor and its inverse (chol.cu): G = R^H R for the Hermitian
+// (complex) or symmetric (real) positive definite q x q matrix G (column
+// major, ld q; upper triangle read, G overwritten as scratch).  Writes
+// Ri = R^-1 (q x q, ld q, zero below the diagonal), rdiag[i] = R_ii (rdiag
+// may be null) and *info_dev = 0, or 1 + the first row whose pivot is not
+// positive (Ri then undefined).  One cluster launch on stream s.
+Status chol_inv(double* G, int q, double* Ri, double* rdiag, int* info_dev, cudaStream_t s);
+Status chol_inv(double2* G, int q, double2* Ri, double* rdiag, int* info_dev, cudaStream_t s);
+int chol_inv_cluster_size(int q, bool complex_matrix);
+
 }  // namespace pwgpu

@@ -170,16 +170,18 @@ __global__ void k_scatter_cols(const S* __restrict__ src, long lds, const int* _
 
 // Subspace matrix Hs (m x m, ld m) over the basis [X | B], X holding nd Ritz
 // vectors with values lam:  [[diag(lam), Z^H], [Z, (G + G^H)/2]],
-// Z = B^H HX (q x nd, ld q), G = B^H HB (q x q, ld q), q = m - nd.
+// Z = B^H HX (q x nd, ld q), G = B^H HB (q x q, ld q), q = m - nd.  When XX
+// (X^H HX, nd x nd, ld nd) is given, X need not be Ritz vectors: the X block
+// is (XX + XX^H)/2.
 template <typename S>
 __global__ void k_assemble_rr(S* __restrict__ Hs, int m, int nd, const double* __restrict__ lam,
-                              const S* __restrict__ Z, const S* __restrict__ G) {
+                              const S* __restrict__ Z, const S* __restrict__ G, const S* __restrict__ XX = nullptr) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long)m * m) return;
   const int r = (int)(t % m), c = (int)(t / m), q = m - nd;
   S v;
   if (r < nd && c < nd) {
-    v = real_scalar<S>(r == c ? lam[r] : 0.0);
+    v = XX ? herm_avg(XX[r + (long)c * nd], XX[c + (long)r * nd]) : real_scalar<S>(r == c ? lam[r] : 0.0);
   } else if (c < nd) {
     v = Z[(r - nd) + (long)c * q];
   } else if (r < nd) {
@@ -266,23 +268,6 @@ Status add_shift(Ctx& c, double* G, double* Id, int q, double shift) {
   return kOk;
 }
 
-// M (rows x q, ld ldm) <- M R^-1 for the upper-triangular q x q R
-Status trsm_right_upper(Ctx& c, const double2* R, int q, double2* M, int rows, long ldm) {
-  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0);
-  if (cublasZtrsm(c.h.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, rows, q,
-                  &one, reinterpret_cast<const cuDoubleComplex*>(R), q, reinterpret_cast<cuDoubleComplex*>(M),
-                  (int)ldm) != CUBLAS_STATUS_SUCCESS)
-    return fail(kCuda, "cublasZtrsm failed (eigensolver)");
-  return kOk;
-}
-Status trsm_right_upper(Ctx& c, const double* R, int q, double* M, int rows, long ldm) {
-  const double one = 1.0;
-  if (cublasDtrsm(c.h.blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, rows, q,
-                  &one, R, q, M, (int)ldm) != CUBLAS_STATUS_SUCCESS)
-    return fail(kCuda, "cublasDtrsm failed (eigensolver)");
-  return kOk;
-}
-
 Status ensure_solver_work(Ctx& c, size_t bytes) {
   const size_t lwork = (bytes + sizeof(double2) - 1) / sizeof(double2);
   if (lwork <= c.w.solver_lwork) return kOk;
@@ -298,32 +283,6 @@ Status ensure_solver(Ctx& c) {
   if (!c.h.solver && cusolverDnCreate(&c.h.solver) != CUSOLVER_STATUS_SUCCESS)
     return fail(kCuda, "cusolverDnCreate failed");
   cusolverDnSetStream(c.h.solver, c.s);
-  return kOk;
-}
-
-// Cholesky of the q x q Gram (upper); info on the device
-Status potrf(Ctx& c, double2* G, int q) {
-  int lwork = 0;
-  auto* g = reinterpret_cast<cuDoubleComplex*>(G);
-  if (cusolverDnZpotrf_bufferSize(c.h.solver, CUBLAS_FILL_MODE_UPPER, q, g, q, &lwork) != CUSOLVER_STATUS_SUCCESS)
-    return fail(kCuda, "cusolverDnZpotrf_bufferSize failed");
-  Status r;
-  if ((r = ensure_solver_work(c, (size_t)lwork * sizeof(double2))) != kOk) return r;
-  if (cusolverDnZpotrf(c.h.solver, CUBLAS_FILL_MODE_UPPER, q, g, q,
-                       reinterpret_cast<cuDoubleComplex*>(c.w.solver_work), lwork, c.w.info) !=
-      CUSOLVER_STATUS_SUCCESS)
-    return fail(kCuda, "cusolverDnZpotrf failed");
-  return kOk;
-}
-Status potrf(Ctx& c, double* G, int q) {
-  int lwork = 0;
-  if (cusolverDnDpotrf_bufferSize(c.h.solver, CUBLAS_FILL_MODE_UPPER, q, G, q, &lwork) != CUSOLVER_STATUS_SUCCESS)
-    return fail(kCuda, "cusolverDnDpotrf_bufferSize failed");
-  Status r;
-  if ((r = ensure_solver_work(c, (size_t)lwork * sizeof(double))) != kOk) return r;
-  if (cusolverDnDpotrf(c.h.solver, CUBLAS_FILL_MODE_UPPER, q, G, q, reinterpret_cast<double*>(c.w.solver_work),
-                       lwork, c.w.info) != CUSOLVER_STATUS_SUCCESS)
-    return fail(kCuda, "cusolverDnDpotrf failed");
   return kOk;
 }
 
@@ -409,14 +368,15 @@ Status chol_qr(Ctx& c, T* Y, T* HY, int q, double shift, bool& ok, double* min_r
     k_set_identity<T><<<blocks_for((long)q * q), 256, 0, c.s>>>(Id, q); count_launch();
     if ((r = add_shift(c, G, Id, q, shift)) != kOk) return r;
   }
-  if ((r = ensure_solver(c)) != kOk) return r;
-  if ((r = potrf(c, G, q)) != kOk) return r;
+  // G = R^H R and Ri = R^-1 in one cluster launch (chol.cu; G is
+  // overwritten); R's diagonal lands in w.colsq
+  T* Ri = as<T>(c.w.Id);
+  if ((r = chol_inv(G, q, Ri, c.w.colsq, c.w.info, c.s)) != kOk) return r;
   int info = 0;
   PW_CUDA_TRY(cudaMemcpyAsync(&info, c.w.info, sizeof(int), cudaMemcpyDeviceToHost, c.s));
   std::vector<double> dg;
   if (min_rdiag) {
     dg.resize(q);
-    k_diag_real<T><<<blocks_for(q), 256, 0, c.s>>>(G, q, q, c.w.colsq); count_launch();
     PW_CUDA_TRY(cudaMemcpyAsync(dg.data(), c.w.colsq, q * sizeof(double), cudaMemcpyDeviceToHost, c.s));
   }
   PW_CUDA_TRY(cudaStreamSynchronize(c.s));
@@ -432,9 +392,6 @@ Status chol_qr(Ctx& c, T* Y, T* HY, int q, double shift, bool& ok, double* min_r
   // Y <- Y R^-1 as one GEMM with the explicit inverse of the small R (a
   // tall-skinny triangular solve is several times slower than the GEMM);
   // w.T and w.HXn are free whenever a block is orthonormalised
-  T* Ri = as<T>(c.w.Id);
-  k_set_identity<T><<<blocks_for((long)q * q), 256, 0, c.s>>>(Ri, q); count_launch();
-  if ((r = trsm_right_upper(c, G, q, Ri, q, q)) != kOk) return r;
   T* tmp[2] = {as<T>(c.w.T), as<T>(c.w.HXn)};
   T* M[2] = {Y, HY};
   for (int i = 0; i < 2; ++i) {
@@ -615,7 +572,16 @@ Status lobpcg_t(Handle& h, EigWork& w, EigVecs& k, int spin, int ik, double v0, 
   // HX in FP64: the residuals below refer to the full-precision operator
   if ((r = apply_op(h, spin, ik, X, n, nd, HX, 0, s)) != kOk) return r;
   out.happ += nd;
-  if ((r = rr_block<T>(c, k, nd)) != kOk) return r;
+  // The Rayleigh-Ritz of X alone is deferred into the first block step: its
+  // subspace matrix takes the full X^H HX block (w.XX), and the residuals of
+  // that step use the Rayleigh quotients diag(X^H HX).  Only a solve that
+  // stops before any block step rotates X by itself (rr_block).
+  T* XX = as<T>(w.XX);
+  if ((r = gemm(c, CUBLAS_OP_C, CUBLAS_OP_N, nd, nd, (int)n, X, n, HX, n, XX, nd)) != kOk) return r;
+  k_diag_real<T><<<blocks_for(nd), 256, 0, s>>>(XX, nd, nd, w.lam); count_launch();
+  PW_CUDA_TRY(cudaMemcpyAsync(k.evals.data(), w.lam, nd * sizeof(double), cudaMemcpyDeviceToHost, s));
+  PW_CUDA_TRY(cudaStreamSynchronize(s));
+  bool first = true;
 
   const double p_drop = precision == 0 ? kPDropFp64 : kPDropMixed;
   T* Tb = as<T>(w.T);
@@ -637,14 +603,20 @@ Status lobpcg_t(Handle& h, EigWork& w, EigVecs& k, int spin, int ik, double v0, 
     PW_CUDA_TRY(cudaStreamSynchronize(s));
     out.max_res = 0.0;
     for (int b = 0; b < nconv; ++b) out.max_res = std::max(out.max_res, std::sqrt(rn[b]));
-    if (out.max_res < tol || out.iters >= max_iter) break;
+    if (out.max_res < tol || out.iters >= max_iter) {
+      if (first && (r = rr_block<T>(c, k, nd)) != kOk) return r;
+      break;
+    }
     // active bands: residual above tol (buffer bands: 10 tol)
     act.clear();
     for (int b = 0; b < nd; ++b)
       if (std::sqrt(rn[b]) > (b < nconv ? tol : 10.0 * tol)) act.push_back(b);
     if ((long)act.size() > n - nd) act.resize((size_t)std::max<long>(0, n - nd));
     const int na = (int)act.size();
-    if (na == 0) break;
+    if (na == 0) {
+      if (first && (r = rr_block<T>(c, k, nd)) != kOk) return r;
+      break;
+    }
     T* W = X + n * nd;
     T* HW = HX + n * nd;
     pt.mark(1, s);
@@ -707,7 +679,7 @@ Status lobpcg_t(Handle& h, EigWork& w, EigVecs& k, int spin, int ik, double v0, 
       }
     }
     const int q = na + npc;
-    if (4 * na <= nd) {
+    if (4 * na <= nd && !first) {
       // few active bands: hard locking.  W and P are orthogonal to every
       // column of X, so [X_a | W | P] (X_a the active Ritz vectors) is an
       // orthonormal basis orthogonal to the converged ones; Rayleigh-Ritz in
@@ -792,8 +764,10 @@ Status lobpcg_t(Handle& h, EigWork& w, EigVecs& k, int spin, int ik, double v0, 
     const int m = nd + q;
     if ((r = gemm(c, CUBLAS_OP_C, CUBLAS_OP_N, q, nd, (int)n, W, n, HX, n, as<T>(w.Z), q)) != kOk) return r;
     if ((r = gemm(c, CUBLAS_OP_C, CUBLAS_OP_N, q, q, (int)n, W, n, HW, n, as<T>(w.G), q)) != kOk) return r;
-    k_assemble_rr<T><<<blocks_for((long)m * m), 256, 0, s>>>(as<T>(w.Hs), m, nd, w.lam0, as<T>(w.Z), as<T>(w.G));
+    k_assemble_rr<T><<<blocks_for((long)m * m), 256, 0, s>>>(as<T>(w.Hs), m, nd, w.lam0, as<T>(w.Z), as<T>(w.G),
+                                                            first ? XX : nullptr);
     count_launch();
+    first = false;
     T* C = nullptr;
     pt.mark(5, s);
     if ((r = subspace_eig<T>(c, m, nd, &C)) != kOk) return r;
@@ -845,6 +819,7 @@ Status eig_work_alloc(EigWork& w, long n, int nd) {
     if ((r = walloc(p, (size_t)n * nd)) != kOk) return r;
   for (double2** p : {&w.Hs, &w.Cs, &w.G, &w.Z, &w.Id})
     if ((r = walloc(p, m * m)) != kOk) return r;
+  if ((r = walloc(&w.XX, (size_t)nd * nd)) != kOk) return r;
   if ((r = walloc(&w.lam, m)) != kOk) return r;
   if ((r = walloc(&w.lam0, m)) != kOk) return r;
   if ((r = walloc(&w.colsq, m)) != kOk) return r;
@@ -859,7 +834,7 @@ void eig_work_release(EigWork& w) {
   auto f = [](void* p) { if (p) cudaFree(p); };
   f(w.T); f(w.HXn); f(w.Pn); f(w.HPn); f(w.Hs); f(w.Cs); f(w.G); f(w.Z); f(w.Id);
   f(w.lam); f(w.lam0); f(w.colsq); f(w.partials); f(w.idx); f(w.status); f(w.solver_work); f(w.info);
-  f(w.eigh_work);
+  f(w.eigh_work); f(w.XX);
   w = EigWork();
 }
 

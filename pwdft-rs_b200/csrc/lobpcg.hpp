@@ -41,6 +41,7 @@ struct EigWork {
   size_t solver_lwork = 0;
   int* info = nullptr;
   double* eigh_work = nullptr;  // scratch of the cluster eigensolver (eigh.cu)
+  double2* XX = nullptr;        // nd x nd: X^H HX at the start of a solve
   size_t eigh_work_len = 0;
 };
 

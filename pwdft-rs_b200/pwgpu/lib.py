@@ -183,6 +183,7 @@ def load_library(path: str = LIB_PATH):
     lib.pwgpu_get_bands.argtypes = [vp, ct.c_int32, ct.c_int32, ct.c_int32, _f64p]
     lib.pwgpu_apply_h_packed.argtypes = [vp, ct.c_int32, _f64p, ct.c_int32, _f64p]
     lib.pwgpu_dense_eigh.argtypes = [ct.c_int32, ct.c_int32, ct.c_int32, _f64p, _f64p, _f64p, _i32p, _f64p]
+    lib.pwgpu_dense_cholesky_inverse.argtypes = [ct.c_int32, ct.c_int32, _f64p, _f64p, _f64p, _i32p, _i32p, _f64p]
     lib.pwgpu_density.argtypes = [vp, ct.c_int32, _f64p, _f64p, _f64p]
     lib.pwgpu_symmetrize.argtypes = [vp, _f64p]
     lib.pwgpu_potentials.argtypes = [vp, _f64p, _f64p, _f64p]
@@ -606,3 +607,26 @@ def dense_eigh(A: np.ndarray, nev: int, timed: bool = False):
                                      _f64(w), z.view(np.float64).ctypes.data_as(_f64p), ct.byref(nc),
                                      ct.byref(ms) if timed else None))
     return (w, z.T, nc.value, ms.value) if timed else (w, z.T, nc.value)
+
+
+def dense_cholesky_inverse(G: np.ndarray, timed: bool = False):
+    """Cholesky factor G = R^H R of a Hermitian / real symmetric positive
+    definite matrix through the device's cluster kernel.  Returns (Ri = R^-1,
+    diag(R), info, cluster CTAs used), plus the kernel's device ms when
+    timed; info = 1 + the first failing pivot row, 0 on success."""
+    lib = load_library()
+    q = G.shape[0]
+    cpx = np.iscomplexobj(G)
+    dt = np.complex128 if cpx else np.float64
+    gf = np.asfortranarray(G, dtype=dt)
+    ri = np.zeros((q, q), dtype=dt)  # filled column-major: transposed view below
+    rd = np.zeros(q)
+    info = ct.c_int32(0)
+    nc = ct.c_int32(0)
+    ms = ct.c_double(0.0)
+    _check(lib, lib.pwgpu_dense_cholesky_inverse(q, 1 if cpx else 0,
+                                                 gf.ravel(order="F").view(np.float64).ctypes.data_as(_f64p),
+                                                 ri.view(np.float64).ctypes.data_as(_f64p), _f64(rd),
+                                                 ct.byref(info), ct.byref(nc), ct.byref(ms) if timed else None))
+    out = (ri.T.copy(), rd, info.value, nc.value)
+    return out + (ms.value,) if timed else out
