@@ -115,9 +115,11 @@ __device__ __forceinline__ void tile_mma(const T* sA, const T* sB, T (&acc)[Tile
 // leading dimension B + 1, upper triangle valid) with warp 0: writes
 // Z_kk = R_kk^-1 into Ri's tile (kd, kd) (zero below the diagonal), R's
 // diagonal into rdiag, and on a failed pivot *info and *flag.  Rows and
-// columns beyond q are treated as the identity.
+// columns beyond q are treated as the identity.  Lane j keeps column j in
+// registers; each finished row of R goes back into sD (row c of the tile),
+// from where the other lanes read it as broadcasts.
 template <typename T>
-__device__ void factor_diag(const T* sD, int q, int kd, T* Ri, double* rdiag, int* info, int* flag) {
+__device__ void factor_diag(T* sD, int q, int kd, T* Ri, double* rdiag, int* info, int* flag) {
   constexpr int B = TileB<T>::value, LD = B + 1;
   if (threadIdx.x >= 32) return;
   const int j = threadIdx.x;
@@ -129,7 +131,9 @@ __device__ void factor_diag(const T* sD, int q, int kd, T* Ri, double* rdiag, in
     a[i] = gj < q ? (i <= j ? sD[i + j * LD] : zero_of(T())) : mk<T>(i == j ? 1.0 : 0.0, 0.0);
     z[i] = zero_of(T());
   }
+  __syncwarp();
   int bad = -1;
+  double rjj = 1.0;  // R_jj, taken at step j (a[] is indexed by compile-time constants only)
 #pragma unroll
   for (int c = 0; c < B; ++c) {
     double d = re(shfl(a[c], c));
@@ -139,15 +143,25 @@ __device__ void factor_diag(const T* sD, int q, int kd, T* Ri, double* rdiag, in
     }
     const double rc = sqrt(d), ir = 1.0 / rc;
     if (j >= c) a[c] = mul(a[c], ir);  // row c of R (lane c: R_cc = rc)
-    T s = zero_of(T());
+    if (j == c) rjj = rc;
+    sD[c + j * LD] = j >= c ? a[c] : zero_of(T());
+    __syncwarp();
+    // trailing rows first: the next pivot depends on them.  Every lane
+    // updates every row (entries below the diagonal of column j hold finite
+    // values that are never read), which keeps a[] in registers
 #pragma unroll
-    for (int l = 0; l < c; ++l) s = add(s, mul(z[l], shfl(a[l], c)));  // Z_jl R_lc
-    z[c] = mul(sub(mk<T>(j == c ? 1.0 : 0.0, 0.0), s), ir);
+    for (int i = c + 1; i < B; ++i) a[i] = sub(a[i], mul(cj(sD[c + i * LD]), a[c]));  // R_ci R_cj
+    // Z_jc = (delta_jc - sum_{l<c} Z_jl R_lc) / R_cc, four partial sums
+    T s0 = zero_of(T()), s1 = zero_of(T()), s2 = zero_of(T()), s3 = zero_of(T());
 #pragma unroll
-    for (int i = c + 1; i < B; ++i) {
-      const T rci = shfl(a[c], i);  // R_ci
-      if (j >= i) a[i] = sub(a[i], mul(cj(rci), a[c]));
+    for (int l = 0; l < c; ++l) {
+      const T t = mul(z[l], sD[l + c * LD]);
+      if ((l & 3) == 0) s0 = add(s0, t);
+      else if ((l & 3) == 1) s1 = add(s1, t);
+      else if ((l & 3) == 2) s2 = add(s2, t);
+      else s3 = add(s3, t);
     }
+    z[c] = mul(sub(mk<T>(j == c ? 1.0 : 0.0, 0.0), add(add(s0, s1), add(s2, s3))), ir);
   }
   // Z row j into Ri (lanes write consecutive rows of each column)
 #pragma unroll
@@ -155,10 +169,94 @@ __device__ void factor_diag(const T* sD, int q, int kd, T* Ri, double* rdiag, in
     const int gc = kd * B + c;
     if (gj < q && gc < q) Ri[gj + (long)gc * q] = z[c];
   }
-  if (gj < q && rdiag) rdiag[gj] = re(a[j]);
+  if (gj < q && rdiag) rdiag[gj] = rjj;
   if (bad >= 0 && kd * B + bad < q && j == 0) {
     *info = kd * B + bad + 1;
     *flag = 1;
+  }
+}
+
+// One tile product of a phase: C (+/-)= op(A) B with op(A) = A^H when ha;
+// C starts from zero unless init.
+template <typename T> struct TileTask {
+  const T* A;
+  int ai, aj;
+  const T* Bm;
+  int bi, bj;
+  T* Cm;
+  int ci, cj;
+  bool ha, sub, init;
+};
+
+// A tile in registers (the load_tile mapping: element e = tid + 256 u).
+template <typename T>
+__device__ __forceinline__ void fetch_regs(const T* M, int q, int ti, int tj, T (&r)[TileMap<T>::UR]) {
+  constexpr int B = TileB<T>::value, UR = TileMap<T>::UR;
+#pragma unroll
+  for (int u = 0; u < UR; ++u) {
+    const int e = threadIdx.x + kCholThreads * u;
+    const int gr = ti * B + e % B, gc = tj * B + e / B;
+    r[u] = (gr < q && gc < q) ? ldcg(M + gr + (long)gc * q) : zero_of(T());
+  }
+}
+template <typename T> __device__ __forceinline__ void regs_to_smem(const T (&r)[TileMap<T>::UR], T* s) {
+  constexpr int B = TileB<T>::value, UR = TileMap<T>::UR, LD = B + 1;
+#pragma unroll
+  for (int u = 0; u < UR; ++u) {
+    const int e = threadIdx.x + kCholThreads * u;
+    s[e % B + (e / B) * LD] = r[u];
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void run_mma(const T* sA, const T* sB, bool ha, bool sub, T (&acc)[TileMap<T>::UR]) {
+  if (ha) {
+    if (sub) tile_mma<T, true, true>(sA, sB, acc);
+    else tile_mma<T, true, false>(sA, sB, acc);
+  } else {
+    if (sub) tile_mma<T, false, true>(sA, sB, acc);
+    else tile_mma<T, false, false>(sA, sB, acc);
+  }
+}
+
+// Run tasks t = first, first + stride, ... < n of a phase, the operand
+// tiles and the starting C of the next task loaded into registers while the
+// current one computes.  fixedA / fixedB: an operand already in shared
+// memory (the task's A or B pointer is then ignored).
+template <typename T, typename Decode>
+__device__ __forceinline__ void run_tasks(int first, int stride, int n, int q, Decode decode, T* sA, T* sB,
+                                          const T* fixedA, const T* fixedB) {
+  constexpr int UR = TileMap<T>::UR;
+  if (first >= n) return;
+  T ra[UR], rb[UR], rc[UR];
+  TileTask<T> cur = decode(first);
+  auto fetch = [&](const TileTask<T>& tk) {
+    if (!fixedA) fetch_regs<T>(tk.A, q, tk.ai, tk.aj, ra);
+    if (!fixedB) fetch_regs<T>(tk.Bm, q, tk.bi, tk.bj, rb);
+    if (tk.init) {
+      load_owned<T>(tk.Cm, q, tk.ci, tk.cj, rc);
+    } else {
+#pragma unroll
+      for (int u = 0; u < UR; ++u) rc[u] = zero_of(T());
+    }
+  };
+  fetch(cur);
+  for (int t = first; t < n; t += stride) {
+    if (!fixedA) regs_to_smem<T>(ra, sA);
+    if (!fixedB) regs_to_smem<T>(rb, sB);
+    T acc[UR];
+#pragma unroll
+    for (int u = 0; u < UR; ++u) acc[u] = rc[u];
+    __syncthreads();
+    TileTask<T> nxt = cur;
+    if (t + stride < n) {
+      nxt = decode(t + stride);
+      fetch(nxt);  // in flight during the product
+    }
+    run_mma<T>(fixedA ? fixedA : sA, fixedB ? fixedB : sB, cur.ha, cur.sub, acc);
+    store_owned<T>(cur.Cm, q, cur.ci, cur.cj, acc);
+    __syncthreads();
+    cur = nxt;
   }
 }
 
@@ -199,28 +297,30 @@ __global__ void __launch_bounds__(kCholThreads, 1) k_chol_inv(T* __restrict__ G,
   for (int k = 0; k < nblk; ++k) {
     if (*cluster.map_shared_rank(&flag, 0) != 0) break;  // same value in every CTA: all leave here
     // ---- B(k): panel R_kj = Z_kk^H G_kj (j > k); inverse column block Z_ik = -S_ik Z_kk (i < k) ----
-    const int nb_tasks = nblk - 1;
-    if (rank < nb_tasks) {
-      load_tile<T>(Ri, q, k, k, sZ);
-      for (int t = rank; t < nb_tasks; t += C) {
-        T acc[UR];
-#pragma unroll
-        for (int u = 0; u < UR; ++u) acc[u] = zero_of(T());
-        if (t < nblk - 1 - k) {
-          const int j = k + 1 + t;
-          load_tile<T>(G, q, k, j, sB);
-          __syncthreads();
-          tile_mma<T, true, false>(sZ, sB, acc);
-          store_owned<T>(G, q, k, j, acc);
-        } else {
-          const int i = t - (nblk - 1 - k);
-          load_tile<T>(Ri, q, i, k, sA);
-          __syncthreads();
-          tile_mma<T, false, true>(sA, sZ, acc);
-          store_owned<T>(Ri, q, i, k, acc);
-        }
-        __syncthreads();
-      }
+    const int npanel = nblk - 1 - k;
+    if (rank < nblk - 1) {
+      load_tile<T>(Ri, q, k, k, sZ);  // Z_kk (visible to all threads after the first barrier below)
+      // panel tasks: A = Z_kk (fixed, conjugate-transposed), B = G_kj (fetched into sB)
+      auto panel = [&](int t) {
+        TileTask<T> tk{};
+        const int j = k + 1 + t;
+        tk.Bm = G; tk.bi = k; tk.bj = j;
+        tk.Cm = G; tk.ci = k; tk.cj = j;
+        tk.ha = true; tk.sub = false; tk.init = false;
+        return tk;
+      };
+      run_tasks<T>(rank, C, npanel, q, panel, sA, sB, sZ, nullptr);
+      // inverse tasks: A = S_ik (fetched into sA), B = Z_kk (fixed)
+      auto zcol = [&](int t) {
+        TileTask<T> tk{};
+        tk.A = Ri; tk.ai = t; tk.aj = k;
+        tk.Cm = Ri; tk.ci = t; tk.cj = k;
+        tk.ha = false; tk.sub = true; tk.init = false;
+        return tk;
+      };
+      // continue the rank's round-robin where the panel list left off
+      const int first = ((rank - npanel) % C + C) % C;
+      run_tasks<T>(first, C, k, q, zcol, sA, sB, nullptr, sZ);
     }
     if (k == nblk - 1) break;
     cluster.sync();
@@ -248,8 +348,8 @@ __global__ void __launch_bounds__(kCholThreads, 1) k_chol_inv(T* __restrict__ G,
     const int workers = C > 1 ? C - 1 : 1;
     const int wid = C > 1 ? rank - 1 : 0;
     if (wid >= 0) {
-      for (int t = wid; t < n_tasks; t += workers) {
-        T acc[UR];
+      auto ctask = [&](int t) {
+        TileTask<T> tk{};
         if (t < n_trail - 1) {
           // trailing tile number t + 1 of the list (k+1,k+1), (k+1,k+2), (k+2,k+2), (k+1,k+3), ...
           int jj = 0, rem = t + 1;
@@ -258,29 +358,21 @@ __global__ void __launch_bounds__(kCholThreads, 1) k_chol_inv(T* __restrict__ G,
             ++jj;
           }
           const int i = k + 1 + rem, j = k + 1 + jj;
-          load_owned<T>(G, q, i, j, acc);
-          load_tile<T>(G, q, k, i, sA);
-          load_tile<T>(G, q, k, j, sB);
-          __syncthreads();
-          tile_mma<T, true, true>(sA, sB, acc);
-          store_owned<T>(G, q, i, j, acc);
+          tk.A = G; tk.ai = k; tk.aj = i;
+          tk.Bm = G; tk.bi = k; tk.bj = j;
+          tk.Cm = G; tk.ci = i; tk.cj = j;
+          tk.ha = true; tk.sub = true; tk.init = true;
         } else {
           const int u2 = t - (n_trail - 1);
           const int i = u2 % (k + 1), j = k + 1 + u2 / (k + 1);
-          if (i == k) {
-#pragma unroll
-            for (int u = 0; u < UR; ++u) acc[u] = zero_of(T());
-          } else {
-            load_owned<T>(Ri, q, i, j, acc);
-          }
-          load_tile<T>(Ri, q, i, k, sA);
-          load_tile<T>(G, q, k, j, sB);
-          __syncthreads();
-          tile_mma<T, false, false>(sA, sB, acc);
-          store_owned<T>(Ri, q, i, j, acc);
+          tk.A = Ri; tk.ai = i; tk.aj = k;
+          tk.Bm = G; tk.bi = k; tk.bj = j;
+          tk.Cm = Ri; tk.ci = i; tk.cj = j;
+          tk.ha = false; tk.sub = false; tk.init = i != k;
         }
-        __syncthreads();
-      }
+        return tk;
+      };
+      run_tasks<T>(wid, workers, n_tasks, q, ctask, sA, sB, nullptr, nullptr);
     }
     cluster.sync();
   }

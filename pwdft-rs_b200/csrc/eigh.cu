@@ -246,11 +246,17 @@ __global__ void __launch_bounds__(kThreads, 1)
   EIGH_MARK(1);
 
   // ---- 1. Householder tridiagonalisation ----
-  // Exchanges are pulled, never pushed: a CTA reads the reflector from the
-  // owner's column and the entries of p from their owners' pbuf (remote
-  // shared-memory loads), since remote stores are several times slower.
+  // Exchanges are pulled, never pushed.  The reflector of a step goes
+  // through L2: its owner writes it to the reflector store in global memory
+  // (which the back-transform reads anyway) and the other CTAs read it from
+  // there, because fifteen CTAs pulling one CTA's shared memory measured
+  // ~5 us a step at m = 540 against well under 1 us from L2.  The entries of
+  // p (spread over all CTAs) and the step's scalars are remote shared-memory
+  // loads; remote stores are several times slower than either.
   // Reflector of column kk, by all threads of its owner: v into the column
-  // (leading 1), (tau, d_kk, e_kk) into the owner's scal of parity kk & 1.
+  // (leading 1) and into the store, (tau, d_kk, e_kk) into the owner's scal
+  // of parity kk & 1.
+  T* vglob_w = reinterpret_cast<T*>(work + vglob_offset(m, nev));
   auto house = [&](int kk) {
     T* col = a_loc + (size_t)(kk >> lgC) * m;
     if (warp == 0) {
@@ -284,8 +290,12 @@ __global__ void __launch_bounds__(kThreads, 1)
     const double* sc2 = scal + 4 * (kk & 1);
     const bool rf = sc2[0] != 0.0 || sc2[1] != 0.0;
     const T scale = mk<T>(hh[0], hh[1]);
-    for (int i = kk + 1 + tid; i < m; i += kThreads)
-      col[i] = i == kk + 1 ? mk<T>(1.0, 0.0) : (rf ? mul(col[i], scale) : mk<T>(0.0, 0.0));
+    T* vg = vglob_w + (size_t)kk * m;
+    for (int i = kk + 1 + tid; i < m; i += kThreads) {
+      const T x = i == kk + 1 ? mk<T>(1.0, 0.0) : (rf ? mul(col[i], scale) : mk<T>(0.0, 0.0));
+      col[i] = x;
+      vg[i] = x;
+    }
   };
 
   if (m > 1 && rank == 0) house(0);
@@ -301,8 +311,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (owner == rank) {
       vb = a_loc + (size_t)(k >> lgC) * m;
     } else {
-      const T* src = cluster.map_shared_rank(a_loc, owner) + (size_t)(k >> lgC) * m;
-      for (int i = k + 1 + tid; i < m; i += kThreads) vbuf[i] = src[i];
+      const T* src = vglob_w + (size_t)k * m;  // written before B1 by the owner; read past L1
+      for (int i = k + 1 + tid; i < m; i += kThreads) vbuf[i] = __ldcg(src + i);
       if (tid < 4) scal[4 * par + tid] = cluster.map_shared_rank(scal, owner)[4 * par + tid];
       vb = vbuf;
       __syncthreads();
@@ -404,8 +414,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     EIGH_SUB(7);
   }
   EIGH_SUB_STORE;
-  // the reflectors to global memory (column k holds v_k on rows k+1 .. m-1), for the back-transform
-  T* vglob_w = reinterpret_cast<T*>(work + vglob_offset(m, nev));
+  // the reflector store complete (column k holds v_k on rows k+1 .. m-1, zero above), for the back-transform
   for (int sl = 0; sl < nown; ++sl) {
     const int k = rank + sl * C;
     const T* col = a_loc + (size_t)sl * m;
