@@ -545,6 +545,7 @@ def kernel_bench(local, steps, warmup, flush, hbm_peak, peak_kind):
 
 
 def main():
+    global BATCH
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
@@ -558,7 +559,9 @@ def main():
     ap.add_argument("--workers", type=int, default=4, help="serve: concurrent jobs on the device")
     ap.add_argument("--serve-requests", type=int, default=60,
                     help="requests of the serving stream replayed after the headline (0: none)")
+    ap.add_argument("--batch", type=int, default=BATCH, help="Si64 cells solved concurrently per step")
     args = ap.parse_args()
+    BATCH = max(1, args.batch)
     world, rank, local = dist_env()
     if args.mode == "serve":
         run_serve(args)

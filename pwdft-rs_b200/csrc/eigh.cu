@@ -104,6 +104,11 @@ constexpr size_t kSmemLimit = 227 * 1024;
 
 using namespace dense;
 
+// The two halves of a cluster barrier (release on arrival, acquire on the
+// wait); every thread of every CTA arrives once, then waits, per phase.
+__device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory"); }
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory"); }
+
 // Shared-memory layout of one CTA (identical on host and device).
 struct Layout {
   size_t a, v, p, s, sc, d, e2, tau, eig, grp, red, hh, total;
@@ -298,13 +303,18 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   };
 
+  // B1 of a step is split: the owner of the next column arrives as soon as
+  // its reflector is out and updates its other columns afterwards, so that
+  // update is off the path the other CTAs wait on; the rest arrive after
+  // their update.  B2 is a full cluster barrier.
   if (m > 1 && rank == 0) house(0);
+  cluster_arrive();
   EIGH_SUB_DECL
   for (int k = 0; k < m - 1; ++k) {
     const int par = k & 1;
     const int owner = k & (C - 1);
     EIGH_SUB(0);
-    cluster.sync();  // B1: the reflector of column k is in its owner's column and scal
+    cluster_wait();  // B1: the reflector of column k is in the store and its owner's scal
     EIGH_SUB(1);
     // pull v (rows k+1 .. m-1) and the step's scalars from the owner
     const T* vb;
@@ -394,6 +404,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int i = k + 1 + tid; i < m; i += kThreads) col[i] = sub(col[i], add(mul(vb[i], cwj), mul(wbuf[i], cvj)));
         __syncthreads();
         house(k + 1);
+        cluster_arrive();
       }
       EIGH_SUB(6);
       for (int gb = warp * gpw; gb < na; gb += kWarps * gpw) {
@@ -409,10 +420,13 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
     } else if (look) {
       house(k + 1);
+      cluster_arrive();
     }
     __syncthreads();
+    if (!look) cluster_arrive();
     EIGH_SUB(7);
   }
+  cluster_wait();  // completes the last arrival
   EIGH_SUB_STORE;
   // the reflector store complete (column k holds v_k on rows k+1 .. m-1, zero above), for the back-transform
   for (int sl = 0; sl < nown; ++sl) {

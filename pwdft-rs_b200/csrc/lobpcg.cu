@@ -772,14 +772,17 @@ Status lobpcg_t(Handle& h, EigWork& w, EigVecs& k, int spin, int ik, double v0, 
     pt.mark(5, s);
     if ((r = subspace_eig<T>(c, m, nd, &C)) != kOk) return r;
     pt.mark(6, s);
-    // new X, HX; new P, HP for the active bands from the (W, P) rows of C
-    if ((r = gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, nd, m, X, n, C, m, Tb, n)) != kOk) return r;
-    if ((r = gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, nd, m, HX, n, C, m, as<T>(w.HXn), n)) != kOk) return r;
+    // new X, HX and new P, HP of the active bands.  T = [W | P] C_wp (C's W, P rows, all nd
+    // columns) is the P part of every new X column: P = T(:, active), X = X C_x + T, so the
+    // W, P products are formed once (likewise for HX, HP)
     PW_CUDA_TRY(cudaMemcpyAsync(w.idx, act.data(), na * sizeof(int), cudaMemcpyHostToDevice, s));
-    T* Ca = C == as<T>(w.Cs) ? as<T>(w.Z) : as<T>(w.Cs);  // q x na gathered columns, ld q
-    k_gather_cols<T><<<dim3(1, na), 256, 0, s>>>(C + nd, m, w.idx, Ca, q, q); count_launch();
-    if ((r = gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, na, q, W, n, Ca, q, Pn, n)) != kOk) return r;
-    if ((r = gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, na, q, HW, n, Ca, q, HPn, n)) != kOk) return r;
+    T* HXn = as<T>(w.HXn);
+    if ((r = gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, nd, q, W, n, C + nd, m, Tb, n)) != kOk) return r;
+    if ((r = gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, nd, q, HW, n, C + nd, m, HXn, n)) != kOk) return r;
+    k_gather_cols<T><<<dim3(c.gx, na), 256, 0, s>>>(Tb, n, w.idx, Pn, n, (int)n); count_launch();
+    k_gather_cols<T><<<dim3(c.gx, na), 256, 0, s>>>(HXn, n, w.idx, HPn, n, (int)n); count_launch();
+    if ((r = gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, nd, nd, X, n, C, m, Tb, n, 1.0)) != kOk) return r;
+    if ((r = gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, nd, nd, HX, n, C, m, HXn, n, 1.0)) != kOk) return r;
     PW_CUDA_TRY(cudaMemcpyAsync(X, Tb, n * nd * sizeof(T), cudaMemcpyDeviceToDevice, s));
     PW_CUDA_TRY(cudaMemcpyAsync(HX, w.HXn, n * nd * sizeof(T), cudaMemcpyDeviceToDevice, s));
     PW_CUDA_TRY(cudaMemcpyAsync(k.evals.data(), w.lam, nd * sizeof(double), cudaMemcpyDeviceToHost, s));
