@@ -64,9 +64,10 @@ BATCH = 4  # Si64 cells solved concurrently in one step
 # each band plus one FP32 V(r) read (the output stays in L2), so it is scaled
 # to a launch's band count as (capture - V) / 22 per band + V.
 XV_TRAFFIC_CAPTURE = (33503744 + 3072, 22)
-# the fused middle kernel (k_yxy<float>) on the same grid: DRAM bytes of one
-# launch and its band count, from one ncu capture (None until captured)
-YXY_TRAFFIC_CAPTURE = (None, 20)
+# the fused middle kernel (k_yxy_ct<float, 8, 9, 8, 9>) on the same grid:
+# dram__bytes_read.sum + dram__bytes_write.sum of one 20-band launch from one
+# ncu capture (the written planes stay in L2), scaled by a launch's bands
+YXY_TRAFFIC_CAPTURE = (17050880, 20)
 
 
 def load_peaks():
