@@ -52,6 +52,9 @@ constexpr int kSmallSolveMax = 64;  // subspace size up to which the one-CTA sol
 // their norm are dropped (FP64 / reduced-precision search directions)
 constexpr double kPDropFp64 = 1e-5;
 constexpr double kPDropMixed = 3e-2;
+// A Cholesky-QR pass is skipped when its block is orthonormal to this
+// (max |Y^H Y - I|): the second pass of CholQR2 then has nothing to fix.
+constexpr double kOrthoSkipTol = 1e-12;
 
 inline unsigned blocks_for(long n, int t = 256) { return (unsigned)std::max<long>(1, (n + t - 1) / t); }
 
@@ -202,6 +205,22 @@ template <typename S> __global__ void k_set_identity(S* __restrict__ A, int m) {
 template <typename S> __global__ void k_diag_real(const S* __restrict__ A, int ld, int m, double* __restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < m) out[i] = real_part(A[i + (long)i * ld]);
+}
+
+// out = max_ij |G_ij - delta_ij| over the q x q Gram matrix (out zeroed by
+// the caller; non-negative doubles order like their bit patterns)
+__device__ __forceinline__ double defect_of(double g, bool diag) { return fabs(diag ? g - 1.0 : g); }
+__device__ __forceinline__ double defect_of(double2 g, bool diag) { return hypot(diag ? g.x - 1.0 : g.x, g.y); }
+template <typename S> __global__ void k_gram_defect(const S* __restrict__ G, int q, double* __restrict__ out) {
+  double v = 0.0;
+  const long nn = (long)q * q;
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < nn; t += (long)gridDim.x * blockDim.x) {
+    const int r = (int)(t % q), cc = (int)(t / q);
+    v = fmax(v, defect_of(G[t], r == cc));
+  }
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0 && v > 0.0)
+    atomicMax(reinterpret_cast<unsigned long long*>(out), (unsigned long long)__double_as_longlong(v));
 }
 
 // real m x m <-> complex (zero imaginary part), for the one-CTA complex solver
@@ -355,14 +374,31 @@ template <typename T> Status project_out(Ctx& c, const T* A, const T* HA, int p,
 
 // One Cholesky-QR pass: G = Y^H Y (+ shift I), G = R^H R, Y <- Y R^-1 (and
 // HY with the same R).  ok = false when the factorisation broke down (Y is
-// left unchanged then).  min_rdiag: smallest diagonal entry of R.
+// left unchanged then).  min_rdiag: smallest diagonal entry of R.  With
+// skip_tol > 0 the pass stops after the Gram matrix when Y is already
+// orthonormal to skip_tol (max |G - I|; *skipped then true), which saves the
+// factorisation and the update products of most second passes.
 template <typename T>
-Status chol_qr(Ctx& c, T* Y, T* HY, int q, double shift, bool& ok, double* min_rdiag = nullptr) {
+Status chol_qr(Ctx& c, T* Y, T* HY, int q, double shift, bool& ok, double* min_rdiag = nullptr,
+               double skip_tol = 0.0, bool* skipped = nullptr) {
   ok = true;
+  if (skipped) *skipped = false;
   if (q == 0) return kOk;
   Status r;
   T* G = as<T>(c.w.G);
   if ((r = gemm(c, CUBLAS_OP_C, CUBLAS_OP_N, q, q, (int)c.n, Y, c.n, Y, c.n, G, q)) != kOk) return r;
+  if (skip_tol > 0.0 && shift == 0.0) {
+    PW_CUDA_TRY(cudaMemsetAsync(c.w.defect, 0, sizeof(double), c.s));
+    k_gram_defect<T><<<std::min<long>(64, blocks_for((long)q * q)), 256, 0, c.s>>>(G, q, c.w.defect); count_launch();
+    double defect = 0.0;
+    PW_CUDA_TRY(cudaMemcpyAsync(&defect, c.w.defect, sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    PW_CUDA_TRY(cudaStreamSynchronize(c.s));
+    if (defect <= skip_tol) {
+      if (skipped) *skipped = true;
+      if (min_rdiag) *min_rdiag = 1.0;
+      return kOk;
+    }
+  }
   if (shift > 0.0) {
     T* Id = as<T>(c.w.Id);
     k_set_identity<T><<<blocks_for((long)q * q), 256, 0, c.s>>>(Id, q); count_launch();
@@ -411,13 +447,15 @@ template <typename T> Status orthonormalize(Ctx& c, T* Y, int q) {
   Status r;
   if ((r = col_norms2(c, (const T*)Y, q, nullptr)) != kOk) return r;
   k_scale_cols_invsqrt<T><<<dim3(c.gx, q), 256, 0, c.s>>>(Y, nullptr, c.n, (int)c.n, c.w.colsq); count_launch();
-  bool ok = false;
-  if ((r = chol_qr(c, Y, (T*)nullptr, q, 0.0, ok)) != kOk) return r;
+  bool ok = false, skipped = false;
+  // an already orthonormal block (the bands carried over from the previous SCF step) needs no pass
+  if ((r = chol_qr(c, Y, (T*)nullptr, q, 0.0, ok, nullptr, kOrthoSkipTol, &skipped)) != kOk) return r;
+  if (skipped) return kOk;
   if (!ok) {
     if ((r = chol_qr(c, Y, (T*)nullptr, q, 1e-10 * q, ok)) != kOk) return r;
     if (!ok) return fail(kNotConverged, "eigensolver: search block is numerically rank deficient");
   }
-  if ((r = chol_qr(c, Y, (T*)nullptr, q, 0.0, ok)) != kOk) return r;
+  if ((r = chol_qr(c, Y, (T*)nullptr, q, 0.0, ok, nullptr, kOrthoSkipTol)) != kOk) return r;
   if (!ok) return fail(kNotConverged, "eigensolver: second Cholesky-QR pass broke down");
   return kOk;
 }
@@ -671,7 +709,7 @@ Status lobpcg_t(Handle& h, EigWork& w, EigVecs& k, int spin, int ik, double v0, 
         if ((r = chol_qr(c, P, HP, npc, 0.0, ok, &rmin)) != kOk) return r;
         if (!ok || rmin < p_drop) {
           npc = 0;  // P block nearly dependent: restart without it
-        } else if ((r = chol_qr(c, P, HP, npc, 0.0, ok)) != kOk) {
+        } else if ((r = chol_qr(c, P, HP, npc, 0.0, ok, nullptr, kOrthoSkipTol)) != kOk) {
           return r;
         } else if (!ok) {
           npc = 0;
@@ -823,6 +861,7 @@ Status eig_work_alloc(EigWork& w, long n, int nd) {
   for (double2** p : {&w.Hs, &w.Cs, &w.G, &w.Z, &w.Id})
     if ((r = walloc(p, m * m)) != kOk) return r;
   if ((r = walloc(&w.XX, (size_t)nd * nd)) != kOk) return r;
+  if ((r = walloc(&w.defect, 2)) != kOk) return r;
   if ((r = walloc(&w.lam, m)) != kOk) return r;
   if ((r = walloc(&w.lam0, m)) != kOk) return r;
   if ((r = walloc(&w.colsq, m)) != kOk) return r;
@@ -837,7 +876,7 @@ void eig_work_release(EigWork& w) {
   auto f = [](void* p) { if (p) cudaFree(p); };
   f(w.T); f(w.HXn); f(w.Pn); f(w.HPn); f(w.Hs); f(w.Cs); f(w.G); f(w.Z); f(w.Id);
   f(w.lam); f(w.lam0); f(w.colsq); f(w.partials); f(w.idx); f(w.status); f(w.solver_work); f(w.info);
-  f(w.eigh_work); f(w.XX);
+  f(w.eigh_work); f(w.XX); f(w.defect);
   w = EigWork();
 }
 

@@ -42,6 +42,7 @@ struct EigWork {
   int* info = nullptr;
   double* eigh_work = nullptr;  // scratch of the cluster eigensolver (eigh.cu)
   double2* XX = nullptr;        // nd x nd: X^H HX at the start of a solve
+  double* defect = nullptr;     // max |Y^H Y - I| of a Cholesky-QR pass
   size_t eigh_work_len = 0;
 };
 
