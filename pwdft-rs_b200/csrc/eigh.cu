@@ -262,11 +262,17 @@ __global__ void __launch_bounds__(kThreads, 1)
   // (leading 1) and into the store, (tau, d_kk, e_kk) into the owner's scal
   // of parity kk & 1.
   T* vglob_w = reinterpret_cast<T*>(work + vglob_offset(m, nev));
-  auto house = [&](int kk) {
+  __shared__ double s2_part[kWarps];  // per-warp partial sums of |col[i]|^2, rows >= kk + 2
+  // have_parts: s2_part already holds the partials (summed while the column was updated)
+  auto house = [&](int kk, bool have_parts) {
     T* col = a_loc + (size_t)(kk >> lgC) * m;
     if (warp == 0) {
       double s2 = 0.0;
-      for (int i = kk + 2 + lane; i < m; i += 32) s2 += abs2(col[i]);
+      if (have_parts) {
+        s2 = lane < kWarps ? s2_part[lane] : 0.0;
+      } else {
+        for (int i = kk + 2 + lane; i < m; i += 32) s2 += abs2(col[i]);
+      }
       s2 = warp_sum(s2);
       if (lane == 0) {
         const T alpha = col[kk + 1];
@@ -307,7 +313,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   // its reflector is out and updates its other columns afterwards, so that
   // update is off the path the other CTAs wait on; the rest arrive after
   // their update.  B2 is a full cluster barrier.
-  if (m > 1 && rank == 0) house(0);
+  if (m > 1 && rank == 0) house(0, false);
   cluster_arrive();
   EIGH_SUB_DECL
   for (int k = 0; k < m - 1; ++k) {
@@ -399,11 +405,19 @@ __global__ void __launch_bounds__(kThreads, 1)
       EIGH_SUB(5);
       if (look) {
         // column k + 1 first, so that its reflector is ready early
+        // (with the norm its reflector needs summed on the way)
         T* col = a_loc + (size_t)((k + 1) >> lgC) * m;
         const T cwj = cj(wbuf[k + 1]), cvj = cj(vb[k + 1]);
-        for (int i = k + 1 + tid; i < m; i += kThreads) col[i] = sub(col[i], add(mul(vb[i], cwj), mul(wbuf[i], cvj)));
+        double s2 = 0.0;
+        for (int i = k + 1 + tid; i < m; i += kThreads) {
+          const T x = sub(col[i], add(mul(vb[i], cwj), mul(wbuf[i], cvj)));
+          col[i] = x;
+          if (i >= k + 3) s2 += abs2(x);
+        }
+        s2 = warp_sum(s2);
+        if (lane == 0) s2_part[warp] = s2;
         __syncthreads();
-        house(k + 1);
+        house(k + 1, true);
         cluster_arrive();
       }
       EIGH_SUB(6);
@@ -419,7 +433,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (int i = k + 1 + r; i < m; i += R) col[i] = sub(col[i], add(mul(vb[i], cwj), mul(wbuf[i], cvj)));
       }
     } else if (look) {
-      house(k + 1);
+      house(k + 1, false);
       cluster_arrive();
     }
     __syncthreads();
