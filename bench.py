@@ -392,6 +392,101 @@ def run_scf_once():
     print("scf once: ok", res["n_iterations"], res["total_energy"])
 
 
+def run_dense():
+    """The eigensolver's two dense kernels on seeded matrices of the Si64
+    solve's subspace sizes, through the C-ABI (CUDA events around each
+    launch, median of five after two warm-ups): the cluster eigensolver
+    (lowest n_d = m/3 pairs, or all for m = 180) and the Cholesky factor with
+    its inverse.  One JSON line; also the short program the dense-kernel
+    profiler captures run."""
+    import torch
+
+    from pwgpu.lib import dense_cholesky_inverse, dense_eigh
+    g = np.random.default_rng(SEED)
+    out = {"mode": "dense", "eigh_ms": {}, "cholesky_inverse_ms": {}, "cusolver_syevd_ms": {},
+           "cusolver_potrf_trsm_ms": {}, "cusolver_note": "torch.linalg (cuSOLVER) on the same matrices, "
+           "all eigenpairs / Cholesky plus triangular inverse, CUDA events, for comparison only"}
+
+    def torch_ms(fn, reps=5):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+
+    for m in (180, 360, 540):
+        nev = m if m <= 180 else m // 3
+        a = g.standard_normal((m, m))
+        a = a + a.T
+        ts = [dense_eigh(a, nev, timed=True)[3] for _ in range(7)][2:]
+        out["eigh_ms"][str(m)] = float(np.median(ts))
+        ta = torch.tensor(a, device="cuda")
+        out["cusolver_syevd_ms"][str(m)] = torch_ms(lambda: torch.linalg.eigh(ta))
+    for q in (180, 360):
+        y = g.standard_normal((3 * q, q))
+        gm = y.T @ y
+        ts = [dense_cholesky_inverse(gm, timed=True)[4] for _ in range(7)][2:]
+        out["cholesky_inverse_ms"][str(q)] = float(np.median(ts))
+        tg = torch.tensor(gm, device="cuda")
+        eye = torch.eye(q, dtype=tg.dtype, device="cuda")
+        out["cusolver_potrf_trsm_ms"][str(q)] = torch_ms(
+            lambda: torch.linalg.solve_triangular(torch.linalg.cholesky(tg), eye, upper=False))
+    print(json.dumps(out))
+
+
+def config4_record(local: int) -> dict:
+    """The batched-k LSDA case (Si8 and C8 conventional cells, 35 Ry, 20 IBZ
+    k-points x 2 spins each, 24 bands, plain FP64 at the reference's default
+    thresholds): each cell solved with its (spin, k) eigensolves on 8
+    concurrent lanes and one at a time, device-synchronised wall time, kernel
+    launches per SCF iteration, and |dE| against the committed oracle
+    fixtures (converged to drho 1e-9, so the bar is the solve's own 1e-5 eV
+    energy threshold)."""
+    import torch
+
+    from pwgpu.config4 import SCF_KW as C4_KW
+    from pwgpu.config4 import config4_system
+    from pwgpu.lib import PwGpu, kernel_launches
+    from pwgpu.upf import load_upf
+    out = {"workload": "si8_c8_lsda_35ry_6x6x6", "cells": {}}
+    wall = {1: 0.0, 8: 0.0}
+    for species, upf in (("Si", "Si.upf"), ("C", "C.upf")):
+        s_, m = config4_system(species, load_upf(os.path.join(ROOT, "tests", "golden", "upf", upf)))
+        with open(os.path.join(ROOT, "tests", "golden", f"config4_{species}_oracle.json")) as f:
+            ref = json.load(f)
+        kw = dict(C4_KW)
+        nb = kw.pop("n_bands")
+        rec = {"n_pw": s_.n_pw, "n_k": len(s_.kpoints)}
+        for lanes in (8, 1):
+            with PwGpu(s_, device=local, lanes=lanes) as dev:
+                dev.scf_run(s_.rho_init_r, nb, starting_magnetization=m, **kw)  # warm-up
+                torch.cuda.synchronize()
+                n0 = kernel_launches()
+                t0 = time.perf_counter()
+                res, _, _, _ = dev.scf_run(s_.rho_init_r, nb, starting_magnetization=m, **kw)
+                torch.cuda.synchronize()
+                dt = time.perf_counter() - t0
+                n1 = kernel_launches() - n0
+            wall[lanes] += dt
+            rec[f"lanes_{lanes}"] = {"s": dt, "scf_iterations": int(res["n_iterations"]),
+                                     "launches_per_scf_iteration": n1 / max(1, int(res["n_iterations"])),
+                                     "dE_vs_oracle_ev": abs(res["total_energy"] - ref["total_energy"]),
+                                     "converged": bool(res["converged"])}
+        out["cells"][species] = rec
+    out["solves_per_s_lanes_8"] = 2.0 / wall[8]
+    out["solves_per_s_sequential"] = 2.0 / wall[1]
+    out["form"] = ("plain FP64; (spin, k) eigensolves of an SCF iteration on 8 host-thread lanes with a stream "
+                   "each, against one at a time; the reference loops k with rayon (scf/driver.rs:461-472)")
+    return out
+
+
 def serving_record(n_requests: int, workers: int) -> dict:
     """Serving workload: the first n_requests requests of the seeded stream
     (Poisson 50/s; Si/C, 2-64 atoms, strain, displacements, 20-35 Ry, Gamma or
@@ -553,14 +648,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="pwgpu", choices=["pwgpu", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="full", choices=["full", "once", "scf-once", "serve"],
+    ap.add_argument("--mode", default="full", choices=["full", "once", "scf-once", "serve", "dense"],
                     help="once: three untimed H|psi> calls per precision; scf-once: one mixed solve; "
-                         "serve: the serving stream through pwgpu_server_* (own JSON line)")
+                         "serve: the serving stream through pwgpu_server_* (own JSON line); "
+                         "dense: the subspace eigensolver and Cholesky kernels alone (own JSON line)")
     ap.add_argument("--requests", type=int, default=200, help="serve: requests of the stream replayed")
     ap.add_argument("--workers", type=int, default=4, help="serve: concurrent jobs on the device")
     ap.add_argument("--serve-requests", type=int, default=60,
                     help="requests of the serving stream replayed after the headline (0: none)")
     ap.add_argument("--batch", type=int, default=BATCH, help="Si64 cells solved concurrently per step")
+    ap.add_argument("--no-config4", action="store_true", help="skip the batched-k LSDA record")
     args = ap.parse_args()
     BATCH = max(1, args.batch)
     world, rank, local = dist_env()
@@ -572,6 +669,9 @@ def main():
         return
     if args.mode == "scf-once":
         run_scf_once()
+        return
+    if args.mode == "dense":
+        run_dense()
         return
     if args.impl == "reference":
         if world > 1:
@@ -711,6 +811,10 @@ def main():
     if rank == 0 and world == 1 and args.serve_requests > 0:
         stage(f"serving stream, first {args.serve_requests} requests")
         serving = serving_record(args.serve_requests, args.workers)
+    c4 = None
+    if rank == 0 and world == 1 and not args.no_config4:
+        stage("batched-k LSDA case (config 4)")
+        c4 = config4_record(local)
     stage("done")
     if rank == 0:
         value = world * BATCH * 1e3 / ms
@@ -750,6 +854,8 @@ def main():
             line["config1_complete_solves"] = c1
         if serving:
             line["serving"] = serving
+        if c4:
+            line["config4"] = c4
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
