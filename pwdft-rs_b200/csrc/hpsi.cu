@@ -424,6 +424,130 @@ bool launch_yxy_ct(const GridMaps& g, cplx<R>* A, const R* vz, int nb, int bpc, 
   }
 }
 
+// K1 and K5 of the fused pipeline with the z transform's two radix stages
+// fixed at compile time (d2 = Z0 * Z1): the first stage of K1 reads the
+// scattered sphere columns from shared memory and its second writes the
+// z-major planes straight to global memory; K5's first stage reads the
+// z-major planes straight from global memory and its second writes shared
+// memory for the sphere gather.  One-dimensional blocks of kZThreads.
+constexpr int kZThreads = 256;
+template <typename R, int Z0, int Z1>
+__global__ void __launch_bounds__(kZThreads) k_zinv_ct(const double2* __restrict__ psi, long ldpsi,
+                                                      cplx<R>* __restrict__ A, const int* __restrict__ col_start,
+                                                      const int* __restrict__ pt_ig, const int* __restrict__ pt_col,
+                                                      const int* __restrict__ pt_z, int ncol, int W, unsigned mW,
+                                                      const cplx<R>* __restrict__ twz) {
+  using C = cplx<R>;
+  constexpr int d2 = Z0 * Z1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  C* scr = buf + W * d2;
+  const int c0 = blockIdx.x * W;
+  const int b = blockIdx.y;
+  const int nl = min(W, ncol - c0);
+  const int tid = threadIdx.x, T = blockDim.x;
+  for (int i = tid; i < W * d2; i += T) buf[i] = cmake<C>(0.0, 0.0);
+  __syncthreads();
+  const double2* ps = psi + (long)b * ldpsi;
+  const int i0 = col_start[c0], i1 = col_start[c0 + nl];
+  for (int i = i0 + tid; i < i1; i += T) buf[pt_z[i] * W + (pt_col[i] - c0)] = to_c<C>(ps[pt_ig[i]]);
+  __syncthreads();
+  C* out = A + (long)b * d2 * ncol + c0;
+  line_fft2_f<+1, Z0, Z1>(W, mW, twz, scr, [&](int e, int l) { return buf[e * W + l]; },
+                          [&](int e, int l, C v) {
+                            if (l < nl) out[(long)e * ncol + l] = v;
+                          });
+}
+
+template <typename R, int Z0, int Z1>
+__global__ void __launch_bounds__(kZThreads) k_zfwd_ct(const cplx<R>* __restrict__ A, const double2* __restrict__ psi,
+                                                      long ldpsi, double2* __restrict__ hpsi, long ldh,
+                                                      const double* __restrict__ kin, double scale,
+                                                      const int* __restrict__ col_start, const int* __restrict__ pt_ig,
+                                                      const int* __restrict__ pt_col, const int* __restrict__ pt_z,
+                                                      int ncol, int W, unsigned mW, const cplx<R>* __restrict__ twz) {
+  using C = cplx<R>;
+  constexpr int d2 = Z0 * Z1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  C* scr = buf + W * d2;
+  const int c0 = blockIdx.x * W;
+  const int b = blockIdx.y;
+  const int nl = min(W, ncol - c0);
+  const int tid = threadIdx.x, T = blockDim.x;
+  const C* in = A + (long)b * d2 * ncol + c0;
+  line_fft2_f<-1, Z0, Z1>(W, mW, twz, scr,
+                          [&](int e, int l) { return l < nl ? in[(long)e * ncol + l] : cmake<C>(0.0, 0.0); },
+                          [&](int e, int l, C v) { buf[e * W + l] = v; });
+  const double2* ps = psi + (long)b * ldpsi;
+  double2* hs = hpsi + (long)b * ldh;
+  const int i0 = col_start[c0], i1 = col_start[c0 + nl];
+  for (int i = i0 + tid; i < i1; i += T) {
+    const int ig = pt_ig[i];
+    const C v = buf[pt_z[i] * W + (pt_col[i] - c0)];
+    const double2 p = ps[ig];
+    const double t = kin[ig];
+    hs[ig] = make_double2((double)v.x * scale + t * p.x, (double)v.y * scale + t * p.y);
+  }
+}
+
+// The compile-time z pass for the two-stage z lengths (72, 40, 25, 24);
+// false for others (the caller runs the generic kernels).
+template <typename R> bool z_ct_ok(const GridMaps& g) {
+  switch (two_stage_key(g.plan[2])) {
+    case 8 * 16 + 9: case 8 * 16 + 5: case 5 * 16 + 5: case 8 * 16 + 3: return true;
+    default: return false;
+  }
+}
+template <typename R>
+void launch_zinv_ct(const GridMaps& g, int W, const double2* psi, long ldpsi, cplx<R>* A, int nb, const cplx<R>* tw,
+                    cudaStream_t s) {
+  const dim3 grid((g.ncol + W - 1) / W, nb);
+  const size_t smem = 2 * (size_t)W * g.d[2] * sizeof(cplx<R>);
+  const unsigned mW = div_magic(W);
+  switch (two_stage_key(g.plan[2])) {
+    case 8 * 16 + 9:
+      k_zinv_ct<R, 8, 9><<<grid, kZThreads, smem, s>>>(psi, ldpsi, A, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, W, mW, tw);
+      break;
+    case 8 * 16 + 5:
+      k_zinv_ct<R, 8, 5><<<grid, kZThreads, smem, s>>>(psi, ldpsi, A, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, W, mW, tw);
+      break;
+    case 5 * 16 + 5:
+      k_zinv_ct<R, 5, 5><<<grid, kZThreads, smem, s>>>(psi, ldpsi, A, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, W, mW, tw);
+      break;
+    default:
+      k_zinv_ct<R, 8, 3><<<grid, kZThreads, smem, s>>>(psi, ldpsi, A, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, W, mW, tw);
+      break;
+  }
+  count_launch();
+}
+template <typename R>
+void launch_zfwd_ct(const GridMaps& g, int W, const cplx<R>* A, const double2* psi, long ldpsi, double2* hpsi, long ldh,
+                    const double* kin, double scale, int nb, const cplx<R>* tw, cudaStream_t s) {
+  const dim3 grid((g.ncol + W - 1) / W, nb);
+  const size_t smem = 2 * (size_t)W * g.d[2] * sizeof(cplx<R>);
+  const unsigned mW = div_magic(W);
+  switch (two_stage_key(g.plan[2])) {
+    case 8 * 16 + 9:
+      k_zfwd_ct<R, 8, 9><<<grid, kZThreads, smem, s>>>(A, psi, ldpsi, hpsi, ldh, kin, scale, g.col_start, g.pt_ig,
+                                                       g.pt_col, g.pt_z, g.ncol, W, mW, tw);
+      break;
+    case 8 * 16 + 5:
+      k_zfwd_ct<R, 8, 5><<<grid, kZThreads, smem, s>>>(A, psi, ldpsi, hpsi, ldh, kin, scale, g.col_start, g.pt_ig,
+                                                       g.pt_col, g.pt_z, g.ncol, W, mW, tw);
+      break;
+    case 5 * 16 + 5:
+      k_zfwd_ct<R, 5, 5><<<grid, kZThreads, smem, s>>>(A, psi, ldpsi, hpsi, ldh, kin, scale, g.col_start, g.pt_ig,
+                                                       g.pt_col, g.pt_z, g.ncol, W, mW, tw);
+      break;
+    default:
+      k_zfwd_ct<R, 8, 3><<<grid, kZThreads, smem, s>>>(A, psi, ldpsi, hpsi, ldh, kin, scale, g.col_start, g.pt_ig,
+                                                       g.pt_col, g.pt_z, g.ncol, W, mW, tw);
+      break;
+  }
+  count_launch();
+}
+
 // V(r) [x][y][z] -> [z][x][y], FP64 and FP32
 __global__ void k_zmajor(const double* __restrict__ vr, double* __restrict__ vz64, float* __restrict__ vz32, int d0,
                          int d1, int d2) {
@@ -644,6 +768,14 @@ Status configure_kernels() {
   set((const void*)k_fft_axis<1>); set((const void*)k_fft_axis<-1>);
   set((const void*)k_x_density);
   set((const void*)k_zinv<double, true>); set((const void*)k_zinv<float, true>);
+  set((const void*)k_zinv_ct<double, 8, 9>); set((const void*)k_zinv_ct<float, 8, 9>);
+  set((const void*)k_zinv_ct<double, 8, 5>); set((const void*)k_zinv_ct<float, 8, 5>);
+  set((const void*)k_zinv_ct<double, 5, 5>); set((const void*)k_zinv_ct<float, 5, 5>);
+  set((const void*)k_zinv_ct<double, 8, 3>); set((const void*)k_zinv_ct<float, 8, 3>);
+  set((const void*)k_zfwd_ct<double, 8, 9>); set((const void*)k_zfwd_ct<float, 8, 9>);
+  set((const void*)k_zfwd_ct<double, 8, 5>); set((const void*)k_zfwd_ct<float, 8, 5>);
+  set((const void*)k_zfwd_ct<double, 5, 5>); set((const void*)k_zfwd_ct<float, 5, 5>);
+  set((const void*)k_zfwd_ct<double, 8, 3>); set((const void*)k_zfwd_ct<float, 8, 3>);
   set((const void*)k_zfwd<double, true>); set((const void*)k_zfwd<float, true>);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute((const void*)k_yxy<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFusedSmemMax);
@@ -734,9 +866,19 @@ static Status autotune_tiles(Handle& h) {
   std::vector<int> cx;
   for (int W : even)
     if (d0 <= 16 * (kThreads / W)) cx.push_back(W);
-  const int wz = best(odd, d2, g.wz, [&](int W) {
-    k_zinv<float><<<dim3((g.ncol + W - 1) / W, nb_in), block_for(W), 2 * (size_t)W * d2 * sizeof(float2), s>>>(
-        psi, h.n_pw, A, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2, div_magic(d2), g.plan[2], g.tw32[2]);
+  // the z width is measured on the kernel the pipeline will run: the
+  // compile-time z pass (one-dimensional blocks, so wider tiles fit) when
+  // the z length has one, else the generic kernel
+  const bool zct = z_ct_ok<float>(g);
+  std::vector<int> zc = odd;
+  if (zct) zc.push_back(81);
+  const int wz = best(zc, d2, g.wz, [&](int W) {
+    if (zct) {
+      launch_zinv_ct<float>(g, W, psi, h.n_pw, A, nb_in, g.tw32[2], s);
+    } else {
+      k_zinv<float><<<dim3((g.ncol + W - 1) / W, nb_in), block_for(W), 2 * (size_t)W * d2 * sizeof(float2), s>>>(
+          psi, h.n_pw, A, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2, div_magic(d2), g.plan[2], g.tw32[2]);
+    }
   });
   const int wy = best(even, d1, g.wy, [&](int W) {
     k_y<float, +1><<<dim3(g.Xp, (d2 + W - 1) / W, nb), block_for(W), 2 * (size_t)W * d1 * sizeof(float2), s>>>(
@@ -942,9 +1084,13 @@ static Status local_chunk(Handle& h, int spin, int ik, const double2* psi, long 
   if (fused_ok<R>(g)) {
     // K1 (z-major A), K234 fused per z-plane, K5
     const R* vz = std::is_same<R, double>::value ? (const R*)h.veff_rz[spin] : (const R*)h.veff_rz32[spin];
-    k_zinv<R, true><<<dim3((g.ncol + wz - 1) / wz, nb), block_for(wz), 2 * (size_t)wz * d2 * sizeof(C), s>>>(
-        psi, ldpsi, A, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2, div_magic(d2), g.plan[2], tw2,
-        div_magic(wz)); count_launch();
+    if (z_ct_ok<R>(g)) {
+      launch_zinv_ct<R>(g, wz, psi, ldpsi, A, nb, tw2, s);
+    } else {
+      k_zinv<R, true><<<dim3((g.ncol + wz - 1) / wz, nb), block_for(wz), 2 * (size_t)wz * d2 * sizeof(C), s>>>(
+          psi, ldpsi, A, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2, div_magic(d2), g.plan[2], tw2,
+          div_magic(wz)); count_launch();
+    }
     mark(tm, 0, s);
     const int groups = std::max(1, std::min(nb, (2 * 148 + d2 - 1) / d2));
     const int bpc = (nb + groups - 1) / groups;
@@ -954,9 +1100,13 @@ static Status local_chunk(Handle& h, int spin, int ik, const double2* psi, long 
           g.plan[0], g.plan[1], tw0, tw1); count_launch();
     }
     mark(tm, 2, s);
-    k_zfwd<R, true><<<dim3((g.ncol + wz - 1) / wz, nb), block_for(wz), 2 * (size_t)wz * d2 * sizeof(C), s>>>(
-        A, psi, ldpsi, hpsi, ldh, h.kp[ik].kinetic, scale, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2,
-        div_magic(d2), g.plan[2], tw2, div_magic(wz)); count_launch();
+    if (z_ct_ok<R>(g)) {
+      launch_zfwd_ct<R>(g, wz, A, psi, ldpsi, hpsi, ldh, h.kp[ik].kinetic, scale, nb, tw2, s);
+    } else {
+      k_zfwd<R, true><<<dim3((g.ncol + wz - 1) / wz, nb), block_for(wz), 2 * (size_t)wz * d2 * sizeof(C), s>>>(
+          A, psi, ldpsi, hpsi, ldh, h.kp[ik].kinetic, scale, g.col_start, g.pt_ig, g.pt_col, g.pt_z, g.ncol, d2,
+          div_magic(d2), g.plan[2], tw2, div_magic(wz)); count_launch();
+    }
     mark(tm, 4, s);
     PW_CUDA_TRY(cudaGetLastError());
     return kOk;

@@ -44,7 +44,7 @@ def check(q, cpx, seed=7):
     return ctas
 
 
-@pytest.mark.parametrize("q", [1, 5, 31, 32, 33, 64, 100, 180, 181, 255, 360, 540])
+@pytest.mark.parametrize("q", [1, 5, 31, 32, 33, 64, 80, 100, 180, 181, 255, 360, 540])
 def test_real(q):
     check(q, False)
 
