@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include <mutex>
+#include <set>
 #include <string>
 
 #include "dense_ops.cuh"
@@ -388,11 +389,18 @@ int pick_chol_cluster(int q, int tile) {
   return 1;
 }
 
+// The cluster-size opt-in is a per-device attribute: set once per device,
+// under a lock (solves on several host threads reach here).
 template <typename T> Status chol_attributes() {
-  static std::once_flag once;
-  static cudaError_t err = cudaSuccess;
-  std::call_once(once, [] { err = cudaFuncSetAttribute(k_chol_inv<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1); });
+  static std::mutex mu;
+  static std::set<int> done;
+  int dev = 0;
+  PW_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count(dev)) return kOk;
+  cudaError_t err = cudaFuncSetAttribute(k_chol_inv<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   if (err != cudaSuccess) return fail(kCuda, std::string("chol_inv attributes: ") + cudaGetErrorString(err));
+  done.insert(dev);
   return kOk;
 }
 

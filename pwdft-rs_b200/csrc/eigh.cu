@@ -41,6 +41,7 @@
 #include <cmath>
 #include <cstdint>
 #include <mutex>
+#include <set>
 #include <string>
 
 #include "handle.hpp"
@@ -833,16 +834,21 @@ int pick_cluster(int m, int tsz) {
   return std::max(c0, want);
 }
 
+// The shared-memory and cluster-size opt-ins are per-device attributes: set
+// once per device, under a lock (solves on several host threads reach here).
 template <typename T> Status set_attributes() {
-  static std::once_flag once;
-  static cudaError_t err = cudaSuccess;
-  std::call_once(once, [] {
-    auto kern = k_eigh_cluster<T>;
-    err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)(kSmemLimit - 2 * kMaxM * sizeof(double)));
-    if (err == cudaSuccess) err = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-  });
+  static std::mutex mu;
+  static std::set<int> done;
+  int dev = 0;
+  PW_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count(dev)) return kOk;
+  auto kern = k_eigh_cluster<T>;
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(kSmemLimit - 2 * kMaxM * sizeof(double)));
+  if (err == cudaSuccess) err = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   if (err != cudaSuccess) return fail(kCuda, std::string("eigh_cluster attributes: ") + cudaGetErrorString(err));
+  done.insert(dev);
   return kOk;
 }
 
