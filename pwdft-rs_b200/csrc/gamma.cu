@@ -377,13 +377,6 @@ Status nonlocal_pq_real(Handle& h, const double* u, long ldu, int nb, cudaStream
   return apply_d_real(h, nb, s);
 }
 
-// Blocks narrower than this keep the FP64 projector GEMMs in the mixed form:
-// both forms then stream the projector matrix once per product (the split
-// operands hold 12 bytes per element against 16 in FP64), so the tensor
-// cores gain little while their 128x128 tiles crowd the batch's other
-// solves (measured on the four-cell Si64 batch).
-constexpr int kMixedRealMinBands = 96;
-
 Status apply_h_real(Handle& h, int spin, const double* u, long ldu, int nb, double* hu, long ldh, int precision,
                     cudaStream_t s) {
   if (!h.gam.on) return fail(kState, "apply_h_real: not a Gamma-real handle");
@@ -399,8 +392,10 @@ Status apply_h_real(Handle& h, int spin, const double* u, long ldu, int nb, doub
   if ((r = apply_local_device(h, spin, 0, h.gam_c1, n, npairs, h.gam_c2, n, precision, s)) != kOk) return r;
   k_pack_pairs<<<grid, 256, 0, s>>>(h.gam_c2, n, nb, hu, ldh, g.half_idx, g.half_neg, g.zero, g.nh);
   count_launch();
-  if (h.n_ch > 0 && precision == 1 && nl_mixed_eligible(h) && nb >= kMixedRealMinBands) {
-    // mixed form, wide blocks: both projector products as 3xBF16 tensor-core GEMMs
+  if (h.n_ch > 0 && precision == 1 && nl_mixed_eligible(h)) {
+    // mixed form: both projector products as 3xBF16 tensor-core GEMMs (every
+    // block width: on the four-cell Si64 batch this measured 1 % above
+    // keeping the FP64 GEMMs for blocks narrower than 48 or 96 bands)
     if ((r = nonlocal_mixed_real(h, u, ldu, nb, hu, ldh, s)) != kOk) return r;
   } else if (h.n_ch > 0) {
     if ((r = nonlocal_pq_real(h, u, ldu, nb, s)) != kOk) return r;
