@@ -315,9 +315,20 @@ __global__ void __launch_bounds__(kThreads) k_yxy(cplx<R>* __restrict__ A, const
 // first stage multiplies by V(r), its second stage keeps only the compact
 // x-planes in the y layout.  Twiddles staged in shared memory.  Buffers:
 // P0 (d0 x d1), P1 (d0 x d1), YB/YS inside P1 while the y-lines are live.
-constexpr int kYxyThreads = 512;
+// Threads per block: one round of butterflies for the larger-radix stage of
+// the x transforms (d1 lines x d0 / max(X0, X1) butterflies: 576 for
+// 72 = 8 x 9), at least 512.  Every stage ends at a block barrier, so a
+// stage that needs a second, mostly idle round costs nearly twice its work.
+// Measured on the 72^3 grid (160-band block, FP32): 512 threads 0.49 ms,
+// 576 0.465 ms, 672 (one round for both stages, registers capped at 40 for
+// two blocks per SM) 0.473 ms.
+template <int X0, int X1, int Y0, int Y1> constexpr int yxy_threads() {
+  constexpr int b = Y0 * Y1 * (X0 < X1 ? X0 : X1);
+  constexpr int t = (b + 31) / 32 * 32;
+  return t < 512 ? 512 : (t > 1024 ? 1024 : t);
+}
 template <typename R, int X0, int X1, int Y0, int Y1>
-__global__ void __launch_bounds__(kYxyThreads) k_yxy_ct(cplx<R>* __restrict__ A, const R* __restrict__ vz, int nb,
+__global__ void __launch_bounds__(yxy_threads<X0, X1, Y0, Y1>(), sizeof(R) == 4 ? 2 : 1) k_yxy_ct(cplx<R>* __restrict__ A, const R* __restrict__ vz, int nb,
                                                        int bpc, int Xp, int Yp, int m0, int m1, int d2, unsigned mXp,
                                                        unsigned mYp, unsigned md1, const cplx<R>* __restrict__ twx,
                                                        const cplx<R>* __restrict__ twy) {
@@ -404,7 +415,7 @@ template <typename R> inline bool fused_ok(const GridMaps& g) {
 template <typename R, int X0, int X1>
 void launch_yxy_ct_n(const GridMaps& g, cplx<R>* A, const R* vz, int nb, int bpc, const cplx<R>* twx,
                      const cplx<R>* twy, cudaStream_t s) {
-  k_yxy_ct<R, X0, X1, X0, X1><<<dim3(g.d[2], (nb + bpc - 1) / bpc), kYxyThreads, yxy_ct_smem<R>(g.d[0], g.d[1]), s>>>(
+  k_yxy_ct<R, X0, X1, X0, X1><<<dim3(g.d[2], (nb + bpc - 1) / bpc), yxy_threads<X0, X1, X0, X1>(), yxy_ct_smem<R>(g.d[0], g.d[1]), s>>>(
       A, vz, nb, bpc, g.Xp, g.Yp, g.m[0], g.m[1], g.d[2], div_magic(g.Xp), div_magic(g.Yp), div_magic(g.d[1]), twx,
       twy);
   count_launch();

@@ -80,28 +80,37 @@ __global__ void k_build_a2(const double2* __restrict__ b, int n_pw, int n_ch, lo
 }
 
 // B1[j][k], j < 2 nb, k < k1pad: column j = [hi | lo | hi] of
-// [psi_r; psi_i] (j < nb) or [psi_i; -psi_r] (j >= nb), band j mod nb.
-// One grid row per column j (blockIdx.y), threads along k.
+// [psi_r; psi_i] (j < nb) or [psi_i; -psi_r] (j >= nb), band j mod nb,
+// zero beyond 6 n_pw.  One thread per element (i, band): it reads psi once
+// and writes its twelve entries (three segments of both columns, real and
+// imaginary halves); rounding is symmetric, so the split of -psi_r is the
+// negated split of psi_r.
 __global__ void k_split_psi(const double2* __restrict__ psi, long ldpsi, int n_pw, int nb, long k1pad,
                             __nv_bfloat16* __restrict__ b1) {
-  const int j = blockIdx.y;
-  const int part = j >= nb;
-  const long band = part ? j - nb : j;
-  const long seg_len = 2L * n_pw;
-  const double2* col = psi + band * ldpsi;
-  __nv_bfloat16* out = b1 + (long)j * k1pad;
-  for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < k1pad; k += (long)gridDim.x * blockDim.x) {
-    __nv_bfloat16 o = __float2bfloat16_rn(0.0f);
-    if (k < 3 * seg_len) {
-      const int seg = k >= 2 * seg_len ? 2 : (k >= seg_len ? 1 : 0);
-      const long r = k - seg * seg_len;
-      const double2 z = col[r < n_pw ? r : r - n_pw];
-      const double v = part == 0 ? (r < n_pw ? z.x : z.y) : (r < n_pw ? z.y : -z.x);
-      __nv_bfloat16 hi, lo;
-      split_bf16(v, hi, lo);
-      o = seg == 1 ? lo : hi;
+  const int band = blockIdx.y;
+  const long seg = 2L * n_pw;
+  const long pad = k1pad - 3 * seg;
+  __nv_bfloat16* c0 = b1 + (long)band * k1pad;
+  __nv_bfloat16* c1 = b1 + (long)(nb + band) * k1pad;
+  const __nv_bfloat16 zero = __float2bfloat16_rn(0.0f);
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n_pw; i += (long)gridDim.x * blockDim.x) {
+    const double2 z = psi[band * ldpsi + i];
+    __nv_bfloat16 hx, lx, hy, ly;
+    split_bf16(z.x, hx, lx);
+    split_bf16(z.y, hy, ly);
+#pragma unroll
+    for (int sg = 0; sg < 3; ++sg) {
+      const long b = sg * seg + i;
+      const bool lo = sg == 1;
+      c0[b] = lo ? lx : hx;
+      c0[b + n_pw] = lo ? ly : hy;
+      c1[b] = lo ? ly : hy;
+      c1[b + n_pw] = __hneg(lo ? lx : hx);
     }
-    out[k] = o;
+    for (long q = i; q < pad; q += n_pw) {
+      c0[3 * seg + q] = zero;
+      c1[3 * seg + q] = zero;
+    }
   }
 }
 
@@ -429,7 +438,7 @@ Status nonlocal_mixed(Handle& h, int ik, const double2* psi, long ldpsi, int nb,
   }
   if ((st = ensure_nl_capacity(h, nb)) != kOk) return st;
   const int n2 = 2 * nb;
-  k_split_psi<<<dim3((unsigned)std::min<long>(64, (m.k1pad + 255) / 256), n2), 256, 0, s>>>(psi, ldpsi, h.n_pw, nb,
+  k_split_psi<<<dim3((unsigned)std::min<long>(64, (h.n_pw + 255) / 256), nb), 256, 0, s>>>(psi, ldpsi, h.n_pw, nb,
                                                                                           m.k1pad, m.b1);
   count_launch();
   const long slice_stride = (long)m.m1pad * n2;
