@@ -148,8 +148,8 @@ def max_over_ranks(values, dist, device):
 
 
 def scf_kwargs():
-    from pwgpu.config3 import FP64_SWITCH, SCF_KW
-    kw = dict(SCF_KW)
+    from pwgpu.config3 import FP64_SWITCH, SCF_KW, SOLVER_KW
+    kw = dict(SCF_KW, **SOLVER_KW)
     nb = kw.pop("n_bands")
     return nb, kw, FP64_SWITCH
 

@@ -204,6 +204,11 @@ typedef struct pwgpu_scf_params {
   int32_t fixed_magnetization;   /* 1: tot_magnetization fixes N_up - N_down (one Fermi level per spin) */
   double tot_magnetization;
   int32_t mixing_period;         /* Periodic Pulay: DIIS every period-th step (<= 0: 3) */
+  /* Eigen-residual target of an SCF step: max(diag_tol, min(diag_tol_cap,
+   * diag_tol_per_drho * last density rms change)) eV; <= 0 selects 3 eV per
+   * e/Å^3 and 3e-2 eV. */
+  double diag_tol_per_drho;
+  double diag_tol_cap;
 } pwgpu_scf_params;
 
 /* ScfResult (scf/mod.rs:269-322) scalars. */

@@ -324,6 +324,8 @@ static Status convert_params(const pwgpu_scf_params* p, ScfParams& q) {
   q.diag_extra_bands = p->diag_extra_bands;
   q.precision = p->precision;
   q.fp64_switch = p->fp64_switch;
+  q.diag_tol_per_drho = p->diag_tol_per_drho > 0.0 ? p->diag_tol_per_drho : 3.0;
+  q.diag_tol_cap = p->diag_tol_cap > 0.0 ? p->diag_tol_cap : 3e-2;
   q.verbose = p->verbose;
   q.starting_magnetization = p->starting_magnetization;
   q.fixed_magnetization = p->fixed_magnetization;

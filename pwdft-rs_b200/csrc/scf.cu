@@ -37,8 +37,6 @@ constexpr double kE2 = 14.399645351950548;
 constexpr double kG2Zero = 1e-12;
 constexpr double kRhoFloor = 1e-30;
 constexpr int kRedBlocks = 512;  // partial sums per reduction (fixed order)
-constexpr double kDiagTolCap = 3e-2;     // eV, loosest eigen-residual target of an SCF step
-constexpr double kDiagTolPerDrho = 3.0;  // eV per (e/Å^3) of the last density rms change
 
 // ---------------------------------------------------------------------------
 // deterministic reductions: partials[blockIdx] then one block sums them
@@ -1192,9 +1190,10 @@ Status scf_run(Handle& h, const ScfParams& p, const double* rho_init, ScfResult&
     // eigen-residual target of this step: the density error it leaves is far
     // below the SCF's own delta rho until the last iterations (measured on
     // the 64-atom cell: 0.1 drho capped at 1e-3 eV took 2.8 s, 3 drho capped
-    // at 3e-2 eV 1.4 s, same converged energy within 3e-5 eV)
+    // at 3e-2 eV 1.4 s, same converged energy within 3e-5 eV; the slope and
+    // cap are parameters, since the best pair depends on the system)
     const double tol = p.single_step ? p.diag_tol
-                                     : std::max(p.diag_tol, std::min(kDiagTolCap, kDiagTolPerDrho *
+                                     : std::max(p.diag_tol, std::min(p.diag_tol_cap, p.diag_tol_per_drho *
                                                 (std::isfinite(last_delta) ? last_delta : 1.0)));
     // preconditioner shift: V_eff(G = 0) = mean of V_eff(r)
     double v0[2] = {0.0, 0.0};

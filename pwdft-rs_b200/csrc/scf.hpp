@@ -26,6 +26,8 @@ struct ScfParams {
   int diag_extra_bands = -1;        // < 0: automatic
   int precision = 0;                // 0 FP64, 1 mixed
   double fp64_switch = 1e-6;        // mixed: FP64 H|psi> once delta rho < this
+  double diag_tol_per_drho = 3.0;   // eigen-residual target of an SCF step: eV per (e/Å^3) of delta rho
+  double diag_tol_cap = 3e-2;       // eV, its loosest value
   int verbose = 0;
   // nspin = 2 (driver_spin.rs:125-167): atom average of the per-species
   // starting_magnetization fractions, and the optional fixed total moment

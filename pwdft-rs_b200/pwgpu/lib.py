@@ -91,7 +91,8 @@ class PwgpuScfParams(ct.Structure):
         ("smearing_sigma", ct.c_double), ("diag_tol", ct.c_double), ("diag_max_iter", ct.c_int32),
         ("diag_extra_bands", ct.c_int32), ("precision", ct.c_int32), ("fp64_switch", ct.c_double),
         ("verbose", ct.c_int32), ("starting_magnetization", ct.c_double), ("fixed_magnetization", ct.c_int32),
-        ("tot_magnetization", ct.c_double), ("mixing_period", ct.c_int32),
+        ("tot_magnetization", ct.c_double), ("mixing_period", ct.c_int32), ("diag_tol_per_drho", ct.c_double),
+        ("diag_tol_cap", ct.c_double),
     ]
 
 
@@ -144,13 +145,15 @@ def scf_params(n_bands: int, max_iter: int = 100, conv_threshold: float = 1e-6, 
                smearing: str = "fermi_dirac", sigma: float = 0.01, diag_tol: float = 1e-8, diag_max_iter: int = 60,
                diag_extra_bands: int = -1, precision: int = 0, fp64_switch: float = 1e-6, verbose: bool = False,
                starting_magnetization: float = 0.0, tot_magnetization=None, mixer: str = "anderson",
-               mixing_period: int = 3) -> "PwgpuScfParams":
-    """The pwgpu_scf_params POD (ScfParams fields, reference defaults)."""
+               mixing_period: int = 3, diag_tol_per_drho: float = 0.0, diag_tol_cap: float = 0.0) -> "PwgpuScfParams":
+    """The pwgpu_scf_params POD (ScfParams fields, reference defaults; the eigen-residual
+    schedule of the SCF steps at 0 selects 3 eV per e/Å^3 of delta rho, capped at 3e-2 eV)."""
     return PwgpuScfParams(n_bands, max_iter, conv_threshold, energy_threshold, mixing_beta, mixing_ndim,
                           mixing_mode(mixer, kerker), q_tf, SMEARING[smearing], sigma, diag_tol, diag_max_iter,
                           diag_extra_bands, precision, fp64_switch, 1 if verbose else 0, starting_magnetization,
                           0 if tot_magnetization is None else 1,
-                          0.0 if tot_magnetization is None else tot_magnetization, mixing_period)
+                          0.0 if tot_magnetization is None else tot_magnetization, mixing_period,
+                          diag_tol_per_drho, diag_tol_cap)
 
 
 _lib = None
@@ -414,13 +417,14 @@ class PwGpu:
                 diag_max_iter: int = 60, diag_extra_bands: int = -1, precision: int = PRECISION_FP64,
                 fp64_switch: float = 1e-6, verbose: bool = False, raise_on_unconverged: bool = True,
                 starting_magnetization: float = 0.0, tot_magnetization=None, mixer: str = "anderson",
-                mixing_period: int = 3):
+                mixing_period: int = 3, diag_tol_per_drho: float = 0.0, diag_tol_cap: float = 0.0):
         """run_scf_unpolarized / run_scf_spin on the device; returns (result dict, eigenvalues
         [nspin * n_k, n_bands] (spin up k-points first), rho_r [nspin * N] (up then down),
         total rho_g in basis order [n_pw])."""
         p = scf_params(n_bands, max_iter, conv_threshold, energy_threshold, mixing_beta, mixing_ndim, kerker, q_tf,
                        smearing, sigma, diag_tol, diag_max_iter, diag_extra_bands, precision, fp64_switch, verbose,
-                       starting_magnetization, tot_magnetization, mixer, mixing_period)
+                       starting_magnetization, tot_magnetization, mixer, mixing_period, diag_tol_per_drho,
+                       diag_tol_cap)
         rho0 = np.ascontiguousarray(rho_init, dtype=np.float64)
         res = PwgpuScfResult()
         ns = self.sys.nspin

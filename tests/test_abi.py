@@ -61,3 +61,34 @@ def test_header_compiles_as_c99_and_cxx(tmp_path):
                     str(src)], check=True)
     subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", "-I", inc, "-x", "c++", str(src)],
                    check=True)
+
+
+def test_ctypes_structs_match_header_layout(tmp_path):
+    """Every field of the ctypes mirrors of the header's PODs sits at the
+    offset the C compiler gives it, and the sizes agree (a field appended to
+    the header without its mirror shows up here)."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        import pytest
+        pytest.skip("gcc not available")
+    mirrors = {"pwgpu_system": L.PwgpuSystem, "pwgpu_options": L.PwgpuOptions,
+               "pwgpu_scf_params": L.PwgpuScfParams, "pwgpu_scf_result": L.PwgpuScfResult,
+               "pwgpu_server_options": L.PwgpuServerOptions, "pwgpu_job_info": L.PwgpuJobInfo,
+               "pwgpu_server_stats": L.PwgpuServerStats}
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "pwgpu.h"', 'int main(void) {']
+    for cname, py in mirrors.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ['  return 0;', '}']
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, py in mirrors.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)

@@ -31,7 +31,7 @@ import pytest
 
 from conftest import GOLDEN
 from oracle import pwdft_oracle as O
-from pwgpu.config3 import FP64_SWITCH, SCF_KW, SI8_SCF_KW, config3_si8_system, config3_system
+from pwgpu.config3 import FP64_SWITCH, SCF_KW, SI8_SCF_KW, SOLVER_KW, config3_si8_system, config3_system
 from pwgpu.lib import PRECISION_FP64, PRECISION_MIXED, PwGpu
 
 pytestmark = pytest.mark.gpu
@@ -57,12 +57,17 @@ def run(s, kw, precision, gamma_complex=False, **extra):
     return res, ev, rho, psi
 
 
+# the library's default eigen-residual schedule and the one the Si64 bench uses
+SCHEDULES = {"default": {}, "si64": SOLVER_KW}
+
+
+@pytest.mark.parametrize("schedule", sorted(SCHEDULES))
 @pytest.mark.parametrize("gamma_complex", [False, True])
-def test_si8_fp64_matches_oracle(si_pp, gamma_complex):
+def test_si8_fp64_matches_oracle(si_pp, gamma_complex, schedule):
     ref = fixture()
     s = config3_si8_system(si_pp)
     assert (s.n_pw, list(s.dims)) == (ref["n_pw"], ref["dims"])
-    res, ev, _, _ = run(s, SI8_SCF_KW, PRECISION_FP64, gamma_complex, diag_tol=1e-10)
+    res, ev, _, _ = run(s, SI8_SCF_KW, PRECISION_FP64, gamma_complex, diag_tol=1e-10, **SCHEDULES[schedule])
     assert res["converged"] == 1
     assert abs(res["total_energy"] - ref["total_energy"]) < E_TOL_FP64
     assert abs(res["harris_foulkes_energy"] - ref["harris_foulkes_energy"]) < E_TOL_FP64
@@ -72,14 +77,27 @@ def test_si8_fp64_matches_oracle(si_pp, gamma_complex):
         assert abs(res[k] - ref["components"][k]) < 1e-6, k
 
 
-def test_si8_mixed_matches_oracle(si_pp):
+@pytest.mark.parametrize("schedule", sorted(SCHEDULES))
+def test_si8_mixed_matches_oracle(si_pp, schedule):
     ref = fixture()
     s = config3_si8_system(si_pp)
-    kw = dict(SCF_KW, n_bands=SI8_SCF_KW["n_bands"])
+    kw = dict(SCF_KW, n_bands=SI8_SCF_KW["n_bands"], **SCHEDULES[schedule])
     res, ev, _, _ = run(s, kw, PRECISION_MIXED)
     assert res["converged"] == 1
     assert abs(res["total_energy"] - ref["total_energy"]) / ref["n_atoms"] < E_TOL_MIXED_ATOM
     assert np.max(np.abs(ev[0] - np.array(ref["eigenvalues"][0]))) < EV_TOL_MIXED
+
+
+def test_schedule_reaches_the_eigensolver(si_pp):
+    """pwgpu_scf_params.diag_tol_per_drho / diag_tol_cap change the work of
+    the solve (band applications) but not its converged energy."""
+    s = config3_si8_system(si_pp)
+    kw = dict(SCF_KW, n_bands=SI8_SCF_KW["n_bands"])
+    r0, _, _, _ = run(s, kw, PRECISION_FP64)
+    r1, _, _, _ = run(s, dict(kw, diag_tol_per_drho=20.0, diag_tol_cap=0.2), PRECISION_FP64)
+    assert r0["converged"] == 1 and r1["converged"] == 1
+    assert r0["h_applications"] != r1["h_applications"]
+    assert abs(r0["total_energy"] - r1["total_energy"]) / 8 < E_TOL_MIXED_ATOM
 
 
 def _si64_state(s):
