@@ -92,3 +92,100 @@ def test_ctypes_structs_match_header_layout(tmp_path):
         assert got[(cname, "size")] == ctypes.sizeof(py), cname
         for fname, _ in py._fields_:
             assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
+
+
+_C_TO_RUST = {"int32_t": "i32", "int64_t": "i64", "double": "f64", "char": "c_char", "void": "c_void",
+              "pwgpu_status": "i32"}
+
+
+def _rust_type(ctype, array=None):
+    """Rust spelling of a C type of the header: `const T*` -> `*const T`,
+    `T**` -> `*mut *mut T`, `const char**` -> `*mut *const c_char`."""
+    ctype = ctype.strip()
+    stars = ctype.count("*")
+    base = ctype.replace("*", " ").split()
+    const = "const" in base
+    base = [b for b in base if b != "const"]
+    assert len(base) == 1, ctype
+    t = _C_TO_RUST.get(base[0], base[0])
+    for i in range(stars):
+        t = ("*const " if (i == 0 and const) else "*mut ") + t
+    if array:
+        t = f"[{t}; {array}]"
+    return t.replace(" ", "")
+
+
+def _header_text():
+    text = open(os.path.join(ROOT, "include", "pwgpu.h")).read()
+    return re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+
+
+def _header_struct(name):
+    m = re.search(r"typedef struct " + name + r"\s*\{(.*?)\}\s*" + name + ";", _header_text(), flags=re.S)
+    assert m, name
+    fields = []
+    for decl in m.group(1).split(";"):
+        decl = decl.strip()
+        if not decl:
+            continue
+        first = re.match(r"((?:const\s+)?\w+\s*\**)\s*(.*)", decl, flags=re.S)
+        ctype, rest = first.group(1), first.group(2)
+        for d in rest.split(","):
+            d = d.strip()
+            stars = len(d) - len(d.lstrip("*"))
+            d = d.lstrip("*").strip()
+            arr = re.match(r"(\w+)\[(\d+)\]", d)
+            if arr:
+                fields.append((arr.group(1), _rust_type(ctype + "*" * stars, arr.group(2))))
+            else:
+                fields.append((d, _rust_type(ctype + "*" * stars)))
+    return fields
+
+
+def _header_function(name):
+    m = re.search(r"([\w\s\*]+?)\b" + name + r"\s*\((.*?)\)\s*;", _header_text(), flags=re.S)
+    assert m, name
+    args = []
+    for a in m.group(2).split(","):
+        a = " ".join(a.split())
+        if a in ("", "void"):
+            continue
+        t = re.match(r"(.*?[\s\*])(\w+)$", a)
+        args.append(_rust_type(t.group(1)))
+    return _rust_type(m.group(1).split("\n")[-1]), args
+
+
+def _rust_block():
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    m = re.search(r"```rust\n(.*?)```", text, flags=re.S)
+    return re.sub(r"//[^\n]*", "", m.group(1))
+
+
+def test_rust_binding_in_integration_matches_header():
+    """The Rust FFI declarations a maintainer would add are
+    the header's: every #[repr(C)] struct field by field (name and type, in
+    order) and every extern fn argument by argument."""
+    rust = _rust_block()
+    structs = re.findall(r"#\[repr\(C\)\]\s*pub struct (\w+)\s*\{(.*?)\}", rust, flags=re.S)
+    checked = set()
+    for name, body in structs:
+        if "_private" in body:
+            assert re.search(r"typedef struct " + name + " " + name + ";", _header_text()), name
+            continue
+        got = []
+        for f in body.split(","):
+            f = f.strip()
+            if f:
+                fm = re.match(r"pub (\w+):\s*(.+)$", f, flags=re.S)
+                got.append((fm.group(1), fm.group(2).replace(" ", "").replace("\n", "")))
+        assert got == _header_struct(name), name
+        checked.add(name)
+    assert {"pwgpu_system", "pwgpu_options", "pwgpu_scf_params", "pwgpu_scf_result"} <= checked
+    fns = re.findall(r"pub fn (\w+)\((.*?)\)\s*->\s*([^;]+);", rust, flags=re.S)
+    assert len(fns) >= 10
+    for name, args, ret in fns:
+        want_ret, want_args = _header_function(name)
+        got_args = [re.match(r"\s*\w+:\s*(.+)$", a, flags=re.S).group(1).replace(" ", "").replace("\n", "")
+                    for a in args.split(",") if a.strip()]
+        assert got_args == want_args, name
+        assert ret.replace(" ", "") == want_ret, name
