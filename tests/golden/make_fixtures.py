@@ -10,7 +10,9 @@ Copied verbatim (data files, not source):
   * pseudopotentials/nc/lda/{Al,As,Cl,Cu,Fe,Ga,Mg,Na,O}.upf (heavy-atom pins)
                                                  -> tests/golden/upf/
   * data/csv/{vloc_g_si,beta_q_si,dij_si,rho_core_g,vgcmp_phase4}_reference.csv,
-    data/csv/vgch_{beta_l,vloc}_heavy.csv        -> tests/golden/csv/
+    data/csv/vgch_{beta_l,vloc}_heavy.csv,
+    data/csv/vgch_sad_heavy{,_samples}.csv (SAD start densities of seven cells)
+                                                 -> tests/golden/csv/
   * data/qe/c_rho_qe.bin (QE's converged C-diamond density, VGCH2BIN bundle)
                                                  -> tests/golden/qe/
 The SCF goldens (E_total, E_F) are constants in tests/test_oracle_pins.py
@@ -23,7 +25,8 @@ import sys
 
 UPFS = ["Si.upf", "Si_hgh.upf", "C.upf"] + [f"{e}.upf" for e in ("Al", "As", "Cl", "Cu", "Fe", "Ga", "Mg", "Na", "O")]
 CSVS = ["vloc_g_si_reference.csv", "beta_q_si_reference.csv", "dij_si_reference.csv",
-        "rho_core_g_reference.csv", "vgcmp_phase4_reference.csv", "vgch_beta_l_heavy.csv", "vgch_vloc_heavy.csv"]
+        "rho_core_g_reference.csv", "vgcmp_phase4_reference.csv", "vgch_beta_l_heavy.csv", "vgch_vloc_heavy.csv",
+        "vgch_sad_heavy.csv", "vgch_sad_heavy_samples.csv"]
 
 
 def main(ref_root: str):
