@@ -15,6 +15,10 @@ Copied verbatim (data files, not source):
                                                  -> tests/golden/csv/
   * data/qe/c_rho_qe.bin (QE's converged C-diamond density, VGCH2BIN bundle)
                                                  -> tests/golden/qe/
+  * data/qe/{cu_fcc,fe_bcc_fm,nacl,c_diamond,mgo}_scf.out (QE's converged
+    bands, weights and Fermi levels) and data/csv/vgch2c_fermi_reference.csv
+    (the Fermi levels the reference's bisection finds on them)
+                                                 -> tests/golden/qe/, tests/golden/csv/
 The SCF goldens (E_total, E_F) are constants in tests/test_oracle_pins.py
 with their reference file:line.
 """
@@ -26,7 +30,8 @@ import sys
 UPFS = ["Si.upf", "Si_hgh.upf", "C.upf"] + [f"{e}.upf" for e in ("Al", "As", "Cl", "Cu", "Fe", "Ga", "Mg", "Na", "O")]
 CSVS = ["vloc_g_si_reference.csv", "beta_q_si_reference.csv", "dij_si_reference.csv",
         "rho_core_g_reference.csv", "vgcmp_phase4_reference.csv", "vgch_beta_l_heavy.csv", "vgch_vloc_heavy.csv",
-        "vgch_sad_heavy.csv", "vgch_sad_heavy_samples.csv"]
+        "vgch_sad_heavy.csv", "vgch_sad_heavy_samples.csv", "vgch2c_fermi_reference.csv"]
+QE_OUTS = [f"{n}_scf.out" for n in ("cu_fcc", "fe_bcc_fm", "nacl", "c_diamond", "mgo")]
 
 
 def main(ref_root: str):
@@ -38,7 +43,8 @@ def main(ref_root: str):
     for f in CSVS:
         shutil.copyfile(os.path.join(ref_root, "data", "csv", f), os.path.join(here, "csv", f))
     os.makedirs(os.path.join(here, "qe"), exist_ok=True)
-    shutil.copyfile(os.path.join(ref_root, "data", "qe", "c_rho_qe.bin"), os.path.join(here, "qe", "c_rho_qe.bin"))
+    for f in ["c_rho_qe.bin"] + QE_OUTS:
+        shutil.copyfile(os.path.join(ref_root, "data", "qe", f), os.path.join(here, "qe", f))
 
 
 if __name__ == "__main__":
