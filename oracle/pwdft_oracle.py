@@ -385,7 +385,7 @@ def density_diff(a, b, omega):
 
 
 # ---------------------------------------------------------------------------
-# Mixing (mixing/anderson.rs:170-266, kerker.rs:18-49, linalg.rs:124-152)
+# Mixing (mixing/anderson.rs:170-266, kerker.rs:18-49, linalg.rs:24-50)
 # ---------------------------------------------------------------------------
 
 def auto_q_tf_squared(n_el, omega):
@@ -498,7 +498,7 @@ def make_mixer(kind, beta, ndim, dims, kerker_weights=None, period=3):
 
 
 def solve_small(a, b):
-    """Partial-pivot LU with the 1e-15 singular-pivot fallback (linalg.rs:124-152)."""
+    """Partial-pivot LU with the 1e-15 singular-pivot fallback (linalg.rs:24-50)."""
     import scipy.linalg as sl
     n = b.size
     if n == 0:

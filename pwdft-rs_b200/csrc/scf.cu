@@ -768,7 +768,7 @@ Status occupations_host(int n_sets, int nb, const double* ev, const double* w, d
   return kOk;
 }
 
-// partial-pivot LU solve with the 1e-15 singular-pivot fallback (linalg.rs:124-152)
+// partial-pivot LU solve with the 1e-15 singular-pivot fallback (linalg.rs:24-50)
 static std::vector<double> solve_small(std::vector<double> a, std::vector<double> b, int n) {
   std::vector<int> piv(n);
   for (int i = 0; i < n; ++i) piv[i] = i;

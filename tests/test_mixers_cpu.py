@@ -9,7 +9,7 @@ the GPU:
   and without Kerker, convergence on a fixed-point problem, history
   trimming);
 * scf/mixing/kerker.rs:56-100 (q_TF range, real preconditioned residual,
-  high-G pass-through) and scf/mixing/linalg.rs:59-66 (the 2x2 solve).
+  high-G pass-through) and scf/mixing/linalg.rs:59-64 (the 2x2 solve).
 
 As in the reference, the "|G|^2" arrays of these tests are synthetic values
 indexed by grid point, and the Kerker weights are P = G^2 / (G^2 + q_TF^2)
@@ -152,6 +152,6 @@ def test_solve_small_two_by_two():
 
 
 def test_solve_small_singular_fallback():
-    """linalg.rs:124-152: a pivot below 1e-15 returns the uniform 1/(n+1)."""
+    """linalg.rs:24-50: a pivot below 1e-15 returns the uniform 1/(n+1)."""
     x = O.solve_small(np.zeros((3, 3)), np.ones(3))
     assert np.allclose(x, 0.25)

@@ -1,5 +1,5 @@
 """Occupations through the library's host code (pwgpu_occupations; no GPU
-work): the reference's smearing unit tests (scf/smearing.rs:268-465) as
+work): the reference's smearing unit tests (scf/smearing.rs:268-461) as
 known answers, and E_F, occupations and TS against the oracle's
 restatement (smearing.rs:38-252) on seeded spectra of several (spin, k)
 sets, every scheme."""

@@ -336,7 +336,7 @@ def test_beta_form_factor_at_q_zero(si_pp):
 
 
 def test_local_potential_symmetry_at_gamma(si_pp):
-    """Si diamond, 204.09 eV (tests/nonlocal_symmetry.rs:157-372): |V_loc(G)|
+    """Si diamond, 204.09 eV (tests/nonlocal_symmetry.rs:157-370): |V_loc(G)|
     with its structure factor is constant over each |G| shell of the basis
     (1e-4), and T + V_loc(G - G') from the FFT-grid lookup carries the
     triply degenerate bands 3-5 at Gamma (spread < 1e-3 eV)."""
@@ -410,7 +410,7 @@ def test_sad_start_density_properties(si_pp):
     """The SAD start density of Si (100 eV) integrates to 8 electrons
     (1e-7), is non-negative, and on a 16^3 grid takes the same value at the
     fractional grid points (1,0,0), (0,1,0) and (0,0,1) (1e-10)
-    (scf/initial_density.rs:226-280)."""
+    (scf/initial_density.rs:226-275)."""
     cr = diamond_primitive("Si", 5.431)
     s = build_system(cr, {"Si": si_pp}, 100.0, gamma_only(), SymmetryInfo.identity_only())
     rho = s.rho_init_r
@@ -433,7 +433,7 @@ def test_hartree_and_density_diff_units():
 
 
 def test_simpson_rule_units():
-    """numerics.rs:62-170 on the host Simpson rule: exact for x^3 on 101
+    """numerics.rs:62-163 on the host Simpson rule: exact for x^3 on 101
     points and x^2 on 51 points (1e-12), within 1e-4 on an even 50-point
     mesh, and sqrt(pi)/2 for exp(-r^2) on [0, 5]."""
     from pwgpu.upf import simpson

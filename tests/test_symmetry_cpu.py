@@ -99,7 +99,7 @@ def test_monkhorst_pack_meshes():
 
 
 def test_basis_properties():
-    """basis.rs:122-185 at 200 eV: 259 plane waves, G = 0 present, every
+    """basis.rs:122-180 at 200 eV: 259 plane waves, G = 0 present, every
     kinetic energy within the cutoff, Miller indices unique."""
     from pwgpu.consts import HBAR2_OVER_2M
     from pwgpu.crystal import BasisSet
