@@ -132,13 +132,14 @@ def test_si64_fp64_iteration_is_the_oracles(si_pp):
 
 
 def test_si64_mixed_form_against_oracle(si_pp):
-    """The benchmarked mixed solve (its own thresholds) against the oracle's
-    energy and eigenvalues at the FP64 fixed point."""
+    """The benchmarked mixed solve (its own thresholds and eigen-residual
+    schedule) against the oracle's energy and eigenvalues at the FP64 fixed
+    point."""
     s = config3_system(si_pp)
     _, _, r1, ev1, _, rho_in1, psi = _si64_state(s)
     chk = O.fixed_point_check(s, rho_in1, psi, SCF_KW["smearing"], SCF_KW["sigma"])
     assert abs(chk["total_energy"] - r1["total_energy"]) < E_TOL_FP64
-    kw = dict(SCF_KW)
+    kw = dict(SCF_KW, **SOLVER_KW)
     nb = kw.pop("n_bands")
     with PwGpu(s) as dev:
         rm, evm, _, _ = dev.scf_run(s.rho_init_r, nb, precision=PRECISION_MIXED, fp64_switch=FP64_SWITCH, **kw)
