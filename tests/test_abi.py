@@ -189,3 +189,59 @@ def test_rust_binding_in_integration_matches_header():
                     for a in args.split(",") if a.strip()]
         assert got_args == want_args, name
         assert ret.replace(" ", "") == want_ret, name
+
+
+def _ctypes_argtypes(name):
+    """ctypes argument types of a header declaration: pointers as void*,
+    int32_t / pwgpu_status as int32, int64_t, double."""
+    _, args = _header_function(name)
+    out = []
+    for a in args:
+        if a.startswith("*"):
+            out.append(ctypes.c_void_p)
+        else:
+            out.append({"i32": ctypes.c_int32, "i64": ctypes.c_int64, "f64": ctypes.c_double}[a])
+    return out
+
+
+_NULL_SWEEP = r"""
+import ctypes, sys
+sys.path[:0] = sys.argv[1:3]
+import test_abi as T
+from pwgpu import lib as L
+lib = ctypes.CDLL(L.LIB_PATH)
+lib.pwgpu_last_error.restype = ctypes.c_char_p
+for name in T.declared_functions():
+    if name in ("pwgpu_version", "pwgpu_last_error"):
+        continue
+    f = getattr(lib, name)
+    f.argtypes = T._ctypes_argtypes(name)
+    f.restype = ctypes.c_int32
+    print(name, f(*[None if t is ctypes.c_void_p else 0 for t in f.argtypes]),
+          (lib.pwgpu_last_error() or b"").decode(errors="replace").replace(" ", "_") or "-", flush=True)
+"""
+
+
+def test_every_entry_point_refuses_null_arguments(tmp_path):
+    """No entry point dereferences a NULL handle, server or array: called
+    with every pointer NULL and every size zero, each returns
+    PWGPU_E_INVALID with a message, and the two destroy calls accept NULL
+    (a no-op, as free(NULL)); the process survives the whole sweep. Runs in
+    a child process, so a crash fails this test instead of the suite."""
+    import subprocess
+    import sys
+    script = tmp_path / "null_sweep.py"
+    script.write_text(_NULL_SWEEP)
+    tests_dir = os.path.join(ROOT, "tests")
+    r = subprocess.run([sys.executable, str(script), tests_dir, os.path.join(ROOT, "pwdft-rs_b200")],
+                       capture_output=True, text=True, timeout=300, cwd=tests_dir)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    got = {l.split()[0]: (int(l.split()[1]), l.split()[2]) for l in r.stdout.splitlines() if l.startswith("pwgpu_")}
+    expected = [n for n in declared_functions() if n not in ("pwgpu_version", "pwgpu_last_error")]
+    assert sorted(got) == sorted(expected)
+    for name, (rc, msg) in got.items():
+        if name in ("pwgpu_destroy", "pwgpu_server_destroy"):
+            assert rc == 0, name
+        else:
+            assert rc == -1, (name, rc)  # PWGPU_E_INVALID
+            assert msg != "-", name
