@@ -143,3 +143,77 @@ def test_spin_and_symmetry_switches(si_pp):
     d3 = parse_deck(si2_deck("basis:\n  ecutwfc: 100.0\n"))
     s3, kw3 = deck_system(d3, {"Si": si_pp})
     assert len(s2.kpoints) >= len(s3.kpoints) and kw3["n_bands"] == min(s3.n_pw, 20)
+
+
+CUBE = "system:\n  lattice: [[1,0,0],[0,1,0],[0,0,1]]\nkpoints:\n  type: monkhorst_pack\n  grid: [2, 2, 2]\n"
+
+
+@pytest.mark.parametrize("field", ["nspin: 2", "mixing_beta: 0.25"])
+def test_pre_rename_electrons_fields_rejected_by_name(field):
+    """settings.rs:854-897: `electrons.nspin` and `electrons.mixing_beta`
+    (moved to `spin_polarized` and `scf.*`) are parse errors naming the field."""
+    with pytest.raises(DeckError) as e:
+        parse_deck(CUBE + "electrons:\n  " + field + "\n")
+    assert e.value.kind == "parse" and field.split(":")[0] in str(e.value)
+
+
+@pytest.mark.parametrize("mode,mixer,kerker", [
+    ("plain", "anderson", False), ("kerker", "anderson", True), ("broyden", "broyden", False),
+    ("broyden_kerker", "broyden", True), ("periodic_pulay", "periodic_pulay", False),
+    ("periodic_pulay_kerker", "periodic_pulay", True)])
+@pytest.mark.parametrize("period", [None, 5])
+def test_mixing_modes_convert_to_the_mixer(si_pp, mode, mixer, kerker, period):
+    """settings.rs:1078-1175, 1389-1418: every MixingModeType parses and
+    converts to its mixer (Kerker with q_TF estimated at run time); Periodic
+    Pulay takes scf.pulay_period, default 3."""
+    extra = f"basis:\n  ecutwfc: 100.0\nscf:\n  mixing_mode: {mode}\n"
+    if period is not None:
+        extra += f"  pulay_period: {period}\n"
+    d = parse_deck(si2_deck(extra))
+    assert d.scf["mixing_mode"] == mode
+    _, kw = deck_system(d, {"Si": si_pp})
+    assert (kw["mixer"], kw["kerker"]) == (mixer, kerker)
+    assert kw["mixing_period"] == (3 if period is None else period)
+
+
+def test_fixed_occupations_with_fixed_smearing():
+    """settings.rs:1468-1483."""
+    d = parse_deck(CUBE + "scf:\n  smearing: fixed\nelectrons:\n  occupations: fixed\n")
+    assert d.scf["smearing"] == "fixed" and d.electrons["occupations"] == "fixed" and d.atoms == []
+
+
+@pytest.mark.parametrize("smearing", ["fermi_dirac", "gaussian", "methfessel_paxton", "cold", "fixed"])
+def test_smearing_names_parse(smearing):
+    """settings.rs:1031-1044, 1419-1434."""
+    assert parse_deck(CUBE + f"scf:\n  smearing: {smearing}\n").scf["smearing"] == smearing
+
+
+@pytest.mark.parametrize("verbosity", ["low", "normal", "high"])
+def test_verbosity_names_parse(verbosity):
+    """settings.rs:428-433, 1060-1067."""
+    assert parse_deck(CUBE + f"output:\n  verbosity: {verbosity}\n").output["verbosity"] == verbosity
+
+
+def test_to_crystal_structure():
+    """settings.rs:968-981: lattice rows as given (Å), fractional positions."""
+    from pwgpu.deck import to_crystal
+    d = parse_deck(si2_deck(a_ang=5.431))
+    c = to_crystal(d)
+    assert [a.symbol for a in c.atoms] == ["Si", "Si"] and tuple(c.atoms[1].frac) == (0.25, 0.25, 0.25)
+    assert abs(c.lattice.a[0]) < 1e-12 and abs(c.lattice.a[1] - 2.7155) < 1e-12
+
+
+def test_deck_contract_follows_the_reference_code_not_its_stale_tests():
+    """Two of the reference's settings tests expect what its own types
+    refuse: settings.rs:829 parses a deck with a `pseudopotentials:` block,
+    but InputSettings (settings.rs:27-68) denies unknown fields and has no
+    such field; settings.rs:1486 expects an unknown element symbol to parse
+    and fail in to_crystal, but AtomInput.symbol is the Element enum
+    (settings.rs:89-92), so the symbol fails at parse time. The deck here
+    follows the types: both are parse errors naming the offending value."""
+    with pytest.raises(DeckError) as e:
+        parse_deck(si2_deck('pseudopotentials:\n  Si: "../pseudopotentials/nc/lda/Si.upf"\n'))
+    assert e.value.kind == "parse" and "pseudopotentials" in str(e.value)
+    with pytest.raises(DeckError) as e:
+        parse_deck(si2_deck().replace("symbol: Si, position: [0.0, 0.0, 0.0]", "symbol: Xz, position: [0.0, 0.0, 0.0]"))
+    assert e.value.kind == "parse" and "Xz" in str(e.value)
