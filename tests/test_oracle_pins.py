@@ -471,3 +471,43 @@ def test_spin_xc_consistency_si(si_pp):
     assert r.n_iterations < 60
     assert abs(r.harris_foulkes_energy - r.total_energy) < 1e-5
     assert abs(r.magnetization) < 0.05
+
+
+def _vloc_bare_coulomb(pp, g, omega):
+    """V_loc(|G|) with the bare Coulomb tail -Z e^2/r subtracted instead of
+    the erf form (the comparison form of vloc_erf_consistency.rs:52-86):
+    (4 pi / Omega) int r^2 [V(r) + Z e^2 / r] j0(G r) dr - 4 pi Z e^2 / (Omega G^2)."""
+    from pwgpu.consts import E2_COULOMB
+    from pwgpu.upf import simpson
+    r = pp.r
+    vs = pp.v_local + pp.z_valence * E2_COULOMB / np.maximum(r, 1e-20)
+    if g < 1e-12:
+        return 4.0 * math.pi / omega * simpson(r * r * vs, pp.rab)
+    gr = g * r
+    j0 = np.where(gr < 1e-10, 1.0 - gr * gr / 6.0, np.sin(gr) / np.where(gr == 0.0, 1.0, gr))
+    return (4.0 * math.pi / omega * simpson(r * r * vs * j0, pp.rab)
+            - 4.0 * math.pi * pp.z_valence * E2_COULOMB / (omega * g * g))
+
+
+def test_vloc_erf_form_equals_bare_coulomb_form(si_pp):
+    """vloc_erf_consistency.rs:118-200: the erf-subtracted V_loc(G) of the
+    host setup (which the device setup matches to 1e-12) equals the
+    bare-Coulomb form on the first 20 |G| shells of Si (a = 5.431 Å,
+    Omega = 40 Å^3) to 1e-6 eV, and at G = 0."""
+    from pwgpu.crystal import fcc_primitive
+    lat = fcc_primitive(5.431)
+    b = np.array([lat.reciprocal().a, lat.reciprocal().b, lat.reciprocal().c])
+    n = np.arange(-6, 7)
+    m = np.stack(np.meshgrid(n, n, n, indexing="ij"), -1).reshape(-1, 3)
+    g = np.sort(np.linalg.norm(m @ b, axis=1))
+    shells = []
+    for x in g[g > 1e-8]:
+        if not shells or x - shells[-1] > 1e-6:
+            shells.append(x)
+        if len(shells) == 20:
+            break
+    omega = 40.0
+    got = v_local_of_g(si_pp, np.array([0.0] + shells), omega)
+    want = np.array([_vloc_bare_coulomb(si_pp, x, omega) for x in [0.0] + shells])
+    assert len(shells) == 20
+    assert np.max(np.abs(got - want)) < 1e-6, np.max(np.abs(got - want))
