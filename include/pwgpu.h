@@ -47,6 +47,7 @@ typedef int32_t pwgpu_status;
 #define PWGPU_E_TIMEOUT (-5)          /* a bounded device wait ran out */
 #define PWGPU_E_NOT_IMPLEMENTED (-6)  /* PwdftError::NotImplemented */
 #define PWGPU_E_STATE (-7)            /* call order violated (e.g. no V_eff set) */
+#define PWGPU_E_PARSE (-8)            /* PwdftError::Parse (malformed pseudopotential file) */
 
 #define PWGPU_PRECISION_FP64 0  /* plain: every H|psi> stage in FP64 */
 #define PWGPU_PRECISION_MIXED 1 /* FFTs and V_eff product in FP32 */
@@ -319,6 +320,50 @@ pwgpu_status pwgpu_potentials(pwgpu_handle* h, const double* rho_r, double* veff
 pwgpu_status pwgpu_mix(pwgpu_handle* h, int32_t channel, int32_t mode, const double* rho_in, const double* rho_out,
                        double* rho_next, double beta, int32_t ndim, int32_t period, double q_tf);
 pwgpu_status pwgpu_mix_reset(pwgpu_handle* h);
+
+/* UPF v2 norm-conserving pseudopotential, read on the host by the library:
+ * parse_upf_body (pseudopotential/upf/parse.rs:20-135) with the scanning of
+ * upf/xml.rs -- each header attribute and data block taken from its first
+ * textual occurrence, PP_RHOATOM zero when absent or unreadable, the NLCC
+ * core charge read when core_correction="T" (zero when the block is
+ * unreadable, empty without it).  Arrays come out in the units of
+ * pwgpu_system's radial fields: r and rab in Å, V_loc in eV, r·beta(r)
+ * divided by sqrt(Å per bohr), D_ij in eV (n_proj x n_proj, row-major),
+ * PP_RHOATOM per Å, core charge in e/Å^3.  A malformed file returns
+ * PWGPU_E_PARSE with the reason in pwgpu_last_error(). */
+typedef struct pwgpu_upf pwgpu_upf;
+
+typedef struct pwgpu_upf_info {
+  char element[8];          /* element symbol, NUL-terminated */
+  double z_valence;
+  int32_t l_max;
+  int32_t n_proj;
+  int32_t mesh;             /* radial mesh points */
+  int32_t has_nlcc;         /* 1: PWGPU_UPF_NLCC holds mesh values (else none) */
+  int32_t has_rho_atom;     /* 1: PP_RHOATOM has a nonzero value */
+} pwgpu_upf_info;
+
+#define PWGPU_UPF_R 0        /* mesh */
+#define PWGPU_UPF_RAB 1      /* mesh */
+#define PWGPU_UPF_LOCAL 2    /* mesh */
+#define PWGPU_UPF_BETA 3     /* mesh, projector `index` (0-based) */
+#define PWGPU_UPF_DIJ 4      /* n_proj * n_proj */
+#define PWGPU_UPF_RHOATOM 5  /* mesh */
+#define PWGPU_UPF_NLCC 6     /* mesh when has_nlcc, else 0 */
+
+/* Parse len bytes of UPF text (UpfPseudoPotential::load's body,
+ * upf/mod.rs:98-135); *out is freed with pwgpu_upf_free. */
+pwgpu_status pwgpu_upf_parse(const char* text, int64_t len, pwgpu_upf** out);
+/* Read and parse a UPF file (UpfPseudoPotential::load_from_path, upf/mod.rs:98). */
+pwgpu_status pwgpu_upf_load(const char* path, pwgpu_upf** out);
+pwgpu_status pwgpu_upf_get_info(const pwgpu_upf* u, pwgpu_upf_info* info);
+/* Copy one array (PWGPU_UPF_*) into out, which holds capacity doubles
+ * (PWGPU_E_INVALID when it is too small). */
+pwgpu_status pwgpu_upf_get_array(const pwgpu_upf* u, int32_t which, int32_t index, double* out, int64_t capacity);
+/* Angular momentum of each projector (n_proj ints). */
+pwgpu_status pwgpu_upf_get_beta_l(const pwgpu_upf* u, int32_t* l);
+/* Free a parsed pseudopotential (NULL is a no-op). */
+pwgpu_status pwgpu_upf_free(pwgpu_upf* u);
 
 /* Occupations of a set of eigenvalues, host FP64, no device work:
  * find_fermi_energy / occupation / entropy_ts (scf/smearing.rs:38-252).

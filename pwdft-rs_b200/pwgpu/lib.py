@@ -21,8 +21,12 @@ PRECISION_MIXED = 1
 
 ERROR_NAMES = {
     -1: "PWGPU_E_INVALID", -2: "PWGPU_E_CUDA", -3: "PWGPU_E_OOM", -4: "PWGPU_E_NOT_CONVERGED",
-    -5: "PWGPU_E_TIMEOUT", -6: "PWGPU_E_NOT_IMPLEMENTED", -7: "PWGPU_E_STATE",
+    -5: "PWGPU_E_TIMEOUT", -6: "PWGPU_E_NOT_IMPLEMENTED", -7: "PWGPU_E_STATE", -8: "PWGPU_E_PARSE",
 }
+PWGPU_E_PARSE = -8
+
+# pwgpu_upf_get_array selectors (PWGPU_UPF_*)
+UPF_R, UPF_RAB, UPF_LOCAL, UPF_BETA, UPF_DIJ, UPF_RHOATOM, UPF_NLCC = range(7)
 
 
 class PwGpuError(RuntimeError):
@@ -132,6 +136,11 @@ class PwgpuServerStats(ct.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class PwgpuUpfInfo(ct.Structure):
+    _fields_ = [("element", ct.c_char * 8), ("z_valence", ct.c_double), ("l_max", ct.c_int32),
+                ("n_proj", ct.c_int32), ("mesh", ct.c_int32), ("has_nlcc", ct.c_int32), ("has_rho_atom", ct.c_int32)]
+
+
 MIXERS = {"anderson": 0, "broyden": 2, "periodic_pulay": 4}
 
 
@@ -215,16 +224,60 @@ def load_library(path: str = LIB_PATH):
     lib.pwgpu_server_result.argtypes = [vp, ct.c_int64, ct.POINTER(PwgpuScfResult), _f64p, ct.POINTER(ct.c_char_p)]
     lib.pwgpu_server_release.argtypes = [vp, ct.c_int64]
     lib.pwgpu_server_get_stats.argtypes = [vp, ct.POINTER(PwgpuServerStats)]
+    lib.pwgpu_upf_parse.argtypes = [ct.c_char_p, ct.c_int64, ct.POINTER(vp)]
+    lib.pwgpu_upf_load.argtypes = [ct.c_char_p, ct.POINTER(vp)]
+    lib.pwgpu_upf_get_info.argtypes = [vp, ct.POINTER(PwgpuUpfInfo)]
+    lib.pwgpu_upf_get_array.argtypes = [vp, ct.c_int32, ct.c_int32, _f64p, ct.c_int64]
+    lib.pwgpu_upf_get_beta_l.argtypes = [vp, _i32p]
+    lib.pwgpu_upf_free.argtypes = [vp]
     for name in ("pwgpu_create", "pwgpu_destroy", "pwgpu_set_veff_g", "pwgpu_apply_h", "pwgpu_apply_h_device",
                  "pwgpu_set_precision", "pwgpu_get_dims", "pwgpu_profile_apply_h", "pwgpu_scf_run", "pwgpu_scf_iter1_from_rho_g",
                  "pwgpu_eigensolve", "pwgpu_density", "pwgpu_symmetrize", "pwgpu_potentials",
                  "pwgpu_small_geneig", "pwgpu_occupations", "pwgpu_mix", "pwgpu_mix_reset", "pwgpu_get_projectors", "pwgpu_initial_density",
                  "pwgpu_get_local_potential", "pwgpu_server_create", "pwgpu_server_destroy",
                  "pwgpu_server_submit", "pwgpu_server_poll", "pwgpu_server_wait", "pwgpu_server_wait_any",
-                 "pwgpu_server_result", "pwgpu_server_release", "pwgpu_server_get_stats"):
+                 "pwgpu_server_result", "pwgpu_server_release", "pwgpu_server_get_stats", "pwgpu_upf_parse",
+                 "pwgpu_upf_load", "pwgpu_upf_get_info", "pwgpu_upf_get_array", "pwgpu_upf_get_beta_l",
+                 "pwgpu_upf_free"):
         getattr(lib, name).restype = ct.c_int32
     _lib = lib
     return lib
+
+
+def _upf_from_handle(lib, h):
+    from .upf import Upf
+    info = PwgpuUpfInfo()
+    _check(lib, lib.pwgpu_upf_get_info(h, ct.byref(info)))
+    mesh, nproj = info.mesh, info.n_proj
+
+    def arr(which, index=0, n=mesh):
+        out = np.zeros(n)
+        _check(lib, lib.pwgpu_upf_get_array(h, which, index, _f64(out), n))
+        return out
+
+    ls = np.zeros(max(nproj, 1), dtype=np.int32)
+    _check(lib, lib.pwgpu_upf_get_beta_l(h, _i32(ls)))
+    core = arr(UPF_NLCC) if info.has_nlcc else np.zeros(0)
+    return Upf(info.element.decode(), info.z_valence, info.l_max, arr(UPF_R), arr(UPF_RAB), arr(UPF_LOCAL),
+               [int(x) for x in ls[:nproj]], [arr(UPF_BETA, i) for i in range(nproj)], arr(UPF_DIJ, n=nproj * nproj),
+               arr(UPF_RHOATOM), core)
+
+
+def load_upf_native(path: str = None, text: str = None):
+    """A UPF read by the library's own parser (pwgpu_upf_load / pwgpu_upf_parse,
+    parse_upf_body, upf/parse.rs:20-135), returned as the same Upf object the
+    Python reader gives; raises PwGpuError(PWGPU_E_PARSE) on a malformed file."""
+    lib = load_library()
+    h = ct.c_void_p()
+    if text is not None:
+        raw = text.encode()
+        _check(lib, lib.pwgpu_upf_parse(raw, len(raw), ct.byref(h)))
+    else:
+        _check(lib, lib.pwgpu_upf_load(os.fsencode(path), ct.byref(h)))
+    try:
+        return _upf_from_handle(lib, h)
+    finally:
+        lib.pwgpu_upf_free(h)
 
 
 def _check(lib, rc):

@@ -75,7 +75,7 @@ def test_ctypes_structs_match_header_layout(tmp_path):
     mirrors = {"pwgpu_system": L.PwgpuSystem, "pwgpu_options": L.PwgpuOptions,
                "pwgpu_scf_params": L.PwgpuScfParams, "pwgpu_scf_result": L.PwgpuScfResult,
                "pwgpu_server_options": L.PwgpuServerOptions, "pwgpu_job_info": L.PwgpuJobInfo,
-               "pwgpu_server_stats": L.PwgpuServerStats}
+               "pwgpu_server_stats": L.PwgpuServerStats, "pwgpu_upf_info": L.PwgpuUpfInfo}
     lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "pwgpu.h"', 'int main(void) {']
     for cname, py in mirrors.items():
         lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
@@ -225,7 +225,7 @@ for name in T.declared_functions():
 def test_every_entry_point_refuses_null_arguments(tmp_path):
     """No entry point dereferences a NULL handle, server or array: called
     with every pointer NULL and every size zero, each returns
-    PWGPU_E_INVALID with a message, and the two destroy calls accept NULL
+    PWGPU_E_INVALID with a message, and the destroy / free calls accept NULL
     (a no-op, as free(NULL)); the process survives the whole sweep. Runs in
     a child process, so a crash fails this test instead of the suite."""
     import subprocess
@@ -240,7 +240,7 @@ def test_every_entry_point_refuses_null_arguments(tmp_path):
     expected = [n for n in declared_functions() if n not in ("pwgpu_version", "pwgpu_last_error")]
     assert sorted(got) == sorted(expected)
     for name, (rc, msg) in got.items():
-        if name in ("pwgpu_destroy", "pwgpu_server_destroy"):
+        if name in ("pwgpu_destroy", "pwgpu_server_destroy", "pwgpu_upf_free"):
             assert rc == 0, name
         else:
             assert rc == -1, (name, rc)  # PWGPU_E_INVALID
