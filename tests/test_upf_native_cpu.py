@@ -108,3 +108,50 @@ def test_accessors_refuse_bad_requests():
     finally:
         assert lib.pwgpu_upf_free(h) == 0
     assert lib.pwgpu_upf_load(b"/nonexistent/X.upf", ct.byref(h)) == -1
+
+
+def _mutations(text, n, seed=20261203):
+    """Seeded random damage to a UPF: cut a span, duplicate a span, swap a
+    character for another, or cut the file short."""
+    rng = np.random.default_rng(seed)
+    alphabet = list('0123456789.-+eE <>/="\n PQRSTUVWXYZ_abc')
+    for _ in range(n):
+        t = text
+        for _ in range(int(rng.integers(1, 4))):
+            kind = int(rng.integers(4))
+            i = int(rng.integers(len(t)))
+            if kind == 0:
+                t = t[:i] + t[i + int(rng.integers(1, 200)):]
+            elif kind == 1:
+                j = i + int(rng.integers(1, 200))
+                t = t[:j] + t[i:j] + t[j:]
+            elif kind == 2:
+                t = t[:i] + alphabet[int(rng.integers(len(alphabet)))] + t[i + 1:]
+            else:
+                t = t[:i]
+        yield t
+
+
+@pytest.mark.parametrize("name", ["Si.upf", "C.upf", "Si_hgh.upf"])
+def test_damaged_files_same_verdict_in_both_readers(name):
+    """On 150 seeded damaged copies of a UPF, the library's reader and the
+    Python reader accept and refuse the same files, and read the same
+    arrays from the files they accept; nothing crashes."""
+    with open(os.path.join(UPF_DIR, name)) as f:
+        text = f.read()
+    accepted = 0
+    for t in _mutations(text, 150):
+        try:
+            want = parse_upf(t)
+        except (UpfError, ValueError):
+            want = None
+        try:
+            got = load_upf_native(text=t)
+        except PwGpuError as e:
+            assert e.code == PWGPU_E_PARSE
+            got = None
+        assert (want is None) == (got is None)
+        if want is not None:
+            _same(got, want)
+            accepted += 1
+    assert 0 < accepted < 150
