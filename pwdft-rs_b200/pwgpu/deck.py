@@ -36,6 +36,7 @@ from __future__ import annotations
 
 import math
 import os
+import re
 from dataclasses import dataclass
 
 import numpy as np
@@ -62,6 +63,72 @@ MIXING_MODES = {  # MixingModeType -> (mixer, kerker), settings.rs:355-377
     "periodic_pulay": ("periodic_pulay", False), "periodic_pulay_kerker": ("periodic_pulay", True),
 }
 FUNCTIONALS = ("pz", "pbe", "pbe0", "hse06")
+
+
+# Plain-scalar typing of the reference's YAML reader (serde_yaml_ng 0.10, the
+# YAML 1.2 core schema as that crate applies it), restated here because
+# PyYAML types plain scalars by YAML 1.1 (`1e-8` a string, `yes`/`on`
+# booleans, `010` octal):
+#   null  ~ null Null NULL and the empty scalar;
+#   bool  true True TRUE false False FALSE only;
+#   int   decimal digits with an optional sign, or 0x / 0o / 0b with digits
+#         of that base; digits with a leading zero (`010`) stay a string;
+#   float a decimal number with a fraction and/or exponent (`1e-8`, `1.`,
+#         `.5`), or .inf / -.inf / .nan in their three spellings; anything
+#         else that is not finite stays a string;
+# everything else, and every quoted scalar, is a string.
+_INT_DEC = re.compile(r"[-+]?[0-9]+\Z")
+_FLOAT_DEC = re.compile(r"[-+]?(?:[0-9]+\.?[0-9]*|\.[0-9]+)(?:[eE][-+]?[0-9]+)?\Z")
+_RADIX = {"0x": 16, "0o": 8, "0b": 2}
+
+
+def _core_scalar(v: str):
+    if v in ("", "~", "null", "Null", "NULL"):
+        return None
+    if v in ("true", "True", "TRUE"):
+        return True
+    if v in ("false", "False", "FALSE"):
+        return False
+    unsigned = v[1:] if v.startswith("+") else v
+    if unsigned[:1] in "+-" and v.startswith("+"):
+        return v
+    for prefix, base in _RADIX.items():
+        if unsigned.startswith(prefix):
+            try:
+                return int(unsigned[2:], base)
+            except ValueError:
+                return v
+    digits = unsigned.lstrip("-")
+    if len(digits) > 1 and digits[0] == "0" and digits.isdigit():
+        return v
+    if _INT_DEC.match(v):
+        return int(v)
+    if unsigned in (".inf", ".Inf", ".INF"):
+        return math.inf
+    if v in ("-.inf", "-.Inf", "-.INF"):
+        return -math.inf
+    if v in (".nan", ".NaN", ".NAN"):
+        return math.nan
+    if _FLOAT_DEC.match(v):
+        f = float(v)
+        return f if math.isfinite(f) else v
+    return v
+
+
+class _DeckLoader(yaml.SafeLoader):
+    """SafeLoader with no implicit typing: every plain scalar arrives as a
+    string node and is typed by _core_scalar."""
+
+
+_DeckLoader.yaml_implicit_resolvers = {}
+
+
+def _construct_str(loader, node):
+    value = loader.construct_scalar(node)
+    return _core_scalar(value) if node.style is None else value
+
+
+_DeckLoader.add_constructor("tag:yaml.org,2002:str", _construct_str)
 
 
 class DeckError(ValueError):
@@ -145,7 +212,7 @@ class Deck:
 def parse_deck(text: str) -> Deck:
     """InputSettings::from_yaml_str: parse and check a deck; defaults filled in."""
     try:
-        raw = yaml.safe_load(text)
+        raw = yaml.load(text, Loader=_DeckLoader)
     except yaml.YAMLError as e:
         raise _parse_err(str(e)) from None
     top = _block(raw, "settings", ("system", "basis", "kpoints", "scf", "electrons", "xc", "symmetry", "output",

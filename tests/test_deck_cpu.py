@@ -217,3 +217,34 @@ def test_deck_contract_follows_the_reference_code_not_its_stale_tests():
     with pytest.raises(DeckError) as e:
         parse_deck(si2_deck().replace("symbol: Si, position: [0.0, 0.0, 0.0]", "symbol: Xz, position: [0.0, 0.0, 0.0]"))
     assert e.value.kind == "parse" and "Xz" in str(e.value)
+
+
+@pytest.mark.parametrize("text,field,value", [
+    ("scf:\n  conv_threshold: 1e-8\n", ("scf", "conv_threshold"), 1e-8),
+    ("scf:\n  energy_threshold: 1E-7\n", ("scf", "energy_threshold"), 1e-7),
+    ("scf:\n  mixing_beta: .5\n", ("scf", "mixing_beta"), 0.5),
+    ("scf:\n  max_iter: 0x40\n", ("scf", "max_iter"), 64),
+    ("scf:\n  n_bands: ~\n", ("scf", "n_bands"), None),
+    ("symmetry:\n  enabled: False\n", ("symmetry", "enabled"), False),
+    ("electrons:\n  tot_magnetization: null\n", ("electrons", "tot_magnetization"), None),
+])
+def test_plain_scalars_typed_as_the_reference_reader_types_them(text, field, value):
+    """The reference reads decks with serde_yaml_ng 0.10 (settings.rs:509-511),
+    which types plain scalars by the YAML 1.2 core rules: an exponent without
+    a dot is a float (PyYAML's YAML 1.1 rules would make `1e-8` a string and
+    refuse the deck), 0x/0o/0b prefixes are integers, ~ and null are null."""
+    d = parse_deck(CUBE + text)
+    assert getattr(d, field[0])[field[1]] == value
+
+
+@pytest.mark.parametrize("text", [
+    "symmetry:\n  enabled: yes\n",        # YAML 1.1 boolean words are strings
+    "output:\n  write_bands: on\n",
+    "scf:\n  max_iter: 010\n",            # leading zero: a string, not octal 8
+    "scf:\n  mixing_beta: '0.5'\n",       # a quoted number stays a string
+    "scf:\n  conv_threshold: 1_0\n",
+])
+def test_yaml_1_1_forms_are_not_numbers_or_booleans(text):
+    with pytest.raises(DeckError) as e:
+        parse_deck(CUBE + text)
+    assert e.value.kind == "parse"
