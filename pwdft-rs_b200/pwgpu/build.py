@@ -19,7 +19,7 @@ INCLUDE = os.path.join(os.path.dirname(PKG_ROOT), "include")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libpwgpu.so")
 
-SOURCES = ["api.cu", "hpsi.cu", "linalg.cu", "lobpcg.cu", "scf.cu", "noalloc.cu", "gemm_bf16.cu", "nl_mixed.cu", "server.cu", "gamma.cu", "setup.cu", "components.cu", "eigh.cu", "chol.cu", "upf.cu"]
+SOURCES = ["api.cu", "hpsi.cu", "linalg.cu", "lobpcg.cu", "scf.cu", "noalloc.cu", "gemm_bf16.cu", "nl_mixed.cu", "server.cu", "gamma.cu", "setup.cu", "components.cu", "eigh.cu", "chol.cu", "upf.cu", "deck.cu"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -131,6 +131,22 @@ def _construct_str(loader, node):
 _DeckLoader.add_constructor("tag:yaml.org,2002:str", _construct_str)
 
 
+def _construct_map(loader, node):
+    """A mapping; a key given twice is an error (serde refuses duplicate
+    fields, PyYAML would keep the last)."""
+    loader.flatten_mapping(node)
+    out = {}
+    for k_node, v_node in node.value:
+        k = loader.construct_object(k_node, deep=True)
+        if k in out:
+            raise yaml.constructor.ConstructorError(None, None, f"duplicate field `{k}`", k_node.start_mark)
+        out[k] = loader.construct_object(v_node, deep=True)
+    return out
+
+
+_DeckLoader.add_constructor("tag:yaml.org,2002:map", _construct_map)
+
+
 class DeckError(ValueError):
     """A deck the reference would refuse: kind is 'parse' (PwdftError::Parse),
     'invalid_param' (InvalidParam, with the parameter's name) or
@@ -312,6 +328,66 @@ def parse_deck(text: str) -> Deck:
     ib = _block(top.get("initial_density"), "initial_density", ("gaussian_sigma",))
     initial = {"gaussian_sigma": _num(ib.get("gaussian_sigma", 1.0), "initial_density.gaussian_sigma")}
     return Deck(lattice, atoms, basis, kpoints, scf, electrons, xc, symmetry, output, initial)
+
+
+def parse_deck_native(text: str) -> Deck:
+    """The same deck read by the library's own reader (pwgpu_deck_parse,
+    csrc/deck.cu), returned as the Deck parse_deck gives; raises DeckError
+    with the same kinds ('parse' for PWGPU_E_PARSE, 'invalid_param' for
+    PWGPU_E_INVALID)."""
+    import ctypes as ct
+
+    from .lib import PwgpuDeckSettings, load_library
+    lib = load_library()
+    raw = text.encode()
+    h = ct.c_void_p()
+    rc = lib.pwgpu_deck_parse(raw, len(raw), ct.byref(h))
+    if rc != 0:
+        msg = lib.pwgpu_last_error().decode(errors="replace")
+        raise DeckError("invalid_param" if rc == -1 else "parse", msg, "shift" if rc == -1 else None)
+    try:
+        st = PwgpuDeckSettings()
+        lib.pwgpu_deck_get_settings(h, ct.byref(st))
+
+        def names(n, width, getter):
+            buf = ct.create_string_buffer(max(n, 1) * width)
+            vals = np.zeros(max(n, 1) * 3)
+            getter(h, buf, vals.ctypes.data_as(ct.POINTER(ct.c_double)))
+            return [buf.raw[k * width:(k + 1) * width].split(b"\0")[0].decode() for k in range(n)], vals
+
+        syms, pos = names(st.n_atoms, 8, lib.pwgpu_deck_get_atoms)
+        msyms, mvals = names(st.n_starting_magnetization, 8, lib.pwgpu_deck_get_starting_magnetization)
+        labels, frac = names(st.n_path, 16, lib.pwgpu_deck_get_band_path)
+    finally:
+        lib.pwgpu_deck_free(h)
+    modes = list(MIXING_MODES)
+    if st.kpoints_type == 0:
+        kpoints = {"type": "monkhorst_pack", "grid": list(st.mp_grid), "shift": tuple(st.mp_shift)}
+    else:
+        kpoints = {"type": "band_path", "npoints": st.band_npoints,
+                   "path": [(labels[k], [float(x) for x in frac[3 * k:3 * k + 3]]) for k in range(st.n_path)]}
+    return Deck(
+        lattice=[[st.lattice[3 * r + c] for c in range(3)] for r in range(3)],
+        atoms=[(syms[a], [float(x) for x in pos[3 * a:3 * a + 3]]) for a in range(st.n_atoms)],
+        basis={"ecutwfc": st.ecutwfc, "ecutrho_ratio": st.ecutrho_ratio,
+               "fft_grid": None if not any(st.fft_grid) else list(st.fft_grid)},
+        kpoints=kpoints,
+        scf={"max_iter": st.max_iter, "conv_threshold": st.conv_threshold, "energy_threshold": st.energy_threshold,
+             "n_bands": None if st.n_bands < 0 else st.n_bands,
+             "eigensolver": ("dense", "iterative")[st.eigensolver], "wfrx_subspace": bool(st.wfrx_subspace),
+             "mixing_beta": st.mixing_beta, "mixing_ndim": st.mixing_ndim, "mixing_mode": modes[st.mixing_mode],
+             "pulay_period": st.pulay_period, "adaptive_beta": bool(st.adaptive_beta),
+             "smearing": SMEARINGS[st.smearing], "smearing_width": st.smearing_width},
+        electrons={"spin_polarized": bool(st.spin_polarized),
+                   "starting_magnetization": {k: float(v) for k, v in zip(msyms, mvals)},
+                   "tot_magnetization": st.tot_magnetization if st.has_tot_magnetization else None,
+                   "occupations": ("smearing", "fixed")[st.occupations]},
+        xc={"functional": FUNCTIONALS[st.functional]},
+        symmetry={"enabled": bool(st.symmetry_enabled), "time_reversal": bool(st.time_reversal),
+                  "tolerance": st.symmetry_tolerance},
+        output={"verbosity": ("low", "normal", "high")[st.verbosity], "write_density": bool(st.write_density),
+                "write_bands": bool(st.write_bands)},
+        initial_density={"gaussian_sigma": st.gaussian_sigma})
 
 
 def load_deck(path: str) -> Deck:

@@ -141,6 +141,22 @@ class PwgpuUpfInfo(ct.Structure):
                 ("n_proj", ct.c_int32), ("mesh", ct.c_int32), ("has_nlcc", ct.c_int32), ("has_rho_atom", ct.c_int32)]
 
 
+class PwgpuDeckSettings(ct.Structure):
+    _fields_ = [("lattice", ct.c_double * 9), ("n_atoms", ct.c_int32), ("ecutwfc", ct.c_double),
+                ("ecutrho_ratio", ct.c_int32), ("fft_grid", ct.c_int32 * 3), ("kpoints_type", ct.c_int32),
+                ("mp_grid", ct.c_int32 * 3), ("mp_shift", ct.c_int32 * 3), ("n_path", ct.c_int32),
+                ("band_npoints", ct.c_int32), ("max_iter", ct.c_int32), ("conv_threshold", ct.c_double),
+                ("energy_threshold", ct.c_double), ("n_bands", ct.c_int32), ("eigensolver", ct.c_int32),
+                ("wfrx_subspace", ct.c_int32), ("mixing_beta", ct.c_double), ("mixing_ndim", ct.c_int32),
+                ("mixing_mode", ct.c_int32), ("pulay_period", ct.c_int32), ("adaptive_beta", ct.c_int32),
+                ("smearing", ct.c_int32), ("smearing_width", ct.c_double), ("spin_polarized", ct.c_int32),
+                ("n_starting_magnetization", ct.c_int32), ("has_tot_magnetization", ct.c_int32),
+                ("tot_magnetization", ct.c_double), ("occupations", ct.c_int32), ("functional", ct.c_int32),
+                ("symmetry_enabled", ct.c_int32), ("time_reversal", ct.c_int32), ("symmetry_tolerance", ct.c_double),
+                ("verbosity", ct.c_int32), ("write_density", ct.c_int32), ("write_bands", ct.c_int32),
+                ("gaussian_sigma", ct.c_double)]
+
+
 MIXERS = {"anderson": 0, "broyden": 2, "periodic_pulay": 4}
 
 
@@ -230,6 +246,12 @@ def load_library(path: str = LIB_PATH):
     lib.pwgpu_upf_get_array.argtypes = [vp, ct.c_int32, ct.c_int32, _f64p, ct.c_int64]
     lib.pwgpu_upf_get_beta_l.argtypes = [vp, _i32p]
     lib.pwgpu_upf_free.argtypes = [vp]
+    lib.pwgpu_deck_parse.argtypes = [ct.c_char_p, ct.c_int64, ct.POINTER(vp)]
+    lib.pwgpu_deck_get_settings.argtypes = [vp, ct.POINTER(PwgpuDeckSettings)]
+    lib.pwgpu_deck_get_atoms.argtypes = [vp, ct.c_char_p, _f64p]
+    lib.pwgpu_deck_get_starting_magnetization.argtypes = [vp, ct.c_char_p, _f64p]
+    lib.pwgpu_deck_get_band_path.argtypes = [vp, ct.c_char_p, _f64p]
+    lib.pwgpu_deck_free.argtypes = [vp]
     for name in ("pwgpu_create", "pwgpu_destroy", "pwgpu_set_veff_g", "pwgpu_apply_h", "pwgpu_apply_h_device",
                  "pwgpu_set_precision", "pwgpu_get_dims", "pwgpu_profile_apply_h", "pwgpu_scf_run", "pwgpu_scf_iter1_from_rho_g",
                  "pwgpu_eigensolve", "pwgpu_density", "pwgpu_symmetrize", "pwgpu_potentials",
@@ -238,7 +260,8 @@ def load_library(path: str = LIB_PATH):
                  "pwgpu_server_submit", "pwgpu_server_poll", "pwgpu_server_wait", "pwgpu_server_wait_any",
                  "pwgpu_server_result", "pwgpu_server_release", "pwgpu_server_get_stats", "pwgpu_upf_parse",
                  "pwgpu_upf_load", "pwgpu_upf_get_info", "pwgpu_upf_get_array", "pwgpu_upf_get_beta_l",
-                 "pwgpu_upf_free"):
+                 "pwgpu_upf_free", "pwgpu_deck_parse", "pwgpu_deck_get_settings", "pwgpu_deck_get_atoms",
+                 "pwgpu_deck_get_starting_magnetization", "pwgpu_deck_get_band_path", "pwgpu_deck_free"):
         getattr(lib, name).restype = ct.c_int32
     _lib = lib
     return lib

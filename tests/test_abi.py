@@ -55,7 +55,7 @@ def test_header_compiles_as_c99_and_cxx(tmp_path):
     if shutil.which("gcc") is None or shutil.which("g++") is None:
         pytest.skip("no host C compiler")
     src = tmp_path / "use_header.c"
-    src.write_text('#include "pwgpu.h"\nint main(void) { return pwgpu_version() == 0; }\n')
+    src.write_text('#include "pwgpu.h"\n#include "pwgpu_deck.h"\nint main(void) { return pwgpu_version() == 0; }\n')
     inc = os.path.join(ROOT, "include")
     subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-fsyntax-only", "-I", inc,
                     str(src)], check=True)
@@ -75,8 +75,10 @@ def test_ctypes_structs_match_header_layout(tmp_path):
     mirrors = {"pwgpu_system": L.PwgpuSystem, "pwgpu_options": L.PwgpuOptions,
                "pwgpu_scf_params": L.PwgpuScfParams, "pwgpu_scf_result": L.PwgpuScfResult,
                "pwgpu_server_options": L.PwgpuServerOptions, "pwgpu_job_info": L.PwgpuJobInfo,
-               "pwgpu_server_stats": L.PwgpuServerStats, "pwgpu_upf_info": L.PwgpuUpfInfo}
-    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "pwgpu.h"', 'int main(void) {']
+               "pwgpu_server_stats": L.PwgpuServerStats, "pwgpu_upf_info": L.PwgpuUpfInfo,
+               "pwgpu_deck_settings": L.PwgpuDeckSettings}
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "pwgpu.h"', '#include "pwgpu_deck.h"',
+             'int main(void) {']
     for cname, py in mirrors.items():
         lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
         for fname, _ in py._fields_:
@@ -116,7 +118,7 @@ def _rust_type(ctype, array=None):
 
 
 def _header_text():
-    text = open(os.path.join(ROOT, "include", "pwgpu.h")).read()
+    text = "".join(open(h).read() for h in sorted(glob.glob(os.path.join(ROOT, "include", "*.h"))))
     return re.sub(r"/\*.*?\*/", "", text, flags=re.S)
 
 
@@ -240,7 +242,7 @@ def test_every_entry_point_refuses_null_arguments(tmp_path):
     expected = [n for n in declared_functions() if n not in ("pwgpu_version", "pwgpu_last_error")]
     assert sorted(got) == sorted(expected)
     for name, (rc, msg) in got.items():
-        if name in ("pwgpu_destroy", "pwgpu_server_destroy", "pwgpu_upf_free"):
+        if name in ("pwgpu_destroy", "pwgpu_server_destroy", "pwgpu_upf_free", "pwgpu_deck_free"):
             assert rc == 0, name
         else:
             assert rc == -1, (name, rc)  # PWGPU_E_INVALID
