@@ -155,52 +155,67 @@ struct Line {
 };
 
 std::string rtrim(std::string s) {
-  while (!s.empty() && (s.back() == ' ' || s.back() == '\t' || s.back() == '\r')) s.pop_back();
+  while (!s.empty() && (s.back() == ' ' || s.back() == '\t' || s.back() == '\r' || s.back() == '\n')) s.pop_back();
   return s;
 }
 std::string trim(const std::string& s) {
   size_t a = 0;
-  while (a < s.size() && (s[a] == ' ' || s[a] == '\t')) ++a;
+  while (a < s.size() && (s[a] == ' ' || s[a] == '\t' || s[a] == '\n')) ++a;
   return rtrim(s.substr(a));
 }
 
-// text of a line with its comment removed (a # at the start or after a blank,
-// outside quotes)
-std::string strip_comment(const std::string& s) {
+// Scan of one line's text outside quoted scalars: a quote or a `[` / `{`
+// opens only where a scalar or collection can start (at the start, or after
+// one of `[ { , : - ?` and blanks); a `#` starts a comment after a blank or
+// right after a closed quote, bracket or comma. Returns the text before the
+// comment; *depth receives the open-bracket count at the end.
+std::string scan_line(const std::string& s, int* depth) {
   bool sq = false, dq = false;
+  char last = '\0';  // last non-blank character outside quotes
+  bool closed = false;  // the previous character closed a quote, a bracket or was a comma
+  int d = 0;
   for (size_t i = 0; i < s.size(); ++i) {
     const char c = s[i];
     if (dq) {
       if (c == '\\') ++i;
-      else if (c == '"') dq = false;
-    } else if (sq) {
-      if (c == '\'') sq = false;
-    } else if (c == '"') {
-      dq = true;
-    } else if (c == '\'') {
-      sq = true;
-    } else if (c == '#' && (i == 0 || s[i - 1] == ' ' || s[i - 1] == '\t')) {
+      else if (c == '"') { dq = false; last = c; closed = true; }
+      continue;
+    }
+    if (sq) {
+      if (c == '\'') {
+        if (i + 1 < s.size() && s[i + 1] == '\'') { ++i; continue; }
+        sq = false; last = c; closed = true;
+      }
+      continue;
+    }
+    const bool can_open = last == '\0' || std::strchr("[{,:-?", last) != nullptr;
+    if (c == '#' && (i == 0 || s[i - 1] == ' ' || s[i - 1] == '\t' || s[i - 1] == '\n' || closed)) {
+      if (depth) *depth = d;
       return s.substr(0, i);
     }
+    closed = false;
+    if (c == ' ' || c == '\t' || c == '\n') continue;
+    if ((c == '"' || c == '\'') && can_open) {
+      (c == '"' ? dq : sq) = true;
+    } else if ((c == '[' || c == '{') && can_open) {
+      ++d;
+    } else if ((c == ']' || c == '}') && d > 0) {
+      --d;
+      closed = true;
+    } else if (c == ',' && d > 0) {
+      closed = true;
+    }
+    last = c;
   }
+  if (depth) *depth = d;
   return s;
 }
 
+std::string strip_comment(const std::string& s) { return scan_line(s, nullptr); }
+
 int bracket_depth(const std::string& s) {
   int d = 0;
-  bool sq = false, dq = false;
-  for (size_t i = 0; i < s.size(); ++i) {
-    const char c = s[i];
-    if (dq) {
-      if (c == '\\') ++i;
-      else if (c == '"') dq = false;
-    } else if (sq) {
-      if (c == '\'') sq = false;
-    } else if (c == '"') dq = true;
-    else if (c == '\'') sq = true;
-    else if (c == '[' || c == '{') ++d;
-    else if (c == ']' || c == '}') --d;
-  }
+  scan_line(s, &d);
   return d;
 }
 
@@ -234,7 +249,7 @@ std::vector<Line> split_lines(const std::string& text) {
     if (body[0] == '%') perr("line " + std::to_string(no) + ": directives are not supported");
     started = true;
     if (!out.empty() && bracket_depth(out.back().text) > 0) {
-      out.back().text += " " + body;  // a flow collection continued on this line
+      out.back().text += "\n" + body;  // a flow collection continued on this line
     } else {
       out.push_back({(int)ind, body, no});
     }
@@ -291,7 +306,7 @@ std::string quoted(const std::string& s, size_t& i, const std::string& at) {
 Node flow(const std::string& s, size_t& i, const std::string& at);
 
 void skip_ws(const std::string& s, size_t& i) {
-  while (i < s.size() && (s[i] == ' ' || s[i] == '\t')) ++i;
+  while (i < s.size() && (s[i] == ' ' || s[i] == '\t' || s[i] == '\n')) ++i;
 }
 
 // one element of a flow collection (a nested collection, a quoted scalar or a
@@ -306,9 +321,17 @@ Node flow_item(const std::string& s, size_t& i, const std::string& at) {
     n.text = quoted(s, i, at);
     return n;
   }
-  size_t j = i;
-  while (j < s.size() && s[j] != ',' && s[j] != ']' && s[j] != '}') ++j;
-  std::string t = trim(s.substr(i, j - i));
+  size_t j = i;  // a plain scalar in a flow collection ends at a flow indicator
+  while (j < s.size() && !std::strchr(",[]{}", s[j])) ++j;
+  std::string t;
+  for (char c : trim(s.substr(i, j - i))) {  // a line break inside a plain scalar folds to one blank
+    if (c == '\n') {
+      while (!t.empty() && t.back() == ' ') t.pop_back();
+      t += ' ';
+    } else {
+      t += c;
+    }
+  }
   i = j;
   unsupported(t, at);
   if (t.find(": ") != std::string::npos) perr(at + "a mapping inside a flow sequence is not supported");
@@ -333,9 +356,18 @@ Node flow(const std::string& s, size_t& i, const std::string& at) {
       if (s[i] == '"' || s[i] == '\'') {
         key = quoted(s, i, at);
       } else {
+        // a plain key ends at a `:` followed by a blank, a flow indicator
+        // (`,` `[` `]` `{` `}`) or the end (a `:` before anything else is part
+        // of the scalar), or at `,` / `}`
         size_t j = i;
-        while (j < s.size() && s[j] != ':' && s[j] != ',' && s[j] != '}') ++j;
-        key = trim(s.substr(i, j - i));
+        while (j < s.size() && s[j] != ',' && s[j] != '}' &&
+               !(s[j] == ':' && (j + 1 == s.size() || std::strchr(" \n,[]{}", s[j + 1]) != nullptr)))
+          ++j;
+        const std::string raw_key = s.substr(i, j - i);
+        if (raw_key.find('\n') != std::string::npos) perr(at + "a mapping key spans lines");
+        key = trim(raw_key);
+        if (!key.empty() && (key[0] == '[' || key[0] == '{')) perr(at + "a collection as a mapping key");
+        unsupported(key, at);
         i = j;
       }
       skip_ws(s, i);

@@ -138,6 +138,8 @@ def _construct_map(loader, node):
     out = {}
     for k_node, v_node in node.value:
         k = loader.construct_object(k_node, deep=True)
+        if isinstance(k, (list, dict)):
+            raise yaml.constructor.ConstructorError(None, None, "a collection as a mapping key", k_node.start_mark)
         if k in out:
             raise yaml.constructor.ConstructorError(None, None, f"duplicate field `{k}`", k_node.start_mark)
         out[k] = loader.construct_object(v_node, deep=True)

@@ -140,3 +140,38 @@ def test_custom_shift_flag_above_one_is_an_invalid_parameter():
         with pytest.raises(DeckError) as e:
             reader(text)
         assert e.value.kind == "invalid_param"
+
+
+def _damaged(text, n, seed):
+    """Seeded random damage: cut a few characters, insert or swap one
+    character from the deck's own alphabet of indicators and digits."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    alphabet = list("0123456789.-+eE [],{}:\n #\"'xyz_")
+    for _ in range(n):
+        t = text
+        for _ in range(int(rng.integers(1, 3))):
+            kind, i = int(rng.integers(3)), int(rng.integers(len(t)))
+            c = alphabet[int(rng.integers(len(alphabet)))]
+            t = (t[:i] + t[i + int(rng.integers(1, 8)):] if kind == 0 else
+                 t[:i] + c + t[i:] if kind == 1 else t[:i] + c + t[i + 1:])
+        yield t
+
+
+@pytest.mark.parametrize("name", ["full", "si2", "band_path", "magnetization_two_species"])
+def test_damaged_decks_same_verdict_in_both_readers(name):
+    """On 300 seeded damaged copies of a deck the two readers accept the same
+    decks with the same settings and refuse the rest with the same kind."""
+    accepted = 0
+    for t in _damaged(VALID[name], 300, seed=sum(map(ord, name))):
+        try:
+            want, wk = parse_deck(t), "ok"
+        except DeckError as e:
+            want, wk = None, e.kind
+        try:
+            got, gk = parse_deck_native(t), "ok"
+        except DeckError as e:
+            got, gk = None, e.kind
+        assert (gk, got) == (wk, want), t
+        accepted += want is not None
+    assert 0 < accepted < 300
