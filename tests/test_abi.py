@@ -247,3 +247,87 @@ def test_every_entry_point_refuses_null_arguments(tmp_path):
         else:
             assert rc == -1, (name, rc)  # PWGPU_E_INVALID
             assert msg != "-", name
+
+
+_C_CALLER = r"""
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include "pwgpu.h"
+#include "pwgpu_deck.h"
+
+/* A C host: read a deck, then the UPF of each species it names, the way a
+ * caller without Python fills pwgpu_system's radial fields. */
+int main(int argc, char** argv) {
+  FILE* f = fopen(argv[1], "rb");
+  if (!f) return 2;
+  char text[1 << 16];
+  size_t n = fread(text, 1, sizeof(text), f);
+  fclose(f);
+  pwgpu_deck* d = NULL;
+  if (pwgpu_deck_parse(text, (int64_t)n, &d) != PWGPU_OK) { printf("deck: %s\n", pwgpu_last_error()); return 3; }
+  pwgpu_deck_settings s;
+  pwgpu_deck_get_settings(d, &s);
+  char* sym = calloc((size_t)s.n_atoms, 8);
+  double* pos = calloc((size_t)s.n_atoms * 3, sizeof(double));
+  pwgpu_deck_get_atoms(d, sym, pos);
+  printf("atoms %d ecut %.3f grid %d %d %d shift %d %d %d nbands %d smearing %d mixing %d\n", s.n_atoms, s.ecutwfc,
+         s.mp_grid[0], s.mp_grid[1], s.mp_grid[2], s.mp_shift[0], s.mp_shift[1], s.mp_shift[2], s.n_bands,
+         s.smearing, s.mixing_mode);
+  for (int a = 0; a < s.n_atoms; ++a) {
+    char path[4096];
+    snprintf(path, sizeof(path), "%s/%s.upf", argv[2], sym + 8 * a);
+    pwgpu_upf* u = NULL;
+    if (pwgpu_upf_load(path, &u) != PWGPU_OK) { printf("upf: %s\n", pwgpu_last_error()); return 4; }
+    pwgpu_upf_info info;
+    pwgpu_upf_get_info(u, &info);
+    double* r = malloc(sizeof(double) * (size_t)info.mesh);
+    pwgpu_upf_get_array(u, PWGPU_UPF_R, 0, r, info.mesh);
+    printf("atom %d %s at %.2f %.2f %.2f: z %.1f nproj %d mesh %d r_last %.6f\n", a, sym + 8 * a, pos[3 * a],
+           pos[3 * a + 1], pos[3 * a + 2], info.z_valence, info.n_proj, info.mesh, r[info.mesh - 1]);
+    free(r);
+    pwgpu_upf_free(u);
+  }
+  /* a malformed deck is refused with PWGPU_E_PARSE and a message */
+  pwgpu_deck* bad = NULL;
+  const char* broken = "system:\n  lattice: [[1,0,0]]\n";
+  int rc = pwgpu_deck_parse(broken, (int64_t)strlen(broken), &bad);
+  printf("broken %d %s\n", rc, rc == PWGPU_E_PARSE && bad == NULL && strlen(pwgpu_last_error()) > 0 ? "refused" : "?");
+  free(sym);
+  free(pos);
+  pwgpu_deck_free(d);
+  return 0;
+}
+"""
+
+
+def test_c_caller_reads_deck_and_pseudopotentials(tmp_path):
+    """A C program linked against libpwgpu.so reads a deck and the UPF of
+    each of its species through the C-ABI alone (what the reference's Rust
+    host would call), with the values the Python readers give."""
+    import shutil
+    import subprocess
+    import pytest
+    from pwgpu.upf import load_upf
+    from conftest import UPF_DIR
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not available")
+    deck = tmp_path / "gaas.yaml"
+    deck.write_text("system:\n  lattice: [[0, 2.83, 2.83], [2.83, 0, 2.83], [2.83, 2.83, 0]]\n  atoms:\n"
+                    "    - {symbol: Ga, position: [0, 0, 0]}\n    - {symbol: As, position: [0.25, 0.25, 0.25]}\n"
+                    "basis:\n  ecutwfc: 272.1\nkpoints:\n  type: monkhorst_pack\n  grid: [4, 4, 4]\n  shift: mp1976\n"
+                    "scf:\n  n_bands: 12\n  smearing: gaussian\n  mixing_mode: broyden_kerker\n")
+    src = tmp_path / "caller.c"
+    src.write_text(_C_CALLER)
+    exe = tmp_path / "caller"
+    libdir = os.path.dirname(L.LIB_PATH)
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                    "-L", libdir, "-lpwgpu", f"-Wl,-rpath,{libdir}"], check=True)
+    out = subprocess.run([str(exe), str(deck), UPF_DIR], check=True, capture_output=True, text=True, timeout=60).stdout
+    lines = out.splitlines()
+    assert lines[0] == "atoms 2 ecut 272.100 grid 4 4 4 shift 1 1 1 nbands 12 smearing 1 mixing 3"
+    for k, el in enumerate(("Ga", "As")):
+        pp = load_upf(os.path.join(UPF_DIR, f"{el}.upf"))
+        assert lines[1 + k].startswith(f"atom {k} {el} at ")
+        assert f"z {pp.z_valence:.1f} nproj {pp.n_proj} mesh {pp.r.size} r_last {pp.r[-1]:.6f}" in lines[1 + k]
+    assert lines[3] == "broken -8 refused"
